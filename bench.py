@@ -1,0 +1,393 @@
+"""Throughput of CapacMD's per-timestep force-and-solve path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c5] [--precision fp64|mixed]
+    python bench.py --impl reference ...      # the reference's own CPU code, same workload
+
+Metric: atom-steps/s -- atoms x MD steps per second of device time, one MD
+step being the reference loop (mpi-main.c:874-1013: thermostat, half kicks,
+drift, RATTLE, and one mpi_force with Sutton-Chen, CPIM RHS, matrix, BiCGSTAB
+and CPIM forces) run resident on the GPU.  Default workload: the 452k-atom
+system (Au2057 icosahedron in 150,000 rigid waters, 16.5 nm periodic box,
+seeded synthetic inputs written in the reference's file formats).
+
+Multi-GPU runs (torchrun) are independent replicas: every rank integrates its
+own copy and nothing is exchanged per step (the path does not shard); value is
+the sum over ranks, timed as the slowest rank.
+
+Printed: one JSON line with value, e2e (the drop-in mpi_force call with host
+buffers, copies included), the roofline of the dominant kernel from CUDA-event
+timings inside the timed region, the CPU baseline (reference code on a bounded
+sample), clocks sampled during the timed region and the kernel-launch count.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD_DESC = {
+    "c5": "Au2057 icosahedron + 150,000 rigid 3-site waters, 452,057 atoms, 16.5 nm periodic box, nvt 300 K",
+    "c3": "2 x Au561 + 30,000 waters, 91,122 atoms, 9.65 nm box, 0.5 V/nm field along z",
+    "c2": "Au309 + 3,000 waters, 9,309 atoms, 4.5 nm box, nvt 300 K",
+    "c4": "Au147 + 1,000 waters, 3,147 atoms, 3.1 nm box",
+    "c1": "Au147 in vacuum, 147 atoms, nve",
+}
+
+
+def _peaks() -> tuple[float, str]:
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 100 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.idx), "-lms", "100"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for k, n in enumerate(names):
+                if p[5 + k].lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def algorithmic_bytes(sim, cls: str, n_atoms: int, n_metal: int, precision: str) -> float:
+    """HBM bytes one launch of a kernel class must move at minimum.
+
+    pair: the list (4 B per entry) plus, per atom, its packed position/charge
+          (32 B, 16 B mixed), list length, type, metal flag, and the force
+          read-modify-write (48 B);
+    spmv: the 4x4-block CPIM matrix (16 entries per ordered metal pair, row
+          padded to a multiple of 32; 8 B, 4 B mixed) plus the input and output
+          vectors (2 x 4M x 8 B).
+    """
+    st = sim.stats()
+    w = 4 if precision == "mixed" else 8
+    if cls == "pair":
+        return 4.0 * st.list_entries + n_atoms * (4 * w + 4 + 4 + 1 + 48)
+    if cls == "spmv":
+        mp = (n_metal + 31) // 32 * 32
+        return 16.0 * w * n_metal * mp + 2 * 4 * n_metal * 8.0
+    if cls == "matrix":
+        mp = (n_metal + 31) // 32 * 32
+        return 16.0 * 8 * n_metal * mp
+    return float("nan")
+
+
+def cpu_reference_sample(paths: dict, n_atoms: int, target_nb_s: float = 6.0) -> dict:
+    """The reference code (oracle/_ref) on a bounded sample of the workload.
+
+    One warm-up force call, then positions drift by dt*v (so the BiCGSTAB warm
+    start is as in MD) and one force call is timed with its nonbonded pair loop
+    restricted to the last fraction f of the pair index -- the share one rank of
+    a 1/f-rank MPI run owns; all other phases run in full.  Per-step time =
+    rest + nonbonded/f (the pair loop is uniform O(N^2) work)."""
+    from oracle import oracle as O
+    if not O.ref_available():
+        return {"unavailable": "reference library oracle/_ref/libcapref.so not built"}
+    ref = O.open_reference(paths, first_force=False)
+    P = n_atoms * (n_atoms - 1) / 2
+    frac = min(1.0, target_nb_s / (11e-9 * P))
+    O.time_sampled_force(ref, frac)  # warm-up: COO allocation, cold solve
+    dt = 0.001
+    for a, v in (("rx", "vx"), ("ry", "vy"), ("rz", "vz")):
+        ref.set(a, ref.get(a) + dt * ref.get(v))
+    t, ph = O.time_sampled_force(ref, frac)
+    nb = ph[4]
+    step = (t - nb) + nb / frac
+    return {"step_s": step, "frac": frac, "wall_s": t, "nonbonded_s": nb, "phases": ph.tolist()}
+
+
+def run_reference_arm(args, world: int, rank: int) -> int:
+    if rank != 0:
+        return 0
+    from capacmd_b200 import configs
+    wl = args.workload
+    paths = configs.cached(wl)
+    n_atoms = int(open(paths["gro"]).readlines()[1])
+    from oracle import oracle as O
+    if not O.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "reference CPU library not built (oracle/_ref)"}))
+        return 0
+    ref = O.open_reference(paths, first_force=False)
+    P = n_atoms * (n_atoms - 1) / 2
+    frac = min(1.0, 4.0 / (11e-9 * P))
+    steps = min(args.steps, 3)
+    O.time_sampled_force(ref, frac)  # one warm-up call
+    per_step = []
+    for _ in range(steps):
+        for a, v in (("rx", "vx"), ("ry", "vy"), ("rz", "vz")):
+            ref.set(a, ref.get(a) + 0.001 * ref.get(v))
+        t, ph = O.time_sampled_force(ref, frac)
+        per_step.append((t - ph[4]) + ph[4] / frac)
+    step_s = float(np.mean(per_step))
+    value = n_atoms / step_s
+    sample = (f"{steps} force calls of the {n_atoms}-atom workload after one warm-up call, positions drifted "
+              f"by dt*v between calls; nonbonded pair loop restricted to the last {frac:.4%} of the pair index "
+              f"(the reference's own rank partition), other phases in full; step time = rest + nonbonded/fraction")
+    print(json.dumps({
+        "impl": "reference", "metric": "atom-steps/s", "value": value, "unit": "atom-steps/s",
+        "n_gpus": world, "steps": steps, "warmup": 1, "ms_per_step": step_s * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD_DESC.get(wl, wl), "name": wl, "parallelism": "1 host thread"},
+        "cpu_baseline": {"value": value, "unit": "atom-steps/s", "cores": 1, "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": "atom-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+    return 0
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c5", choices=sorted(WORKLOAD_DESC))
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--e2e-calls", type=int, default=20)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        return run_reference_arm(args, world, rank)
+
+    import torch
+    import torch.distributed as dist
+    import capacmd_b200 as cm
+    from capacmd_b200 import configs
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+    if rank == 0:
+        paths = configs.cached(args.workload)
+    if world > 1:
+        dist.barrier()
+    paths = configs.cached(args.workload)
+
+    prec = cm.PREC_MIXED if args.precision == "mixed" else cm.PREC_FP64
+    desc = cm.Desc.from_paths(paths)
+    sim = cm.Simulation(desc, precision=prec, device=local)
+    N, M = desc.n_atoms, desc.n_metal
+    sim.md_init()
+    sim.md_steps(args.warmup)
+
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.15)
+    cm.lib().capac_profile_enable(sim._p, 1)
+    l0 = sim.kernel_launches()
+    ms = ctypes_time(sim, args.steps)
+    launches = sim.kernel_launches() - l0
+    prof = {}
+    for cls in ("pair", "spmv", "matrix", "cpim_metal", "cpim_rhs", "qsc", "list_build", "solver_vec"):
+        prof[cls] = profile_get(sim, cls)
+    cm.lib().capac_profile_enable(sim._p, 0)
+    clk = clocks.stop()
+    torch.cuda.synchronize()
+    if world > 1:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    value = N * args.steps * world / (ms / 1e3)
+    st = sim.stats()
+
+    # dominant kernel and its roofline
+    peak, peak_kind = _peaks()
+    dom = max(("pair", "spmv", "matrix"), key=lambda k: prof[k][1])
+    n_launch, tot_ms = prof[dom]
+    if dom == "spmv":
+        n_launch = spmv_effective(sim, n_launch)
+    avg_s = tot_ms / max(n_launch, 1) / 1e3
+    bytes_launch = algorithmic_bytes(sim, dom, N, M, args.precision)
+    achieved = bytes_launch / avg_s / 1e9 if avg_s > 0 else None
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak if achieved else None, "traffic": _traffic(args.workload, dom),
+                "kernel": dom, "algorithmic_bytes_per_launch": bytes_launch, "avg_launch_ms": avg_s * 1e3,
+                "launches": n_launch, "peak_kind": peak_kind}
+
+    # end to end through the drop-in mpi_force with pinned host buffers
+    e2e = None
+    if not args.no_e2e:
+        e2e = e2e_drop_in(sim, desc, args.e2e_calls, torch)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        r = cpu_reference_sample(paths, N)
+        if "unavailable" in r:
+            cpu = {"value": None, "unit": "atom-steps/s", "cores": 1, "kind": "reference", "sample": r["unavailable"]}
+        else:
+            cpu = {"value": N / r["step_s"], "unit": "atom-steps/s", "cores": 1, "kind": "reference",
+                   "sample": (f"one reference force call (after a warm-up call) of the {N}-atom workload with the "
+                              f"nonbonded pair loop restricted to the last {r['frac']:.4%} of the pair index, other "
+                              f"phases in full; step = rest + nonbonded/fraction = {r['step_s']:.1f} s")}
+
+    if rank == 0:
+        ps = sim.phase_times()
+        line = {
+            "metric": "atom-steps/s", "value": value, "unit": "atom-steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.precision == "fp64" else "f32 pair/SpMV + f64 refinement",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD_DESC[args.workload], "name": args.workload,
+                       "atoms": N, "metal_atoms": M, "cpim_unknowns": desc.n_mat, "precision": args.precision,
+                       "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+                       "l2": "inputs larger than L2 (neighbour list and CPIM matrix > 126 MB)"},
+            "ns_per_day": args.steps / (ms / 1e3) * 0.001 * 86400 * 1e-3 * 1e3,
+            "solver": {"iterations_last": st.solver_iterations, "rel_residual_last": st.solver_rel_residual,
+                       "spmv_ms_total": prof["spmv"][1]},
+            "kernel_ms": {k: v[1] for k, v in prof.items()},
+            "phase_ms_last_force": {"list": ps[10], "qsc": ps[1], "cpim_vec": ps[6], "cpim_matrix": ps[5],
+                                    "cpim_solve": ps[7], "nonbonded": ps[4], "cpim_force": ps[8]},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "gpu_launches": launches,
+        }
+        print(json.dumps(line))
+    sim.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def ctypes_time(sim, steps: int) -> float:
+    import ctypes
+    import capacmd_b200 as cm
+    out = ctypes.c_double(0.0)
+    lib = cm.lib()
+    lib.capac_time_md_steps.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+    cm._check(lib.capac_time_md_steps(sim._p, int(steps), ctypes.byref(out)))
+    return out.value
+
+
+def profile_get(sim, cls: str) -> tuple[int, float]:
+    import ctypes
+    import capacmd_b200 as cm
+    lib = cm.lib()
+    lib.capac_profile_get.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.POINTER(ctypes.c_long),
+                                      ctypes.POINTER(ctypes.c_double)]
+    n, ms = ctypes.c_long(0), ctypes.c_double(0.0)
+    cm._check(lib.capac_profile_get(sim._p, cls.encode(), ctypes.byref(n), ctypes.byref(ms)))
+    return int(n.value), float(ms.value)
+
+
+def spmv_effective(sim, launched: int) -> int:
+    """SpMV launches that did work (the solver over-issues a few per solve that
+    return immediately once it has converged)."""
+    n, _ = profile_get(sim, "spmv_effective")
+    return n if n > 0 else launched
+
+
+def _traffic(workload: str, kernel: str):
+    """DRAM bytes per launch measured by ncu for this kernel and workload, if a
+    capture summary is committed (profiles/ncu_traffic.json)."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "ncu_traffic.json")) as f:
+            return json.load(f).get(workload, {}).get(kernel)
+    except Exception:
+        return None
+
+
+def e2e_drop_in(sim, desc, calls: int, torch) -> dict:
+    """atom-steps/s through capac_mpi_force with pinned host buffers: positions
+    (and the induced-vector warm start) copied in, forces, energies, virial and
+    the induced vector copied out, every call."""
+    import ctypes
+    import capacmd_b200 as cm
+    N, n = desc.n_atoms, max(desc.n_mat, 1)
+
+    def pinned(k):
+        return torch.empty(k, dtype=torch.float64, pin_memory=True).numpy()
+
+    rx, ry, rz = pinned(N), pinned(N), pinned(N)
+    rx[:], ry[:], rz[:] = sim.get("rx"), sim.get("ry"), sim.get("rz")
+    vx, vy, vz = sim.get("vx"), sim.get("vy"), sim.get("vz")
+    fx, fy, fz, pot, vir, pq = pinned(N), pinned(N), pinned(N), pinned(15), pinned(9), pinned(n)
+    pq[:] = sim.get("vec_pq") if desc.n_mat else 0.0
+    lib = cm.lib()
+    ptr = lambda a: a.ctypes.data  # noqa: E731
+    h2d = 3 * N * 8 + desc.n_mat * 8
+    d2h = 3 * N * 8 + 15 * 8 + 9 * 8 + desc.n_mat * 8
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(calls):
+        rx += 0.0001 * vx
+        ry += 0.0001 * vy
+        rz += 0.0001 * vz
+        cm._check(lib.capac_mpi_force(sim._p, ptr(rx), ptr(ry), ptr(rz), ptr(fx), ptr(fy), ptr(fz), ptr(pot),
+                                      ptr(vir), ptr(pq) if desc.n_mat else None, None, None, None))
+    dt = time.perf_counter() - t0
+    return {"value": N * calls / dt, "unit": "atom-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+            "calls": calls, "ms_per_call": dt / calls * 1e3,
+            "what": "one drop-in mpi_force per step (host positions in, host forces/energies/virial/vec_pq out); "
+                    "the MD integration of the drop-in mode runs in the caller"}
+
+
+if __name__ == "__main__":
+    sys.exit(main())

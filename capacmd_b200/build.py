@@ -1,0 +1,84 @@
+"""Build the CUDA library in-tree (sm_100a) and the CPU oracles.
+
+    python -m capacmd_b200.build            # library + oracle (+ reference oracle if its sources exist)
+
+The library is ``capacmd_b200/libcapacmd_gpu.so``: host C++ (input parsing,
+orchestration, C ABI) and the sm_100a kernels, linked against the CUDA runtime.
+"""
+from __future__ import annotations
+
+import concurrent.futures as cf
+import os
+import shutil
+import subprocess
+import sys
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+CSRC = os.path.join(PKG, "csrc")
+OBJ = os.path.join(ROOT, "build", "obj")
+LIB = os.path.join(PKG, "libcapacmd_gpu.so")
+REF_SRC = "/root/reference"
+
+SOURCES = ["io.cpp", "api.cu", "k_list.cu", "k_pair.cu", "k_cpim.cu", "k_md.cu", "k_mixed.cu"]
+
+
+def nvcc() -> str:
+    for cand in (shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def _flags() -> list[str]:
+    return ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
+            "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall", f"-I{os.path.join(ROOT, 'include')}", f"-I{CSRC}",
+            "--expt-relaxed-constexpr"]
+
+
+def _compile(src: str, verbose: bool) -> str:
+    out = os.path.join(OBJ, os.path.splitext(src)[0] + ".o")
+    path = os.path.join(CSRC, src)
+    deps = [path] + [os.path.join(CSRC, h) for h in os.listdir(CSRC) if h.endswith((".h", ".cuh"))]
+    deps.append(os.path.join(ROOT, "include", "capacmd.h"))
+    if os.path.exists(out) and os.path.getmtime(out) >= max(os.path.getmtime(d) for d in deps):
+        return out
+    cmd = [nvcc()] + _flags() + ["-c", path, "-o", out]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+    return out
+
+
+def build_library(verbose: bool = False) -> str:
+    os.makedirs(OBJ, exist_ok=True)
+    srcs = [s for s in SOURCES if os.path.exists(os.path.join(CSRC, s))]
+    with cf.ThreadPoolExecutor(max_workers=min(8, len(srcs))) as ex:
+        objs = list(ex.map(lambda s: _compile(s, verbose), srcs))
+    if not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(o) for o in objs):
+        cmd = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", LIB] + objs + [
+            "-lcudart"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+    return LIB
+
+
+def build_oracle(verbose: bool = False) -> None:
+    """Compile the C restatement and, where its sources exist, the reference."""
+    odir = os.path.join(ROOT, "oracle")
+    subprocess.run(["make", "-s", "-C", odir], check=True)
+    if os.path.isdir(REF_SRC):
+        subprocess.run(["make", "-s", "-C", odir, "ref", f"REF={REF_SRC}"], check=True)
+
+
+def main() -> int:
+    verbose = "-v" in sys.argv
+    build_library(verbose)
+    build_oracle(verbose)
+    print(LIB)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,792 @@
+// C ABI of the force-and-solve path: context set-up, the mpi_force-equivalent
+// orchestration (force.c:2097-2320), the MD loop (mpi-main.c:874-1013) and
+// state transfer.  All state lives on one device; one stream orders the work.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "ctx.h"
+
+namespace capac {
+
+namespace {
+thread_local std::string g_last_error;
+
+template <class T>
+T *dalloc(size_t n)
+{
+    T *p = nullptr;
+    CAPAC_CUDA(cudaMalloc(&p, sizeof(T) * (n > 0 ? n : 1)));
+    return p;
+}
+
+template <class T>
+T *dupload(const T *h, size_t n, cudaStream_t s)
+{
+    T *p = dalloc<T>(n);
+    if (n > 0 && h) CAPAC_CUDA(cudaMemcpyAsync(p, h, sizeof(T) * n, cudaMemcpyHostToDevice, s));
+    return p;
+}
+
+void check_ctx(capac_ctx *c)
+{
+    if (!c) throw Error(CAPAC_ERR_INVALID, "null context");
+}
+
+void check_flags(capac_ctx *c)
+{
+    CAPAC_CUDA(cudaMemcpyAsync(c->h_flags, c->flags, sizeof(int) * 4, cudaMemcpyDeviceToHost, c->stream));
+    CAPAC_CUDA(cudaStreamSynchronize(c->stream));
+    if (c->h_flags[2]) {
+        const bool first = c->h_flags[2] & 1;
+        CAPAC_CUDA(cudaMemsetAsync(c->flags + 2, 0, sizeof(int), c->stream));
+        throw Error(CAPAC_ERR_RATTLE, first ? "RATTLE_1 not converged!" : "RATTLE_2 not converged!");
+    }
+}
+
+void record(capac_ctx *c, int k) { CAPAC_CUDA(cudaEventRecord(c->ev[k], c->stream)); }
+
+// One mpi_force equivalent on the device state; solve = false keeps the
+// induced vector as it is.
+void force(capac_ctx *c, bool solve = true)
+{
+    cudaStream_t s = c->stream;
+    record(c, 0);
+    launch_list_maintenance(c, false);
+    launch_pack_positions(c);
+    CAPAC_CUDA(cudaMemsetAsync(c->fx, 0, sizeof(double) * c->N, s));
+    CAPAC_CUDA(cudaMemsetAsync(c->fy, 0, sizeof(double) * c->N, s));
+    CAPAC_CUDA(cudaMemsetAsync(c->fz, 0, sizeof(double) * c->N, s));
+    CAPAC_CUDA(cudaMemsetAsync(c->pot, 0, sizeof(double) * 15, s));
+    CAPAC_CUDA(cudaMemsetAsync(c->vir, 0, sizeof(double) * 9, s));
+    record(c, 1);
+    const bool cpim = c->M > 0 && c->use_cpff;
+    if (c->M > 0) launch_qsc(c);
+    record(c, 2);
+    if (cpim) launch_cpim_rhs(c);
+    record(c, 3);
+    if (cpim) launch_cpim_matrix(c);
+    record(c, 4);
+    int st = CAPAC_OK;
+    if (cpim && solve) st = run_bicgstab(c);
+    record(c, 5);
+    launch_pair_forces(c, 0);
+    record(c, 6);
+    if (cpim) launch_cpim_metal_forces(c);
+    launch_external_field(c);
+    record(c, 7);
+    if (st != CAPAC_OK) {
+        char msg[160];
+        snprintf(msg, sizeof msg, "Error: bicg_stab not converged. rTr= %e, bTb= %e", c->h_ss->rTr, c->h_ss->bTb);
+        throw Error(st, msg);
+    }
+}
+
+void md_step(capac_ctx *c)
+{
+    const long step = ++c->md_step;
+    const bool nvt = c->ensemble == CAPAC_NVT;
+    launch_heating(c, step);
+    if (nvt) launch_nhc(c);
+    launch_md_half_kick(c, nvt);
+    launch_md_drift(c);
+    launch_rattle(c, 0);
+    force(c);
+    check_flags(c);
+    launch_sum_potential(c);
+    launch_md_half_kick(c, false);
+    launch_rattle(c, 1);
+    launch_kinetic(c);
+    if (nvt) {
+        launch_nhc(c);
+        launch_scale_velocities(c);
+    }
+    launch_remove_com(c);
+    launch_kinetic(c);
+    if (step % c->n_save == 0) {
+        launch_apply_pbc(c);
+        launch_fmax_rms(c);
+    }
+}
+
+double *state_array(capac_ctx *c, const std::string &n, int *count)
+{
+    const int N = c->N;
+    struct E { const char *nm; double *p; int cnt; } tab[] = {
+        {"rx", c->rx, N}, {"ry", c->ry, N}, {"rz", c->rz, N}, {"vx", c->vx, N}, {"vy", c->vy, N},
+        {"vz", c->vz, N}, {"fx", c->fx, N}, {"fy", c->fy, N}, {"fz", c->fz, N},
+        {"potential", c->pot, 15}, {"virial", c->vir, 9},
+        {"vec_pq", c->vec_pq, c->M > 0 ? c->n_mat : 0}, {"vec_ext", c->vec_ext, c->M > 0 ? c->n_mat : 0},
+        {"diag_relay", c->diag, c->M > 0 ? c->n_mat : 0}, {"inv_sqrt_dens", c->isd, c->M},
+    };
+    for (auto &e : tab) {
+        if (n == e.nm) {
+            *count = e.cnt;
+            return e.p;
+        }
+    }
+    return nullptr;
+}
+
+}  // namespace
+
+void set_last_error(const std::string &msg) { g_last_error = msg; }
+
+constexpr int kProfSlots = 4096;
+
+void prof_flush(capac_ctx *c)
+{
+    Profiler &p = c->prof;
+    if (p.used == 0) return;
+    CAPAC_CUDA(cudaStreamSynchronize(c->stream));
+    for (int s = 0; s < p.used; ++s) {
+        float ms = 0.f;
+        CAPAC_CUDA(cudaEventElapsedTime(&ms, p.ev[2 * s], p.ev[2 * s + 1]));
+        p.ms[p.cls[s]] += ms;
+        p.count[p.cls[s]] += 1;
+    }
+    p.used = 0;
+}
+
+void prof_begin(capac_ctx *c, int cls)
+{
+    Profiler &p = c->prof;
+    if (!p.on) return;
+    if (p.used == kProfSlots) prof_flush(c);
+    p.cls[p.used] = cls;
+    CAPAC_CUDA(cudaEventRecord(p.ev[2 * p.used], c->stream));
+}
+
+void prof_end(capac_ctx *c)
+{
+    Profiler &p = c->prof;
+    if (!p.on) return;
+    CAPAC_CUDA(cudaEventRecord(p.ev[2 * p.used + 1], c->stream));
+    ++p.used;
+}
+
+void cuda_check(cudaError_t e, const char *what)
+{
+    if (e != cudaSuccess) throw Error(CAPAC_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+}  // namespace capac
+
+using namespace capac;
+
+extern "C" {
+
+const char *capac_last_error(void) { return g_last_error.c_str(); }
+
+void capac_options_default(capac_options *o)
+{
+    if (!o) return;
+    memset(o, 0, sizeof *o);
+    o->precision = CAPAC_PREC_FP64;
+    o->device = 0;
+    o->skin = 0.2;
+    o->list_every = 0;
+    o->max_neighbors = 0;
+    o->solver_tol = 0.0;
+    o->refine_tol = 1.0e-10;
+}
+
+int capac_create(const capac_desc *d, const capac_options *opt, capac_ctx **out)
+{
+    return guard([&] {
+        if (!d || !out) throw Error(CAPAC_ERR_INVALID, "null argument");
+        *out = nullptr;
+        if (d->n_bonded_terms > 0 || d->n_vsites_total > 0)
+            throw Error(CAPAC_ERR_UNSUPPORTED, "bonded terms and virtual sites are outside this path");
+        if (d->n_atoms <= 1 || d->n_atoms >= (1 << kIdxBits))
+            throw Error(CAPAC_ERR_INVALID, "atom count out of range");
+        if (d->n_types <= 0 || d->n_types > 255) throw Error(CAPAC_ERR_INVALID, "type count out of range");
+        if (d->r_cut <= 0.0) throw Error(CAPAC_ERR_INVALID, "cut_off_radius must be positive");
+        for (int a = 0; a < 3; ++a)
+            if (!(d->box[a] > 0.0)) throw Error(CAPAC_ERR_INVALID, "box lengths must be positive");
+        for (int k = 0; k < d->n_nps; ++k)
+            if (d->n_metal == 0 || d->np_start[k] < d->metal_min || d->np_end[k] > d->metal_max ||
+                d->np_start[k] > d->np_end[k])
+                throw Error(CAPAC_ERR_INVALID, "START_END_CHG range outside MM_METAL");
+        if (d->n_nps > 256) throw Error(CAPAC_ERR_UNSUPPORTED, "more than 256 nanoparticles");
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+            throw Error(CAPAC_ERR_NO_DEVICE, "no CUDA device");
+        capac_options o;
+        capac_options_default(&o);
+        if (opt) o = *opt;
+        if (o.skin <= 0.0) o.skin = 0.2;
+        if (o.device < 0 || o.device >= ndev) throw Error(CAPAC_ERR_NO_DEVICE, "device ordinal out of range");
+        cudaDeviceProp prop;
+        CAPAC_CUDA(cudaGetDeviceProperties(&prop, o.device));
+        if (prop.major != 10) throw Error(CAPAC_ERR_NO_DEVICE, std::string("needs an sm_100 device, found ") + prop.name);
+        CAPAC_CUDA(cudaSetDevice(o.device));
+
+        capac_ctx *c = new capac_ctx();
+        try {
+            c->opt = o;
+            c->device = o.device;
+            derive(d, &c->c);
+            c->N = d->n_atoms;
+            c->M = d->n_metal;
+            c->n_nps = d->n_nps;
+            c->n_mat = c->c.n_mat;
+            c->n_mols = d->n_mols;
+            c->mol_types = d->mol_types;
+            c->ensemble = d->ensemble;
+            c->fix_metal = d->fix_metal;
+            c->use_cpff = d->use_cpff;
+            c->n_save = d->n_save > 0 ? d->n_save : 1;
+            c->n_heating = d->n_heating;
+            c->dt = d->dt;
+            c->metal_min = d->metal_min;
+            c->has_cstr = d->n_cstr_total > 0;
+            CAPAC_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+            cudaStream_t s = c->stream;
+            for (auto &e : c->ev) CAPAC_CUDA(cudaEventCreate(&e));
+            const size_t N = c->N;
+
+            // state
+            c->rx = dupload(d->rx, N, s); c->ry = dupload(d->ry, N, s); c->rz = dupload(d->rz, N, s);
+            c->vx = dupload(d->vx, N, s); c->vy = dupload(d->vy, N, s); c->vz = dupload(d->vz, N, s);
+            c->fx = dalloc<double>(N); c->fy = dalloc<double>(N); c->fz = dalloc<double>(N);
+            c->ox = dalloc<double>(N); c->oy = dalloc<double>(N); c->oz = dalloc<double>(N);
+            c->rx0 = dalloc<double>(N); c->ry0 = dalloc<double>(N); c->rz0 = dalloc<double>(N);
+            c->pos4 = dalloc<double4>(N);
+            if (o.precision == CAPAC_PREC_MIXED) c->pos4f = dalloc<float4>(N);
+
+            // topology
+            c->type = dupload(d->atom_type, N, s);
+            c->mol_id = dupload(d->mol_id, N, s);
+            c->mol_type = dupload(d->mol_type, N, s);
+            c->atom_in_mol = dupload(d->atom_in_mol, N, s);
+            c->is_metal = dupload(d->is_metal, N, s);
+            c->charge = dupload(d->charge, N, s);
+            c->mass = dupload(d->mass, N, s);
+            c->inv_mass = dupload(d->inv_mass, N, s);
+            const int T = d->mol_types;
+            size_t excl_n = 0;
+            for (int m = 0; m < T; ++m) excl_n = std::max(excl_n, (size_t)d->excl_offset[m] + (size_t)d->mol_atoms[m] * d->mol_atoms[m]);
+            c->mol_atoms = dupload(d->mol_atoms, T, s);
+            c->excl_offset = dupload(d->excl_offset, T, s);
+            c->excl = dupload(d->excl, excl_n, s);
+            const int NT = d->n_types;
+            std::vector<double4> par(NT * NT);
+            for (int k = 0; k < NT * NT; ++k) par[k] = make_double4(d->nb_c6[k], d->nb_c12[k], d->nb_a[k], d->nb_b[k]);
+            c->nb_funct = dupload(d->nb_funct, (size_t)NT * NT, s);
+            c->nb_par = dupload(par.data(), par.size(), s);
+            c->mol_first = dupload(d->mol_first, d->n_mols, s);
+            c->mol_last = dupload(d->mol_last, d->n_mols, s);
+            c->cstr_off = dupload(d->cstr_offset, T, s);
+            c->cstr_cnt = dupload(d->cstr_count, T, s);
+            size_t ncs = 0;
+            for (int m = 0; m < T; ++m) ncs = std::max(ncs, (size_t)d->cstr_offset[m] + d->cstr_count[m]);
+            c->cstr_i = dupload(d->cstr_i, ncs, s);
+            c->cstr_j = dupload(d->cstr_j, ncs, s);
+            c->cstr_r = dupload(d->cstr_r, ncs, s);
+            c->h_np_start.assign(d->np_start, d->np_start + d->n_nps);
+            c->h_np_end.assign(d->np_end, d->np_end + d->n_nps);
+            c->np_start = dupload(d->np_start, d->n_nps, s);
+            c->np_end = dupload(d->np_end, d->n_nps, s);
+            c->np_charge = dupload(d->np_charge, d->n_nps, s);
+
+            // parameters
+            DevParams &P = c->P;
+            for (int a = 0; a < 3; ++a) {
+                P.box.L[a] = d->box[a];
+                P.box.H[a] = d->box[a] * 0.5;
+            }
+            P.N = c->N;
+            P.M = c->M;
+            P.n_mat = c->n_mat;
+            P.n_nps = c->n_nps;
+            P.n_types = NT;
+            P.metal_min = c->M > 0 ? d->metal_min : 0;
+            P.use_vdw = d->use_vdw;
+            P.use_coulomb = d->use_coulomb;
+            P.rc = d->r_cut;
+            P.rc2 = c->c.r_cut2;
+            P.list_r2 = (d->r_cut + o.skin) * (d->r_cut + o.skin);
+            P.inv_rc12 = c->c.inv_rc12;
+            P.inv_rc6 = c->c.inv_rc6;
+            P.w_alpha = d->w_alpha;
+            P.w_a2_sqrtpi = c->c.w_a2_sqrtpi;
+            P.w_const = c->c.w_const;
+            P.w_erfc_arcut = c->c.w_erfc_arcut;
+            P.inv_polar = c->c.inv_polar;
+            P.inv_capac = c->c.inv_capac;
+            P.inv_r_qq = c->c.inv_r_qq;
+            P.inv_r_pq = c->c.inv_r_pq;
+            P.inv_r_pp = c->c.inv_r_pp;
+            P.qsc_eps = d->qsc_eps;
+            P.qsc_c = d->qsc_c;
+            P.qsc_a = d->qsc_a;
+            P.qsc_n = d->qsc_n;
+            P.qsc_m = d->qsc_m;
+            for (int a = 0; a < 3; ++a) P.efield[a] = d->efield[a];
+            P.type = c->type;
+            P.mol_id = c->mol_id;
+            P.mol_type = c->mol_type;
+            P.atom_in_mol = c->atom_in_mol;
+            P.is_metal = c->is_metal;
+            P.charge = c->charge;
+            P.mass = c->mass;
+            P.inv_mass = c->inv_mass;
+            P.mol_atoms = c->mol_atoms;
+            P.excl_offset = c->excl_offset;
+            P.excl = c->excl;
+            P.nb_funct = c->nb_funct;
+            P.nb_par = c->nb_par;
+            P.np_start = c->np_start;
+            P.np_end = c->np_end;
+            P.np_charge = c->np_charge;
+
+            // neighbour list: capacity from the densest plausible environment
+            {
+                const double V = d->box[0] * d->box[1] * d->box[2];
+                const double rl = d->r_cut + o.skin;
+                const double sphere = 4.0 / 3.0 * M_PI * rl * rl * rl;
+                double dens = std::max((double)N / V, 60.0);  // at least metallic gold density
+                long est = (long)(1.25 * dens * sphere) + 64;
+                if (o.max_neighbors > 0) est = o.max_neighbors;
+                est = std::min<long>(est, (long)N);
+                c->cap = (int)((est + 31) & ~31L);
+            }
+            c->nbr = dalloc<uint32_t>(N * (size_t)c->cap);
+            c->nnb = dalloc<int>(N);
+            c->cell_key = dalloc<int>(N);
+            c->cell_key_sorted = dalloc<int>(N);
+            c->atom_ids = dalloc<int>(N);
+            c->cell_atoms = dalloc<int>(N);
+            c->flags = dalloc<int>(4);
+            CAPAC_CUDA(cudaMemsetAsync(c->flags, 0, sizeof(int) * 4, s));
+            CAPAC_CUDA(cudaMallocHost(&c->h_flags, sizeof(int) * 4));
+
+            // metal / CPIM
+            if (c->M > 0) {
+                const int M = c->M, n = c->n_mat;
+                c->Mp = (M + 31) & ~31;
+                c->isd = dalloc<double>(M);
+                c->vec_ext = dalloc<double>(n);
+                c->vec_pq = dalloc<double>(n);
+                c->diag = dalloc<double>(n);
+                CAPAC_CUDA(cudaMemsetAsync(c->vec_ext, 0, sizeof(double) * n, s));
+                CAPAC_CUDA(cudaMemsetAsync(c->vec_pq, 0, sizeof(double) * n, s));
+                std::vector<double> diag(n, 1.0);
+                for (int i = 0; i < M; ++i) {
+                    diag[3 * i] = diag[3 * i + 1] = diag[3 * i + 2] = c->c.inv_polar;
+                    diag[3 * M + i] = -c->c.inv_capac;
+                }
+                CAPAC_CUDA(cudaMemcpyAsync(c->diag, diag.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s));
+                CAPAC_CUDA(cudaStreamSynchronize(s));
+                if (c->use_cpff) {
+                    c->mat = dalloc<double>((size_t)M * 16 * c->Mp);
+                    c->bw = dalloc<double>((size_t)n * 11);
+                    CAPAC_CUDA(cudaMemsetAsync(c->bw, 0, sizeof(double) * n * 11, s));
+                }
+                c->nnz = 0;
+            }
+            c->ss = dalloc<SolverScalars>(1);
+            CAPAC_CUDA(cudaMemsetAsync(c->ss, 0, sizeof(SolverScalars), s));
+            CAPAC_CUDA(cudaMallocHost(&c->h_ss, sizeof(SolverScalars)));
+            memset(c->h_ss, 0, sizeof(SolverScalars));
+
+            c->partials_cap = partials_needed(c);
+            c->partials = dalloc<double>(c->partials_cap);
+            c->pot = dalloc<double>(15);
+            c->vir = dalloc<double>(9);
+            CAPAC_CUDA(cudaMemsetAsync(c->pot, 0, sizeof(double) * 15, s));
+            CAPAC_CUDA(cudaMemsetAsync(c->vir, 0, sizeof(double) * 9, s));
+            ThermoState th;
+            memset(&th, 0, sizeof th);
+            th.ref_temp = d->ref_temp;
+            th.ext_temp = d->ref_temp;
+            th.kT = c->c.kT;
+            th.scale = 1.0;
+            th.vQ[0] = d->vq0;
+            c->th = dupload(&th, 1, s);
+            CAPAC_CUDA(cudaMallocHost(&c->h_th, sizeof(ThermoState)));
+            c->h_ss->done = 0;
+            CAPAC_CUDA(cudaStreamSynchronize(s));
+            *out = c;
+        } catch (...) {
+            capac_destroy(c);
+            throw;
+        }
+    });
+}
+
+int capac_destroy(capac_ctx *c)
+{
+    if (!c) return CAPAC_OK;
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    void *dev[] = {c->rx, c->ry, c->rz, c->vx, c->vy, c->vz, c->fx, c->fy, c->fz, c->ox, c->oy, c->oz,
+                   c->rx0, c->ry0, c->rz0, c->pos4, c->pos4f, c->type, c->mol_id, c->mol_type,
+                   c->atom_in_mol, c->is_metal, c->charge, c->mass, c->inv_mass, c->mol_atoms,
+                   c->excl_offset, c->excl, c->nb_funct, c->nb_par, c->mol_first, c->mol_last, c->cstr_off,
+                   c->cstr_cnt, c->cstr_i, c->cstr_j, c->cstr_r, c->np_start, c->np_end, c->np_charge,
+                   c->nbr, c->nnb, c->cell_key, c->cell_key_sorted, c->atom_ids, c->cell_atoms,
+                   c->cell_start, c->cell_end, c->sort_tmp, c->flags, c->isd, c->vec_ext, c->vec_pq,
+                   c->diag, c->mat, c->matf, c->bw, c->bwf, c->ss, c->partials, c->pot, c->vir, c->th};
+    for (void *p : dev)
+        if (p) cudaFree(p);
+    if (c->h_flags) cudaFreeHost(c->h_flags);
+    if (c->h_ss) cudaFreeHost(c->h_ss);
+    if (c->h_th) cudaFreeHost(c->h_th);
+    for (auto &e : c->ev)
+        if (e) cudaEventDestroy(e);
+    for (auto &e : c->prof.ev)
+        if (e) cudaEventDestroy(e);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return CAPAC_OK;
+}
+
+int capac_force(capac_ctx *c)
+{
+    return guard([&] {
+        check_ctx(c);
+        force(c);
+        check_flags(c);
+    });
+}
+
+int capac_mpi_force(capac_ctx *c, const double *rx, const double *ry, const double *rz, double *fx, double *fy,
+                    double *fz, double *potential, double *virial, double *vec_pq, double *vec_ext,
+                    double *diag_relay, double *inv_sqrt_dens)
+{
+    return guard([&] {
+        check_ctx(c);
+        if (!rx || !ry || !rz) throw Error(CAPAC_ERR_INVALID, "positions are required");
+        cudaStream_t s = c->stream;
+        const size_t nb = sizeof(double) * c->N;
+        CAPAC_CUDA(cudaMemcpyAsync(c->rx, rx, nb, cudaMemcpyHostToDevice, s));
+        CAPAC_CUDA(cudaMemcpyAsync(c->ry, ry, nb, cudaMemcpyHostToDevice, s));
+        CAPAC_CUDA(cudaMemcpyAsync(c->rz, rz, nb, cudaMemcpyHostToDevice, s));
+        if (vec_pq && c->M > 0)
+            CAPAC_CUDA(cudaMemcpyAsync(c->vec_pq, vec_pq, sizeof(double) * c->n_mat, cudaMemcpyHostToDevice, s));
+        force(c);
+        if (fx) CAPAC_CUDA(cudaMemcpyAsync(fx, c->fx, nb, cudaMemcpyDeviceToHost, s));
+        if (fy) CAPAC_CUDA(cudaMemcpyAsync(fy, c->fy, nb, cudaMemcpyDeviceToHost, s));
+        if (fz) CAPAC_CUDA(cudaMemcpyAsync(fz, c->fz, nb, cudaMemcpyDeviceToHost, s));
+        if (potential) CAPAC_CUDA(cudaMemcpyAsync(potential, c->pot, sizeof(double) * 15, cudaMemcpyDeviceToHost, s));
+        if (virial) CAPAC_CUDA(cudaMemcpyAsync(virial, c->vir, sizeof(double) * 9, cudaMemcpyDeviceToHost, s));
+        if (c->M > 0) {
+            const size_t mb = sizeof(double) * c->n_mat;
+            if (vec_pq) CAPAC_CUDA(cudaMemcpyAsync(vec_pq, c->vec_pq, mb, cudaMemcpyDeviceToHost, s));
+            if (vec_ext) CAPAC_CUDA(cudaMemcpyAsync(vec_ext, c->vec_ext, mb, cudaMemcpyDeviceToHost, s));
+            if (diag_relay) CAPAC_CUDA(cudaMemcpyAsync(diag_relay, c->diag, mb, cudaMemcpyDeviceToHost, s));
+            if (inv_sqrt_dens)
+                CAPAC_CUDA(cudaMemcpyAsync(inv_sqrt_dens, c->isd, sizeof(double) * c->M, cudaMemcpyDeviceToHost, s));
+        }
+        check_flags(c);
+    });
+}
+
+int capac_force_given_pq(capac_ctx *c)
+{
+    return guard([&] {
+        check_ctx(c);
+        force(c, false);
+        check_flags(c);
+    });
+}
+
+int capac_cpim_matvec(capac_ctx *c, const double *x, double *y)
+{
+    return guard([&] {
+        check_ctx(c);
+        if (!x || !y) throw Error(CAPAC_ERR_INVALID, "null argument");
+        if (c->M == 0 || !c->mat) throw Error(CAPAC_ERR_INVALID, "no CPIM matrix in this system");
+        double *dx = c->bw + (size_t)W_Y_SLOT * c->n_mat, *dy = c->bw + (size_t)W_V_SLOT * c->n_mat;
+        const size_t nb = sizeof(double) * c->n_mat;
+        CAPAC_CUDA(cudaMemcpyAsync(dx, x, nb, cudaMemcpyHostToDevice, c->stream));
+        launch_cpim_spmv(c, dx, dy);
+        CAPAC_CUDA(cudaMemcpyAsync(y, dy, nb, cudaMemcpyDeviceToHost, c->stream));
+        CAPAC_CUDA(cudaStreamSynchronize(c->stream));
+    });
+}
+
+int capac_qsc(capac_ctx *c)
+{
+    return guard([&] {
+        check_ctx(c);
+        launch_pack_positions(c);
+        if (c->M > 0) launch_qsc(c);
+        CAPAC_CUDA(cudaStreamSynchronize(c->stream));
+    });
+}
+
+int capac_cpff_vec_ext(capac_ctx *c)
+{
+    return guard([&] {
+        check_ctx(c);
+        if (c->M == 0) return;
+        launch_list_maintenance(c, false);
+        launch_pack_positions(c);
+        launch_cpim_rhs(c);
+        CAPAC_CUDA(cudaStreamSynchronize(c->stream));
+    });
+}
+
+int capac_cpff_mat_relay(capac_ctx *c, long *nnz)
+{
+    return guard([&] {
+        check_ctx(c);
+        if (c->M == 0 || !c->mat) return;
+        launch_pack_positions(c);
+        launch_cpim_matrix(c);
+        CAPAC_CUDA(cudaStreamSynchronize(c->stream));
+        // entries the reference's COO form would hold (cpff.c:245-516):
+        // 16 per off-diagonal block, 4 per diagonal block, 2 per NP member
+        if (nnz) {
+            long lam = 0;
+            for (int k = 0; k < c->n_nps; ++k) lam += 2L * (c->h_np_end[k] - c->h_np_start[k] + 1);
+            *nnz = 16L * c->M * (c->M - 1) + 4L * c->M + lam;
+        }
+    });
+}
+
+int capac_bicgstab(capac_ctx *c, int *iterations)
+{
+    return guard([&] {
+        check_ctx(c);
+        if (c->M == 0 || !c->mat) return;
+        const int st = run_bicgstab(c);
+        if (iterations) *iterations = c->last_iters;
+        if (st != CAPAC_OK) throw Error(st, "Error: bicg_stab not converged.");
+    });
+}
+
+int capac_cpff_force(capac_ctx *c)
+{
+    return guard([&] {
+        check_ctx(c);
+        if (c->M == 0 || !c->use_cpff) return;
+        launch_list_maintenance(c, false);
+        launch_pack_positions(c);
+        launch_pair_forces(c, 1);
+        launch_cpim_metal_forces(c);
+        CAPAC_CUDA(cudaStreamSynchronize(c->stream));
+    });
+}
+
+int capac_md_init(capac_ctx *c)
+{
+    return guard([&] {
+        check_ctx(c);
+        force(c);
+        check_flags(c);
+        launch_sum_potential(c);
+        launch_remove_com(c);
+        launch_kinetic(c);
+        CAPAC_CUDA(cudaMemcpyAsync(c->h_th, c->th, sizeof(ThermoState), cudaMemcpyDeviceToHost, c->stream));
+        CAPAC_CUDA(cudaStreamSynchronize(c->stream));
+        c->h_th->first_temp = c->h_th->inst_temp;
+        c->h_th->ext_temp = c->h_th->ref_temp;
+        CAPAC_CUDA(cudaMemcpyAsync(c->th, c->h_th, sizeof(ThermoState), cudaMemcpyHostToDevice, c->stream));
+        launch_fmax_rms(c);
+        CAPAC_CUDA(cudaStreamSynchronize(c->stream));
+        c->md_step = 0;
+    });
+}
+
+int capac_md_steps(capac_ctx *c, int n)
+{
+    return guard([&] {
+        check_ctx(c);
+        if (n < 0) throw Error(CAPAC_ERR_INVALID, "negative step count");
+        for (int k = 0; k < n; ++k) md_step(c);
+        CAPAC_CUDA(cudaStreamSynchronize(c->stream));
+        check_flags(c);
+    });
+}
+
+int capac_get(capac_ctx *c, const char *name, double *out)
+{
+    int count = -1;
+    const int st = guard([&] {
+        check_ctx(c);
+        if (!name || !out) throw Error(CAPAC_ERR_INVALID, "null argument");
+        std::string n(name);
+        CAPAC_CUDA(cudaStreamSynchronize(c->stream));
+        int cnt = 0;
+        if (double *p = state_array(c, n, &cnt)) {
+            if (cnt > 0) CAPAC_CUDA(cudaMemcpy(out, p, sizeof(double) * cnt, cudaMemcpyDeviceToHost));
+            count = cnt;
+            return;
+        }
+        if (n == "vQ" || n == "thermo" || n == "fmax_rms") {
+            ThermoState th;
+            CAPAC_CUDA(cudaMemcpy(&th, c->th, sizeof th, cudaMemcpyDeviceToHost));
+            if (n == "vQ") {
+                memcpy(out, th.vQ, sizeof th.vQ);
+                count = kNhc;
+            } else if (n == "thermo") {
+                out[0] = th.eksum;
+                out[1] = th.inst_temp;
+                out[2] = th.ref_temp;
+                out[3] = c->c.ndf;
+                count = 4;
+            } else {
+                out[0] = th.fmax;
+                out[1] = th.frms;
+                count = 2;
+            }
+            return;
+        }
+        if (n == "box") {
+            for (int a = 0; a < 3; ++a) {
+                out[a] = c->P.box.L[a];
+                out[3 + a] = c->P.box.H[a];
+            }
+            count = 6;
+            return;
+        }
+        throw Error(CAPAC_ERR_INVALID, "unknown array " + n);
+    });
+    return st == CAPAC_OK ? count : st;
+}
+
+int capac_set(capac_ctx *c, const char *name, const double *in)
+{
+    int count = -1;
+    const int st = guard([&] {
+        check_ctx(c);
+        if (!name || !in) throw Error(CAPAC_ERR_INVALID, "null argument");
+        std::string n(name);
+        CAPAC_CUDA(cudaStreamSynchronize(c->stream));
+        int cnt = 0;
+        double *p = state_array(c, n, &cnt);
+        if (!p || n == "potential" || n == "virial" || n == "inv_sqrt_dens" || n == "diag_relay")
+            throw Error(CAPAC_ERR_INVALID, "array " + n + " cannot be set");
+        if (cnt > 0) CAPAC_CUDA(cudaMemcpy(p, in, sizeof(double) * cnt, cudaMemcpyHostToDevice));
+        if (n == "rx" || n == "ry" || n == "rz") c->list_valid = false;
+        count = cnt;
+    });
+    return st == CAPAC_OK ? count : st;
+}
+
+int capac_get_stats(capac_ctx *c, capac_stats *out)
+{
+    return guard([&] {
+        check_ctx(c);
+        if (!out) throw Error(CAPAC_ERR_INVALID, "null argument");
+        memset(out, 0, sizeof *out);
+        out->solver_iterations = c->last_iters;
+        out->solver_outer = c->last_outer;
+        out->solver_rel_residual = c->last_rel_res;
+        out->list_builds = c->list_builds;
+        out->list_capacity = c->cap;
+        out->md_step = c->md_step;
+        if (c->list_valid) {
+            std::vector<int> nn(c->N);
+            CAPAC_CUDA(cudaStreamSynchronize(c->stream));
+            CAPAC_CUDA(cudaMemcpy(nn.data(), c->nnb, sizeof(int) * c->N, cudaMemcpyDeviceToHost));
+            long tot = 0, mx = 0;
+            for (int v : nn) {
+                tot += v;
+                mx = std::max<long>(mx, v);
+            }
+            out->list_entries = tot;
+            out->max_neighbors = mx;
+        }
+    });
+}
+
+int capac_pair_fingerprint(capac_ctx *c, int from_list, long *count, unsigned long long *hash)
+{
+    return guard([&] {
+        check_ctx(c);
+        if (!count || !hash) throw Error(CAPAC_ERR_INVALID, "null argument");
+        launch_pair_fingerprint(c, from_list, count, hash);
+    });
+}
+
+int capac_phase_times(capac_ctx *c, double out_ms[15])
+{
+    return guard([&] {
+        check_ctx(c);
+        CAPAC_CUDA(cudaStreamSynchronize(c->stream));
+        for (int k = 0; k < 15; ++k) out_ms[k] = 0.0;
+        auto span = [&](int a, int b) {
+            float ms = 0.f;
+            if (cudaEventElapsedTime(&ms, c->ev[a], c->ev[b]) != cudaSuccess) return 0.0;
+            return (double)ms;
+        };
+        out_ms[10] = span(0, 1);  // list maintenance and packing
+        out_ms[1] = span(1, 2);   // Sutton-Chen density + force
+        out_ms[6] = span(2, 3);   // CPIM vector
+        out_ms[5] = span(3, 4);   // CPIM matrix
+        out_ms[7] = span(4, 5);   // CPIM solve
+        out_ms[4] = span(5, 6);   // nonbonded (+ water side of CPIM)
+        out_ms[8] = span(6, 7);   // CPIM force, external field
+        out_ms[0] = span(0, 7);
+    });
+}
+
+long capac_kernel_launches(capac_ctx *c) { return c ? c->launches : 0; }
+
+int capac_time_md_steps(capac_ctx *c, int n, double *ms)
+{
+    return guard([&] {
+        check_ctx(c);
+        if (!ms || n < 0) throw Error(CAPAC_ERR_INVALID, "bad argument");
+        CAPAC_CUDA(cudaEventRecord(c->ev[14], c->stream));
+        for (int k = 0; k < n; ++k) md_step(c);
+        CAPAC_CUDA(cudaEventRecord(c->ev[15], c->stream));
+        CAPAC_CUDA(cudaEventSynchronize(c->ev[15]));
+        float t = 0.f;
+        CAPAC_CUDA(cudaEventElapsedTime(&t, c->ev[14], c->ev[15]));
+        *ms = t;
+        check_flags(c);
+    });
+}
+
+int capac_profile_enable(capac_ctx *c, int on)
+{
+    return guard([&] {
+        check_ctx(c);
+        Profiler &p = c->prof;
+        if (p.ev.empty()) {
+            p.ev.resize(2 * kProfSlots);
+            p.cls.resize(kProfSlots);
+            for (auto &e : p.ev) CAPAC_CUDA(cudaEventCreate(&e));
+        }
+        prof_flush(c);
+        for (int k = 0; k < K_NCLASS; ++k) {
+            p.count[k] = 0;
+            p.ms[k] = 0.0;
+        }
+        p.spmv_effective = 0;
+        p.on = on != 0;
+    });
+}
+
+int capac_profile_get(capac_ctx *c, const char *cls, long *launches, double *total_ms)
+{
+    return guard([&] {
+        check_ctx(c);
+        if (!cls || !launches || !total_ms) throw Error(CAPAC_ERR_INVALID, "null argument");
+        static const char *names[K_NCLASS] = {"pair", "spmv", "matrix", "cpim_metal", "cpim_rhs",
+                                              "qsc", "list_build", "solver_vec", "integrate"};
+        prof_flush(c);
+        if (0 == strcmp(cls, "spmv_effective")) {
+            *launches = c->prof.spmv_effective;
+            *total_ms = 0.0;
+            return;
+        }
+        for (int k = 0; k < K_NCLASS; ++k) {
+            if (0 == strcmp(cls, names[k])) {
+                *launches = c->prof.count[k];
+                *total_ms = c->prof.ms[k];
+                return;
+            }
+        }
+        throw Error(CAPAC_ERR_INVALID, std::string("unknown kernel class ") + cls);
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,198 @@
+// Device-resident state of one simulation and the launchers of its kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "capacmd.h"
+#include "capac_internal.h"
+#include "device.cuh"
+
+namespace capac {
+
+// Scalars of one BiCGSTAB solve, kept in device memory (bicg_stab.c:280-303).
+struct SolverScalars {
+    double bTb, crit, rho, rho_old, alpha, omega, rTr, rho_next;
+    double res0;     // refinement: FP64 residual norm^2 at the sweep start
+    int iter, done, status, pad;
+};
+
+// Thermostat and integrator scalars (System, typedef.h:353-401).
+struct ThermoState {
+    double eksum, inst_temp, ref_temp, first_temp, ext_temp, kT, scale;
+    double vQ[kNhc], aQ[kNhc];
+    double vcom[4];
+    double fmax, frms;
+};
+
+// Read-only parameters passed by value to the kernels.
+struct DevParams {
+    Box box;
+    int N, M, n_mat, n_nps, n_types, metal_min;
+    int use_vdw, use_coulomb;
+    double rc, rc2, list_r2;  // list_r2 = (rc + skin)^2
+    double inv_rc12, inv_rc6, w_alpha, w_a2_sqrtpi, w_const, w_erfc_arcut;
+    double inv_polar, inv_capac, inv_r_qq, inv_r_pq, inv_r_pp;
+    double qsc_eps, qsc_c, qsc_a;
+    int qsc_n, qsc_m;
+    double efield[3];
+    // per atom
+    const int *type, *mol_id, *mol_type, *atom_in_mol;
+    const unsigned char *is_metal;
+    const double *charge, *mass, *inv_mass;
+    // per molecule type
+    const int *mol_atoms, *excl_offset;
+    const unsigned char *excl;
+    const int *nb_funct;
+    const double4 *nb_par;  // (c6, c12, a, b)
+    // nanoparticles
+    const int *np_start, *np_end;
+    const double *np_charge;
+};
+
+// Kernel classes for the event-based profiler.
+enum KClass { K_PAIR = 0, K_SPMV, K_MATRIX, K_CPIM_METAL, K_CPIM_RHS, K_QSC, K_LIST, K_SOLVER_VEC, K_INTEGRATE, K_NCLASS };
+
+// Pool of CUDA event pairs bracketing launches while profiling is on.
+struct Profiler {
+    bool on = false;
+    std::vector<cudaEvent_t> ev;  // 2 per slot
+    std::vector<int> cls;
+    int used = 0;
+    long count[K_NCLASS] = {};
+    double ms[K_NCLASS] = {};
+    long spmv_effective = 0;  // SpMV launches that did work (1 + 2 per iteration per solve)
+};
+
+}  // namespace capac
+
+struct capac_ctx {
+    capac::DevParams P{};
+    capac_consts c{};
+    capac_options opt{};
+    int N = 0, M = 0, n_mat = 0, n_nps = 0, n_mols = 0, mol_types = 0;
+    int ensemble = 0, fix_metal = 0, use_cpff = 0, n_save = 1, n_heating = 0;
+    int metal_min = 0;
+    double dt = 0.0;
+    bool has_cstr = false;
+    cudaStream_t stream = nullptr;
+    long launches = 0;
+    long md_step = 0;
+    long list_builds = 0;
+    int device = 0;
+
+    // host copies needed on the host side
+    std::vector<int> h_np_start, h_np_end;
+
+    // state (SoA, FP64)
+    double *rx = nullptr, *ry = nullptr, *rz = nullptr, *vx = nullptr, *vy = nullptr, *vz = nullptr;
+    double *fx = nullptr, *fy = nullptr, *fz = nullptr, *ox = nullptr, *oy = nullptr, *oz = nullptr;
+    double4 *pos4 = nullptr;  // (x, y, z, q) packed for gathers
+    float4 *pos4f = nullptr;  // mixed path: FP32 copy
+    // topology
+    int *type = nullptr, *mol_id = nullptr, *mol_type = nullptr, *atom_in_mol = nullptr;
+    unsigned char *is_metal = nullptr;
+    double *charge = nullptr, *mass = nullptr, *inv_mass = nullptr;
+    int *mol_atoms = nullptr, *excl_offset = nullptr;
+    unsigned char *excl = nullptr;
+    int *nb_funct = nullptr;
+    double4 *nb_par = nullptr;
+    int *mol_first = nullptr, *mol_last = nullptr, *cstr_off = nullptr, *cstr_cnt = nullptr;
+    int *cstr_i = nullptr, *cstr_j = nullptr;
+    double *cstr_r = nullptr;
+    int *np_start = nullptr, *np_end = nullptr;
+    double *np_charge = nullptr;
+
+    // neighbour list
+    int cap = 0;             // entries per atom
+    uint32_t *nbr = nullptr; // [N * cap]
+    int *nnb = nullptr;      // [N]
+    double *rx0 = nullptr, *ry0 = nullptr, *rz0 = nullptr;  // positions at the last build
+    int ncell[3] = {1, 1, 1};
+    double cell_len[3] = {0, 0, 0};
+    int n_cells = 1;
+    int *cell_key = nullptr, *cell_key_sorted = nullptr, *atom_ids = nullptr, *cell_atoms = nullptr;
+    int *cell_start = nullptr, *cell_end = nullptr;
+    void *sort_tmp = nullptr;
+    size_t sort_tmp_bytes = 0;
+    int *flags = nullptr;      // [0] rebuild needed, [1] list overflow max count, [2] rattle error
+    int *h_flags = nullptr;    // pinned mirror
+    bool list_valid = false;
+
+    // metal / CPIM
+    int Mp = 0;                  // M padded to a multiple of 32
+    double *isd = nullptr;       // inv_sqrt_dens [M]
+    double *vec_ext = nullptr, *vec_pq = nullptr, *diag = nullptr;  // [n_mat]
+    double *mat = nullptr;       // [M * 16 * Mp] 4x4 blocks, plane layout
+    float *matf = nullptr;       // mixed path copy
+    double *bw = nullptr;        // BiCGSTAB work vectors, 11 * n_mat
+    float *bwf = nullptr;        // mixed path inner-solve vectors
+    capac::SolverScalars *ss = nullptr;
+    capac::SolverScalars *h_ss = nullptr;  // pinned
+    long nnz = 0;
+    int last_iters = 0, last_outer = 0;
+    double last_rel_res = 0.0;
+
+    // reductions and outputs
+    double *partials = nullptr;
+    size_t partials_cap = 0;     // doubles
+    double *pot = nullptr, *vir = nullptr;  // [15], [9]
+    capac::ThermoState *th = nullptr;
+    capac::ThermoState *h_th = nullptr;
+
+    // timing
+    cudaEvent_t ev[16] = {};
+    float phase_ms[15] = {};
+    capac::Profiler prof;
+};
+
+namespace capac {
+
+void cuda_check(cudaError_t e, const char *what);
+#define CAPAC_CUDA(call) ::capac::cuda_check((call), #call)
+
+// Kernel launchers (one stream; every launch is counted).
+void launch_pack_positions(capac_ctx *c);
+void launch_list_maintenance(capac_ctx *c, bool force_rebuild);
+void launch_pair_forces(capac_ctx *c, int mode);  // mode: 0 full, 1 CPIM water side only
+void launch_qsc(capac_ctx *c);
+void launch_cpim_rhs(capac_ctx *c);
+void launch_cpim_matrix(capac_ctx *c);
+int run_bicgstab(capac_ctx *c);  // returns status
+void launch_cpim_spmv(capac_ctx *c, const double *x, double *y);  // plain y = A x
+constexpr int W_Y_SLOT = 7, W_V_SLOT = 4;  // BiCGSTAB work-vector slots used as scratch
+void launch_cpim_metal_forces(capac_ctx *c);
+void launch_external_field(capac_ctx *c);
+void launch_finalize(capac_ctx *c, int nblocks, int K, const int *slots_pot, const int *slots_vir);
+void launch_pair_fingerprint(capac_ctx *c, int from_list, long *count, unsigned long long *hash);
+
+// integrator
+void launch_md_half_kick(capac_ctx *c, bool with_nhc_scale);
+void launch_md_drift(capac_ctx *c);
+void launch_rattle(capac_ctx *c, int second);
+void launch_kinetic(capac_ctx *c);
+void launch_nhc(capac_ctx *c);
+void launch_scale_velocities(capac_ctx *c);
+void launch_remove_com(capac_ctx *c);
+void launch_apply_pbc(capac_ctx *c);
+void launch_fmax_rms(capac_ctx *c);
+void launch_heating(capac_ctx *c, long step);
+void launch_sum_potential(capac_ctx *c);
+
+size_t partials_needed(const capac_ctx *c);
+
+// Profiler hooks: a ProfScope brackets the launches issued in its lifetime.
+void prof_begin(capac_ctx *c, int cls);
+void prof_end(capac_ctx *c);
+void prof_flush(capac_ctx *c);
+struct ProfScope {
+    capac_ctx *c;
+    ProfScope(capac_ctx *cc, int cls) : c(cc) { prof_begin(c, cls); }
+    ~ProfScope() { prof_end(c); }
+};
+
+inline unsigned grid_for(long n, int block) { return (unsigned)((n + block - 1) / block); }
+
+}  // namespace capac

@@ -1,0 +1,765 @@
+// Sutton-Chen and CPIM kernels, FP64, plus the deterministic reductions.
+//
+// Metal atoms are contiguous (MM_METAL min..max).  The CPIM system of size
+// n_mat = 4M + n_NPs is the reference's (cpff.c:205-519): per ordered metal
+// pair (i, j) a 4x4 block over (p_x, p_y, p_z, q) of each atom,
+//
+//     [ A_ij (3x3)   m_ij ]     A_ij = -(c1 (3 r r^T - r^2 I) - c2 r r^T)
+//     [ -m_ij^T      C_ij ]     m_ij = c3 r,  C_ij = -erf(r/R_qq)/r
+//
+// with diagonal blocks diag(1/polar x3, -1/capac), and the charge-neutrality
+// rows/columns (+1 between an NP's Lagrange multiplier and its charges).
+// Blocks are stored densely (the reference has no cut-off here either) as 16
+// planes per block row: mat[(i*16 + e)*Mp + j], e = 4*row + col, so a warp
+// reading consecutive j of one plane is fully coalesced.
+#include "terms.cuh"
+
+namespace capac {
+
+// ---------------------------------------------------------- reductions
+
+struct Slots {
+    int pot[24];
+    int vir[24];
+};
+
+__global__ void __launch_bounds__(256) k_finalize(const double *__restrict__ partials, int nblocks, int K,
+                                                  Slots s, double *pot, double *vir)
+{
+    __shared__ double sh[32];
+    for (int k = 0; k < K; ++k) {
+        double v = 0.0;
+        for (int b = threadIdx.x; b < nblocks; b += blockDim.x) v += partials[(size_t)b * K + k];
+        double t[1] = {v};
+        block_sum<1>(t, sh);
+        if (threadIdx.x == 0) {
+            if (s.pot[k] >= 0) pot[s.pot[k]] += t[0];
+            if (s.vir[k] >= 0) vir[s.vir[k]] += t[0];
+        }
+    }
+}
+
+void launch_finalize(capac_ctx *c, int nblocks, int K, const int *slots_pot, const int *slots_vir)
+{
+    Slots s;
+    for (int k = 0; k < 24; ++k) {
+        s.pot[k] = k < K ? slots_pot[k] : -1;
+        s.vir[k] = k < K ? slots_vir[k] : -1;
+    }
+    k_finalize<<<1, 256, 0, c->stream>>>(c->partials, nblocks, K, s, c->pot, c->vir);
+    ++c->launches;
+}
+
+// --------------------------------------------------------- Sutton-Chen
+
+// mpi_qsc_dens, force.c:385-461: rho_i = sum_{j != i, r < rc} (a/r)^m.
+__global__ void __launch_bounds__(256) k_qsc_density(DevParams P, const double4 *__restrict__ pos4, double *isd)
+{
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (i >= P.M) return;
+    const double4 pi = pos4[P.metal_min + i];
+    double rho = 0.0;
+    for (int j = lane; j < P.M; j += 32) {
+        if (j == i) continue;
+        const double4 pj = pos4[P.metal_min + j];
+        double dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
+        image(dx, dy, dz, P.box);
+        const double r2 = norm2_exact(dx, dy, dz);
+        if (r2 < P.rc2) rho += pow(P.qsc_a / sqrt(r2), (double)P.qsc_m);
+    }
+    rho = warp_sum(rho);
+    if (lane == 0) isd[i] = 1.0 / sqrt(rho);
+}
+
+// mpi_qsc_force, force.c:468-542: forces on i only, virial halved.
+__global__ void __launch_bounds__(256) k_qsc_force(DevParams P, const double4 *__restrict__ pos4,
+                                                   const double *__restrict__ isd, double *fx, double *fy,
+                                                   double *fz, double *partials)
+{
+    __shared__ double sh[32 * 10];
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    double acc[10] = {0.0};  // energy, virial[9]
+    if (i < P.M) {
+        const double4 pi = pos4[P.metal_min + i];
+        const double cm2 = P.qsc_c * P.qsc_m / 2.0;
+        double f0 = 0.0, f1 = 0.0, f2 = 0.0;
+        for (int j = lane; j < P.M; j += 32) {
+            if (j == i) continue;
+            const double4 pj = pos4[P.metal_min + j];
+            double dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
+            image(dx, dy, dz, P.box);
+            const double r2 = norm2_exact(dx, dy, dz);
+            if (r2 >= P.rc2) continue;
+            const double r = sqrt(r2), ar = P.qsc_a / r;
+            const double an = pow(ar, (double)P.qsc_n), am = pow(ar, (double)P.qsc_m);
+            const double f = P.qsc_eps * (P.qsc_n * an - cm2 * (isd[i] + isd[j]) * am) / r2;
+            const double gx = f * dx, gy = f * dy, gz = f * dz;
+            f0 -= gx; f1 -= gy; f2 -= gz;
+            acc[1] -= dx * gx * 0.5; acc[2] -= dx * gy * 0.5; acc[3] -= dx * gz * 0.5;
+            acc[4] -= dy * gx * 0.5; acc[5] -= dy * gy * 0.5; acc[6] -= dy * gz * 0.5;
+            acc[7] -= dz * gx * 0.5; acc[8] -= dz * gy * 0.5; acc[9] -= dz * gz * 0.5;
+            acc[0] += P.qsc_eps * an * 0.5;
+        }
+        f0 = warp_sum(f0);
+        f1 = warp_sum(f1);
+        f2 = warp_sum(f2);
+        if (lane == 0) {
+            const int a = P.metal_min + i;
+            fx[a] += f0;
+            fy[a] += f1;
+            fz[a] += f2;
+            acc[0] -= P.qsc_eps * P.qsc_c / isd[i];
+        }
+    }
+    block_partials<10>(acc, sh, partials);
+}
+
+void launch_qsc(capac_ctx *c)
+{
+    const unsigned grid = grid_for((long)c->M * 32, 256);
+    {
+        ProfScope ps(c, K_QSC);
+        k_qsc_density<<<grid, 256, 0, c->stream>>>(c->P, c->pos4, c->isd);
+        k_qsc_force<<<grid, 256, 0, c->stream>>>(c->P, c->pos4, c->isd, c->fx, c->fy, c->fz, c->partials);
+    }
+    c->launches += 2;
+    static const int pot_slots[10] = {1, -1, -1, -1, -1, -1, -1, -1, -1, -1};
+    static const int vir_slots[10] = {-1, 0, 1, 2, 3, 4, 5, 6, 7, 8};
+    launch_finalize(c, (int)grid, 10, pot_slots, vir_slots);
+}
+
+// ------------------------------------------------------------ CPIM RHS
+
+// mpi_cpff_vec_ext, cpff.c:43-198: field and potential of the permanent
+// charges inside the cut-off at each metal atom, converted to atomic units,
+// plus the uniform external field; NP total charges in the last rows.
+__global__ void __launch_bounds__(256) k_cpim_rhs(DevParams P, const double4 *__restrict__ pos4,
+                                                  const uint32_t *__restrict__ nbr, const int *__restrict__ nnb,
+                                                  int cap, double *vec_ext)
+{
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (blockIdx.x == 0 && threadIdx.x < P.n_nps) vec_ext[4 * P.M + threadIdx.x] = P.np_charge[threadIdx.x];
+    if (i >= P.M) return;
+    const int im = P.metal_min + i;
+    const double4 pi = pos4[im];
+    double ex = 0.0, ey = 0.0, ez = 0.0, v = 0.0;
+    const uint32_t *row = nbr + (size_t)im * cap;
+    for (int k = lane; k < nnb[im]; k += 32) {
+        const int j = nb_index(row[k]);
+        if (P.is_metal[j]) continue;
+        const double4 pj = pos4[j];
+        if (pj.w == 0.0) continue;
+        double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+        image(dx, dy, dz, P.box);
+        const double r2 = norm2_exact(dx, dy, dz);
+        if (r2 >= P.rc2) continue;
+        const double r = sqrt(r2);
+        double ef, vf;
+        if (P.use_coulomb == 1) {
+            const double ec = erfc(P.w_alpha * r), eg = exp(-P.w_alpha * P.w_alpha * r2);
+            ef = kFQQ * pj.w * (ec / r2 + P.w_a2_sqrtpi * eg / r - P.w_const) / r;
+            vf = kFQQ * pj.w * (ec / r - P.w_erfc_arcut + P.w_const * (r - P.rc));
+        } else {
+            ef = kFQQ * pj.w / (r2 * r);
+            vf = kFQQ * pj.w / r;
+        }
+        const double s = ef * kConvE;
+        ex += s * dx;
+        ey += s * dy;
+        ez += s * dz;
+        v += vf * kConvV;
+    }
+    ex = warp_sum(ex);
+    ey = warp_sum(ey);
+    ez = warp_sum(ez);
+    v = warp_sum(v);
+    if (lane == 0) {
+        vec_ext[3 * i + 0] = ex + P.efield[0] * kConvE;
+        vec_ext[3 * i + 1] = ey + P.efield[1] * kConvE;
+        vec_ext[3 * i + 2] = ez + P.efield[2] * kConvE;
+        const double vext = P.efield[0] * pi.x + P.efield[1] * pi.y + P.efield[2] * pi.z;
+        vec_ext[3 * P.M + i] = v - vext * kConvV;
+    }
+}
+
+void launch_cpim_rhs(capac_ctx *c)
+{
+    ProfScope ps(c, K_CPIM_RHS);
+    k_cpim_rhs<<<grid_for((long)c->M * 32 + 32, 256), 256, 0, c->stream>>>(c->P, c->pos4, c->nbr, c->nnb, c->cap,
+                                                                            c->vec_ext);
+    ++c->launches;
+}
+
+// ------------------------------------------------------- CPIM matrix
+
+// One thread per ordered pair (i, j); 16 coalesced plane writes.
+__global__ void __launch_bounds__(128) k_cpim_matrix(DevParams P, const double4 *__restrict__ pos4, int Mp,
+                                                     double *__restrict__ mat)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blockIdx.y;
+    if (j >= Mp) return;
+    double e[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) e[k] = 0.0;
+    if (j < P.M) {
+        if (j == i) {
+            e[0] = e[5] = e[10] = keep_entry(P.inv_polar);
+            e[15] = keep_entry(-P.inv_capac);
+        } else {
+            const double4 pi = pos4[P.metal_min + i], pj = pos4[P.metal_min + j];
+            double r[3] = {pj.x - pi.x, pj.y - pi.y, pj.z - pi.z};
+            image(r[0], r[1], r[2], P.box);
+            r[0] *= kNm2Bohr;
+            r[1] *= kNm2Bohr;
+            r[2] *= kNm2Bohr;
+            const double r2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2], rr = sqrt(r2);
+            const double ipp = P.inv_r_pp, ipq = P.inv_r_pq;
+            const double gpp = exp(-(r2 * ipp * ipp));
+            const double c1 = 1.0 / (r2 * r2 * rr) * (erf(rr * ipp) - 2.0 * kInvSqrtPi * ipp * rr * gpp);
+            const double c2 = 4.0 * kInvSqrtPi * (ipp * ipp * ipp) / r2 * gpp;
+            const double gpq = exp(-(r2 * ipq * ipq));
+            const double c3 = 1.0 / (r2 * rr) * (erf(rr * ipq) - 2.0 * kInvSqrtPi * ipq * rr * gpq);
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+#pragma unroll
+                for (int b = 0; b < 3; ++b) {
+                    const double dab = a == b ? 1.0 : 0.0;
+                    e[4 * a + b] = keep_entry(-(c1 * (3.0 * r[a] * r[b] - dab * r2) - c2 * r[a] * r[b]));
+                }
+                e[4 * a + 3] = keep_entry(c3 * r[a]);
+                e[12 + a] = keep_entry(-c3 * r[a]);
+            }
+            e[15] = keep_entry(-erf(rr * P.inv_r_qq) / rr);
+        }
+    }
+    double *base = mat + (size_t)i * 16 * Mp + j;
+#pragma unroll
+    for (int k = 0; k < 16; ++k) base[(size_t)k * Mp] = e[k];
+}
+
+void launch_cpim_matrix(capac_ctx *c)
+{
+    dim3 grid(grid_for(c->Mp, 128), c->M);
+    ProfScope ps(c, K_MATRIX);
+    k_cpim_matrix<<<grid, 128, 0, c->stream>>>(c->P, c->pos4, c->Mp, c->mat);
+    ++c->launches;
+}
+
+// ------------------------------------------------------------ SpMV
+
+// y = A x for the CPIM system, one block per row block (metal atom) plus one
+// block per Lagrange row.  Epilogue: per-block dot partials
+//   DOT_R0:  (r0, y)            -> partials[b*2]
+//   DOT_KT:  Kt = K y; (Kt, z), (Kt, Kt) -> partials[b*2], partials[b*2+1]
+enum { DOT_NONE = 0, DOT_R0 = 1, DOT_KT = 2 };
+
+template <int DOT>
+__global__ void __launch_bounds__(256) k_spmv(DevParams P, int Mp, const double *__restrict__ mat,
+                                              const double *__restrict__ x, double *__restrict__ y,
+                                              const double *__restrict__ d1, const double *__restrict__ d2,
+                                              double *__restrict__ partials, const SolverScalars *ss)
+{
+    __shared__ double sh[32 * 4];
+    if (ss && ss->done) return;
+    const int M = P.M;
+    const int b = blockIdx.x;
+    if (b < M) {
+        const double *row = mat + (size_t)b * 16 * Mp;
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+        for (int j = threadIdx.x; j < M; j += blockDim.x) {
+            const double xv[4] = {x[3 * j], x[3 * j + 1], x[3 * j + 2], x[3 * M + j]};
+#pragma unroll
+            for (int r = 0; r < 4; ++r)
+#pragma unroll
+                for (int cc = 0; cc < 4; ++cc) acc[r] += row[(size_t)(4 * r + cc) * Mp + j] * xv[cc];
+        }
+        block_sum<4>(acc, sh);
+        if (threadIdx.x == 0) {
+            const int im = P.metal_min + b;
+            for (int k = 0; k < P.n_nps; ++k)
+                if (im >= P.np_start[k] && im <= P.np_end[k]) acc[3] += x[4 * M + k];
+            const int rows[4] = {3 * b, 3 * b + 1, 3 * b + 2, 3 * M + b};
+            double p0 = 0.0, p1 = 0.0;
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                y[rows[r]] = acc[r];
+                if (DOT == DOT_R0) p0 += d1[rows[r]] * acc[r];
+                if (DOT == DOT_KT) {
+                    const double kt = d2[rows[r]] * acc[r];
+                    p0 += kt * d1[rows[r]];
+                    p1 += kt * kt;
+                }
+            }
+            if (DOT != DOT_NONE) {
+                partials[2 * b] = p0;
+                partials[2 * b + 1] = p1;
+            }
+        }
+    } else {
+        const int k = b - M;
+        double acc[1] = {0.0};
+        for (int a = P.np_start[k] + threadIdx.x; a <= P.np_end[k]; a += blockDim.x)
+            acc[0] += x[3 * M + (a - P.metal_min)];
+        block_sum<1>(acc, sh);
+        if (threadIdx.x == 0) {
+            const int rowi = 4 * M + k;
+            y[rowi] = acc[0];
+            if (DOT == DOT_R0) partials[2 * b] = d1[rowi] * acc[0], partials[2 * b + 1] = 0.0;
+            if (DOT == DOT_KT) {
+                const double kt = acc[0];  // K = 1 on Lagrange rows
+                partials[2 * b] = kt * d1[rowi];
+                partials[2 * b + 1] = kt * kt;
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------ BiCGSTAB
+
+// Work vector slots inside bw (bicg_stab.c:280-290).
+enum { W_AX = 0, W_R0, W_R, W_P, W_V, W_S, W_T, W_Y, W_Z, W_KT, W_K };
+
+// Fixed-order sum of `nb` two-wide partials into out[0..1] (single block).
+__device__ __forceinline__ void sum_partials2(const double *partials, int nb, double *sh, double &s0, double &s1)
+{
+    double v[2] = {0.0, 0.0};
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+        v[0] += partials[2 * b];
+        v[1] += partials[2 * b + 1];
+    }
+    block_sum<2>(v, sh);
+    s0 = v[0];
+    s1 = v[1];
+}
+
+__global__ void __launch_bounds__(256) k_vec_dot(int n, const double *__restrict__ a, const double *__restrict__ b,
+                                                 double *partials)
+{
+    __shared__ double sh[64];
+    double v[2] = {0.0, 0.0};
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) v[0] = a[k] * b[k];
+    block_sum<2>(v, sh);
+    if (threadIdx.x == 0) {
+        partials[2 * blockIdx.x] = v[0];
+        partials[2 * blockIdx.x + 1] = 0.0;
+    }
+}
+
+// bTb, early exit and criterion (bicg_stab.c:296-303).
+__global__ void k_bcg_start(const double *partials, int nb, double tol, SolverScalars *ss)
+{
+    __shared__ double sh[64];
+    double s0, s1;
+    sum_partials2(partials, nb, sh, s0, s1);
+    if (threadIdx.x == 0) {
+        ss->bTb = s0;
+        ss->crit = s0 * tol;
+        ss->rho_old = ss->alpha = ss->omega = 1.0;
+        ss->iter = 0;
+        ss->status = 0;
+        ss->done = s0 < 1.0e-10 ? 1 : 0;
+        ss->rTr = 0.0;
+    }
+}
+
+// r0 = r = b - Ax, p = v = 0, K = 1/diag (1 on Lagrange rows); (r0, r) partials.
+__global__ void __launch_bounds__(256) k_bcg_init(int n, int n4, const double *__restrict__ b,
+                                                  const double *__restrict__ diag, double *bw, double *partials,
+                                                  const SolverScalars *ss)
+{
+    __shared__ double sh[64];
+    if (ss->done) return;
+    double v[2] = {0.0, 0.0};
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) {
+        const double r = b[k] - bw[W_AX * n + k];
+        bw[W_R0 * n + k] = r;
+        bw[W_R * n + k] = r;
+        bw[W_V * n + k] = 0.0;
+        bw[W_P * n + k] = 0.0;
+        bw[W_K * n + k] = k < n4 ? 1.0 / diag[k] : 1.0;
+        v[0] = r * r;
+    }
+    block_sum<2>(v, sh);
+    if (threadIdx.x == 0) {
+        partials[2 * blockIdx.x] = v[0];
+        partials[2 * blockIdx.x + 1] = 0.0;
+    }
+}
+
+__global__ void k_bcg_rho0(const double *partials, int nb, SolverScalars *ss)
+{
+    __shared__ double sh[64];
+    if (ss->done) return;
+    double s0, s1;
+    sum_partials2(partials, nb, sh, s0, s1);
+    if (threadIdx.x == 0) ss->rho = s0;
+}
+
+// p = r + beta (p - omega v), y = K p (bicg_stab.c:371-404); the iteration-0
+// early exit on rho < 1e-10 (bicg_stab.c:368).
+__global__ void __launch_bounds__(256) k_bcg_p(int n, double *bw, SolverScalars *ss)
+{
+    if (ss->done) return;
+    if (ss->iter == 0 && ss->rho < 1.0e-10) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) ss->done = 1;
+        return;
+    }
+    const double beta = (ss->rho / ss->rho_old) * (ss->alpha / ss->omega), om = ss->omega;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const double p = bw[W_R * n + k] + beta * (bw[W_P * n + k] - om * bw[W_V * n + k]);
+    bw[W_P * n + k] = p;
+    bw[W_Y * n + k] = p * bw[W_K * n + k];
+}
+
+__global__ void k_bcg_alpha(const double *partials, int nb, SolverScalars *ss)
+{
+    __shared__ double sh[64];
+    if (ss->done) return;
+    double s0, s1;
+    sum_partials2(partials, nb, sh, s0, s1);
+    if (threadIdx.x == 0) ss->alpha = ss->rho / s0;
+}
+
+// s = r - alpha v, z = K s (bicg_stab.c:418-449).
+__global__ void __launch_bounds__(256) k_bcg_s(int n, double *bw, const SolverScalars *ss)
+{
+    if (ss->done) return;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const double s = bw[W_R * n + k] - ss->alpha * bw[W_V * n + k];
+    bw[W_S * n + k] = s;
+    bw[W_Z * n + k] = s * bw[W_K * n + k];
+}
+
+__global__ void k_bcg_omega(const double *partials, int nb, SolverScalars *ss)
+{
+    __shared__ double sh[64];
+    if (ss->done) return;
+    double s0, s1;
+    sum_partials2(partials, nb, sh, s0, s1);
+    if (threadIdx.x == 0) ss->omega = s0 / s1;
+}
+
+// x += alpha y + omega z, r = s - omega t; (r, r) and (r0, r) partials
+// (bicg_stab.c:490-529).
+__global__ void __launch_bounds__(256) k_bcg_x(int n, double *bw, double *x, double *partials,
+                                               const SolverScalars *ss)
+{
+    __shared__ double sh[64];
+    if (ss->done) return;
+    double v[2] = {0.0, 0.0};
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) {
+        x[k] += ss->alpha * bw[W_Y * n + k] + ss->omega * bw[W_Z * n + k];
+        const double r = bw[W_S * n + k] - ss->omega * bw[W_T * n + k];
+        bw[W_R * n + k] = r;
+        v[0] = r * r;
+        v[1] = bw[W_R0 * n + k] * r;
+    }
+    block_sum<2>(v, sh);
+    if (threadIdx.x == 0) {
+        partials[2 * blockIdx.x] = v[0];
+        partials[2 * blockIdx.x + 1] = v[1];
+    }
+}
+
+// Convergence test and MAX_ITER handling (bicg_stab.c:523-571).
+__global__ void k_bcg_check(const double *partials, int nb, SolverScalars *ss)
+{
+    __shared__ double sh[64];
+    if (ss->done) return;
+    double rTr, r0r;
+    sum_partials2(partials, nb, sh, rTr, r0r);
+    if (threadIdx.x == 0) {
+        ss->rho_old = ss->rho;
+        ss->rho = r0r;
+        ss->rTr = rTr;
+        ss->iter += 1;
+        if (rTr < ss->crit) {
+            ss->done = 1;
+        } else if (ss->iter > kMaxIter) {
+            ss->done = 1;
+            ss->status = rTr < ss->crit * 100.0 ? 1 : -1;  // 1: loosened criterion accepted
+        }
+    }
+}
+
+namespace {
+
+void spmv(capac_ctx *c, int dot, const double *x, double *y, const double *d1, const double *d2,
+          const SolverScalars *ss)
+{
+    const int nb = c->M + c->n_nps;
+    ProfScope ps(c, K_SPMV);
+    if (dot == DOT_R0)
+        k_spmv<DOT_R0><<<nb, 256, 0, c->stream>>>(c->P, c->Mp, c->mat, x, y, d1, d2, c->partials, ss);
+    else if (dot == DOT_KT)
+        k_spmv<DOT_KT><<<nb, 256, 0, c->stream>>>(c->P, c->Mp, c->mat, x, y, d1, d2, c->partials, ss);
+    else
+        k_spmv<DOT_NONE><<<nb, 256, 0, c->stream>>>(c->P, c->Mp, c->mat, x, y, d1, d2, c->partials, ss);
+    ++c->launches;
+}
+
+}  // namespace
+
+void launch_cpim_spmv(capac_ctx *c, const double *x, double *y)
+{
+    spmv(c, DOT_NONE, x, y, nullptr, nullptr, nullptr);
+}
+
+// mpi_precon_bicg_stab_COO (bicg_stab.c:253-573) on the device; the host only
+// polls the done flag every few iterations.
+int run_bicgstab(capac_ctx *c)
+{
+    const int n = c->n_mat, n4 = 4 * c->M;
+    const int nbv = (int)grid_for(n, 256);
+    const int nbm = c->M + c->n_nps;
+    cudaStream_t s = c->stream;
+    double *bw = c->bw;
+    auto W = [&](int k) { return bw + (size_t)k * n; };
+    const double tol = c->opt.solver_tol > 0.0 ? c->opt.solver_tol : 1.0e-8;
+
+    k_vec_dot<<<nbv, 256, 0, s>>>(n, c->vec_ext, c->vec_ext, c->partials);
+    k_bcg_start<<<1, 256, 0, s>>>(c->partials, nbv, tol, c->ss);
+    spmv(c, DOT_NONE, c->vec_pq, W(W_AX), nullptr, nullptr, c->ss);
+    k_bcg_init<<<nbv, 256, 0, s>>>(n, n4, c->vec_ext, c->diag, bw, c->partials, c->ss);
+    k_bcg_rho0<<<1, 256, 0, s>>>(c->partials, nbv, c->ss);
+    c->launches += 4;
+
+    const int chunk = 4;
+    for (int it = 0; it <= kMaxIter + chunk; it += chunk) {
+        for (int q = 0; q < chunk; ++q) {
+            {
+                ProfScope ps(c, K_SOLVER_VEC);
+                k_bcg_p<<<nbv, 256, 0, s>>>(n, bw, c->ss);
+            }
+            spmv(c, DOT_R0, W(W_Y), W(W_V), W(W_R0), nullptr, c->ss);
+            {
+                ProfScope ps(c, K_SOLVER_VEC);
+                k_bcg_alpha<<<1, 256, 0, s>>>(c->partials, nbm, c->ss);
+                k_bcg_s<<<nbv, 256, 0, s>>>(n, bw, c->ss);
+            }
+            spmv(c, DOT_KT, W(W_Z), W(W_T), W(W_Z), W(W_K), c->ss);
+            {
+                ProfScope ps(c, K_SOLVER_VEC);
+                k_bcg_omega<<<1, 256, 0, s>>>(c->partials, nbm, c->ss);
+                k_bcg_x<<<nbv, 256, 0, s>>>(n, bw, c->vec_pq, c->partials, c->ss);
+                k_bcg_check<<<1, 256, 0, s>>>(c->partials, nbv, c->ss);
+            }
+            c->launches += 6;
+        }
+        CAPAC_CUDA(cudaMemcpyAsync(c->h_ss, c->ss, sizeof(SolverScalars), cudaMemcpyDeviceToHost, s));
+        CAPAC_CUDA(cudaStreamSynchronize(s));
+        if (c->h_ss->done) break;
+    }
+    c->last_iters = c->h_ss->iter;
+    c->last_outer = 1;
+    if (c->prof.on && c->h_ss->bTb >= 1.0e-10) c->prof.spmv_effective += 1 + 2L * c->h_ss->iter;
+    c->last_rel_res = c->h_ss->bTb > 0 ? sqrt(c->h_ss->rTr / c->h_ss->bTb) : 0.0;
+    if (!c->h_ss->done || c->h_ss->status < 0) return CAPAC_ERR_NOT_CONVERGED;
+    if (c->h_ss->status == 1)
+        fprintf(stderr, "Note: Loosen bicg_stab convergence criteria to 1e-6 for this step.\n");
+    return CAPAC_OK;
+}
+
+// ------------------------------------------------- CPIM metal-side forces
+
+// mpi_cpff_force (cpff.c:526-950) for one metal atom per block: metal -
+// permanent-charge terms over its list, self terms, dense metal - metal
+// damped T0/T1/T2 terms (forces on i only, virial halved), external field on
+// the induced charge and dipole.  Energies [9..14] and the virial go to
+// per-block partials.
+__global__ void __launch_bounds__(256) k_cpim_metal(DevParams P, const double4 *__restrict__ pos4,
+                                                    const uint32_t *__restrict__ nbr, const int *__restrict__ nnb,
+                                                    int cap, const double *__restrict__ pq, double *fx, double *fy,
+                                                    double *fz, double *partials)
+{
+    __shared__ double sh[32 * 18];
+    const int i = blockIdx.x;
+    const int M = P.M;
+    const int im = P.metal_min + i;
+    const double4 pi4 = pos4[im];
+    const double qi = pq[3 * M + i];
+    const double pi[3] = {pq[3 * i], pq[3 * i + 1], pq[3 * i + 2]};
+    // acc: f[3], e9..e14 (6), vir[9]
+    double acc[18];
+#pragma unroll
+    for (int k = 0; k < 18; ++k) acc[k] = 0.0;
+
+    // metal - permanent charge, MD units (cpff.c:578-724)
+    const uint32_t *row = nbr + (size_t)im * cap;
+    for (int k = threadIdx.x; k < nnb[im]; k += blockDim.x) {
+        const int j = nb_index(row[k]);
+        if (P.is_metal[j]) continue;
+        const double4 pj = pos4[j];
+        if (pj.w == 0.0) continue;
+        double r[3] = {pi4.x - pj.x, pi4.y - pj.y, pi4.z - pj.z};
+        image(r[0], r[1], r[2], P.box);
+        const double r2 = norm2_exact(r[0], r[1], r[2]);
+        if (r2 >= P.rc2) continue;
+        double f[3], a0, ec;
+        cpim_charge_pair(P, r, r2, pj.w, qi, pi, f, a0, ec);
+        const double rr = sqrt(r2);
+        if (P.use_coulomb == 1)
+            acc[4] += kFQQ * pj.w * qi * (ec / rr - P.w_erfc_arcut + P.w_const * (rr - P.rc));
+        else
+            acc[4] += kFQQ * pj.w * qi / rr;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) acc[5] += -kFQQ * pj.w * pi[a] / kNm2Bohr * a0 * r[a];
+        acc[0] += f[0];
+        acc[1] += f[1];
+        acc[2] += f[2];
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b = 0; b < 3; ++b) acc[9 + 3 * a + b] += -r[a] * f[b];
+    }
+
+    // metal - metal, atomic units (cpff.c:752-926)
+    const double iqq = P.inv_r_qq, ipq = P.inv_r_pq, ipp = P.inv_r_pp;
+    const double ipq3 = ipq * ipq * ipq, ipp3 = ipp * ipp * ipp, ipp5 = ipp3 * ipp * ipp;
+    for (int j = threadIdx.x; j < M; j += blockDim.x) {
+        if (j == i) continue;
+        const double4 pj4 = pos4[P.metal_min + j];
+        double r[3] = {pj4.x - pi4.x, pj4.y - pi4.y, pj4.z - pi4.z};
+        image(r[0], r[1], r[2], P.box);
+        r[0] *= kNm2Bohr;
+        r[1] *= kNm2Bohr;
+        r[2] *= kNm2Bohr;
+        const double r2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2], rr = sqrt(r2);
+        const double ir3 = 1.0 / (r2 * rr), ir5 = ir3 / r2, ir7 = ir5 / r2;
+        const double qj = pq[3 * M + j];
+        const double pj[3] = {pq[3 * j], pq[3 * j + 1], pq[3 * j + 2]};
+        double f[3] = {0.0, 0.0, 0.0};
+        // charge - charge
+        const double gqq = exp(-(r2 * iqq * iqq)), erq = erf(rr * iqq);
+        const double A0 = ir3 * (erq - 2.0 * kInvSqrtPi * iqq * rr * gqq);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) f[a] += A0 * r[a] * kFqqAu2 * qi * qj;
+        acc[6] += kFqqAu1 * qi * qj * erq / rr * 0.5;
+        // charge - dipole
+        const double gpq = exp(-(r2 * ipq * ipq));
+        const double tpq = erf(rr * ipq) - 2.0 * kInvSqrtPi * ipq * rr * gpq;
+        const double Apq0 = ir3 * tpq, A1 = ir5 * tpq, B1 = 4.0 * kInvSqrtPi * ipq3 / r2 * gpq;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+#pragma unroll
+            for (int b = 0; b < 3; ++b) {
+                const double dab = a == b ? 1.0 : 0.0;
+                const double T = A1 * (3.0 * r[a] * r[b] - dab * r2) - B1 * r[a] * r[b];
+                f[b] += -T * kFqqAu2 * qi * pj[a];
+                f[b] += T * kFqqAu2 * qj * pi[a];
+            }
+            acc[7] += -kFqqAu1 * qi * pj[a] * r[a] * Apq0 * 0.5;
+            acc[7] += kFqqAu1 * qj * pi[a] * r[a] * Apq0 * 0.5;
+        }
+        // dipole - dipole
+        const double gpp = exp(-(r2 * ipp * ipp)), erp = erf(rr * ipp);
+        const double App1 = ir5 * (erp - 2.0 * kInvSqrtPi * ipp * rr * gpp);
+        const double Bpp1 = 4.0 * kInvSqrtPi * ipp3 / r2 * gpp;
+        const double A2 = ir7 * (3.0 * erp - 6.0 * kInvSqrtPi * ipp * rr * gpp -
+                                 4.0 * (r2 * rr) * kInvSqrtPi * ipp3 * gpp);
+        const double B2 = 8.0 * kInvSqrtPi * ipp5 / r2 * gpp;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+#pragma unroll
+            for (int b = 0; b < 3; ++b) {
+                const double dab = a == b ? 1.0 : 0.0;
+#pragma unroll
+                for (int cc = 0; cc < 3; ++cc) {
+                    const double dbc = b == cc ? 1.0 : 0.0, dca = cc == a ? 1.0 : 0.0;
+                    f[cc] += -(A2 * (5.0 * r[a] * r[b] * r[cc] - r2 * (r[a] * dbc + r[b] * dca + r[cc] * dab)) -
+                               B2 * r[a] * r[b] * r[cc]) * kFqqAu2 * pi[a] * pj[b];
+                }
+                acc[8] += -kFqqAu1 * pi[a] * pj[b] * ((3.0 * r[a] * r[b] - dab * r2) * App1 - r[a] * r[b] * Bpp1) * 0.5;
+            }
+        }
+        acc[0] -= f[0];
+        acc[1] -= f[1];
+        acc[2] -= f[2];
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b = 0; b < 3; ++b) acc[9 + 3 * a + b] += -r[a] * f[b] * 0.5;
+    }
+    block_sum<18>(acc, sh);
+    if (threadIdx.x == 0) {
+        // self terms (cpff.c:729-742)
+        acc[6] += 0.5 * kFQQ * qi * qi * (P.inv_capac * kNm2Bohr);
+        for (int a = 0; a < 3; ++a) acc[8] += 0.5 * kFQQ * pi[a] * pi[a] * (P.inv_polar * kNm2Bohr);
+        // external field on the induced charge and dipole (cpff.c:930-948)
+        acc[0] += P.efield[0] * qi;
+        acc[1] += P.efield[1] * qi;
+        acc[2] += P.efield[2] * qi;
+        acc[3] -= P.efield[0] * qi * pi4.x + P.efield[1] * qi * pi4.y + P.efield[2] * qi * pi4.z;
+        acc[3] -= P.efield[0] * pi[0] + P.efield[1] * pi[1] + P.efield[2] * pi[2];
+        fx[im] += acc[0];
+        fy[im] += acc[1];
+        fz[im] += acc[2];
+        for (int k = 0; k < 15; ++k) partials[(size_t)blockIdx.x * 15 + k] = acc[3 + k];
+    }
+}
+
+void launch_cpim_metal_forces(capac_ctx *c)
+{
+    {
+        ProfScope ps(c, K_CPIM_METAL);
+        k_cpim_metal<<<c->M, 256, 0, c->stream>>>(c->P, c->pos4, c->nbr, c->nnb, c->cap, c->vec_pq, c->fx, c->fy,
+                                                   c->fz, c->partials);
+    }
+    ++c->launches;
+    static const int pot_slots[15] = {9, 10, 11, 12, 13, 14, -1, -1, -1, -1, -1, -1, -1, -1, -1};
+    static const int vir_slots[15] = {-1, -1, -1, -1, -1, -1, 0, 1, 2, 3, 4, 5, 6, 7, 8};
+    launch_finalize(c, c->M, 15, pot_slots, vir_slots);
+}
+
+// ------------------------------------- external field on fixed charges
+
+// force.c:2251-2260
+__global__ void __launch_bounds__(256) k_external_field(DevParams P, const double4 *__restrict__ pos4, double *fx,
+                                                        double *fy, double *fz, double *partials)
+{
+    __shared__ double sh[32];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double e[1] = {0.0};
+    if (i < P.N) {
+        const double4 p = pos4[i];
+        const double q = p.w;
+        fx[i] += P.efield[0] * q;
+        fy[i] += P.efield[1] * q;
+        fz[i] += P.efield[2] * q;
+        e[0] = -(P.efield[0] * q * p.x + P.efield[1] * q * p.y + P.efield[2] * q * p.z);
+    }
+    block_partials<1>(e, sh, partials);
+}
+
+void launch_external_field(capac_ctx *c)
+{
+    if (c->P.efield[0] == 0.0 && c->P.efield[1] == 0.0 && c->P.efield[2] == 0.0) return;
+    const unsigned grid = grid_for(c->N, 256);
+    k_external_field<<<grid, 256, 0, c->stream>>>(c->P, c->pos4, c->fx, c->fy, c->fz, c->partials);
+    ++c->launches;
+    static const int pot_slots[1] = {9};
+    static const int vir_slots[1] = {-1};
+    launch_finalize(c, (int)grid, 1, pot_slots, vir_slots);
+}
+
+size_t partials_needed(const capac_ctx *c)
+{
+    const size_t pair_blocks = grid_for((long)c->N * 32, 256);
+    size_t need = pair_blocks * 11;
+    need = std::max(need, (size_t)grid_for((long)c->N, 256) * 16);
+    need = std::max(need, (size_t)(c->M + c->n_nps + 8) * 16);
+    need = std::max(need, (size_t)grid_for((long)c->n_mols, 256) * 16);
+    need = std::max(need, (size_t)grid_for((long)c->n_mat, 256) * 4);
+    return need + 64;
+}
+
+}  // namespace capac

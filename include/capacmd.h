@@ -1,0 +1,250 @@
+/*
+ * capacmd.h -- C ABI of the B200 (sm_100a) implementation of CapacMD's
+ * per-timestep force-and-solve path.
+ *
+ * Every entry point takes plain pointers and sizes and returns an int status
+ * (CAPAC_OK or a negative CAPAC_ERR_*); capac_last_error() gives the message
+ * of the most recent failure on the calling thread.  The reference reports the
+ * same failures with printf + exit(1); a caller that wants that behaviour
+ * checks the status and exits.
+ *
+ * Reference interfaces replaced (paths inside the CapacMD project):
+ *   system input      read_settings/read_gro/read_param_1/2/assign_indices
+ *                     (file.h:30-80, file.c:74-203, file.c:286-1099)
+ *                     -> capac_desc_load
+ *   derived constants mpi-main.c:170-203, 315-323, 548-552 -> capac_desc_derive
+ *   one force call    mpi_force (force.h:100-103)
+ *                     -> capac_force (device-resident state) and
+ *                        capac_mpi_force (host buffers in and out)
+ *   CPIM stages       mpi_cpff_vec_ext (cpff.h:30-33) -> capac_cpff_vec_ext
+ *                     mpi_cpff_mat_relay_COO (cpff.h:39-40) -> capac_cpff_mat_relay
+ *                     mpi_precon_bicg_stab_COO (bicg_stab.h:58-59) -> capac_bicgstab
+ *                     mpi_cpff_force (cpff.h:46-48) -> capac_cpff_force
+ *   integrator        rattle_1st/rattle_2nd (force.h:85-95), apply_pbc
+ *                     (force.h:37-38), get_fmax_rms (force.h:79),
+ *                     kinetic_energy/remove_comm/nose_hoover_chain
+ *                     (thermostat.h:31-45), MD loop (mpi-main.c:874-1013)
+ *                     -> capac_md_steps and the per-stage entry points below.
+ *
+ * Units follow the reference: nm, ps, kJ/mol, e, amu; the CPIM vector is in
+ * atomic units (e*Bohr for dipoles, e for charges).  The CPIM vector layout is
+ * the reference's: [0,3M) dipoles x,y,z per metal atom, [3M,4M) charges,
+ * [4M,4M+n_NPs) Lagrange multipliers (mpi-main.c:572-591).
+ */
+#ifndef CAPACMD_H
+#define CAPACMD_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+#define CAPAC_OK 0
+#define CAPAC_ERR_INVALID (-1)        /* bad argument or inconsistent input */
+#define CAPAC_ERR_IO (-2)             /* input file missing or malformed */
+#define CAPAC_ERR_CUDA (-3)           /* CUDA runtime failure */
+#define CAPAC_ERR_NOT_CONVERGED (-4)  /* BiCGSTAB above 100x tolerance after MAX_ITER (bicg_stab.c:561-570) */
+#define CAPAC_ERR_RATTLE (-5)         /* RATTLE did not converge (force.c:1990-1994, 2083-2087) */
+#define CAPAC_ERR_UNSUPPORTED (-6)    /* input uses a term outside this path (bonded terms, vsites) */
+#define CAPAC_ERR_CAPACITY (-7)       /* a fixed-capacity buffer is too small for this input */
+#define CAPAC_ERR_NO_DEVICE (-8)      /* no usable sm_100 device */
+
+const char *capac_last_error(void);
+
+/* ------------------------------------------------------- enumerations */
+#define CAPAC_RUN_MD 0
+#define CAPAC_RUN_EM 1
+#define CAPAC_RUN_CG 2
+#define CAPAC_NVE 0
+#define CAPAC_NVT 1
+
+#define CAPAC_PREC_FP64 0   /* plain FP64 path: reference arithmetic on the GPU */
+#define CAPAC_PREC_MIXED 1  /* FP32 pair terms, FP32 CPIM matrix/SpMV, FP64 refinement */
+
+/* ------------------------------------------------- system description
+ * Everything the reference reads from mdset.txt, param.txt and the .gro file,
+ * flattened into arrays.  Arrays are owned by whoever built the struct:
+ * capac_desc_load allocates them (free with capac_desc_free); a caller that
+ * fills the struct itself keeps ownership.
+ */
+typedef struct capac_desc {
+    /* mdset.txt (RunSet, typedef.h:200-242; keys file.c:90-124) */
+    int run_type;     /* CAPAC_RUN_* */
+    int ensemble;     /* CAPAC_NVE / CAPAC_NVT */
+    int n_steps, n_save, n_heating, em_steps;
+    double dt, r_cut, w_alpha, ref_temp, tau_temp, em_length, em_tol;
+    int use_vdw;      /* 1: shifted-force LJ ("shifted"), 0: plain cut-off */
+    int use_coulomb;  /* 1: damped shifted force ("wolf_sum"), 0: plain cut-off */
+    int fix_metal, use_cpff;
+    double efield[3]; /* kJ mol^-1 nm^-1 e^-1 (input V/nm times 96.4853363969351) */
+
+    /* param.txt (Topol, typedef.h:298-338; Metal, typedef.h:245-288) */
+    double scale_lj, scale_qq;
+    int n_atoms, n_mols, n_types, mol_types;
+    int *mol_num;          /* [mol_types] molecules of each type */
+    int *mol_atoms;        /* [mol_types] atoms per molecule of each type */
+    int *nb_funct;         /* [n_types*n_types] 1 LJ, 2 Buckingham, 3 Morse, 4 erf-vdW */
+    double *nb_c6, *nb_c12, *nb_a, *nb_b; /* [n_types*n_types] */
+    int *excl_offset;      /* [mol_types] start of a mol_atoms^2 exclusion matrix */
+    unsigned char *excl;   /* exclusion matrices, row-major */
+    int *cstr_offset;      /* [mol_types] first constraint of the type */
+    int *cstr_count;       /* [mol_types] constraints per molecule of the type */
+    int *cstr_i, *cstr_j;  /* constraint atom indices within the molecule */
+    double *cstr_r;        /* constraint lengths, nm */
+    int n_cstr_total;      /* constraints in the whole system (for ndf) */
+    int n_bonded_terms;    /* bonds+pairs+angles+dihedrals over all molecule types */
+    int n_vsites_total;    /* virtual sites in the whole system */
+    int metal_min, metal_max, n_metal;
+    int qsc_n, qsc_m;
+    double qsc_eps, qsc_c, qsc_a;
+    double cpff_polar, cpff_capac; /* atomic units */
+    int n_nps;
+    int *np_start, *np_end;        /* [n_nps] atom index ranges, inclusive */
+    double *np_charge;             /* [n_nps] total charge, e */
+
+    /* per atom (Atom_Info, typedef.h:146-152; filled as assign_indices, file.c:1031-1099) */
+    int *atom_type, *mol_id, *mol_type, *atom_in_mol;
+    unsigned char *is_metal;
+    double *charge, *mass, *inv_mass;
+    int *mol_first, *mol_last;     /* [n_mols] Mol_Info */
+
+    /* .gro (read_gro, file.c:138-203) */
+    double box[3];
+    double *rx, *ry, *rz, *vx, *vy, *vz;
+    double vq0, vp;                /* thermostat velocities from the title line */
+} capac_desc;
+
+/* Constants the reference derives at start-up. */
+typedef struct capac_consts {
+    double r_cut2, w_a2_sqrtpi, w_const, w_erfc_arcut; /* mpi-main.c:170-178 */
+    double inv_rc12, inv_rc6;                          /* mpi-main.c:202-203 */
+    double inv_polar, inv_capac, inv_r_qq, inv_r_pq, inv_r_pp; /* mpi-main.c:315-323 */
+    int ndf;                                           /* mpi-main.c:548 */
+    double kT, q_mass, dt_2;                           /* mpi-main.c:551-562 */
+    int n_mat;                                         /* 4*n_metal + n_nps */
+} capac_consts;
+
+/* Parse the three reference input files.  On success *out owns all arrays. */
+int capac_desc_load(const char *gro_path, const char *param_path, const char *mdset_path,
+                    capac_desc **out);
+void capac_desc_free(capac_desc *d);
+int capac_desc_derive(const capac_desc *d, capac_consts *out);
+/* Copy a named per-system array of a description into out (doubles).  Names:
+ * rx ry rz vx vy vz charge mass box.  Returns the count written or <0. */
+int capac_desc_get(const capac_desc *d, const char *name, double *out);
+/* Sizes of a description: atoms, molecules, metal atoms, NPs, n_mat. */
+int capac_desc_info(const capac_desc *d, int *n_atoms, int *n_mols, int *n_metal, int *n_nps, int *n_mat);
+
+/* ------------------------------------------------------- GPU context */
+typedef struct capac_options {
+    int precision;          /* CAPAC_PREC_FP64 or CAPAC_PREC_MIXED */
+    int device;             /* CUDA device ordinal */
+    double skin;            /* neighbour-list skin, nm (default 0.2) */
+    int list_every;         /* forced list rebuild interval in steps, 0 = displacement only */
+    int max_neighbors;      /* 0 = estimate from density */
+    double solver_tol;      /* rTr < solver_tol * bTb; 0 = reference 1e-8 (bicg_stab.c:303) */
+    double refine_tol;      /* mixed path: FP64 relative residual target (default 1e-10) */
+} capac_options;
+
+void capac_options_default(capac_options *o);
+
+typedef struct capac_ctx capac_ctx;
+
+int capac_create(const capac_desc *d, const capac_options *opt, capac_ctx **out);
+int capac_destroy(capac_ctx *ctx);
+
+/* One full force evaluation on the device-resident state, mpi_force semantics
+ * (force.c:2097-2320): zero forces/energies/virial, nonbonded pairs, Sutton-Chen
+ * density and forces, CPIM RHS, matrix, BiCGSTAB (warm-started from the
+ * current induced vector), CPIM forces, external field on permanent charges.
+ * potential[0] is left for the caller (sum_potential). */
+int capac_force(capac_ctx *ctx);
+
+/* mpi_force with host buffers (drop-in mode): copies positions in, evaluates,
+ * copies forces, energies, virial and the CPIM vectors out.  vec_pq is in/out
+ * (warm start, as Metal.vec_pq).  Any output pointer may be NULL.
+ * Sizes: rx..fz n_atoms, potential 15, virial 9, vec_pq/vec_ext/diag_relay
+ * n_mat, inv_sqrt_dens n_metal. */
+int capac_mpi_force(capac_ctx *ctx, const double *rx, const double *ry, const double *rz,
+                    double *fx, double *fy, double *fz, double *potential, double *virial,
+                    double *vec_pq, double *vec_ext, double *diag_relay, double *inv_sqrt_dens);
+
+/* CPIM stages on the device state, for stage-by-stage checks. */
+int capac_qsc(capac_ctx *ctx);                          /* mpi_qsc_dens + mpi_qsc_force */
+int capac_cpff_vec_ext(capac_ctx *ctx);                 /* mpi_cpff_vec_ext */
+int capac_cpff_mat_relay(capac_ctx *ctx, long *nnz);    /* mpi_cpff_mat_relay_COO */
+int capac_bicgstab(capac_ctx *ctx, int *iterations);    /* mpi_precon_bicg_stab_COO */
+int capac_cpff_force(capac_ctx *ctx);                   /* mpi_cpff_force */
+
+/* y = A x with the CPIM matrix of the last assembly; x and y are host arrays
+ * of n_mat doubles in the reference layout (mpi_mat_vec_COO, bicg_stab.c:46-63). */
+int capac_cpim_matvec(capac_ctx *ctx, const double *x, double *y);
+
+/* capac_force without the BiCGSTAB solve: every term is evaluated with the
+ * induced vector currently held (set with capac_set "vec_pq"). */
+int capac_force_given_pq(capac_ctx *ctx);
+
+/* MD steps on the device (mpi-main.c:874-1013, file output left out):
+ * heating ramp, Nose-Hoover chain (nvt), half kick, drift, RATTLE, force,
+ * half kick, RATTLE, kinetic energy, Nose-Hoover chain, COM removal; every
+ * n_save steps apply_pbc and get_fmax_rms. */
+int capac_md_steps(capac_ctx *ctx, int n_steps);
+
+/* The reference's start-up after the first mpi_force (mpi-main.c:614-655):
+ * sum_potential, remove_comm, kinetic_energy, first/ext temperature. */
+int capac_md_init(capac_ctx *ctx);
+
+/* State transfer.  Names for per-atom arrays (n_atoms doubles):
+ * rx ry rz vx vy vz fx fy fz.  Others: potential(15) virial(9) vec_pq vec_ext
+ * diag_relay (n_mat) inv_sqrt_dens(n_metal) vQ(10) thermo(4: eKsum inst_temp
+ * ref_temp ndf) box(6).  capac_get returns the count written, <0 on error. */
+int capac_get(capac_ctx *ctx, const char *name, double *out);
+int capac_set(capac_ctx *ctx, const char *name, const double *in);
+
+/* Statistics of the last force call: BiCGSTAB iterations, neighbour-list
+ * rebuilds so far, list entries, pairs inside the cut-off. */
+typedef struct capac_stats {
+    int solver_iterations;
+    int solver_outer;           /* refinement sweeps (mixed path) */
+    double solver_rel_residual; /* sqrt(rTr/bTb) at exit */
+    long list_builds;
+    long list_entries;
+    long max_neighbors;
+    int list_capacity;
+    long md_step;
+} capac_stats;
+int capac_get_stats(capac_ctx *ctx, capac_stats *out);
+
+/* Pair-set fingerprint of the current positions: number of nonbonded pairs
+ * j<i inside the cut-off that the reference loop (force.c:1419-1473) visits,
+ * and a 64-bit order-independent hash of those (i,j).  from_list = 1 reads
+ * the neighbour list, 0 enumerates all N(N-1)/2 pairs on the GPU. */
+int capac_pair_fingerprint(capac_ctx *ctx, int from_list, long *count, unsigned long long *hash);
+
+/* Per-phase device times of the last force call in ms, in the reference's
+ * time_used slots (mpi-main.c:119-128): 1 QSC density, 2 QSC force,
+ * 4 nonbonded, 5 CPIM matrix, 6 CPIM vector, 7 CPIM solve, 8 CPIM force. */
+int capac_phase_times(capac_ctx *ctx, double out_ms[15]);
+
+/* Number of kernels this library launched since the context was created. */
+long capac_kernel_launches(capac_ctx *ctx);
+
+/* Device time of the MD steps, measured with CUDA events on the library's
+ * stream around n_steps of capac_md_steps. */
+int capac_time_md_steps(capac_ctx *ctx, int n_steps, double *ms);
+
+/* Per-kernel device times.  While enabled, every launch of the kernels named
+ * below is bracketed by CUDA events on the library's stream; capac_profile_get
+ * returns the launch count and total milliseconds of one kernel class since
+ * the last capac_profile_enable.  Classes: "pair", "spmv", "matrix",
+ * "cpim_metal", "cpim_rhs", "qsc", "list_build", "solver_vec", "integrate". */
+int capac_profile_enable(capac_ctx *ctx, int on);
+int capac_profile_get(capac_ctx *ctx, const char *cls, long *launches, double *total_ms);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CAPACMD_H */

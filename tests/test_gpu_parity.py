@@ -1,0 +1,152 @@
+"""FP64 GPU path against the oracle and the reference's golden outputs.
+
+Every call goes through the C ABI (libcapacmd_gpu.so via ctypes).  Bars:
+  * pair set: identical (count and order-independent hash) to the reference
+    loop, from the neighbour list and from an all-pairs GPU enumeration;
+  * everything outside the BiCGSTAB iterate (RHS, matrix action, Sutton-Chen
+    densities, forces/energies/virial for a given induced vector): 1e-10
+    relative (normwise), in practice ~1e-14;
+  * the induced vector with the reference's stopping rule: meets the rule
+    (relative residual < 1e-4) -- its digits beyond that depend on rounding;
+  * tight solve (rTr < 1e-26 bTb): induced charges/dipoles and forces within
+    1e-10 relative of the oracle's tight solve;
+  * 100 MD steps, tight solve: total-energy trace within 1e-8 relative.
+"""
+import numpy as np
+import pytest
+
+import capacmd_b200 as cm
+from capacmd_b200 import configs
+from oracle.oracle import Oracle
+from conftest import GOLDEN_CASES, golden_paths, golden_ref, rel_err, slot_rel_err
+
+pytestmark = pytest.mark.gpu
+
+TIGHT = 1e-26
+
+
+@pytest.fixture(autouse=True)
+def _need_gpu(gpu_available):
+    if not gpu_available:
+        pytest.fail("no sm_100 GPU: GPU tests must run on a B200")
+
+
+def _pair(case, tol=0.0):
+    d = cm.Desc.from_paths(golden_paths(case))
+    return d, cm.Simulation(d, solver_tol=tol), Oracle(d, solver_tol=tol or 1e-8)
+
+
+@pytest.mark.parametrize("case", GOLDEN_CASES)
+def test_pair_set_identical(case):
+    d, s, o = _pair(case)
+    g = golden_ref(case)
+    ref = (int(g["pair_count"]), int(g["pair_hash"]))
+    assert s.pair_fingerprint(from_list=True) == ref
+    assert s.pair_fingerprint(from_list=False) == ref
+
+
+@pytest.mark.parametrize("case", GOLDEN_CASES)
+def test_forces_given_reference_pq(case):
+    d, s, o = _pair(case)
+    g = golden_ref(case)
+    s.force()  # builds the list and the matrix
+    if d.n_mat > 0:
+        s.set("vec_pq", g["vec_pq"])
+    cm.lib().capac_force_given_pq(s._p)
+    for k in ("fx", "fy", "fz"):
+        assert rel_err(s.get(k), g[k]) < 1e-10, k
+    assert slot_rel_err(s.get("potential")[1:], g["potential"][1:]) < 1e-10
+    assert rel_err(s.get("virial"), g["virial"]) < 1e-10
+
+
+@pytest.mark.parametrize("case", GOLDEN_CASES)
+def test_solve_inputs(case):
+    d, s, o = _pair(case)
+    g = golden_ref(case)
+    s.force()
+    if d.n_mat == 0:
+        return
+    assert rel_err(s.get("vec_ext"), g["vec_ext"]) < 1e-12
+    assert rel_err(s.get("inv_sqrt_dens"), g["inv_sqrt_dens"]) < 1e-13
+    assert rel_err(s.get("diag_relay"), g["diag_relay"]) == 0.0
+    y = np.zeros(d.n_mat)
+    x = np.ascontiguousarray(g["mv_x"])
+    assert cm.lib().capac_cpim_matvec(s._p, x.ctypes.data, y.ctypes.data) == 0
+    assert rel_err(y, g["mv_y"]) < 1e-12
+
+
+@pytest.mark.parametrize("case", ["t_au55w", "t_2np", "c1_field"])
+def test_default_solve_meets_reference_rule(case):
+    d, s, o = _pair(case)
+    g = golden_ref(case)
+    s.force()
+    o.force()
+    x = s.get("vec_pq")
+    b = g["vec_ext"]
+    r = b - o.matvec(x)
+    assert float(r @ r) < 1e-8 * float(b @ b)
+    assert abs(s.stats().solver_iterations - o.iterations()) <= 4
+
+
+@pytest.mark.parametrize("case", GOLDEN_CASES)
+def test_tight_solve_and_forces(case):
+    d, s, o = _pair(case, TIGHT)
+    s.force()
+    assert o.force() == 0
+    if d.n_mat > 0:
+        assert rel_err(s.get("vec_pq"), o.get("vec_pq")) < 1e-10
+    for k in ("fx", "fy", "fz"):
+        assert rel_err(s.get(k), o.get(k)) < 1e-10, k
+    assert slot_rel_err(s.get("potential")[1:], o.get("potential")[1:]) < 1e-9
+
+
+def test_drop_in_call_with_host_buffers():
+    d, s, o = _pair("t_2np")
+    g = golden_ref("t_2np")
+    out = s.mpi_force(d.get("rx"), d.get("ry"), d.get("rz"), vec_pq=np.zeros(d.n_mat))
+    b = g["vec_ext"]
+    r = b - o.matvec(out["vec_pq"]) if o.force() == 0 else None
+    assert float(r @ r) < 1e-8 * float(b @ b)
+    assert rel_err(out["vec_ext"], g["vec_ext"]) < 1e-12
+
+
+@pytest.mark.parametrize("case", ["c1", "t_water", "t_2np"])
+def test_md_100_steps_energy_trace(case):
+    d, s, o = _pair(case, TIGHT)
+    s.md_init()
+    assert o.force() == 0
+    o.md_init()
+    es, eo = [], []
+    for _ in range(100):
+        s.md_steps(1)
+        assert o.md_steps(1) == 0
+        es.append(s.get("potential")[0] + 0.5 * s.get("thermo")[0])
+        eo.append(o.get("potential")[0] + 0.5 * o.get("thermo")[0])
+    es, eo = np.array(es), np.array(eo)
+    assert np.max(np.abs(es - eo) / np.abs(eo)) < 1e-8
+    assert rel_err(s.get("rx"), o.get("rx")) < 1e-8
+
+
+def test_reference_md_trace_without_solve_noise():
+    d, s, o = _pair("c1")
+    g = golden_ref("c1")
+    s.md_init()
+    pots = []
+    for _ in range(len(g["md_potential"])):
+        s.md_steps(1)
+        pots.append(s.get("potential")[0])
+    assert rel_err(np.array(pots), g["md_potential"][:, 0]) < 1e-10
+    for k in ("rx", "vx", "vz"):
+        assert rel_err(s.get(k), g["md_" + k]) < 1e-10
+
+
+def test_medium_system_pair_set_and_forces():
+    p = configs.cached("c4")
+    d = cm.Desc.from_paths(p)
+    s = cm.Simulation(d, solver_tol=TIGHT)
+    o = Oracle(d, solver_tol=TIGHT)
+    assert s.pair_fingerprint(True) == s.pair_fingerprint(False) == o.pair_fingerprint()
+    s.force()
+    assert o.force() == 0
+    assert rel_err(s.forces(), o.forces()) < 1e-10
+    assert rel_err(s.get("vec_pq"), o.get("vec_pq")) < 1e-10
