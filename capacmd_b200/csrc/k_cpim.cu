@@ -195,57 +195,36 @@ void launch_cpim_rhs(capac_ctx *c)
 
 // ------------------------------------------------------- CPIM matrix
 
-// One thread per ordered pair (i, j); 16 coalesced plane writes.
+// One thread per ordered pair (i, j); 16 coalesced plane writes.  The entries
+// are computed in FP64 and stored as T (double on the FP64 path, float on the
+// mixed path).
+template <typename T>
 __global__ void __launch_bounds__(128) k_cpim_matrix(DevParams P, const double4 *__restrict__ pos4, int Mp,
-                                                     double *__restrict__ mat)
+                                                     T *__restrict__ mat)
 {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     const int i = blockIdx.y;
     if (j >= Mp) return;
     double e[16];
-#pragma unroll
-    for (int k = 0; k < 16; ++k) e[k] = 0.0;
     if (j < P.M) {
-        if (j == i) {
-            e[0] = e[5] = e[10] = keep_entry(P.inv_polar);
-            e[15] = keep_entry(-P.inv_capac);
-        } else {
-            const double4 pi = pos4[P.metal_min + i], pj = pos4[P.metal_min + j];
-            double r[3] = {pj.x - pi.x, pj.y - pi.y, pj.z - pi.z};
-            image(r[0], r[1], r[2], P.box);
-            r[0] *= kNm2Bohr;
-            r[1] *= kNm2Bohr;
-            r[2] *= kNm2Bohr;
-            const double r2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2], rr = sqrt(r2);
-            const double ipp = P.inv_r_pp, ipq = P.inv_r_pq;
-            const double gpp = exp(-(r2 * ipp * ipp));
-            const double c1 = 1.0 / (r2 * r2 * rr) * (erf(rr * ipp) - 2.0 * kInvSqrtPi * ipp * rr * gpp);
-            const double c2 = 4.0 * kInvSqrtPi * (ipp * ipp * ipp) / r2 * gpp;
-            const double gpq = exp(-(r2 * ipq * ipq));
-            const double c3 = 1.0 / (r2 * rr) * (erf(rr * ipq) - 2.0 * kInvSqrtPi * ipq * rr * gpq);
+        cpim_block(P, pos4[P.metal_min + i], pos4[P.metal_min + j], i == j, e);
+    } else {
 #pragma unroll
-            for (int a = 0; a < 3; ++a) {
-#pragma unroll
-                for (int b = 0; b < 3; ++b) {
-                    const double dab = a == b ? 1.0 : 0.0;
-                    e[4 * a + b] = keep_entry(-(c1 * (3.0 * r[a] * r[b] - dab * r2) - c2 * r[a] * r[b]));
-                }
-                e[4 * a + 3] = keep_entry(c3 * r[a]);
-                e[12 + a] = keep_entry(-c3 * r[a]);
-            }
-            e[15] = keep_entry(-erf(rr * P.inv_r_qq) / rr);
-        }
+        for (int k = 0; k < 16; ++k) e[k] = 0.0;
     }
-    double *base = mat + (size_t)i * 16 * Mp + j;
+    T *base = mat + (size_t)i * 16 * Mp + j;
 #pragma unroll
-    for (int k = 0; k < 16; ++k) base[(size_t)k * Mp] = e[k];
+    for (int k = 0; k < 16; ++k) base[(size_t)k * Mp] = (T)e[k];
 }
 
 void launch_cpim_matrix(capac_ctx *c)
 {
     dim3 grid(grid_for(c->Mp, 128), c->M);
     ProfScope ps(c, K_MATRIX);
-    k_cpim_matrix<<<grid, 128, 0, c->stream>>>(c->P, c->pos4, c->Mp, c->mat);
+    if (c->matf)
+        k_cpim_matrix<float><<<grid, 128, 0, c->stream>>>(c->P, c->pos4, c->Mp, c->matf);
+    else
+        k_cpim_matrix<double><<<grid, 128, 0, c->stream>>>(c->P, c->pos4, c->Mp, c->mat);
     ++c->launches;
 }
 
@@ -257,8 +236,12 @@ void launch_cpim_matrix(capac_ctx *c)
 //   DOT_KT:  Kt = K y; (Kt, z), (Kt, Kt) -> partials[b*2], partials[b*2+1]
 enum { DOT_NONE = 0, DOT_R0 = 1, DOT_KT = 2 };
 
-template <int DOT>
-__global__ void __launch_bounds__(256) k_spmv(DevParams P, int Mp, const double *__restrict__ mat,
+// T: stored entry type (double, or float on the mixed path; accumulation is
+// FP64 either way).  FREE: no stored matrix, every block is recomputed in FP64
+// from the positions (the FP64 residual of the mixed path's refinement).
+template <int DOT, typename T, bool FREE>
+__global__ void __launch_bounds__(256) k_spmv(DevParams P, int Mp, const T *__restrict__ mat,
+                                              const double4 *__restrict__ pos4,
                                               const double *__restrict__ x, double *__restrict__ y,
                                               const double *__restrict__ d1, const double *__restrict__ d2,
                                               double *__restrict__ partials, const SolverScalars *ss)
@@ -268,14 +251,24 @@ __global__ void __launch_bounds__(256) k_spmv(DevParams P, int Mp, const double 
     const int M = P.M;
     const int b = blockIdx.x;
     if (b < M) {
-        const double *row = mat + (size_t)b * 16 * Mp;
+        const T *row = FREE ? nullptr : mat + (size_t)b * 16 * Mp;
         double acc[4] = {0.0, 0.0, 0.0, 0.0};
+        double4 pb = FREE ? pos4[P.metal_min + b] : make_double4(0, 0, 0, 0);
         for (int j = threadIdx.x; j < M; j += blockDim.x) {
             const double xv[4] = {x[3 * j], x[3 * j + 1], x[3 * j + 2], x[3 * M + j]};
+            if (FREE) {
+                double e[16];
+                cpim_block(P, pb, pos4[P.metal_min + j], j == b, e);
 #pragma unroll
-            for (int r = 0; r < 4; ++r)
+                for (int r = 0; r < 4; ++r)
 #pragma unroll
-                for (int cc = 0; cc < 4; ++cc) acc[r] += row[(size_t)(4 * r + cc) * Mp + j] * xv[cc];
+                    for (int cc = 0; cc < 4; ++cc) acc[r] += e[4 * r + cc] * xv[cc];
+            } else {
+#pragma unroll
+                for (int r = 0; r < 4; ++r)
+#pragma unroll
+                    for (int cc = 0; cc < 4; ++cc) acc[r] += (double)row[(size_t)(4 * r + cc) * Mp + j] * xv[cc];
+            }
         }
         block_sum<4>(acc, sh);
         if (threadIdx.x == 0) {
@@ -498,12 +491,24 @@ void spmv(capac_ctx *c, int dot, const double *x, double *y, const double *d1, c
 {
     const int nb = c->M + c->n_nps;
     ProfScope ps(c, K_SPMV);
-    if (dot == DOT_R0)
-        k_spmv<DOT_R0><<<nb, 256, 0, c->stream>>>(c->P, c->Mp, c->mat, x, y, d1, d2, c->partials, ss);
-    else if (dot == DOT_KT)
-        k_spmv<DOT_KT><<<nb, 256, 0, c->stream>>>(c->P, c->Mp, c->mat, x, y, d1, d2, c->partials, ss);
-    else
-        k_spmv<DOT_NONE><<<nb, 256, 0, c->stream>>>(c->P, c->Mp, c->mat, x, y, d1, d2, c->partials, ss);
+    cudaStream_t s = c->stream;
+    if (c->matf) {
+        if (dot == DOT_R0)
+            k_spmv<DOT_R0, float, false><<<nb, 256, 0, s>>>(c->P, c->Mp, c->matf, c->pos4, x, y, d1, d2, c->partials, ss);
+        else if (dot == DOT_KT)
+            k_spmv<DOT_KT, float, false><<<nb, 256, 0, s>>>(c->P, c->Mp, c->matf, c->pos4, x, y, d1, d2, c->partials, ss);
+        else
+            k_spmv<DOT_NONE, float, false><<<nb, 256, 0, s>>>(c->P, c->Mp, c->matf, c->pos4, x, y, d1, d2, c->partials,
+                                                              ss);
+    } else {
+        if (dot == DOT_R0)
+            k_spmv<DOT_R0, double, false><<<nb, 256, 0, s>>>(c->P, c->Mp, c->mat, c->pos4, x, y, d1, d2, c->partials, ss);
+        else if (dot == DOT_KT)
+            k_spmv<DOT_KT, double, false><<<nb, 256, 0, s>>>(c->P, c->Mp, c->mat, c->pos4, x, y, d1, d2, c->partials, ss);
+        else
+            k_spmv<DOT_NONE, double, false><<<nb, 256, 0, s>>>(c->P, c->Mp, c->mat, c->pos4, x, y, d1, d2,
+                                                               c->partials, ss);
+    }
     ++c->launches;
 }
 

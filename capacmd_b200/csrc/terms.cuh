@@ -49,4 +49,43 @@ __device__ __forceinline__ void cpim_charge_pair(const DevParams &P, const doubl
     }
 }
 
+// The 4x4 CPIM block of the ordered metal pair (i, j) in FP64, entries
+// e[4*row + col] over (p_x, p_y, p_z, q): mpi_cpff_mat_relay_COO,
+// cpff.c:245-436.  r = r_j - r_i (pbc_12) in Bohr; diagonal block when same.
+// Entries with |e| <= 1e-15 are dropped as in the reference (typedef.h:89-93).
+__device__ __forceinline__ void cpim_block(const DevParams &P, const double4 &pi, const double4 &pj, bool same,
+                                           double e[16])
+{
+#pragma unroll
+    for (int k = 0; k < 16; ++k) e[k] = 0.0;
+    if (same) {
+        e[0] = e[5] = e[10] = keep_entry(P.inv_polar);
+        e[15] = keep_entry(-P.inv_capac);
+        return;
+    }
+    double r[3] = {pj.x - pi.x, pj.y - pi.y, pj.z - pi.z};
+    image(r[0], r[1], r[2], P.box);
+    r[0] *= kNm2Bohr;
+    r[1] *= kNm2Bohr;
+    r[2] *= kNm2Bohr;
+    const double r2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2], rr = sqrt(r2);
+    const double ipp = P.inv_r_pp, ipq = P.inv_r_pq;
+    const double gpp = exp(-(r2 * ipp * ipp));
+    const double c1 = 1.0 / (r2 * r2 * rr) * (erf(rr * ipp) - 2.0 * kInvSqrtPi * ipp * rr * gpp);
+    const double c2 = 4.0 * kInvSqrtPi * (ipp * ipp * ipp) / r2 * gpp;
+    const double gpq = exp(-(r2 * ipq * ipq));
+    const double c3 = 1.0 / (r2 * rr) * (erf(rr * ipq) - 2.0 * kInvSqrtPi * ipq * rr * gpq);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+#pragma unroll
+        for (int b = 0; b < 3; ++b) {
+            const double dab = a == b ? 1.0 : 0.0;
+            e[4 * a + b] = keep_entry(-(c1 * (3.0 * r[a] * r[b] - dab * r2) - c2 * r[a] * r[b]));
+        }
+        e[4 * a + 3] = keep_entry(c3 * r[a]);
+        e[12 + a] = keep_entry(-c3 * r[a]);
+    }
+    e[15] = keep_entry(-erf(rr * P.inv_r_qq) / rr);
+}
+
 }  // namespace capac
