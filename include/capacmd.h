@@ -186,6 +186,28 @@ int capac_cpim_matvec(capac_ctx *ctx, const double *x, double *y);
  * induced vector currently held (set with capac_set "vec_pq"). */
 int capac_force_given_pq(capac_ctx *ctx);
 
+/* CPIM solve that allocates no device memory.  No counterpart in the
+ * reference: it serves callers that cannot call cudaMalloc -- a host code that
+ * hands all device memory to its own pool at start-up and forbids later
+ * allocations, or a per-time-step caller for which an allocation (which may
+ * synchronise the device) is not acceptable.  Same Jacobi-preconditioned
+ * BiCGSTAB as capac_bicgstab, on arrays the caller owns (device pointers):
+ *   mat   the 4x4-block matrix, mat[(i*16 + 4*row + col)*mat_stride + j] for
+ *         block row i and block column j of n_metal metal atoms, rows/cols of a
+ *         block ordered (p_x, p_y, p_z, q);
+ *   rhs, diag  n_mat = 4*n_metal + n_nps values, reference vector layout;
+ *   x     in: warm start, out: solution.
+ * np_start/np_end are HOST arrays of metal-local atom ranges.  tol: criterion
+ * rTr < tol*bTb (0 = 1e-8).  stream: a cudaStream_t, NULL for the default.
+ * Limits: n_mat <= 16384 and n_nps <= 16 (CAPAC_ERR_CAPACITY beyond).  The
+ * work space is one static device array of about 1.2 MB that every device
+ * loading the library holds until exit; the first call on a device looks up
+ * its address (make that first call before any stream capture).  All calls
+ * share the work space, so calls that overlap on the GPU race. */
+int capac_bicgstab_static(const double *mat, int n_metal, int mat_stride, int n_nps, const int *np_start,
+                          const int *np_end, const double *rhs, const double *diag, double *x, double tol,
+                          int *iterations, void *stream);
+
 /* MD steps on the device (mpi-main.c:874-1013, file output left out):
  * heating ramp, Nose-Hoover chain (nvt), half kick, drift, RATTLE, force,
  * half kick, RATTLE, kinetic energy, Nose-Hoover chain, COM removal; every
