@@ -113,17 +113,19 @@ def algorithmic_bytes(sim, cls: str, n_atoms: int, n_metal: int, precision: str)
     pair: the list (4 B per entry) plus, per atom, its packed position/charge
           (32 B, 16 B mixed), list length, type, metal flag, and the force
           read-modify-write (48 B);
-    spmv: the 4x4-block CPIM matrix (16 entries per ordered metal pair, row
-          padded to a multiple of 32; 8 B, 4 B mixed) plus the input and output
-          vectors (2 x 4M x 8 B).
+    spmv: the symmetric packed 4x4-block CPIM matrix (10 entries per unordered
+          metal pair in 32 x 32-atom tiles over the upper triangle; 8 B, 4 B
+          mixed), the per-tile partial sums written and read back (nT^2 x 128 x
+          8 B each way) and the input and output vectors.
     """
     st = sim.stats()
     w = 4 if precision == "mixed" else 8
     if cls == "pair":
-        return 4.0 * st.list_entries + n_atoms * (4 * w + 4 + 4 + 1 + 48)
+        return 4.0 * st.list_entries + n_atoms * (32 + 4 + 4 + 1 + 48)
     if cls == "spmv":
-        mp = (n_metal + 31) // 32 * 32
-        return 16.0 * w * n_metal * mp + 2 * 4 * n_metal * 8.0
+        nt = (n_metal + 31) // 32
+        tiles = nt * (nt + 1) // 2
+        return 10.0 * w * 1024 * tiles + 2 * nt * nt * 128 * 8.0 + 2 * 4 * n_metal * 8.0
     if cls == "matrix":
         mp = (n_metal + 31) // 32 * 32
         return 16.0 * 8 * n_metal * mp
@@ -203,6 +205,8 @@ def main() -> int:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--e2e-calls", type=int, default=20)
+    ap.add_argument("--solver-kernel", type=int, default=0, choices=[0, 1],
+                    help="0: persistent cooperative BiCGSTAB launch per solve, 1: a launch per vector step")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -230,7 +234,7 @@ def main() -> int:
 
     prec = cm.PREC_MIXED if args.precision == "mixed" else cm.PREC_FP64
     desc = cm.Desc.from_paths(paths)
-    sim = cm.Simulation(desc, precision=prec, device=local)
+    sim = cm.Simulation(desc, precision=prec, device=local, solver_kernel=args.solver_kernel)
     N, M = desc.n_atoms, desc.n_metal
     sim.md_init()
     sim.md_steps(args.warmup)
@@ -246,8 +250,10 @@ def main() -> int:
     ms = ctypes_time(sim, args.steps)
     launches = sim.kernel_launches() - l0
     prof = {}
-    for cls in ("pair", "spmv", "matrix", "cpim_metal", "cpim_rhs", "qsc", "list_build", "solver_vec"):
+    for cls in ("pair", "spmv", "matrix", "cpim_metal", "cpim_rhs", "qsc", "list_build", "solver_vec", "resid",
+                "solve"):
         prof[cls] = profile_get(sim, cls)
+    n_spmv = spmv_effective(sim, 0)
     cm.lib().capac_profile_enable(sim._p, 0)
     clk = clocks.stop()
     torch.cuda.synchronize()
@@ -261,12 +267,19 @@ def main() -> int:
 
     # dominant kernel and its roofline
     peak, peak_kind = _peaks()
-    dom = max(("pair", "spmv", "matrix"), key=lambda k: prof[k][1])
+    dom = max(("pair", "spmv", "matrix", "solve"), key=lambda k: prof[k][1])
     n_launch, tot_ms = prof[dom]
     if dom == "spmv":
-        n_launch = spmv_effective(sim, n_launch)
+        n_launch = n_spmv or n_launch
     avg_s = tot_ms / max(n_launch, 1) / 1e3
-    bytes_launch = algorithmic_bytes(sim, dom, N, M, args.precision)
+    if dom == "solve":
+        # one launch = a whole solve: its SpMV products plus the BiCGSTAB
+        # vector updates (19 n doubles per iteration beyond the products)
+        iters = max(n_spmv - n_launch, 0) / 2
+        bytes_launch = (n_spmv * algorithmic_bytes(sim, "spmv", N, M, args.precision)
+                        + iters * 19 * desc.n_mat * 8.0) / max(n_launch, 1)
+    else:
+        bytes_launch = algorithmic_bytes(sim, dom, N, M, args.precision)
     achieved = bytes_launch / avg_s / 1e9 if avg_s > 0 else None
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak if achieved else None, "traffic": _traffic(args.workload, dom),
@@ -301,9 +314,12 @@ def main() -> int:
                        "atoms": N, "metal_atoms": M, "cpim_unknowns": desc.n_mat, "precision": args.precision,
                        "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
                        "l2": "inputs larger than L2 (neighbour list and CPIM matrix > 126 MB)"},
-            "ns_per_day": args.steps / (ms / 1e3) * 0.001 * 86400 * 1e-3 * 1e3,
-            "solver": {"iterations_last": st.solver_iterations, "rel_residual_last": st.solver_rel_residual,
-                       "spmv_ms_total": prof["spmv"][1]},
+            "ns_per_day": args.steps / (ms / 1e3) * 0.001 * 86.4,  # steps/s x dt(ps) x s/day / ps-per-ns
+            "solver": {"iterations_last": st.solver_iterations, "sweeps_last": st.solver_outer,
+                       "initial_rel_residual_last": st.solver_initial_rel_residual,
+                       "rel_residual_last": st.solver_rel_residual,
+                       "ms_per_solve": (prof["spmv"][1] + prof["solver_vec"][1] + prof["resid"][1]
+                                        + prof["solve"][1]) / args.steps},
             "kernel_ms": {k: v[1] for k, v in prof.items()},
             "phase_ms_last_force": {"list": ps[10], "qsc": ps[1], "cpim_vec": ps[6], "cpim_matrix": ps[5],
                                     "cpim_solve": ps[7], "nonbonded": ps[4], "cpim_force": ps[8]},

@@ -45,14 +45,16 @@ class CapacError(RuntimeError):
 class Options(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int), ("device", ctypes.c_int), ("skin", ctypes.c_double),
                 ("list_every", ctypes.c_int), ("max_neighbors", ctypes.c_int),
-                ("solver_tol", ctypes.c_double), ("refine_tol", ctypes.c_double)]
+                ("solver_tol", ctypes.c_double), ("refine_tol", ctypes.c_double),
+                ("matrix_layout", ctypes.c_int), ("predictor", ctypes.c_int), ("solver_kernel", ctypes.c_int)]
 
 
 class Stats(ctypes.Structure):
     _fields_ = [("solver_iterations", ctypes.c_int), ("solver_outer", ctypes.c_int),
                 ("solver_rel_residual", ctypes.c_double), ("list_builds", ctypes.c_long),
                 ("list_entries", ctypes.c_long), ("max_neighbors", ctypes.c_long),
-                ("list_capacity", ctypes.c_int), ("md_step", ctypes.c_long)]
+                ("list_capacity", ctypes.c_int), ("md_step", ctypes.c_long),
+                ("solver_initial_rel_residual", ctypes.c_double)]
 
 
 class Consts(ctypes.Structure):
@@ -152,12 +154,14 @@ class Simulation:
     """Device-resident state of one system on one B200."""
 
     def __init__(self, desc: Desc, precision: int = PREC_FP64, device: int = 0, skin: float = 0.2,
-                 solver_tol: float = 0.0, refine_tol: float = 1e-10, max_neighbors: int = 0):
+                 solver_tol: float = 0.0, refine_tol: float = 1e-11, max_neighbors: int = 0,
+                 matrix_layout: int = 0, predictor: int = 1, solver_kernel: int = 0):
         self.desc = desc
         o = Options()
         lib().capac_options_default(ctypes.byref(o))
         o.precision, o.device, o.skin = precision, device, skin
         o.solver_tol, o.refine_tol, o.max_neighbors = solver_tol, refine_tol, max_neighbors
+        o.matrix_layout, o.predictor, o.solver_kernel = matrix_layout, predictor, solver_kernel
         self._p = ctypes.c_void_p()
         _check(lib().capac_create(desc.ptr, ctypes.byref(o), ctypes.byref(self._p)))
         self.n_atoms = desc.n_atoms

@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 
@@ -70,7 +71,7 @@ void force(capac_ctx *c, bool solve = true)
     if (cpim) launch_cpim_matrix(c);
     record(c, 4);
     int st = CAPAC_OK;
-    if (cpim && solve) st = run_bicgstab(c);
+    if (cpim && solve) st = c->opt.precision == CAPAC_PREC_MIXED ? run_refined_solve(c) : run_bicgstab(c);
     record(c, 5);
     launch_pair_forces(c, 0);
     record(c, 6);
@@ -154,6 +155,17 @@ void prof_begin(capac_ctx *c, int cls)
 {
     Profiler &p = c->prof;
     if (!p.on) return;
+    if (SolveGraph *g = c->capturing) {
+        // inside a capture: the replay records a pair of the graph's own events
+        cudaEvent_t a, b;
+        CAPAC_CUDA(cudaEventCreate(&a));
+        CAPAC_CUDA(cudaEventCreate(&b));
+        g->ev.push_back(a);
+        g->ev.push_back(b);
+        g->cls.push_back(cls);
+        CAPAC_CUDA(cudaEventRecordWithFlags(a, c->stream, cudaEventRecordExternal));
+        return;
+    }
     if (p.used == kProfSlots) prof_flush(c);
     p.cls[p.used] = cls;
     CAPAC_CUDA(cudaEventRecord(p.ev[2 * p.used], c->stream));
@@ -163,8 +175,24 @@ void prof_end(capac_ctx *c)
 {
     Profiler &p = c->prof;
     if (!p.on) return;
+    if (SolveGraph *g = c->capturing) {
+        CAPAC_CUDA(cudaEventRecordWithFlags(g->ev.back(), c->stream, cudaEventRecordExternal));
+        return;
+    }
     CAPAC_CUDA(cudaEventRecord(p.ev[2 * p.used + 1], c->stream));
     ++p.used;
+}
+
+// After a replay of a profiled graph has completed: add its event pairs.
+void prof_graph_replayed(capac_ctx *c, const SolveGraph &g)
+{
+    if (!c->prof.on || !g.prof) return;
+    for (size_t k = 0; k < g.cls.size(); ++k) {
+        float ms = 0.f;
+        CAPAC_CUDA(cudaEventElapsedTime(&ms, g.ev[2 * k], g.ev[2 * k + 1]));
+        c->prof.ms[g.cls[k]] += ms;
+        c->prof.count[g.cls[k]] += 1;
+    }
 }
 
 void cuda_check(cudaError_t e, const char *what)
@@ -190,7 +218,10 @@ void capac_options_default(capac_options *o)
     o->list_every = 0;
     o->max_neighbors = 0;
     o->solver_tol = 0.0;
-    o->refine_tol = 1.0e-10;
+    o->refine_tol = 1.0e-11;
+    o->matrix_layout = 0;
+    o->predictor = 1;
+    o->solver_kernel = 0;
 }
 
 int capac_create(const capac_desc *d, const capac_options *opt, capac_ctx **out)
@@ -228,6 +259,8 @@ int capac_create(const capac_desc *d, const capac_options *opt, capac_ctx **out)
         try {
             c->opt = o;
             c->device = o.device;
+            c->num_sms = prop.multiProcessorCount;
+            c->use_graphs = getenv("CAPAC_NO_GRAPHS") == nullptr;
             derive(d, &c->c);
             c->N = d->n_atoms;
             c->M = d->n_metal;
@@ -255,7 +288,6 @@ int capac_create(const capac_desc *d, const capac_options *opt, capac_ctx **out)
             c->ox = dalloc<double>(N); c->oy = dalloc<double>(N); c->oz = dalloc<double>(N);
             c->rx0 = dalloc<double>(N); c->ry0 = dalloc<double>(N); c->rz0 = dalloc<double>(N);
             c->pos4 = dalloc<double4>(N);
-            if (o.precision == CAPAC_PREC_MIXED) c->pos4f = dalloc<float4>(N);
 
             // topology
             c->type = dupload(d->atom_type, N, s);
@@ -382,7 +414,26 @@ int capac_create(const capac_desc *d, const capac_options *opt, capac_ctx **out)
                 CAPAC_CUDA(cudaMemcpyAsync(c->diag, diag.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s));
                 CAPAC_CUDA(cudaStreamSynchronize(s));
                 if (c->use_cpff) {
-                    c->mat = dalloc<double>((size_t)M * 16 * c->Mp);
+                    const bool mixed = o.precision == CAPAC_PREC_MIXED;
+                    if (o.matrix_layout == 0) {
+                        const size_t ne = sym_matrix_elems(M);
+                        c->msym = mixed ? (void *)dalloc<float>(ne) : (void *)dalloc<double>(ne);
+                        c->sympart = dalloc<double>(sym_partial_doubles(M));
+                        if (o.solver_kernel == 0) c->coop_grid = coop_grid_size(c->device, mixed);
+                        if (c->coop_grid > 0) {
+                            c->coop_bp = dalloc<double>((size_t)6 * c->coop_grid);
+                            c->coop_bar = dalloc<unsigned char>(coop_barrier_bytes());
+                        }
+                    } else if (mixed) {
+                        c->matf = dalloc<float>((size_t)M * 16 * c->Mp);
+                    } else {
+                        c->mat = dalloc<double>((size_t)M * 16 * c->Mp);
+                    }
+                    if (mixed) {
+                        c->rres = dalloc<double>(n);
+                        c->dcorr = dalloc<double>(n);
+                        c->xprev = dalloc<double>(n);
+                    }
                     c->bw = dalloc<double>((size_t)n * 11);
                     CAPAC_CUDA(cudaMemsetAsync(c->bw, 0, sizeof(double) * n * 11, s));
                 }
@@ -429,7 +480,7 @@ int capac_destroy(capac_ctx *c)
                    c->cstr_cnt, c->cstr_i, c->cstr_j, c->cstr_r, c->np_start, c->np_end, c->np_charge,
                    c->nbr, c->nnb, c->cell_key, c->cell_key_sorted, c->atom_ids, c->cell_atoms,
                    c->cell_start, c->cell_end, c->sort_tmp, c->flags, c->isd, c->vec_ext, c->vec_pq,
-                   c->diag, c->mat, c->matf, c->bw, c->bwf, c->ss, c->partials, c->pot, c->vir, c->th};
+                   c->diag, c->mat, c->matf, c->msym, c->sympart, c->coop_bp, c->coop_bar, c->rres, c->dcorr, c->xprev, c->bw, c->bwf, c->ss, c->partials, c->pot, c->vir, c->th};
     for (void *p : dev)
         if (p) cudaFree(p);
     if (c->h_flags) cudaFreeHost(c->h_flags);
@@ -439,6 +490,11 @@ int capac_destroy(capac_ctx *c)
         if (e) cudaEventDestroy(e);
     for (auto &e : c->prof.ev)
         if (e) cudaEventDestroy(e);
+    for (auto &g : c->graphs) {
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+        for (auto &e : g.ev)
+            if (e) cudaEventDestroy(e);
+    }
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return CAPAC_OK;
@@ -499,7 +555,7 @@ int capac_cpim_matvec(capac_ctx *c, const double *x, double *y)
     return guard([&] {
         check_ctx(c);
         if (!x || !y) throw Error(CAPAC_ERR_INVALID, "null argument");
-        if (c->M == 0 || !c->mat) throw Error(CAPAC_ERR_INVALID, "no CPIM matrix in this system");
+        if (c->M == 0 || (!c->mat && !c->matf && !c->msym)) throw Error(CAPAC_ERR_INVALID, "no CPIM matrix in this system");
         double *dx = c->bw + (size_t)W_Y_SLOT * c->n_mat, *dy = c->bw + (size_t)W_V_SLOT * c->n_mat;
         const size_t nb = sizeof(double) * c->n_mat;
         CAPAC_CUDA(cudaMemcpyAsync(dx, x, nb, cudaMemcpyHostToDevice, c->stream));
@@ -535,7 +591,7 @@ int capac_cpff_mat_relay(capac_ctx *c, long *nnz)
 {
     return guard([&] {
         check_ctx(c);
-        if (c->M == 0 || !c->mat) return;
+        if (c->M == 0 || (!c->mat && !c->matf && !c->msym)) return;
         launch_pack_positions(c);
         launch_cpim_matrix(c);
         CAPAC_CUDA(cudaStreamSynchronize(c->stream));
@@ -553,8 +609,8 @@ int capac_bicgstab(capac_ctx *c, int *iterations)
 {
     return guard([&] {
         check_ctx(c);
-        if (c->M == 0 || !c->mat) return;
-        const int st = run_bicgstab(c);
+        if (c->M == 0 || (!c->mat && !c->matf && !c->msym)) return;
+        const int st = c->opt.precision == CAPAC_PREC_MIXED ? run_refined_solve(c) : run_bicgstab(c);
         if (iterations) *iterations = c->last_iters;
         if (st != CAPAC_OK) throw Error(st, "Error: bicg_stab not converged.");
     });
@@ -664,6 +720,7 @@ int capac_set(capac_ctx *c, const char *name, const double *in)
             throw Error(CAPAC_ERR_INVALID, "array " + n + " cannot be set");
         if (cnt > 0) CAPAC_CUDA(cudaMemcpy(p, in, sizeof(double) * cnt, cudaMemcpyHostToDevice));
         if (n == "rx" || n == "ry" || n == "rz") c->list_valid = false;
+        if (n == "vec_pq") c->n_solves = 0;  // a new warm start restarts the predictor history
         count = cnt;
     });
     return st == CAPAC_OK ? count : st;
@@ -678,6 +735,7 @@ int capac_get_stats(capac_ctx *c, capac_stats *out)
         out->solver_iterations = c->last_iters;
         out->solver_outer = c->last_outer;
         out->solver_rel_residual = c->last_rel_res;
+        out->solver_initial_rel_residual = c->last_init_res;
         out->list_builds = c->list_builds;
         out->list_capacity = c->cap;
         out->md_step = c->md_step;
@@ -771,7 +829,7 @@ int capac_profile_get(capac_ctx *c, const char *cls, long *launches, double *tot
         check_ctx(c);
         if (!cls || !launches || !total_ms) throw Error(CAPAC_ERR_INVALID, "null argument");
         static const char *names[K_NCLASS] = {"pair", "spmv", "matrix", "cpim_metal", "cpim_rhs",
-                                              "qsc", "list_build", "solver_vec", "integrate"};
+                                              "qsc", "list_build", "solver_vec", "integrate", "resid", "solve"};
         prof_flush(c);
         if (0 == strcmp(cls, "spmv_effective")) {
             *launches = c->prof.spmv_effective;

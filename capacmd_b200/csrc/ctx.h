@@ -14,8 +14,9 @@ namespace capac {
 
 // Scalars of one BiCGSTAB solve, kept in device memory (bicg_stab.c:280-303).
 struct SolverScalars {
-    double bTb, crit, rho, rho_old, alpha, omega, rTr, rho_next;
+    double bTb, crit, rho, rho_old, alpha, omega, rTr, skip;
     double res0;     // refinement: FP64 residual norm^2 at the sweep start
+    double rr0;      // (r, r) of the warm start
     int iter, done, status, pad;
 };
 
@@ -53,7 +54,11 @@ struct DevParams {
 };
 
 // Kernel classes for the event-based profiler.
-enum KClass { K_PAIR = 0, K_SPMV, K_MATRIX, K_CPIM_METAL, K_CPIM_RHS, K_QSC, K_LIST, K_SOLVER_VEC, K_INTEGRATE, K_NCLASS };
+enum KClass {
+    K_PAIR = 0, K_SPMV, K_MATRIX, K_CPIM_METAL, K_CPIM_RHS, K_QSC, K_LIST, K_SOLVER_VEC, K_INTEGRATE, K_RESID,
+    K_SOLVE,  // persistent solver: a whole BiCGSTAB solve in one launch
+    K_NCLASS
+};
 
 // Pool of CUDA event pairs bracketing launches while profiling is on.
 struct Profiler {
@@ -64,6 +69,17 @@ struct Profiler {
     long count[K_NCLASS] = {};
     double ms[K_NCLASS] = {};
     long spmv_effective = 0;  // SpMV launches that did work (1 + 2 per iteration per solve)
+};
+
+// A captured chunk of solver iterations, replayed with cudaGraphLaunch.
+struct SolveGraph {
+    const double *b = nullptr;
+    double *x = nullptr;
+    bool prof = false;                 // captured with event-record nodes
+    cudaGraphExec_t exec = nullptr;
+    long kernels = 0;                  // kernels per replay
+    std::vector<int> cls;              // kernel class of each event pair
+    std::vector<cudaEvent_t> ev;       // event pairs recorded by the replay
 };
 
 }  // namespace capac
@@ -82,6 +98,7 @@ struct capac_ctx {
     long md_step = 0;
     long list_builds = 0;
     int device = 0;
+    int num_sms = 148;
 
     // host copies needed on the host side
     std::vector<int> h_np_start, h_np_end;
@@ -127,13 +144,21 @@ struct capac_ctx {
     double *vec_ext = nullptr, *vec_pq = nullptr, *diag = nullptr;  // [n_mat]
     double *mat = nullptr;       // [M * 16 * Mp] 4x4 blocks, plane layout
     float *matf = nullptr;       // mixed path copy
+    void *msym = nullptr;        // symmetric packed tiles (float on the mixed path, else double)
+    double *sympart = nullptr;   // per-tile partial sums of the symmetric SpMV
+    int coop_grid = 0;           // blocks of the persistent solver (0: per-step launches)
+    double *coop_bp = nullptr;   // its per-block dot partials, 6 * coop_grid
+    void *coop_bar = nullptr;    // its grid barrier
     double *bw = nullptr;        // BiCGSTAB work vectors, 11 * n_mat
-    float *bwf = nullptr;        // mixed path inner-solve vectors
+    float *bwf = nullptr;        // (unused)
+    double *rres = nullptr, *dcorr = nullptr;  // mixed path: FP64 residual and correction, n_mat each
+    double *xprev = nullptr;     // mixed path: previous step's solution (warm-start extrapolation)
+    int n_solves = 0;            // completed solves (the extrapolation needs two)
     capac::SolverScalars *ss = nullptr;
     capac::SolverScalars *h_ss = nullptr;  // pinned
     long nnz = 0;
     int last_iters = 0, last_outer = 0;
-    double last_rel_res = 0.0;
+    double last_rel_res = 0.0, last_init_res = 0.0;
 
     // reductions and outputs
     double *partials = nullptr;
@@ -146,6 +171,9 @@ struct capac_ctx {
     cudaEvent_t ev[16] = {};
     float phase_ms[15] = {};
     capac::Profiler prof;
+    std::vector<capac::SolveGraph> graphs;
+    capac::SolveGraph *capturing = nullptr;  // set while a solver chunk is being captured
+    bool use_graphs = true;
 };
 
 namespace capac {
@@ -161,8 +189,21 @@ void launch_qsc(capac_ctx *c);
 void launch_cpim_rhs(capac_ctx *c);
 void launch_cpim_matrix(capac_ctx *c);
 int run_bicgstab(capac_ctx *c);  // returns status
+int run_refined_solve(capac_ctx *c);  // mixed path: FP64 refinement around FP32-matrix BiCGSTAB
 void launch_cpim_spmv(capac_ctx *c, const double *x, double *y);  // plain y = A x
+// symmetric packed storage (k_cpim_sym.cu)
+int sym_tiles(int M);
+size_t sym_matrix_elems(int M);
+size_t sym_partial_doubles(int M);
+void launch_sym_assemble(capac_ctx *c);
+int sym_reduce_blocks(const capac_ctx *c);
+void launch_sym_spmv(capac_ctx *c, int dot, const double *x, double *y, const double *d1, const double *d2,
+                     const SolverScalars *ss);
 constexpr int W_Y_SLOT = 7, W_V_SLOT = 4;  // BiCGSTAB work-vector slots used as scratch
+// persistent cooperative solver (k_solve_coop.cu)
+int coop_grid_size(int device, bool mixed);
+size_t coop_barrier_bytes();
+int bicgstab_coop(capac_ctx *c, const double *b, double *x, double tol, double skip);
 void launch_cpim_metal_forces(capac_ctx *c);
 void launch_external_field(capac_ctx *c);
 void launch_finalize(capac_ctx *c, int nblocks, int K, const int *slots_pot, const int *slots_vir);
@@ -187,6 +228,7 @@ size_t partials_needed(const capac_ctx *c);
 void prof_begin(capac_ctx *c, int cls);
 void prof_end(capac_ctx *c);
 void prof_flush(capac_ctx *c);
+void prof_graph_replayed(capac_ctx *c, const SolveGraph &g);
 struct ProfScope {
     capac_ctx *c;
     ProfScope(capac_ctx *cc, int cls) : c(cc) { prof_begin(c, cls); }

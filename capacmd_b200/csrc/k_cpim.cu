@@ -219,6 +219,10 @@ __global__ void __launch_bounds__(128) k_cpim_matrix(DevParams P, const double4 
 
 void launch_cpim_matrix(capac_ctx *c)
 {
+    if (c->msym) {
+        launch_sym_assemble(c);
+        return;
+    }
     dim3 grid(grid_for(c->Mp, 128), c->M);
     ProfScope ps(c, K_MATRIX);
     if (c->matf)
@@ -343,8 +347,11 @@ __global__ void __launch_bounds__(256) k_vec_dot(int n, const double *__restrict
     }
 }
 
-// bTb, early exit and criterion (bicg_stab.c:296-303).
-__global__ void k_bcg_start(const double *partials, int nb, double tol, SolverScalars *ss)
+// bTb, early exit and criterion (bicg_stab.c:296-303).  `skip` is the
+// absolute threshold of the reference's two early exits (bTb < 1e-10 and, on
+// the first iteration, rho < 1e-10); refinement sweeps, whose right-hand
+// sides are small residuals, pass a threshold that only catches exact zero.
+__global__ void k_bcg_start(const double *partials, int nb, double tol, double skip, SolverScalars *ss)
 {
     __shared__ double sh[64];
     double s0, s1;
@@ -355,7 +362,8 @@ __global__ void k_bcg_start(const double *partials, int nb, double tol, SolverSc
         ss->rho_old = ss->alpha = ss->omega = 1.0;
         ss->iter = 0;
         ss->status = 0;
-        ss->done = s0 < 1.0e-10 ? 1 : 0;
+        ss->skip = skip;
+        ss->done = s0 < skip ? 1 : 0;
         ss->rTr = 0.0;
     }
 }
@@ -391,7 +399,11 @@ __global__ void k_bcg_rho0(const double *partials, int nb, SolverScalars *ss)
     if (ss->done) return;
     double s0, s1;
     sum_partials2(partials, nb, sh, s0, s1);
-    if (threadIdx.x == 0) ss->rho = s0;
+    if (threadIdx.x == 0) {
+        ss->rho = s0;  // (r0, r) with r = r0
+        ss->rTr = s0;
+        ss->rr0 = s0;
+    }
 }
 
 // p = r + beta (p - omega v), y = K p (bicg_stab.c:371-404); the iteration-0
@@ -399,7 +411,7 @@ __global__ void k_bcg_rho0(const double *partials, int nb, SolverScalars *ss)
 __global__ void __launch_bounds__(256) k_bcg_p(int n, double *bw, SolverScalars *ss)
 {
     if (ss->done) return;
-    if (ss->iter == 0 && ss->rho < 1.0e-10) {
+    if (ss->iter == 0 && ss->rho < ss->skip) {
         if (blockIdx.x == 0 && threadIdx.x == 0) ss->done = 1;
         return;
     }
@@ -411,13 +423,31 @@ __global__ void __launch_bounds__(256) k_bcg_p(int n, double *bw, SolverScalars 
     bw[W_Y * n + k] = p * bw[W_K * n + k];
 }
 
+// Status when BiCGSTAB breaks down (a zero or non-finite alpha or omega, which
+// the reference does not guard against and which it would carry into NaN):
+// the iterate stays at the last finite x.  Accepted like the reference's
+// MAX_ITER fallback when rTr < 100 crit (status 1), otherwise an error (-1).
+// rTr of iteration 0 is the initial residual, stored by k_bcg_rho0.
+__device__ __forceinline__ int breakdown_status(const SolverScalars *ss)
+{
+    return ss->rTr < ss->crit * 100.0 ? 1 : -2;  // -2: restartable breakdown
+}
+
 __global__ void k_bcg_alpha(const double *partials, int nb, SolverScalars *ss)
 {
     __shared__ double sh[64];
     if (ss->done) return;
     double s0, s1;
     sum_partials2(partials, nb, sh, s0, s1);
-    if (threadIdx.x == 0) ss->alpha = ss->rho / s0;
+    if (threadIdx.x == 0) {
+        const double a = ss->rho / s0;
+        if (isfinite(a)) {
+            ss->alpha = a;
+        } else {  // breakdown: keep x as it is and judge the last residual
+            ss->done = 1;
+            ss->status = breakdown_status(ss);
+        }
+    }
 }
 
 // s = r - alpha v, z = K s (bicg_stab.c:418-449).
@@ -437,7 +467,15 @@ __global__ void k_bcg_omega(const double *partials, int nb, SolverScalars *ss)
     if (ss->done) return;
     double s0, s1;
     sum_partials2(partials, nb, sh, s0, s1);
-    if (threadIdx.x == 0) ss->omega = s0 / s1;
+    if (threadIdx.x == 0) {
+        const double w = s0 / s1;
+        if (isfinite(w) && w != 0.0) {
+            ss->omega = w;
+        } else {  // breakdown before x is touched
+            ss->done = 1;
+            ss->status = breakdown_status(ss);
+        }
+    }
 }
 
 // x += alpha y + omega z, r = s - omega t; (r, r) and (r0, r) partials
@@ -489,6 +527,10 @@ namespace {
 void spmv(capac_ctx *c, int dot, const double *x, double *y, const double *d1, const double *d2,
           const SolverScalars *ss)
 {
+    if (c->msym) {
+        launch_sym_spmv(c, dot, x, y, d1, d2, ss);
+        return;
+    }
     const int nb = c->M + c->n_nps;
     ProfScope ps(c, K_SPMV);
     cudaStream_t s = c->stream;
@@ -519,27 +561,84 @@ void launch_cpim_spmv(capac_ctx *c, const double *x, double *y)
     spmv(c, DOT_NONE, x, y, nullptr, nullptr, nullptr);
 }
 
-// mpi_precon_bicg_stab_COO (bicg_stab.c:253-573) on the device; the host only
-// polls the done flag every few iterations.
-int run_bicgstab(capac_ctx *c)
+// y = A x with every block recomputed in FP64 from the positions.
+void spmv_free(capac_ctx *c, const double *x, double *y)
 {
+    const int nb = c->M + c->n_nps;
+    ProfScope ps(c, K_RESID);
+    k_spmv<DOT_NONE, double, true><<<nb, 256, 0, c->stream>>>(c->P, c->Mp, nullptr, c->pos4, x, y, nullptr, nullptr,
+                                                              c->partials, nullptr);
+    ++c->launches;
+}
+
+// r = b - Ax; partials of (r, r).
+__global__ void __launch_bounds__(256) k_residual(int n, const double *__restrict__ b, const double *__restrict__ Ax,
+                                                  double *__restrict__ r, double *partials)
+{
+    __shared__ double sh[64];
+    double v[2] = {0.0, 0.0};
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) {
+        const double rk = b[k] - Ax[k];
+        r[k] = rk;
+        v[0] = rk * rk;
+    }
+    block_sum<2>(v, sh);
+    if (threadIdx.x == 0) {
+        partials[2 * blockIdx.x] = v[0];
+        partials[2 * blockIdx.x + 1] = 0.0;
+    }
+}
+
+__global__ void k_residual_final(const double *partials, int nb, SolverScalars *ss)
+{
+    __shared__ double sh[64];
+    double s0, s1;
+    sum_partials2(partials, nb, sh, s0, s1);
+    if (threadIdx.x == 0) ss->res0 = s0;
+}
+
+__global__ void __launch_bounds__(256) k_axpy1(int n, const double *__restrict__ d, double *__restrict__ x)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) x[k] += d[k];
+}
+
+// Warm-start predictor: x <- 2 x - x_prev, x_prev <- old x (linear
+// extrapolation of the last two solutions); `first` only records x.
+__global__ void __launch_bounds__(256) k_predict(int n, int first, double *__restrict__ x, double *__restrict__ xprev)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const double t = x[k];
+    if (!first) x[k] = 2.0 * t - xprev[k];
+    xprev[k] = t;
+}
+
+// Jacobi-preconditioned BiCGSTAB (bicg_stab.c:253-573) on A x = b with the
+// stored matrix (FP64, or FP32 on the mixed path), x warm-started.  The host
+// polls the done flag every few iterations.  Returns the status; the solver
+// scalars are left in c->h_ss.
+int bicgstab_core(capac_ctx *c, const double *b, double *x, double tol, double skip)
+{
+    if (c->coop_grid > 0) return bicgstab_coop(c, b, x, tol, skip);
     const int n = c->n_mat, n4 = 4 * c->M;
     const int nbv = (int)grid_for(n, 256);
-    const int nbm = c->M + c->n_nps;
+    const int nbm = c->msym ? sym_reduce_blocks(c) : c->M + c->n_nps;  // blocks writing SpMV dot partials
     cudaStream_t s = c->stream;
     double *bw = c->bw;
     auto W = [&](int k) { return bw + (size_t)k * n; };
-    const double tol = c->opt.solver_tol > 0.0 ? c->opt.solver_tol : 1.0e-8;
 
-    k_vec_dot<<<nbv, 256, 0, s>>>(n, c->vec_ext, c->vec_ext, c->partials);
-    k_bcg_start<<<1, 256, 0, s>>>(c->partials, nbv, tol, c->ss);
-    spmv(c, DOT_NONE, c->vec_pq, W(W_AX), nullptr, nullptr, c->ss);
-    k_bcg_init<<<nbv, 256, 0, s>>>(n, n4, c->vec_ext, c->diag, bw, c->partials, c->ss);
+    k_vec_dot<<<nbv, 256, 0, s>>>(n, b, b, c->partials);
+    k_bcg_start<<<1, 256, 0, s>>>(c->partials, nbv, tol, skip, c->ss);
+    spmv(c, DOT_NONE, x, W(W_AX), nullptr, nullptr, c->ss);
+    k_bcg_init<<<nbv, 256, 0, s>>>(n, n4, b, c->diag, bw, c->partials, c->ss);
     k_bcg_rho0<<<1, 256, 0, s>>>(c->partials, nbv, c->ss);
     c->launches += 4;
 
     const int chunk = 4;
-    for (int it = 0; it <= kMaxIter + chunk; it += chunk) {
+    // One chunk of iterations; every kernel returns at once after convergence.
+    auto issue_chunk = [&]() {
         for (int q = 0; q < chunk; ++q) {
             {
                 ProfScope ps(c, K_SOLVER_VEC);
@@ -555,23 +654,135 @@ int run_bicgstab(capac_ctx *c)
             {
                 ProfScope ps(c, K_SOLVER_VEC);
                 k_bcg_omega<<<1, 256, 0, s>>>(c->partials, nbm, c->ss);
-                k_bcg_x<<<nbv, 256, 0, s>>>(n, bw, c->vec_pq, c->partials, c->ss);
+                k_bcg_x<<<nbv, 256, 0, s>>>(n, bw, x, c->partials, c->ss);
                 k_bcg_check<<<1, 256, 0, s>>>(c->partials, nbv, c->ss);
             }
             c->launches += 6;
         }
+    };
+    // The chunk only touches buffers fixed for the context's lifetime, so it
+    // is captured once per (b, x, profiling) and replayed as a CUDA graph.
+    SolveGraph *g = nullptr;
+    if (c->use_graphs) {
+        for (auto &sg : c->graphs)
+            if (sg.b == b && sg.x == x && sg.prof == c->prof.on) g = &sg;
+        if (!g) {
+            c->graphs.emplace_back();
+            g = &c->graphs.back();
+            g->b = b;
+            g->x = x;
+            g->prof = c->prof.on;
+            const long l0 = c->launches;
+            cudaGraph_t graph;
+            CAPAC_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+            c->capturing = g;
+            issue_chunk();
+            c->capturing = nullptr;
+            CAPAC_CUDA(cudaStreamEndCapture(s, &graph));
+            CAPAC_CUDA(cudaGraphInstantiate(&g->exec, graph, 0));
+            CAPAC_CUDA(cudaGraphDestroy(graph));
+            g->kernels = c->launches - l0;
+            c->launches = l0;
+        }
+    }
+    for (int it = 0; it <= kMaxIter + chunk; it += chunk) {
+        if (g) {
+            CAPAC_CUDA(cudaGraphLaunch(g->exec, s));
+            c->launches += g->kernels;
+        } else {
+            issue_chunk();
+        }
         CAPAC_CUDA(cudaMemcpyAsync(c->h_ss, c->ss, sizeof(SolverScalars), cudaMemcpyDeviceToHost, s));
         CAPAC_CUDA(cudaStreamSynchronize(s));
+        if (g) prof_graph_replayed(c, *g);
         if (c->h_ss->done) break;
     }
-    c->last_iters = c->h_ss->iter;
-    c->last_outer = 1;
-    if (c->prof.on && c->h_ss->bTb >= 1.0e-10) c->prof.spmv_effective += 1 + 2L * c->h_ss->iter;
-    c->last_rel_res = c->h_ss->bTb > 0 ? sqrt(c->h_ss->rTr / c->h_ss->bTb) : 0.0;
+    if (c->prof.on && c->h_ss->bTb >= skip) c->prof.spmv_effective += 1 + 2L * c->h_ss->iter;
     if (!c->h_ss->done || c->h_ss->status < 0) return CAPAC_ERR_NOT_CONVERGED;
-    if (c->h_ss->status == 1)
-        fprintf(stderr, "Note: Loosen bicg_stab convergence criteria to 1e-6 for this step.\n");
-    return CAPAC_OK;
+    return c->h_ss->status == 1 ? 1 : CAPAC_OK;
+}
+
+// The reference's solve: rTr < tol * bTb with its early exits.
+int run_bicgstab(capac_ctx *c)
+{
+    const double tol = c->opt.solver_tol > 0.0 ? c->opt.solver_tol : 1.0e-8;
+    int st = bicgstab_core(c, c->vec_ext, c->vec_pq, tol, 1.0e-10);
+    int iters = c->h_ss->iter, starts = 1;
+    // A breakdown (zero or non-finite alpha/omega) leaves x at its last finite
+    // value; restart from there with a fresh shadow residual, as is standard
+    // for BiCGSTAB (the reference would carry the NaN to MAX_ITER and exit).
+    while (c->h_ss->status == -2 && starts < 8) {
+        // not the reference's first iteration: only an exact zero ends it early
+        st = bicgstab_core(c, c->vec_ext, c->vec_pq, tol, 1.0e-300);
+        iters += c->h_ss->iter;
+        ++starts;
+    }
+    c->last_iters = iters;
+    c->last_outer = starts;
+    c->last_rel_res = c->h_ss->bTb > 0 ? sqrt(c->h_ss->rTr / c->h_ss->bTb) : 0.0;
+    c->last_init_res = c->h_ss->bTb > 0 ? sqrt(c->h_ss->rr0 / c->h_ss->bTb) : 0.0;
+    if (st == 1) fprintf(stderr, "Note: Loosen bicg_stab convergence criteria to 1e-6 for this step.\n");
+    return st < 0 ? st : CAPAC_OK;
+}
+
+// Mixed path: FP64 iterative refinement.  Each sweep recomputes the residual
+// r = b - A x in FP64 (matrix-free: every block rebuilt from the positions in
+// FP64, so no FP64 matrix is stored), solves A d = r with BiCGSTAB on the FP32
+// matrix (FP64 vectors, inner products and accumulation) to a relative
+// residual of 1e-5, and updates x += d, until |r| <= refine_tol |b|.  The
+// reference's zero-field early exit (bTb < 1e-10) is kept.
+int run_refined_solve(capac_ctx *c)
+{
+    const int n = c->n_mat;
+    const int nbv = (int)grid_for(n, 256);
+    cudaStream_t s = c->stream;
+    const double rtol = c->opt.refine_tol > 0.0 ? c->opt.refine_tol : 1.0e-11;
+    const double inner_tol = 1.0e-10;  // (1e-5)^2
+    const int max_sweeps = 12;
+
+    k_vec_dot<<<nbv, 256, 0, s>>>(n, c->vec_ext, c->vec_ext, c->partials);
+    k_bcg_start<<<1, 256, 0, s>>>(c->partials, nbv, 1.0, 1.0e-10, c->ss);
+    c->launches += 2;
+    CAPAC_CUDA(cudaMemcpyAsync(c->h_ss, c->ss, sizeof(SolverScalars), cudaMemcpyDeviceToHost, s));
+    CAPAC_CUDA(cudaStreamSynchronize(s));
+    c->last_iters = 0;
+    c->last_outer = 0;
+    c->last_rel_res = 0.0;
+    if (c->h_ss->done) return CAPAC_OK;  // zero right-hand side: keep x
+    const double bTb = c->h_ss->bTb;
+    if (c->opt.predictor == 1 && c->xprev) {
+        k_predict<<<nbv, 256, 0, s>>>(n, c->n_solves == 0 ? 1 : 0, c->vec_pq, c->xprev);
+        ++c->launches;
+    }
+    ++c->n_solves;
+    double rr = 0.0;
+    int total = 0, sweep = 0;
+    for (;; ++sweep) {
+        spmv_free(c, c->vec_pq, c->bw + (size_t)W_AX * n);
+        k_residual<<<nbv, 256, 0, s>>>(n, c->vec_ext, c->bw + (size_t)W_AX * n, c->rres, c->partials);
+        k_residual_final<<<1, 256, 0, s>>>(c->partials, nbv, c->ss);
+        c->launches += 2;
+        CAPAC_CUDA(cudaMemcpyAsync(c->h_ss, c->ss, sizeof(SolverScalars), cudaMemcpyDeviceToHost, s));
+        CAPAC_CUDA(cudaStreamSynchronize(s));
+        rr = c->h_ss->res0;
+        if (sweep == 0) c->last_init_res = sqrt(rr / bTb);
+        if (rr <= rtol * rtol * bTb || sweep == max_sweeps) break;
+        CAPAC_CUDA(cudaMemsetAsync(c->dcorr, 0, sizeof(double) * n, s));
+        const int st = bicgstab_core(c, c->rres, c->dcorr, inner_tol, 1.0e-300);
+        total += c->h_ss->iter;
+        if (st < 0 && c->h_ss->iter == 0) break;  // no progress possible
+        k_axpy1<<<nbv, 256, 0, s>>>(n, c->dcorr, c->vec_pq);
+        ++c->launches;
+    }
+    c->last_iters = total;
+    c->last_outer = sweep;
+    c->last_rel_res = sqrt(rr / bTb);
+    if (rr <= rtol * rtol * bTb) return CAPAC_OK;
+    if (rr < 1.0e-8 * bTb) {  // the reference's own criterion still holds
+        fprintf(stderr, "Note: refinement stopped at relative residual %.3e\n", c->last_rel_res);
+        return CAPAC_OK;
+    }
+    return CAPAC_ERR_NOT_CONVERGED;
 }
 
 // ------------------------------------------------- CPIM metal-side forces

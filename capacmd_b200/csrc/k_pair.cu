@@ -1,163 +1,406 @@
-// Nonbonded pair forces over the full neighbour list, FP64.
+// Nonbonded pair forces over the full neighbour list (FP64 and mixed).
 //
 // Per pair this is compute_nonbonded / compute_erf_vdw / compute_morse /
 // compute_buckingham (force.c:591-816) as dispatched by mpi_nonb_pair
 // (force.c:1476-1528): LJ shifted force + damped shifted force Coulomb
 // (funct 1), Buckingham (2), Morse (3), erf-damped vdW (4).
 //
-// One warp owns atom i and walks its list; every pair is visited from both
-// ends, so forces need no atomics and each end adds half of the pair energy
-// and virial.  The cut-off test uses the reference's r^2 rounding.
+// One warp owns an atom i at a time (grid-stride over atoms) and walks its
+// list; every pair is visited from both ends, so forces need no atomics and
+// each end adds half of the pair energy and virial.  The cut-off test is done
+// in FP64 with the reference's r^2 rounding, so both precisions keep exactly
+// the reference's pair set.  Candidates that pass it are compacted into a
+// per-warp queue in shared memory and the pair math runs on full warps.
 //
 // The same traversal adds, on each charged non-metal atom, the force from the
 // induced charges and dipoles of metal neighbours inside the cut-off: the
 // water side of the metal-water loop of mpi_cpff_force (cpff.c:578-724).  The
 // metal side, with energies [10],[11] and the virial, is k_cpim_metal.
+//
+// Mixed path: coordinate differences and the cut-off in FP64, the pair terms
+// in FP32, force sums per lane with Kahan compensation, energies and virial
+// gathered per atom in FP32 and summed across atoms in FP64.
+#include <algorithm>
+
 #include "terms.cuh"
 
 namespace capac {
 
 namespace {
 
-// Force factor (force on j = f * rvec) and energies of one nonbonded pair.
+constexpr int kPairWarps = 8;  // warps per block
+
+// FP32 constants of the run.
+struct PairConstsF {
+    float rc, inv_rc, inv_rc12, inv_rc6, alpha, a2_sqrtpi, w_const, w_erfc_arcut, fqq;
+    int use_vdw, use_coulomb;
+};
+
+// FP64 pair term (force on j = f * rvec), reference formulas with the
+// divisions by r, r^2, r^6, r^12 turned into products with 1/r.
 __device__ __forceinline__ double pair_term(const DevParams &P, int k, double qi, double qj, double r2,
                                             double &e_qq, double &e_vdw)
 {
     const int fn = P.nb_funct[k];
     const double4 pr = P.nb_par[k];  // (c6, c12, a, b)
-    const double r = sqrt(r2);
-    if (fn == 4) {  // compute_erf_vdw, force.c:591-632
+    const double r = sqrt(r2), rinv = 1.0 / r, r2inv = rinv * rinv;
+    if (fn == 4) {  // compute_erf_vdw, force.c:591-632 (width = a)
         if (pr.x != 0.0 || pr.y != 0.0) {
-            const double r6 = r2 * r2 * r2, r12 = r6 * r6;
-            const double a12 = pr.y / r12, a6 = pr.x / r6, u = r / pr.z, eu = erf(u);
+            const double r6inv = r2inv * r2inv * r2inv;
+            const double a12 = pr.y * r6inv * r6inv, a6 = pr.x * r6inv, u = r / pr.z, eu = erf(u);
             e_vdw += (a12 - a6) * eu;
-            return ((12.0 * a12 - 6.0 * a6) / r * eu - (a12 - a6) * 2.0 * kInvSqrtPi * exp(-u * u) / pr.z) / r;
+            return ((12.0 * a12 - 6.0 * a6) * rinv * eu - (a12 - a6) * 2.0 * kInvSqrtPi * exp(-u * u) / pr.z) * rinv;
         }
         return 0.0;
     }
     if (fn == 3) {  // compute_morse, force.c:639-667 (D = A, a = B, R = C6)
         const double e1 = exp(-pr.w * (r - pr.x)), e2 = e1 * e1;
         e_vdw += pr.z * (e2 - 2.0 * e1);
-        return 2.0 * pr.z * pr.w * (e2 - e1) / r;
+        return 2.0 * pr.z * pr.w * (e2 - e1) * rinv;
     }
     if (fn == 2) {  // compute_buckingham, force.c:674-703 (A, B, C6)
-        const double r6 = r2 * r2 * r2, r8 = r6 * r2, eb = exp(-pr.w * r);
-        e_vdw += pr.z * eb - pr.x / r6;
-        return pr.z * eb * pr.w / r - 6.0 * pr.x / r8;
+        const double r6inv = r2inv * r2inv * r2inv, eb = exp(-pr.w * r);
+        e_vdw += pr.z * eb - pr.x * r6inv;
+        return pr.z * eb * pr.w * rinv - 6.0 * pr.x * r6inv * r2inv;
     }
     // funct 1: compute_nonbonded, force.c:710-816 (not a 1-4 pair)
     double f = 0.0;
     if (pr.x != 0.0 || pr.y != 0.0) {
-        const double r6 = r2 * r2 * r2, r12 = r6 * r6;
+        const double r6inv = r2inv * r2inv * r2inv, r12inv = r6inv * r6inv;
         if (P.use_vdw == 1) {
-            const double fr = 12.0 * pr.y / r12 - 6.0 * pr.x / r6;
+            const double fr = 12.0 * pr.y * r12inv - 6.0 * pr.x * r6inv;
             const double fc = 12.0 * pr.y * P.inv_rc12 - 6.0 * pr.x * P.inv_rc6;
-            f = (fr - fc) / r2;
-            e_vdw += (pr.y / r12 - pr.x / r6) + (r - P.rc) * fc / P.rc - (pr.y * P.inv_rc12 - pr.x * P.inv_rc6);
+            f = (fr - fc) * r2inv;
+            e_vdw += (pr.y * r12inv - pr.x * r6inv) + (r - P.rc) * fc / P.rc - (pr.y * P.inv_rc12 - pr.x * P.inv_rc6);
         } else {
-            f = (pr.y * 2.0 / r12 - pr.x / r6) * 6.0 / r2;
-            e_vdw += pr.y / r12 - pr.x / r6;
+            f = (pr.y * 2.0 * r12inv - pr.x * r6inv) * 6.0 * r2inv;
+            e_vdw += pr.y * r12inv - pr.x * r6inv;
         }
     }
     if (qi != 0.0 && qj != 0.0) {
+        const double qq = kFQQ * qi * qj;
         if (P.use_coulomb == 1) {
             const double a = P.w_alpha, ec = erfc(a * r);
-            f += kFQQ * qi * qj * ((ec / r2 + P.w_a2_sqrtpi * exp(-a * a * r2) / r) - P.w_const) / r;
-            e_qq += kFQQ * qi * qj * (ec / r - P.w_erfc_arcut + P.w_const * (r - P.rc));
+            f += qq * ((ec * r2inv + P.w_a2_sqrtpi * exp(-a * a * r2) * rinv) - P.w_const) * rinv;
+            e_qq += qq * (ec * rinv - P.w_erfc_arcut + P.w_const * (r - P.rc));
         } else {
-            f += kFQQ * qi * qj / (r2 * r);
-            e_qq += kFQQ * qi * qj / r;
+            f += qq * r2inv * rinv;
+            e_qq += qq * rinv;
         }
     }
     return f;
 }
 
-}  // namespace
-
-template <bool NONBONDED, bool CPIM>
-__global__ void __launch_bounds__(256) k_pair_f64(DevParams P, const double4 *__restrict__ pos4,
-                                                  const uint32_t *__restrict__ nbr, const int *__restrict__ nnb,
-                                                  int cap, const double *__restrict__ vec_pq,
-                                                  double *__restrict__ fx, double *__restrict__ fy,
-                                                  double *__restrict__ fz, double *__restrict__ partials)
+// The same terms in FP32.
+__device__ __forceinline__ float pair_term_f(const DevParams &P, const PairConstsF &K, int k, float qi, float qj,
+                                             float r2, float &e_qq, float &e_vdw)
 {
+    const int fn = P.nb_funct[k];
+    const double4 pd = P.nb_par[k];
+    const float c6 = (float)pd.x, c12 = (float)pd.y, pa = (float)pd.z, pb = (float)pd.w;
+    const float rinv = rsqrtf(r2), r = r2 * rinv, r2inv = rinv * rinv;
+    if (fn == 4) {
+        if (c6 != 0.f || c12 != 0.f) {
+            const float r6inv = r2inv * r2inv * r2inv;
+            const float a12 = c12 * r6inv * r6inv, a6 = c6 * r6inv, u = r / pa, eu = erff(u);
+            e_vdw += (a12 - a6) * eu;
+            return ((12.f * a12 - 6.f * a6) * rinv * eu - (a12 - a6) * 2.f * (float)kInvSqrtPi * expf(-u * u) / pa) *
+                   rinv;
+        }
+        return 0.f;
+    }
+    if (fn == 3) {
+        const float e1 = expf(-pb * (r - c6)), e2 = e1 * e1;
+        e_vdw += pa * (e2 - 2.f * e1);
+        return 2.f * pa * pb * (e2 - e1) * rinv;
+    }
+    if (fn == 2) {
+        const float r6inv = r2inv * r2inv * r2inv, eb = expf(-pb * r);
+        e_vdw += pa * eb - c6 * r6inv;
+        return pa * eb * pb * rinv - 6.f * c6 * r6inv * r2inv;
+    }
+    float f = 0.f;
+    if (c6 != 0.f || c12 != 0.f) {
+        const float r6inv = r2inv * r2inv * r2inv, r12inv = r6inv * r6inv;
+        if (K.use_vdw == 1) {
+            const float fr = 12.f * c12 * r12inv - 6.f * c6 * r6inv;
+            const float fc = 12.f * c12 * K.inv_rc12 - 6.f * c6 * K.inv_rc6;
+            f = (fr - fc) * r2inv;
+            e_vdw += (c12 * r12inv - c6 * r6inv) + (r - K.rc) * fc * K.inv_rc - (c12 * K.inv_rc12 - c6 * K.inv_rc6);
+        } else {
+            f = (c12 * 2.f * r12inv - c6 * r6inv) * 6.f * r2inv;
+            e_vdw += c12 * r12inv - c6 * r6inv;
+        }
+    }
+    if (qi != 0.f && qj != 0.f) {
+        const float qq = K.fqq * qi * qj;
+        if (K.use_coulomb == 1) {
+            const float ar = K.alpha * r, ec = erfcf(ar);
+            f += qq * ((ec * r2inv + K.a2_sqrtpi * expf(-ar * ar) * rinv) - K.w_const) * rinv;
+            e_qq += qq * (ec * rinv - K.w_erfc_arcut + K.w_const * (r - K.rc));
+        } else {
+            f += qq * r2inv * rinv;
+            e_qq += qq * rinv;
+        }
+    }
+    return f;
+}
+
+// CPIM force on a metal atom from a permanent charge (the atom receives the
+// opposite), FP32; r = metal - atom (cpim_charge_pair in FP32).
+__device__ __forceinline__ void cpim_charge_pair_f(const PairConstsF &K, const float r[3], float r2, float q_perm,
+                                                   float q_ind, const float p[3], float f[3])
+{
+    const float rinv = rsqrtf(r2), rr = r2 * rinv, r2inv = rinv * rinv;
+    float a0, ec = 0.f, eg = 0.f;
+    if (K.use_coulomb == 1) {
+        ec = erfcf(K.alpha * rr);
+        eg = expf(-K.alpha * K.alpha * r2);
+        a0 = (ec * r2inv + K.a2_sqrtpi * eg * rinv - K.w_const) * rinv;
+    } else {
+        a0 = r2inv * rinv;
+    }
+    const float s = K.fqq * q_perm;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) f[a] = a0 * r[a] * s * q_ind;
+    const float pr = p[0] * r[0] + p[1] * r[1] + p[2] * r[2];
+    const float sp = s / (float)kNm2Bohr;
+    const float ir3 = r2inv * rinv, ir5 = ir3 * r2inv;
+    if (K.use_coulomb == 1) {
+        const float al3 = K.alpha * K.alpha * K.alpha;
+        const float a1 = ir5 * (ec + K.a2_sqrtpi * rr * eg);
+        const float b1 = 4.f * (float)kInvSqrtPi * al3 * r2inv * eg;
+        const float c1 = K.w_const * ir3;
+        // sum_a T_ab p_a, T_ab = a1 (3 r_a r_b - d_ab r^2) + b1 r_a r_b - c1 (r_a r_b - d_ab r^2)
+#pragma unroll
+        for (int b = 0; b < 3; ++b)
+            f[b] -= (a1 * (3.f * pr * r[b] - p[b] * r2) + b1 * pr * r[b] - c1 * (pr * r[b] - p[b] * r2)) * sp;
+    } else {
+#pragma unroll
+        for (int b = 0; b < 3; ++b) f[b] -= (3.f * pr * r[b] - p[b] * r2) * ir5 * sp;
+    }
+}
+
+// Per-lane force accumulator: plain FP64, or Kahan-compensated FP32.
+template <typename Real>
+struct Acc;
+template <>
+struct Acc<double> {
+    double s = 0.0;
+    __device__ __forceinline__ void add(double v) { s += v; }
+    __device__ __forceinline__ double value() const { return s; }
+};
+template <>
+struct Acc<float> {
+    float s = 0.f, c = 0.f;
+    __device__ __forceinline__ void add(float v)
+    {
+        const float y = v - c;
+        const float t = s + y;
+        c = (t - s) - y;
+        s = t;
+    }
+    __device__ __forceinline__ double value() const { return (double)s - (double)c; }
+};
+
+// A candidate inside the cut-off, parked in the warp's queue.
+struct Cand {
+    double dx, dy, dz, r2, qj;
+    uint32_t e;
+    int pad;
+};
+
+template <typename Real, bool NONBONDED, bool CPIM>
+__global__ void __launch_bounds__(kPairWarps * 32) k_pair(DevParams P, PairConstsF K, const double4 *__restrict__ pos4,
+                                                           const uint32_t *__restrict__ nbr,
+                                                           const int *__restrict__ nnb, int cap,
+                                                           const double *__restrict__ vec_pq, double *__restrict__ fx,
+                                                           double *__restrict__ fy, double *__restrict__ fz,
+                                                           double *__restrict__ partials)
+{
+    __shared__ Cand queue[kPairWarps][64];
     __shared__ double sh[32 * 11];
-    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    double acc[11] = {0.0};  // fx fy fz e_qq e_vdw vir[9] -> packed below
-    double f3[3] = {0.0, 0.0, 0.0};
-    if (i < P.N) {
+    __shared__ double wacc[kPairWarps][8];  // per warp: e_qq, e_vdw, virial xx xy xz yy yz zz
+    const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const unsigned lt_mask = (1u << lane) - 1u;
+    Cand *Q = queue[wib];
+    if (lane < 8) wacc[wib][lane] = 0.0;
+    __syncwarp();
+    const int stride = gridDim.x * kPairWarps;
+    for (int i = blockIdx.x * kPairWarps + wib; i < P.N; i += stride) {
         const double4 pi = pos4[i];
-        const int ti = P.type[i];
-        const bool metal_i = P.is_metal[i] != 0;
+        const int trow = P.type[i] * P.n_types;
+        const bool cpim_i = CPIM && P.is_metal[i] == 0 && pi.w != 0.0;
         const int n = nnb[i];
         const uint32_t *row = nbr + (size_t)i * cap;
-        for (int k = lane; k < n; k += 32) {
-            const uint32_t e = row[k];
-            const int j = nb_index(e);
-            const double4 pj = pos4[j];
-            double dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
-            image(dx, dy, dz, P.box);
-            const double r2 = norm2_exact(dx, dy, dz);
-            if (r2 >= P.rc2) continue;
+        Acc<Real> f0, f1, f2;
+        Real e_qq = 0, e_vdw = 0;
+        Real v[6];  // the pair virial is symmetric: xx xy xz yy yz zz
+#pragma unroll
+        for (int q = 0; q < 6; ++q) v[q] = 0;
+
+        auto process = [&](const Cand &c) {
+            const Real dx = (Real)c.dx, dy = (Real)c.dy, dz = (Real)c.dz;
             if (NONBONDED) {
-                const double f = pair_term(P, ti * P.n_types + nb_type(e), pi.w, pj.w, r2, acc[0], acc[1]);
-                f3[0] -= f * dx;
-                f3[1] -= f * dy;
-                f3[2] -= f * dz;
-                // virial -= r_a (f r_b), half per visit
-                const double fjx = f * dx, fjy = f * dy, fjz = f * dz;
-                acc[2] -= 0.5 * dx * fjx; acc[3] -= 0.5 * dx * fjy; acc[4] -= 0.5 * dx * fjz;
-                acc[5] -= 0.5 * dy * fjx; acc[6] -= 0.5 * dy * fjy; acc[7] -= 0.5 * dy * fjz;
-                acc[8] -= 0.5 * dz * fjx; acc[9] -= 0.5 * dz * fjy; acc[10] -= 0.5 * dz * fjz;
+                Real f;
+                if constexpr (sizeof(Real) == 8)
+                    f = pair_term(P, trow + nb_type(c.e), pi.w, c.qj, c.r2, e_qq, e_vdw);
+                else
+                    f = pair_term_f(P, K, trow + nb_type(c.e), (float)pi.w, (float)c.qj, (float)c.r2, e_qq, e_vdw);
+                const Real gx = f * dx, gy = f * dy, gz = f * dz;
+                f0.add(-gx);
+                f1.add(-gy);
+                f2.add(-gz);
+                v[0] -= dx * gx; v[1] -= dx * gy; v[2] -= dx * gz;
+                v[3] -= dy * gy; v[4] -= dy * gz; v[5] -= dz * gz;
             }
-            if (CPIM && !metal_i && pi.w != 0.0 && P.is_metal[j]) {
-                const int jm = j - P.metal_min;
-                const double r[3] = {dx, dy, dz};  // metal - atom
-                const double pind[3] = {vec_pq[3 * jm], vec_pq[3 * jm + 1], vec_pq[3 * jm + 2]};
-                double f[3], a0, ec;
-                cpim_charge_pair(P, r, r2, pi.w, vec_pq[3 * P.M + jm], pind, f, a0, ec);
-                f3[0] -= f[0];
-                f3[1] -= f[1];
-                f3[2] -= f[2];
+            if (cpim_i) {
+                const int j = nb_index(c.e);
+                if (P.is_metal[j]) {
+                    const int jm = j - P.metal_min;
+                    if constexpr (sizeof(Real) == 8) {
+                        const double r[3] = {c.dx, c.dy, c.dz};  // metal - atom
+                        const double p[3] = {vec_pq[3 * jm], vec_pq[3 * jm + 1], vec_pq[3 * jm + 2]};
+                        double g[3], a0, ec;
+                        cpim_charge_pair(P, r, c.r2, pi.w, vec_pq[3 * P.M + jm], p, g, a0, ec);
+                        f0.add(-g[0]);
+                        f1.add(-g[1]);
+                        f2.add(-g[2]);
+                    } else {
+                        const float r[3] = {(float)c.dx, (float)c.dy, (float)c.dz};
+                        const float p[3] = {(float)vec_pq[3 * jm], (float)vec_pq[3 * jm + 1],
+                                            (float)vec_pq[3 * jm + 2]};
+                        float g[3];
+                        cpim_charge_pair_f(K, r, (float)c.r2, (float)pi.w, (float)vec_pq[3 * P.M + jm], p, g);
+                        f0.add(-g[0]);
+                        f1.add(-g[1]);
+                        f2.add(-g[2]);
+                    }
+                }
+            }
+        };
+
+        int qn = 0;  // queue fill, warp-uniform
+        for (int base = 0; base < n; base += 32) {
+            const int k = base + lane;
+            bool ok = false;
+            Cand c;
+            if (k < n) {
+                const uint32_t e = row[k];
+                const double4 pj = pos4[nb_index(e)];
+                double dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
+                image(dx, dy, dz, P.box);
+                const double r2 = norm2_exact(dx, dy, dz);
+                ok = r2 < P.rc2;
+                c.dx = dx;
+                c.dy = dy;
+                c.dz = dz;
+                c.r2 = r2;
+                c.qj = pj.w;
+                c.e = e;
+            }
+            const unsigned ballot = __ballot_sync(0xffffffffu, ok);
+            if (ok) Q[qn + __popc(ballot & lt_mask)] = c;
+            qn += __popc(ballot);
+            __syncwarp();
+            if (qn >= 32) {
+                process(Q[lane]);
+                __syncwarp();
+                if (lane < qn - 32) Q[lane] = Q[lane + 32];
+                __syncwarp();
+                qn -= 32;
             }
         }
-        f3[0] = warp_sum(f3[0]);
-        f3[1] = warp_sum(f3[1]);
-        f3[2] = warp_sum(f3[2]);
+        if (lane < qn) process(Q[lane]);
+        __syncwarp();
+
+        const double s0 = warp_sum(f0.value()), s1 = warp_sum(f1.value()), s2 = warp_sum(f2.value());
         if (lane == 0) {
-            fx[i] += f3[0];
-            fy[i] += f3[1];
-            fz[i] += f3[2];
+            fx[i] += s0;
+            fy[i] += s1;
+            fz[i] += s2;
         }
-        acc[0] *= 0.5;
-        acc[1] *= 0.5;
+        if (NONBONDED) {
+            const double t[8] = {warp_sum((double)e_qq), warp_sum((double)e_vdw), warp_sum((double)v[0]),
+                                 warp_sum((double)v[1]), warp_sum((double)v[2]), warp_sum((double)v[3]),
+                                 warp_sum((double)v[4]), warp_sum((double)v[5])};
+            if (lane == 0) {
+#pragma unroll
+                for (int q = 0; q < 8; ++q) wacc[wib][q] += 0.5 * t[q];
+            }
+        }
     }
-    if (NONBONDED) block_partials<11>(acc, sh, partials);
+    if (NONBONDED) {
+        __syncthreads();
+        // acc: e_qq, e_vdw, virial[9] (mirrored from the symmetric six)
+        double acc[11] = {0.0};
+        if (threadIdx.x < kPairWarps) {
+            const double *w = wacc[threadIdx.x];
+            acc[0] = w[0];
+            acc[1] = w[1];
+            acc[2] = w[2]; acc[3] = w[3]; acc[4] = w[4];
+            acc[5] = w[3]; acc[6] = w[5]; acc[7] = w[6];
+            acc[8] = w[4]; acc[9] = w[6]; acc[10] = w[7];
+        }
+        block_partials<11>(acc, sh, partials);
+    }
+}
+
+PairConstsF pair_consts_f(const capac_ctx *c)
+{
+    PairConstsF K;
+    K.rc = (float)c->P.rc;
+    K.inv_rc = (float)(1.0 / c->P.rc);
+    K.inv_rc12 = (float)c->P.inv_rc12;
+    K.inv_rc6 = (float)c->P.inv_rc6;
+    K.alpha = (float)c->P.w_alpha;
+    K.a2_sqrtpi = (float)c->P.w_a2_sqrtpi;
+    K.w_const = (float)c->P.w_const;
+    K.w_erfc_arcut = (float)c->P.w_erfc_arcut;
+    K.fqq = (float)kFQQ;
+    K.use_vdw = c->P.use_vdw;
+    K.use_coulomb = c->P.use_coulomb;
+    return K;
+}
+
+template <typename Real>
+void launch_pair_t(capac_ctx *c, int mode, unsigned grid)
+{
+    const PairConstsF K = pair_consts_f(c);
+    const bool cpim = c->M > 0 && c->use_cpff;
+    ProfScope ps(c, K_PAIR);
+    if (mode == 0 && cpim)
+        k_pair<Real, true, true><<<grid, kPairWarps * 32, 0, c->stream>>>(c->P, K, c->pos4, c->nbr, c->nnb, c->cap,
+                                                                          c->vec_pq, c->fx, c->fy, c->fz, c->partials);
+    else if (mode == 0)
+        k_pair<Real, true, false><<<grid, kPairWarps * 32, 0, c->stream>>>(c->P, K, c->pos4, c->nbr, c->nnb, c->cap,
+                                                                           c->vec_pq, c->fx, c->fy, c->fz, c->partials);
+    else
+        k_pair<Real, false, true><<<grid, kPairWarps * 32, 0, c->stream>>>(c->P, K, c->pos4, c->nbr, c->nnb, c->cap,
+                                                                           c->vec_pq, c->fx, c->fy, c->fz, c->partials);
+    ++c->launches;
+}
+
+}  // namespace
+
+unsigned pair_grid(const capac_ctx *c)
+{
+    const long need = (c->N + kPairWarps - 1) / kPairWarps;
+    const long cap = (long)c->num_sms * 16;
+    return (unsigned)std::max(1L, std::min(need, cap));
 }
 
 void launch_pair_forces(capac_ctx *c, int mode)
 {
-    const unsigned grid = grid_for((long)c->N * 32, 256);
+    const unsigned grid = pair_grid(c);
+    if (c->opt.precision == CAPAC_PREC_MIXED)
+        launch_pair_t<float>(c, mode, grid);
+    else
+        launch_pair_t<double>(c, mode, grid);
     if (mode == 0) {
-        {
-            ProfScope ps(c, K_PAIR);
-            if (c->M > 0 && c->use_cpff)
-                k_pair_f64<true, true><<<grid, 256, 0, c->stream>>>(c->P, c->pos4, c->nbr, c->nnb, c->cap,
-                                                                    c->vec_pq, c->fx, c->fy, c->fz, c->partials);
-            else
-                k_pair_f64<true, false><<<grid, 256, 0, c->stream>>>(c->P, c->pos4, c->nbr, c->nnb, c->cap,
-                                                                     c->vec_pq, c->fx, c->fy, c->fz, c->partials);
-        }
-        ++c->launches;
         static const int pot_slots[11] = {7, 8, -1, -1, -1, -1, -1, -1, -1, -1, -1};
         static const int vir_slots[11] = {-1, -1, 0, 1, 2, 3, 4, 5, 6, 7, 8};
         launch_finalize(c, (int)grid, 11, pot_slots, vir_slots);
-    } else {
-        ProfScope ps(c, K_PAIR);
-        k_pair_f64<false, true><<<grid, 256, 0, c->stream>>>(c->P, c->pos4, c->nbr, c->nnb, c->cap, c->vec_pq,
-                                                             c->fx, c->fy, c->fz, c->partials);
-        ++c->launches;
     }
 }
 

@@ -145,7 +145,13 @@ typedef struct capac_options {
     int list_every;         /* forced list rebuild interval in steps, 0 = displacement only */
     int max_neighbors;      /* 0 = estimate from density */
     double solver_tol;      /* rTr < solver_tol * bTb; 0 = reference 1e-8 (bicg_stab.c:303) */
-    double refine_tol;      /* mixed path: FP64 relative residual target (default 1e-10) */
+    double refine_tol;      /* mixed path: FP64 relative residual target (default 1e-11: within the
+                               1e-10 asked of the refinement, with room for ill-conditioned metal
+                               clusters, where 1e-10 leaves charge errors near 1e-8) */
+    int matrix_layout;      /* CPIM matrix: 0 symmetric packed 4x4 blocks (default), 1 full 4x4 blocks */
+    int predictor;          /* mixed path warm start: 0 last solution, 1 linear extrapolation (default) */
+    int solver_kernel;      /* BiCGSTAB on the symmetric layout: 0 one persistent cooperative launch per
+                               solve when the device supports it (default), 1 a launch per vector step */
 } capac_options;
 
 void capac_options_default(capac_options *o);
@@ -236,6 +242,7 @@ typedef struct capac_stats {
     long max_neighbors;
     int list_capacity;
     long md_step;
+    double solver_initial_rel_residual; /* sqrt(rTr/bTb) of the warm start */
 } capac_stats;
 int capac_get_stats(capac_ctx *ctx, capac_stats *out);
 
@@ -261,7 +268,10 @@ int capac_time_md_steps(capac_ctx *ctx, int n_steps, double *ms);
  * below is bracketed by CUDA events on the library's stream; capac_profile_get
  * returns the launch count and total milliseconds of one kernel class since
  * the last capac_profile_enable.  Classes: "pair", "spmv", "matrix",
- * "cpim_metal", "cpim_rhs", "qsc", "list_build", "solver_vec", "integrate". */
+ * "cpim_metal", "cpim_rhs", "qsc", "list_build", "solver_vec", "integrate",
+ * "resid" (mixed path FP64 residual), "solve" (persistent solver: one launch
+ * per BiCGSTAB solve) and "spmv_effective" (SpMV products that did work, with
+ * total_ms 0). */
 int capac_profile_enable(capac_ctx *ctx, int on);
 int capac_profile_get(capac_ctx *ctx, const char *cls, long *launches, double *total_ms);
 

@@ -346,43 +346,53 @@ static int cpim_solve(orc *o)
     const double bTb = dot(n, b, b);
     if (bTb < 1.0e-10) return 0;
     const double crit = bTb * o->solver_tol;
-    matvec(o, x, Ax);
-    for (int k = 0; k < n; ++k) {
-        r0[k] = b[k] - Ax[k];
-        r[k] = r0[k];
-        v[k] = p[k] = 0.0;
-        K[k] = k < 4 * M ? 1.0 / o->diag[k] : 1.0;
+    /* A breakdown (alpha or omega zero or non-finite) restarts from the last
+     * finite x; the reference has no such guard and would carry the NaN to
+     * MAX_ITER.  It does not occur at the reference's own tolerance on the
+     * golden inputs; tight-tolerance runs can reach it near the FP64 floor. */
+    for (int start = 0; start < 8; ++start) {
+        matvec(o, x, Ax);
+        for (int k = 0; k < n; ++k) {
+            r0[k] = b[k] - Ax[k];
+            r[k] = r0[k];
+            v[k] = p[k] = 0.0;
+            K[k] = k < 4 * M ? 1.0 / o->diag[k] : 1.0;
+        }
+        double rho_old = 1.0, omega = 1.0, alpha = 1.0, rTr = dot(n, r, r);
+        int iter = 0, broke = 0;
+        for (;;) {
+            const double rho = dot(n, r0, r);
+            if (rho < 1.0e-10 && iter == 0 && start == 0) return 0;
+            const double beta = (rho / rho_old) * (alpha / omega);
+            for (int k = 0; k < n; ++k) {
+                p[k] = r[k] + beta * (p[k] - omega * v[k]);
+                y[k] = p[k] * K[k];
+            }
+            matvec(o, y, v);
+            alpha = rho / dot(n, r0, v);
+            if (!isfinite(alpha)) { broke = 1; break; }
+            for (int k = 0; k < n; ++k) {
+                s[k] = r[k] - alpha * v[k];
+                z[k] = s[k] * K[k];
+            }
+            matvec(o, z, t);
+            for (int k = 0; k < n; ++k) Kt[k] = t[k] * K[k];
+            omega = dot(n, Kt, z) / dot(n, Kt, Kt);
+            if (!isfinite(omega) || omega == 0.0) { broke = 1; break; }
+            for (int k = 0; k < n; ++k) {
+                x[k] += alpha * y[k] + omega * z[k];
+                r[k] = s[k] - omega * t[k];
+            }
+            rho_old = rho;
+            ++iter;
+            ++o->iterations;
+            rTr = dot(n, r, r);
+            if (rTr < crit) return 0;
+            if (iter > MAX_ITER) return rTr < crit * 100.0 ? 0 : -1;
+        }
+        if (broke && rTr < crit * 100.0) return 0;
     }
-    double rho_old = 1.0, omega = 1.0, alpha = 1.0;
-    int iter = 0;
-    for (;;) {
-        const double rho = dot(n, r0, r);
-        if (rho < 1.0e-10 && iter == 0) return 0;
-        const double beta = (rho / rho_old) * (alpha / omega);
-        for (int k = 0; k < n; ++k) {
-            p[k] = r[k] + beta * (p[k] - omega * v[k]);
-            y[k] = p[k] * K[k];
-        }
-        matvec(o, y, v);
-        alpha = rho / dot(n, r0, v);
-        for (int k = 0; k < n; ++k) {
-            s[k] = r[k] - alpha * v[k];
-            z[k] = s[k] * K[k];
-        }
-        matvec(o, z, t);
-        for (int k = 0; k < n; ++k) Kt[k] = t[k] * K[k];
-        omega = dot(n, Kt, z) / dot(n, Kt, Kt);
-        for (int k = 0; k < n; ++k) {
-            x[k] += alpha * y[k] + omega * z[k];
-            r[k] = s[k] - omega * t[k];
-        }
-        rho_old = rho;
-        ++iter;
-        o->iterations = iter;
-        const double rTr = dot(n, r, r);
-        if (rTr < crit) return 0;
-        if (iter > MAX_ITER) return rTr < crit * 100.0 ? 0 : -1;
-    }
+    return -1;
 }
 
 /* mpi_cpff_force, cpff.c:526-950 (metal atoms assumed first, as in every

@@ -23,7 +23,9 @@ from conftest import GOLDEN_CASES, golden_paths, golden_ref, rel_err, slot_rel_e
 pytestmark = pytest.mark.gpu
 
 TIGHT = 1e-26
-TIGHT_MEDIUM = 1e-24  # the CPU oracle stagnates near rTr/bTb ~ 1e-24 on the 3.1k-atom system
+# On the 3.1k-atom system BiCGSTAB reaches its FP64 floor near a relative
+# residual of 7e-12 and breaks down (NaN) if asked for less than ~1e-12.
+TIGHT_MEDIUM = 1e-22
 
 
 @pytest.fixture(autouse=True)

@@ -1,0 +1,83 @@
+"""The persistent cooperative BiCGSTAB against the launch-per-step solver.
+
+Both run the same algorithm (bicg_stab.c:253-573) on the symmetric packed
+matrix; they differ only in the order of floating-point sums, so tight solves
+agree to rounding and reference-rule solves meet the same criterion.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+import capacmd_b200 as cm
+from conftest import golden_paths, rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(autouse=True)
+def _need_gpu(gpu_available):
+    if not gpu_available:
+        pytest.fail("no sm_100 GPU: GPU tests must run on a B200")
+
+
+def _solve_launches(sim):
+    n, ms = ctypes.c_long(), ctypes.c_double()
+    assert cm.lib().capac_profile_get(sim._p, b"solve", ctypes.byref(n), ctypes.byref(ms)) == 0
+    return n.value
+
+
+def _pair(case, prec, tol):
+    d = cm.Desc.from_paths(golden_paths(case))
+    coop = cm.Simulation(d, precision=prec, solver_tol=tol, solver_kernel=0)
+    step = cm.Simulation(d, precision=prec, solver_tol=tol, solver_kernel=1)
+    for s in (coop, step):
+        assert cm.lib().capac_profile_enable(s._p, 1) == 0
+        s.force()
+    return d, coop, step
+
+
+@pytest.mark.parametrize("case", ["t_au55w", "t_2np", "c1_field"])
+@pytest.mark.parametrize("prec", [cm.PREC_FP64, cm.PREC_MIXED])
+def test_persistent_solver_matches_stepwise_tight(case, prec):
+    d, coop, step = _pair(case, prec, 1e-26 if prec == cm.PREC_FP64 else 0.0)
+    assert _solve_launches(coop) > 0, "persistent solver did not run"
+    assert _solve_launches(step) == 0
+    # FP64: both solve to rTr < 1e-26 bTb; mixed: both refine to a relative
+    # residual of 1e-10, which leaves the charges within the 1e-8 bar
+    bar = 1e-10 if prec == cm.PREC_FP64 else 1e-8
+    assert rel_err(coop.get("vec_pq"), step.get("vec_pq")) < bar
+    assert rel_err(coop.forces(), step.forces()) < bar
+
+
+@pytest.mark.parametrize("case", ["t_au55w", "t_2np", "c1_field"])
+def test_persistent_solver_meets_reference_rule(case):
+    d, coop, step = _pair(case, cm.PREC_FP64, 0.0)
+    st_c, st_s = coop.stats(), step.stats()
+    # rTr < 1e-8 bTb (bicg_stab.c:303, 523)
+    assert st_c.solver_rel_residual < 1e-4
+    assert st_s.solver_rel_residual < 1e-4
+    # same algorithm: the iteration counts differ by rounding only
+    assert abs(st_c.solver_iterations - st_s.solver_iterations) <= max(3, st_s.solver_iterations // 5)
+    # the answer is the reference's up to the 1e-4 stopping rule
+    assert rel_err(coop.get("vec_pq"), step.get("vec_pq")) < 1e-2
+
+
+def test_persistent_solver_zero_field_exit():
+    # Au147 in vacuum without a field: bTb = 0, the reference's early exit
+    d, coop, step = _pair("c1", cm.PREC_FP64, 0.0)
+    assert np.all(coop.get("vec_pq") == 0.0)
+    assert np.all(step.get("vec_pq") == 0.0)
+    assert coop.stats().solver_iterations == 0
+
+
+def test_persistent_solver_md_steps():
+    # several solves in a row, warm-started, through the integrator
+    d = cm.Desc.from_paths(golden_paths("c1_field"))
+    coop = cm.Simulation(d, solver_tol=1e-26, solver_kernel=0)
+    step = cm.Simulation(d, solver_tol=1e-26, solver_kernel=1)
+    for s in (coop, step):
+        s.md_init()
+        s.md_steps(5)
+    assert rel_err(coop.positions(), step.positions()) < 1e-11
+    assert rel_err(coop.get("vec_pq"), step.get("vec_pq")) < 1e-9
