@@ -220,7 +220,7 @@ void capac_options_default(capac_options *o)
     o->solver_tol = 0.0;
     o->refine_tol = 1.0e-11;
     o->matrix_layout = 0;
-    o->predictor = 1;
+    o->predictor = 2;
     o->solver_kernel = 0;
 }
 
@@ -421,7 +421,7 @@ int capac_create(const capac_desc *d, const capac_options *opt, capac_ctx **out)
                         c->sympart = dalloc<double>(sym_partial_doubles(M));
                         if (o.solver_kernel == 0) c->coop_grid = coop_grid_size(c->device, mixed);
                         if (c->coop_grid > 0) {
-                            c->coop_bp = dalloc<double>((size_t)6 * c->coop_grid);
+                            c->coop_bp = dalloc<double>(coop_partial_doubles(c->coop_grid));
                             c->coop_bar = dalloc<unsigned char>(coop_barrier_bytes());
                         }
                     } else if (mixed) {
@@ -432,7 +432,7 @@ int capac_create(const capac_desc *d, const capac_options *opt, capac_ctx **out)
                     if (mixed) {
                         c->rres = dalloc<double>(n);
                         c->dcorr = dalloc<double>(n);
-                        c->xprev = dalloc<double>(n);
+                        c->xprev = dalloc<double>((size_t)3 * n);
                     }
                     c->bw = dalloc<double>((size_t)n * 11);
                     CAPAC_CUDA(cudaMemsetAsync(c->bw, 0, sizeof(double) * n * 11, s));

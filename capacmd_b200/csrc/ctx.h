@@ -147,13 +147,13 @@ struct capac_ctx {
     void *msym = nullptr;        // symmetric packed tiles (float on the mixed path, else double)
     double *sympart = nullptr;   // per-tile partial sums of the symmetric SpMV
     int coop_grid = 0;           // blocks of the persistent solver (0: per-step launches)
-    double *coop_bp = nullptr;   // its per-block dot partials, 6 * coop_grid
+    double *coop_bp = nullptr;   // its per-block dot partials
     void *coop_bar = nullptr;    // its grid barrier
     double *bw = nullptr;        // BiCGSTAB work vectors, 11 * n_mat
     float *bwf = nullptr;        // (unused)
     double *rres = nullptr, *dcorr = nullptr;  // mixed path: FP64 residual and correction, n_mat each
-    double *xprev = nullptr;     // mixed path: previous step's solution (warm-start extrapolation)
-    int n_solves = 0;            // completed solves (the extrapolation needs two)
+    double *xprev = nullptr;     // mixed path: the three solutions before the last (warm-start extrapolation)
+    int n_solves = 0;            // completed solves since the history was reset
     capac::SolverScalars *ss = nullptr;
     capac::SolverScalars *h_ss = nullptr;  // pinned
     long nnz = 0;
@@ -203,6 +203,7 @@ constexpr int W_Y_SLOT = 7, W_V_SLOT = 4;  // BiCGSTAB work-vector slots used as
 // persistent cooperative solver (k_solve_coop.cu)
 int coop_grid_size(int device, bool mixed);
 size_t coop_barrier_bytes();
+size_t coop_partial_doubles(int grid);
 int bicgstab_coop(capac_ctx *c, const double *b, double *x, double tol, double skip);
 void launch_cpim_metal_forces(capac_ctx *c);
 void launch_external_field(capac_ctx *c);

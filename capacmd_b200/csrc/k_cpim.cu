@@ -604,15 +604,21 @@ __global__ void __launch_bounds__(256) k_axpy1(int n, const double *__restrict__
     if (k < n) x[k] += d[k];
 }
 
-// Warm-start predictor: x <- 2 x - x_prev, x_prev <- old x (linear
-// extrapolation of the last two solutions); `first` only records x.
-__global__ void __launch_bounds__(256) k_predict(int n, int first, double *__restrict__ x, double *__restrict__ xprev)
+// Warm-start predictor: polynomial extrapolation of the last solutions.
+// x is the last solution x_n, hist holds x_{n-1}, x_{n-2}, x_{n-3} (n each);
+// order 1: 2 x_n - x_{n-1}; 2: 3 x_n - 3 x_{n-1} + x_{n-2};
+// 3: 4 x_n - 6 x_{n-1} + 4 x_{n-2} - x_{n-3}; 0 or less only records x_n.
+__global__ void __launch_bounds__(256) k_predict(int n, int order, double *__restrict__ x, double *__restrict__ hist)
 {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
-    const double t = x[k];
-    if (!first) x[k] = 2.0 * t - xprev[k];
-    xprev[k] = t;
+    const double t = x[k], h1 = hist[k], h2 = hist[n + k], h3 = hist[2 * (size_t)n + k];
+    if (order == 1) x[k] = 2.0 * t - h1;
+    else if (order == 2) x[k] = 3.0 * (t - h1) + h2;
+    else if (order == 3) x[k] = 4.0 * (t + h2) - 6.0 * h1 - h3;
+    hist[2 * (size_t)n + k] = h2;
+    hist[n + k] = h1;
+    hist[k] = t;
 }
 
 // Jacobi-preconditioned BiCGSTAB (bicg_stab.c:253-573) on A x = b with the
@@ -729,15 +735,16 @@ int run_bicgstab(capac_ctx *c)
 // r = b - A x in FP64 (matrix-free: every block rebuilt from the positions in
 // FP64, so no FP64 matrix is stored), solves A d = r with BiCGSTAB on the FP32
 // matrix (FP64 vectors, inner products and accumulation) to a relative
-// residual of 1e-5, and updates x += d, until |r| <= refine_tol |b|.  The
-// reference's zero-field early exit (bTb < 1e-10) is kept.
+// residual of 1e-5 (on the last sweep only as far as the target needs), and
+// updates x += d, until |r| <= refine_tol |b|.  The reference's zero-field
+// early exit (bTb < 1e-10) is kept.
+constexpr double kInnerReduction = 1.0e-5;
 int run_refined_solve(capac_ctx *c)
 {
     const int n = c->n_mat;
     const int nbv = (int)grid_for(n, 256);
     cudaStream_t s = c->stream;
     const double rtol = c->opt.refine_tol > 0.0 ? c->opt.refine_tol : 1.0e-11;
-    const double inner_tol = 1.0e-10;  // (1e-5)^2
     const int max_sweeps = 12;
 
     k_vec_dot<<<nbv, 256, 0, s>>>(n, c->vec_ext, c->vec_ext, c->partials);
@@ -750,8 +757,10 @@ int run_refined_solve(capac_ctx *c)
     c->last_rel_res = 0.0;
     if (c->h_ss->done) return CAPAC_OK;  // zero right-hand side: keep x
     const double bTb = c->h_ss->bTb;
-    if (c->opt.predictor == 1 && c->xprev) {
-        k_predict<<<nbv, 256, 0, s>>>(n, c->n_solves == 0 ? 1 : 0, c->vec_pq, c->xprev);
+    if (c->opt.predictor > 0 && c->xprev) {
+        // the warm start of the first solve is not a solution: history
+        // entries count from the second solve on
+        k_predict<<<nbv, 256, 0, s>>>(n, std::min(c->opt.predictor, c->n_solves - 1), c->vec_pq, c->xprev);
         ++c->launches;
     }
     ++c->n_solves;
@@ -768,7 +777,11 @@ int run_refined_solve(capac_ctx *c)
         if (sweep == 0) c->last_init_res = sqrt(rr / bTb);
         if (rr <= rtol * rtol * bTb || sweep == max_sweeps) break;
         CAPAC_CUDA(cudaMemsetAsync(c->dcorr, 0, sizeof(double) * n, s));
-        const int st = bicgstab_core(c, c->rres, c->dcorr, inner_tol, 1.0e-300);
+        // reduce the residual by 1e-5, or, on the last sweep, by what is
+        // left to the target with a margin of 3
+        const double need = 0.3 * rtol * sqrt(bTb / rr);
+        const double tau = std::min(std::max(need, kInnerReduction), 0.1);
+        const int st = bicgstab_core(c, c->rres, c->dcorr, tau * tau, 1.0e-300);
         total += c->h_ss->iter;
         if (st < 0 && c->h_ss->iter == 0) break;  // no progress possible
         k_axpy1<<<nbv, 256, 0, s>>>(n, c->dcorr, c->vec_pq);

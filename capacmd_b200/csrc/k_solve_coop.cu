@@ -1,25 +1,39 @@
 // BiCGSTAB for the CPIM system in one persistent, cooperatively launched
-// kernel (symmetric packed 4x4-block matrix, FP32 or FP64 entries).
+// kernel on the symmetric packed 4x4-block matrix (FP32 or FP64 entries).
 //
 // Same algorithm and stopping rules as bicgstab_core (bicg_stab.c:253-573,
-// plus the breakdown guard); the host launches one kernel per solve instead of
-// about ten small kernels per iteration.  Phases of one iteration, each ended
-// by a grid barrier:
-//   P  p = r + beta (p - omega v), y = K p
-//   T  tile SpMV of y -> partials          R  v = A y, partials of (r0, v)
-//   S  alpha; s = r - alpha v, z = K s
-//   T  tile SpMV of z -> partials          R  t = A z, Kt, partials of (Kt, z), (Kt, Kt)
-//   X  omega; x += alpha y + omega z, r = s - omega t, partials of (r, r), (r0, r)
-// Every block reduces the per-block dot partials itself, in one fixed order,
-// so all blocks compute bit-identical scalars and take the same branch at
-// every test.
+// with the breakdown guard); the host launches one kernel per solve instead
+// of about ten small kernels per iteration.  One block per SM.  Each block
+// owns the tiles t = blockIdx.x + k * gridDim.x and streams them from HBM
+// into a two-stage shared-memory ring with bulk asynchronous copies
+// (cp.async.bulk + mbarrier); the matrix does not change during a solve, so
+// the ring runs on across phases and iterations.
 //
-// The grid barrier is a counter/generation pair in global memory with a
-// bounded wait: a block that polls more than 2^24 times sets the error word
-// and leaves; every block checks that word after each barrier and returns,
-// and the host reports the error.  The launch is cooperative, so either all
-// blocks are resident or the launch fails.
-#include <cooperative_groups.h>
+// An iteration, with a grid barrier after each of its four phases:
+//   P  tile pass of y = K p, p = r + beta (p - omega v), r = s - omega t,
+//      all formed on the fly; the owner of diagonal tile (I, I) stores r, p
+//      and y of block row I and applies the previous iteration's
+//      x += alpha y + omega z to it
+//   V  v = A y from the tile partials (fixed order), partials of (r0, v)
+//   S  alpha; tile pass of z = K s, s = r - alpha v formed on the fly;
+//      the diagonal-tile owner stores s and z
+//   T  t = A z, Kt, partials of (Kt, z), (Kt, Kt), (r0, s), (r0, t), (s, s),
+//      (s, t), (t, t): omega, rho = (r0, s - omega t) and (r, r) follow
+//      without a pass of their own
+// p and v are double-buffered, since blocks form y from the old p and v
+// while others store the new ones.  Every block sums the per-block dot
+// partials itself in one fixed order, so all blocks compute bit-identical
+// scalars and take the same branch at every test.  (r, r) from the merged
+// dots differs from the directly summed one by rounding only; the value
+// returned is summed directly from the final residual.
+//
+// Every wait is bounded.  The grid barrier (counter and generation word)
+// gives up after 2^24 polls, a ring-stage wait after 2^20 polls of at most
+// 1 us each; either sets the error word, the block then waits (bounded) for
+// its own copies in flight and returns, the other blocks give up at their
+// next barrier, and the host reports the error.  The launch is cooperative,
+// so either all blocks are resident or the launch fails.
+#include <cstdint>
 
 #include "terms.cuh"
 
@@ -29,36 +43,107 @@ namespace {
 
 constexpr int kT = 32;
 constexpr int kPlanes = 10;
-constexpr size_t kTileElems = (size_t)kPlanes * kT * kT;
+constexpr int kTileElems = kPlanes * kT * kT;
 constexpr int kBlock = 256;
+constexpr int kRingBytes = 160 * 1024;  // 4 FP32 tiles or 2 FP64 tiles
+constexpr int kChunkTiles = 16;         // tiles whose inputs a pass gathers at once
+constexpr int kGroups = 4;              // partial-sum groups per output row in the reduce phases
+constexpr int kBatch = 16;              // partials one thread loads at once in the reduce phases
 constexpr long kSpinLimit = 1L << 24;
+constexpr long kWaitPolls = 1L << 20;
+constexpr unsigned kSuspendNs = 1000;
+
+enum { MODE_X = 0, MODE_P = 1, MODE_S = 2 };
 
 __host__ __device__ __forceinline__ size_t tile_index(int I, int J, int nT)
 {
     return (size_t)I * nT - (size_t)I * (I - 1) / 2 + (size_t)(J - I);
 }
-__device__ __forceinline__ size_t elem_offset(int p, int a, int b)
+__device__ __forceinline__ int elem_offset(int p, int a, int b)
 {
-    return ((size_t)p * (kT / 4) + (b >> 2)) * (kT * 4) + (size_t)a * 4 + (b & 3);
+    return ((p * (kT / 4) + (b >> 2)) * (kT * 4)) + a * 4 + (b & 3);
 }
-__device__ __forceinline__ void load4(const float *p, double out[4])
+__device__ __forceinline__ void lds4(const float *p, float out[4])
 {
     const float4 v = *reinterpret_cast<const float4 *>(p);
     out[0] = v.x; out[1] = v.y; out[2] = v.z; out[3] = v.w;
 }
-__device__ __forceinline__ void load4(const double *p, double out[4])
+__device__ __forceinline__ void lds4(const double *p, double out[4])
 {
     const double2 u = *reinterpret_cast<const double2 *>(p);
     const double2 v = *reinterpret_cast<const double2 *>(p + 2);
     out[0] = u.x; out[1] = u.y; out[2] = v.x; out[3] = v.y;
 }
 
+// Sums of 16 values over the 32 lanes of a warp by recursive halving: at
+// each step a lane keeps half of its values and adds the partner's copy of
+// that half (8 + 4 + 2 + 1 exchanges), then one last exchange; 16 shuffles
+// instead of 80.  Lanes 2v and 2v + 1 return the sum of value v (v = 4 k + c
+// of cb[k][c]).  The order of additions is fixed.
+__device__ __forceinline__ double warp_sum16(double (&cb)[4][4], int lane)
+{
+    double v[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = cb[i >> 2][i & 3];
+#pragma unroll
+    for (int half = 8, m = 16; half >= 1; half >>= 1, m >>= 1) {
+        const bool upper = (lane & m) != 0;
+#pragma unroll
+        for (int i = 0; i < half; ++i) {
+            const double send = upper ? v[i] : v[i + half];
+            const double keep = upper ? v[i + half] : v[i];
+            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, m);
+        }
+    }
+    return v[0] + __shfl_xor_sync(0xffffffffu, v[0], 1);
+}
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init()
+{
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+// One bulk copy global -> shared completing on `bar` (no multicast).
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, unsigned bytes, uint64_t *bar)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity)
+{
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity), "r"(kSuspendNs)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity)
+{
+    for (long i = 0; i < kWaitPolls; ++i)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
 }  // namespace
 
-struct CoopBarrier {
+struct CoopSync {
     unsigned count;
     unsigned gen;
-    int error;
+    int error;  // 1 grid barrier timed out, 2 ring-stage wait timed out
     int pad;
 };
 
@@ -68,19 +153,19 @@ struct CoopArgs {
     const int *np_start, *np_end;
     const void *mat;
     double *part;  // nT * nT * 128 tile partials
-    double *bp;    // dot partials: 3 sets of 2 doubles per block
+    double *bp;    // dot partials: 2 sets of 2 doubles per block
     const double *b, *diag;
-    double *x;
-    double *r0, *r, *p, *v, *s, *t, *y, *z, *K;
+    double *x, *r0, *r, *s, *t, *y, *z, *K;
+    double *p[2], *v[2];
     double tol, skip;
     SolverScalars *ss;
-    CoopBarrier *bar;
+    CoopSync *sync;
 };
 
 namespace {
 
-// Bounded grid barrier; false if any block gave up waiting.
-__device__ bool grid_barrier(CoopBarrier *bar)
+// Bounded grid barrier; false if any block gave up.
+__device__ bool grid_barrier(CoopSync *bar)
 {
     __shared__ int ok;
     __syncthreads();
@@ -97,7 +182,7 @@ __device__ bool grid_barrier(CoopBarrier *bar)
             long spins = 0;
             while (*gen == g) {
                 if (++spins > kSpinLimit) {
-                    atomicExch(&bar->error, 1);
+                    atomicCAS(&bar->error, 0, 1);
                     break;
                 }
                 __nanosleep(32);
@@ -110,135 +195,303 @@ __device__ bool grid_barrier(CoopBarrier *bar)
     return ok != 0;
 }
 
-// Sum the per-block dot partials in a fixed order; every block gets the same.
-__device__ void sum_bp(const double *bp, int nb, double &a, double &b)
+// Dot partials: kBp doubles per block.  sum_bp sums them over the blocks
+// in one fixed order, so every block gets the same K sums.
+constexpr int kBp = 8;
+template <int K>
+__device__ void sum_bp(const double *bp, int nb, double (&out)[K])
 {
-    __shared__ double sh[64];
-    __shared__ double out[2];
-    double v[2] = {0.0, 0.0};
-    for (int k = threadIdx.x; k < nb; k += blockDim.x) {
-        v[0] += __ldcg(bp + 2 * k);
-        v[1] += __ldcg(bp + 2 * k + 1);
-    }
-    block_sum<2>(v, sh);
-    if (threadIdx.x == 0) {
-        out[0] = v[0];
-        out[1] = v[1];
-    }
+    __shared__ double sh[8 * kBp];
+    __shared__ double res[kBp];
+    double v[K];
+#pragma unroll
+    for (int q = 0; q < K; ++q) v[q] = 0.0;
+    for (int k = threadIdx.x; k < nb; k += blockDim.x)
+#pragma unroll
+        for (int q = 0; q < K; ++q) v[q] += __ldcg(bp + (size_t)kBp * k + q);
+    block_sum<K>(v, sh);
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int q = 0; q < K; ++q) res[q] = v[q];
     __syncthreads();
-    a = out[0];
-    b = out[1];
+#pragma unroll
+    for (int q = 0; q < K; ++q) out[q] = res[q];
     __syncthreads();
 }
 
-__device__ void put_bp(double *bp, double a, double b)
+template <int K>
+__device__ void put_bp(double *bp, double (&v)[K])
 {
-    __shared__ double sh[64];
-    double v[2] = {a, b};
-    block_sum<2>(v, sh);
-    if (threadIdx.x == 0) {
-        bp[2 * blockIdx.x] = v[0];
-        bp[2 * blockIdx.x + 1] = v[1];
-    }
+    __shared__ double sh[8 * kBp];
+    block_sum<K>(v, sh);
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int q = 0; q < K; ++q) bp[(size_t)kBp * blockIdx.x + q] = v[q];
 }
 
-// Tile SpMV of `in` into the tile partials (as k_sym_tiles).
+// Scalars of the current tile pass.
+struct PassScalars {
+    double beta, omega, alpha;  // MODE_P: beta, and omega, alpha of the previous iteration; MODE_S: alpha
+    int cur;    // p[cur], v[cur] are the old p and v (MODE_P); v[cur] is the new v (MODE_S)
+    int first;  // MODE_P of the first iteration: r is stored, no update of x is pending
+};
+
+// MODE_P, one CPIM row: the residual r = s - omega t of the previous
+// iteration (stored r on the first), the new p, and on `store` the row's
+// deferred updates: r, and x += alpha y + omega z of the previous iteration
+// (y is read before it is overwritten).  Returns the new p.
+__device__ __forceinline__ double p_row(const CoopArgs &A, const PassScalars &S, int row, bool store)
+{
+    const double r = S.first ? __ldcg(A.r + row) : fma(-S.omega, __ldcg(A.t + row), __ldcg(A.s + row));
+    const double pn = fma(S.beta, fma(-S.omega, __ldcg(A.v[S.cur] + row), __ldcg(A.p[S.cur] + row)), r);
+    if (store) {
+        if (!S.first) {
+            A.r[row] = r;
+            A.x[row] += S.alpha * __ldcg(A.y + row) + S.omega * __ldcg(A.z + row);
+        }
+        A.p[S.cur ^ 1][row] = pn;
+    }
+    return pn;
+}
+
+// The ring of tiles of one block: Stages = kRingBytes / tile bytes slots;
+// sequence number q -> slot q % Stages, whose k-th use waits for parity
+// k & 1; tile of q = blockIdx.x + (q mod n_my) * gridDim.x.  Every thread
+// counts `consumed`; thread 0 alone issues the copies and counts `issued`
+// (always consumed + Stages).
 template <typename T>
-__device__ void tiles_phase(const CoopArgs &A, const double *in)
+struct Ring {
+    static constexpr int Stages = kRingBytes / (int)(kTileElems * sizeof(T));
+    T *buf;
+    uint64_t *bar;  // Stages mbarriers
+    long issued, consumed;
+    int n_my;
+    __device__ int tile_of(long q) const { return blockIdx.x + (int)(q % n_my) * gridDim.x; }
+    __device__ T *stage(int st) const { return buf + (size_t)st * kTileElems; }
+    __device__ void issue(const T *mat)  // thread 0
+    {
+        const long q = issued++;
+        const int st = (int)(q % Stages);
+        bulk_load(stage(st), mat + (size_t)tile_of(q) * kTileElems, kTileElems * sizeof(T), bar + st);
+    }
+    // thread 0: bounded wait for every copy still in flight
+    __device__ void drain()
+    {
+        for (long q = consumed; q < issued; ++q) mbar_wait(bar + (q % Stages), (unsigned)((q / Stages) & 1));
+        consumed = issued;
+    }
+};
+
+// Shared arrays of a tile pass (one copy for all pass kinds).  The pass
+// inputs are held in the matrix's type: the products run in FP32 on the
+// FP32 matrix, and every sum across columns or tiles is in FP64.
+template <typename T>
+struct PassSmem {
+    T in[kChunkTiles][2][kT][4];  // pass inputs of the chunk's tiles: block rows I and J
+    double rowacc[8][kT][4];
+    double colacc[kT][4];
+    int tile_i[kChunkTiles], tile_j[kChunkTiles];
+    int wait_ok;
+};
+
+// Tile pass: partial products of the block's tiles with the pass input.
+// The inputs of up to kChunkTiles tiles are gathered in one batch of
+// independent loads before the tiles are processed.  Returns false when a
+// ring wait timed out.
+template <typename T, int MODE>
+__device__ bool tiles_pass(const CoopArgs &A, const PassScalars &S, Ring<T> &ring, PassSmem<T> &sm)
 {
-    __shared__ double xr[kT][4], xc[kT][4];
-    __shared__ double rowacc[8][kT][4];
-    __shared__ double colacc[kT][4];
-    const T *mat = static_cast<const T *>(A.mat);
+    constexpr int Stages = Ring<T>::Stages;
     const int M = A.M;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    for (int t = blockIdx.x; t < A.ntiles; t += gridDim.x) {
-        int I = 0;
-        while (tile_index(I + 1, I + 1, A.nT) <= (size_t)t && I + 1 < A.nT) ++I;
-        const int J = I + (int)((size_t)t - tile_index(I, I, A.nT));
-        {
-            const int side = threadIdx.x >> 7, q = threadIdx.x & 127, at = q >> 2, comp = q & 3;
+    const int side = threadIdx.x >> 7, q4 = threadIdx.x & 127, at = q4 >> 2, comp = q4 & 3;
+
+    // the Lagrange rows of the stored vectors (K = 1 there)
+    if (MODE != MODE_X && threadIdx.x == 0) {
+        for (int k = blockIdx.x; k < A.n_nps; k += gridDim.x) {
+            const int row = A.n4 + k;
+            if (MODE == MODE_P) {
+                A.y[row] = p_row(A, S, row, true);
+            } else {
+                const double sn = fma(-S.alpha, __ldcg(A.v[S.cur] + row), __ldcg(A.r + row));
+                A.s[row] = sn;
+                A.z[row] = sn;
+            }
+        }
+    }
+
+    for (int c0 = 0; c0 < ring.n_my; c0 += kChunkTiles) {
+        const int nc = min(kChunkTiles, ring.n_my - c0);
+        if (threadIdx.x < nc) {
+            const int t = blockIdx.x + (c0 + threadIdx.x) * gridDim.x;
+            int I = 0;
+            while (tile_index(I + 1, I + 1, A.nT) <= (size_t)t && I + 1 < A.nT) ++I;
+            sm.tile_i[threadIdx.x] = I;
+            sm.tile_j[threadIdx.x] = I + (int)((size_t)t - tile_index(I, I, A.nT));
+        }
+        __syncthreads();
+        // gather: thread (side, atom, comp) of every tile of the chunk
+#pragma unroll 4
+        for (int kk = 0; kk < nc; ++kk) {
+            const int I = sm.tile_i[kk], J = sm.tile_j[kk];
             const int atom = (side ? J : I) * kT + at;
             double val = 0.0;
-            if (atom < M) val = __ldcg(in + (comp < 3 ? 3 * atom + comp : 3 * M + atom));
-            if (side == 0) xr[at][comp] = val;
-            else xc[at][comp] = val;
+            if (atom < M) {
+                const int row = comp < 3 ? 3 * atom + comp : 3 * M + atom;
+                if (MODE == MODE_X) {
+                    val = __ldcg(A.x + row);
+                } else if (MODE == MODE_P) {
+                    const bool owner = I == J && side == 0;  // the diagonal-tile owner stores block row I
+                    val = __dmul_rn(__ldcg(A.K + row), p_row(A, S, row, owner));
+                    if (owner) A.y[row] = val;
+                } else {
+                    const double sn = fma(-S.alpha, __ldcg(A.v[S.cur] + row), __ldcg(A.r + row));
+                    val = __dmul_rn(__ldcg(A.K + row), sn);
+                    if (I == J && side == 0) {
+                        A.s[row] = sn;
+                        A.z[row] = val;
+                    }
+                }
+            }
+            sm.in[kk][side][at][comp] = (T)val;
         }
         __syncthreads();
-        const T *tile = mat + (size_t)t * kTileElems;
-        const int a = lane;
-        double vv[kPlanes][4];
+
+        for (int kk = 0; kk < nc; ++kk) {
+            const int I = sm.tile_i[kk], J = sm.tile_j[kk];
+            const long q = ring.consumed;
+            const int st = (int)(q % Stages);
+            const unsigned parity = (unsigned)((q / Stages) & 1);
+            if (threadIdx.x == 0) sm.wait_ok = mbar_wait(ring.bar + st, parity) ? 1 : 0;
+            __syncthreads();
+            if (!sm.wait_ok) return false;
+            // every thread observes the completed phase before reading the stage
+            // (it has completed: this returns at the first poll)
+            mbar_wait(ring.bar + st, parity);
+            const T *tile = ring.stage(st);
+            const T(*xr)[4] = sm.in[kk][0];
+            const T(*xc)[4] = sm.in[kk][1];
+            const int a = lane;
+            T ra[4] = {0, 0, 0, 0};
+            T cb[4][4];
+            const T xa0 = xr[a][0], xa1 = xr[a][1], xa2 = xr[a][2], xa3 = xr[a][3];
+            {
+                T vv[kPlanes][4];
 #pragma unroll
-        for (int pl = 0; pl < kPlanes; ++pl) load4(tile + elem_offset(pl, a, 4 * w), vv[pl]);
-        double ra[4] = {0.0, 0.0, 0.0, 0.0};
-        double cb[4][4];
+                for (int pl = 0; pl < kPlanes; ++pl) lds4(tile + elem_offset(pl, a, 4 * w), vv[pl]);
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const int b = 4 * w + k;
-            const double Axx = vv[0][k], Axy = vv[1][k], Axz = vv[2][k], Ayy = vv[3][k], Ayz = vv[4][k],
-                         Azz = vv[5][k], m0 = vv[6][k], m1 = vv[7][k], m2 = vv[8][k], C = vv[9][k];
-            const double xb0 = xc[b][0], xb1 = xc[b][1], xb2 = xc[b][2], xb3 = xc[b][3];
-            const double xa0 = xr[a][0], xa1 = xr[a][1], xa2 = xr[a][2], xa3 = xr[a][3];
-            ra[0] += Axx * xb0 + Axy * xb1 + Axz * xb2 + m0 * xb3;
-            ra[1] += Axy * xb0 + Ayy * xb1 + Ayz * xb2 + m1 * xb3;
-            ra[2] += Axz * xb0 + Ayz * xb1 + Azz * xb2 + m2 * xb3;
-            ra[3] += -(m0 * xb0 + m1 * xb1 + m2 * xb2) + C * xb3;
-            cb[k][0] = Axx * xa0 + Axy * xa1 + Axz * xa2 - m0 * xa3;
-            cb[k][1] = Axy * xa0 + Ayy * xa1 + Ayz * xa2 - m1 * xa3;
-            cb[k][2] = Axz * xa0 + Ayz * xa1 + Azz * xa2 - m2 * xa3;
-            cb[k][3] = m0 * xa0 + m1 * xa1 + m2 * xa2 + C * xa3;
+                for (int k4 = 0; k4 < 4; ++k4) {
+                    const int b = 4 * w + k4;
+                    const T Axx = vv[0][k4], Axy = vv[1][k4], Axz = vv[2][k4], Ayy = vv[3][k4], Ayz = vv[4][k4],
+                            Azz = vv[5][k4], m0 = vv[6][k4], m1 = vv[7][k4], m2 = vv[8][k4], C = vv[9][k4];
+                    const T xb0 = xc[b][0], xb1 = xc[b][1], xb2 = xc[b][2], xb3 = xc[b][3];
+                    ra[0] += Axx * xb0 + Axy * xb1 + Axz * xb2 + m0 * xb3;
+                    ra[1] += Axy * xb0 + Ayy * xb1 + Ayz * xb2 + m1 * xb3;
+                    ra[2] += Axz * xb0 + Ayz * xb1 + Azz * xb2 + m2 * xb3;
+                    ra[3] += -(m0 * xb0 + m1 * xb1 + m2 * xb2) + C * xb3;
+                    cb[k4][0] = Axx * xa0 + Axy * xa1 + Axz * xa2 - m0 * xa3;
+                    cb[k4][1] = Axy * xa0 + Ayy * xa1 + Ayz * xa2 - m1 * xa3;
+                    cb[k4][2] = Axz * xa0 + Ayz * xa1 + Azz * xa2 - m2 * xa3;
+                    cb[k4][3] = m0 * xa0 + m1 * xa1 + m2 * xa2 + C * xa3;
+                }
+            }
+            // column sums over the warp's 32 rows: lane 2v and 2v + 1 end
+            // with value v = 4 k + c
+            double cbd[4][4];
+#pragma unroll
+            for (int k4 = 0; k4 < 4; ++k4)
+#pragma unroll
+                for (int c = 0; c < 4; ++c) cbd[k4][c] = (double)cb[k4][c];
+            const double colsum = warp_sum16(cbd, lane);
+#pragma unroll
+            for (int c = 0; c < 4; ++c) sm.rowacc[w][a][c] = (double)ra[c];
+            if ((lane & 1) == 0) {
+                const int v = lane >> 1;
+                sm.colacc[4 * w + (v >> 2)][v & 3] = colsum;
+            }
+            __syncthreads();  // the stage is free again
+            ++ring.consumed;  // every thread keeps the same count
+            if (threadIdx.x == 0) ring.issue(static_cast<const T *>(A.mat));  // the tile this slot holds next
+            double *pr = A.part + ((size_t)I * A.nT + J) * (kT * 4);
+            double *pc = A.part + ((size_t)J * A.nT + I) * (kT * 4);
+            if (threadIdx.x < kT * 4) {
+                const int aa = threadIdx.x >> 2, c = threadIdx.x & 3;
+                double s = 0.0;
+#pragma unroll
+                for (int ww = 0; ww < 8; ++ww) s += sm.rowacc[ww][aa][c];
+                pr[threadIdx.x] = I == J ? s + sm.colacc[aa][c] : s;
+            } else if (I != J) {
+                const int c = threadIdx.x - kT * 4;
+                pc[c] = sm.colacc[c >> 2][c & 3];
+            }
         }
-#pragma unroll
-        for (int k = 0; k < 4; ++k)
-#pragma unroll
-            for (int q = 0; q < 4; ++q) cb[k][q] = warp_sum(cb[k][q]);
-#pragma unroll
-        for (int q = 0; q < 4; ++q) rowacc[w][a][q] = ra[q];
-        if (lane == 0) {
-#pragma unroll
-            for (int k = 0; k < 4; ++k)
-#pragma unroll
-                for (int q = 0; q < 4; ++q) colacc[4 * w + k][q] = cb[k][q];
-        }
-        __syncthreads();
-        double *pr = A.part + ((size_t)I * A.nT + J) * (kT * 4);
-        double *pc = A.part + ((size_t)J * A.nT + I) * (kT * 4);
-        if (threadIdx.x < kT * 4) {
-            const int aa = threadIdx.x >> 2, q = threadIdx.x & 3;
-            double s = 0.0;
-#pragma unroll
-            for (int ww = 0; ww < 8; ++ww) s += rowacc[ww][aa][q];
-            pr[threadIdx.x] = I == J ? s + colacc[aa][q] : s;
-        } else if (I != J) {
-            const int q = threadIdx.x - kT * 4;
-            pc[q] = colacc[q >> 2][q & 3];
-        }
-        __syncthreads();
+        __syncthreads();  // rowacc, colacc and the chunk inputs are free again
+    }
+    return true;
+}
+
+enum { RED_START = 0, RED_V = 1, RED_T = 2 };
+
+// The dot contributions of one output row (see reduce_pass).
+template <int RED>
+__device__ __forceinline__ void reduce_row(const CoopArgs &A, const PassScalars &S, int row, double out, double in,
+                                           double Krow, double (&d)[7])
+{
+    if (RED == RED_START) {
+        const double rk = A.b[row] - out;
+        A.r0[row] = rk;
+        A.r[row] = rk;
+        d[0] += rk * rk;
+    } else if (RED == RED_V) {
+        A.v[S.cur ^ 1][row] = out;
+        d[0] += __ldcg(A.r0 + row) * out;
+    } else {
+        A.t[row] = out;
+        const double kt = Krow * out, sr = __ldcg(A.s + row), r0 = __ldcg(A.r0 + row);
+        d[0] += kt * in;  // (K t, z)
+        d[1] += kt * kt;
+        d[2] += r0 * sr;
+        d[3] += r0 * out;
+        d[4] += sr * sr;
+        d[5] += sr * out;
+        d[6] += out * out;
     }
 }
 
-// out = A in: sums the tile partials of each row in a fixed order (8 groups
-// per output combined by shuffles), adds the diagonal block and the
-// neutrality couplings.  Returns this thread's dot contributions:
-//   DOT 0: (d1, out)            DOT 1: Kt = K out, (Kt, d1), (Kt, Kt)
-template <int DOT>
-__device__ void reduce_phase(const CoopArgs &A, const double *in, double *out, const double *d1, double &p0,
-                             double &p1)
+// out = A in from the tile partials (kGroups groups per output, combined by
+// shuffles in a fixed order), the diagonal and the neutrality couplings.
+// RED_START: r0 = r = b - A x, dot (r, r).  RED_V: v = A y, dot (r0, v).
+// RED_T: t = A z and the dots (K t, z), (K t, K t), (r0, s), (r0, t), (s, s),
+// (s, t), (t, t), from which omega, the next rho and (r, r) of r = s - omega t
+// follow without another pass.  Writes the block's dot partials to bp.
+template <int RED>
+__device__ void reduce_pass(const CoopArgs &A, const PassScalars &S, double *bp)
 {
     const int M = A.M;
-    const long nwork = (long)A.nT * 128 * 8;
+    const double *in = RED == RED_START ? A.x : (RED == RED_V ? A.y : A.z);
+    double d[7] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    const long nwork = (long)A.nT * 128 * kGroups;
     const long gthreads = (long)gridDim.x * blockDim.x;
     for (long base = 0; base < nwork; base += gthreads) {
         const long id = base + (long)blockIdx.x * blockDim.x + threadIdx.x;
+        const int g = (int)(id % kGroups), o = (int)((id / kGroups) & 127), I = (int)(id / (128 * kGroups));
         double s = 0.0;
-        const int g = (int)(id & 7), o = (int)((id >> 3) & 127), I = (int)(id >> 10);
         if (id < nwork) {
+            // kBatch independent loads in flight, summed in a fixed order
             const double *src = A.part + (size_t)I * A.nT * (kT * 4) + o;
-            for (int Kk = g; Kk < A.nT; Kk += 8) s += __ldcg(src + (size_t)Kk * (kT * 4));
+            for (int K0 = g; K0 < A.nT; K0 += kBatch * kGroups) {
+                double vals[kBatch];
+#pragma unroll
+                for (int u = 0; u < kBatch; ++u) {
+                    const int Kk = K0 + u * kGroups;
+                    vals[u] = Kk < A.nT ? __ldcg(src + (size_t)Kk * (kT * 4)) : 0.0;
+                }
+#pragma unroll
+                for (int u = 0; u < kBatch; ++u) s += vals[u];
+            }
         }
         s += __shfl_xor_sync(0xffffffffu, s, 1);
         s += __shfl_xor_sync(0xffffffffu, s, 2);
-        s += __shfl_xor_sync(0xffffffffu, s, 4);
         if (id < nwork && g == 0) {
             const int atom = I * kT + (o >> 2), comp = o & 3;
             if (atom < M) {
@@ -250,177 +503,169 @@ __device__ void reduce_phase(const CoopArgs &A, const double *in, double *out, c
                     s += -A.inv_capac * xin;
                     const int im = A.metal_min + atom;
                     for (int k = 0; k < A.n_nps; ++k)
-                        if (im >= A.np_start[k] && im <= A.np_end[k]) s += __ldcg(in + 4 * M + k);
+                        if (im >= A.np_start[k] && im <= A.np_end[k]) s += __ldcg(in + A.n4 + k);
                 }
-                out[row] = s;
-                if (DOT == 0) p0 += __ldcg(d1 + row) * s;
-                if (DOT == 1) {
-                    const double kt = __ldcg(A.K + row) * s;
-                    p0 += kt * __ldcg(d1 + row);
-                    p1 += kt * kt;
-                }
+                reduce_row<RED>(A, S, row, s, xin, RED == RED_T ? __ldcg(A.K + row) : 0.0, d);
             }
         }
     }
-    // Lagrange rows: sum of the NP's charges of `in`
-    for (int k = blockIdx.x; k < A.n_nps; k += gridDim.x) {
+    // Lagrange rows: the sum of the nanoparticle's charges of `in`
+    for (int k = (int)gridDim.x - 1 - (int)blockIdx.x; k < A.n_nps; k += gridDim.x) {
         __shared__ double sh[32];
         double acc[1] = {0.0};
         for (int at = A.np_start[k] + threadIdx.x; at <= A.np_end[k]; at += blockDim.x)
             acc[0] += __ldcg(in + 3 * M + (at - A.metal_min));
         block_sum<1>(acc, sh);
         if (threadIdx.x == 0) {
-            const int row = 4 * M + k;
-            out[row] = acc[0];
-            if (DOT == 0) p0 += __ldcg(d1 + row) * acc[0];
-            if (DOT == 1) {
-                p0 += acc[0] * __ldcg(d1 + row);  // K = 1 on Lagrange rows
-                p1 += acc[0] * acc[0];
-            }
+            const int row = A.n4 + k;
+            reduce_row<RED>(A, S, row, acc[0], __ldcg(in + row), 1.0, d);  // K = 1 on Lagrange rows
         }
         __syncthreads();
+    }
+    if (RED == RED_T) {
+        put_bp<7>(bp, d);
+    } else {
+        double d1[1] = {d[0]};
+        put_bp<1>(bp, d1);
     }
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kBlock) k_bicgstab_coop(CoopArgs A)
+__global__ void __launch_bounds__(kBlock, 1) k_bicgstab_coop(CoopArgs A)
 {
+    extern __shared__ __align__(128) unsigned char ring_smem[];
+    constexpr int Stages = Ring<T>::Stages;
+    __shared__ __align__(8) uint64_t ring_bar[Stages];
+    __shared__ PassSmem<T> psm;
     SolverScalars *ss = A.ss;
     const int n = A.n;
     const long gthreads = (long)gridDim.x * blockDim.x;
     const long tid = (long)blockIdx.x * blockDim.x + threadIdx.x;
     const int nb = gridDim.x;
-    // Separate partial sets per dot kind: a block may write the x/r partials
-    // while a slower block still reads the omega partials (no barrier lies
-    // between those two phases).
-    double *bpV = A.bp, *bpT = A.bp + 2 * nb, *bpX = A.bp + 4 * nb;
-    double a1;
+    double *bpA = A.bp, *bpB = A.bp + (size_t)kBp * nb;
 
-    // start: bTb, Ax0, r0 = r = b - A x, p = v = 0, K
+    Ring<T> ring;
+    ring.buf = reinterpret_cast<T *>(ring_smem);
+    ring.bar = ring_bar;
+    ring.issued = ring.consumed = 0;
+    ring.n_my = (int)blockIdx.x < A.ntiles ? (A.ntiles - 1 - (int)blockIdx.x) / nb + 1 : 0;
+    if (threadIdx.x == 0) {
+        for (int st = 0; st < Stages; ++st) mbar_init(ring_bar + st, 1);
+        fence_mbar_init();
+        if (ring.n_my > 0)
+            for (int st = 0; st < Stages; ++st) ring.issue(static_cast<const T *>(A.mat));
+    }
+    __syncthreads();
+
+    PassScalars S{0.0, 0.0, 0.0, 0, 1};
+    int iter = 0, status = 0;
+    double bTb = 0.0, crit = 0.0, rTr = 0.0, rr0 = 0.0;
+    bool ok = true;
+
+    // start: bTb, K, p = v = 0 (first buffers)
     {
-        double pb = 0.0;
+        double pb[1] = {0.0};
         for (long k = tid; k < n; k += gthreads) {
             const double bk = A.b[k];
-            pb += bk * bk;
+            pb[0] += bk * bk;
             A.K[k] = k < A.n4 ? 1.0 / A.diag[k] : 1.0;
+            A.p[0][k] = 0.0;
+            A.v[0][k] = 0.0;
         }
-        put_bp(bpX, pb, 0.0);
+        put_bp<1>(bpA, pb);
     }
-    if (!grid_barrier(A.bar)) return;
-    double bTb;
-    sum_bp(bpX, nb, bTb, a1);
-    const double crit = bTb * A.tol;
-    if (bTb < A.skip) {
-        if (tid == 0) {
-            ss->bTb = bTb;
-            ss->iter = 0;
-            ss->done = 1;
-            ss->status = 0;
-            ss->rTr = 0.0;
-            ss->rr0 = 0.0;
-        }
-        return;
+    ok = grid_barrier(A.sync);
+    if (ok) {
+        double t1[1];
+        sum_bp<1>(bpA, nb, t1);
+        bTb = t1[0];
+        crit = bTb * A.tol;
     }
-    tiles_phase<T>(A, A.x);
-    if (!grid_barrier(A.bar)) return;
-    {
-        double q0 = 0.0, q1 = 0.0;
-        reduce_phase<2>(A, A.x, A.t, nullptr, q0, q1);  // t = A x (no dots)
+    bool done = !ok || bTb < A.skip;  // zero right-hand side: x stays (bicg_stab.c:303-307)
+    if (!done) {
+        ok = tiles_pass<T, MODE_X>(A, S, ring, psm) && grid_barrier(A.sync);
+        if (ok) reduce_pass<RED_START>(A, S, bpB);
+        ok = ok && grid_barrier(A.sync);
+        done = !ok;
     }
-    if (!grid_barrier(A.bar)) return;
-    {
-        double pr = 0.0;
-        for (long k = tid; k < n; k += gthreads) {
-            const double rk = A.b[k] - __ldcg(A.t + k);
-            A.r0[k] = rk;
-            A.r[k] = rk;
-            A.p[k] = 0.0;
-            A.v[k] = 0.0;
-            pr += rk * rk;
-        }
-        put_bp(bpX, pr, 0.0);
+    double rho = 0.0, rho_old = 1.0, alpha = 1.0, omega = 1.0;
+    if (!done) {
+        double t1[1];
+        sum_bp<1>(bpB, nb, t1);
+        rho = rTr = rr0 = t1[0];
+        if (rho < A.skip) done = true;  // warm start already converged (bicg_stab.c:368)
     }
-    if (!grid_barrier(A.bar)) return;
-    double rho;
-    sum_bp(bpX, nb, rho, a1);
-    double rTr = rho, rr0 = rho, rho_old = 1.0, alpha = 1.0, omega = 1.0;
-    int iter = 0, status = 0, done = 0;
-    if (rho < A.skip) done = 1;  // warm start already converged (bicg_stab.c:368)
-
+    bool pending = false;  // x += alpha y + omega z of the last iteration not yet applied
     while (!done) {
-        // P
-        const double beta = (rho / rho_old) * (alpha / omega);
-        for (long k = tid; k < n; k += gthreads) {
-            const double pk = __ldcg(A.r + k) + beta * (__ldcg(A.p + k) - omega * __ldcg(A.v + k));
-            A.p[k] = pk;
-            A.y[k] = pk * __ldcg(A.K + k);
+        S.beta = (rho / rho_old) * (alpha / omega);
+        S.omega = omega;
+        S.alpha = alpha;
+        ok = tiles_pass<T, MODE_P>(A, S, ring, psm) && grid_barrier(A.sync);
+        if (!ok) break;
+        S.first = 0;
+        reduce_pass<RED_V>(A, S, bpA);
+        if (!grid_barrier(A.sync)) {
+            ok = false;
+            break;
         }
-        if (!grid_barrier(A.bar)) return;
-        tiles_phase<T>(A, A.y);
-        if (!grid_barrier(A.bar)) return;
-        {
-            double q0 = 0.0, q1 = 0.0;
-            reduce_phase<0>(A, A.y, A.v, A.r0, q0, q1);
-            put_bp(bpV, q0, 0.0);
-        }
-        if (!grid_barrier(A.bar)) return;
-        // S
-        double r0v;
-        sum_bp(bpV, nb, r0v, a1);
-        const double al = rho / r0v;
-        if (!isfinite(al)) {
+        double r0v[1];
+        sum_bp<1>(bpA, nb, r0v);
+        const double al = rho / r0v[0];
+        if (!isfinite(al)) {  // breakdown: x is the start of this iteration
             status = rTr < crit * 100.0 ? 1 : -2;
             break;
         }
         alpha = al;
-        for (long k = tid; k < n; k += gthreads) {
-            const double sk = __ldcg(A.r + k) - alpha * __ldcg(A.v + k);
-            A.s[k] = sk;
-            A.z[k] = sk * __ldcg(A.K + k);
+        S.cur ^= 1;  // v[cur] and p[cur] are now the new ones
+        S.alpha = alpha;
+        ok = tiles_pass<T, MODE_S>(A, S, ring, psm) && grid_barrier(A.sync);
+        if (!ok) break;
+        reduce_pass<RED_T>(A, S, bpB);
+        if (!grid_barrier(A.sync)) {
+            ok = false;
+            break;
         }
-        if (!grid_barrier(A.bar)) return;
-        tiles_phase<T>(A, A.z);
-        if (!grid_barrier(A.bar)) return;
-        {
-            double q0 = 0.0, q1 = 0.0;
-            reduce_phase<1>(A, A.z, A.t, A.z, q0, q1);
-            put_bp(bpT, q0, q1);
-        }
-        if (!grid_barrier(A.bar)) return;
-        // X
-        double ktz, ktkt;
-        sum_bp(bpT, nb, ktz, ktkt);
-        const double om = ktz / ktkt;
+        double d[7];
+        sum_bp<7>(bpB, nb, d);
+        const double om = d[0] / d[1];
         if (!isfinite(om) || om == 0.0) {
             status = rTr < crit * 100.0 ? 1 : -2;
             break;
         }
         omega = om;
-        {
-            double q0 = 0.0, q1 = 0.0;
-            for (long k = tid; k < n; k += gthreads) {
-                A.x[k] += alpha * __ldcg(A.y + k) + omega * __ldcg(A.z + k);
-                const double rk = __ldcg(A.s + k) - omega * __ldcg(A.t + k);
-                A.r[k] = rk;
-                q0 += rk * rk;
-                q1 += __ldcg(A.r0 + k) * rk;
-            }
-            put_bp(bpX, q0, q1);
-        }
-        if (!grid_barrier(A.bar)) return;
-        double r0r;
-        sum_bp(bpX, nb, rTr, r0r);
+        // r = s - omega t: (r0, r) and (r, r) from the merged dots
         rho_old = rho;
-        rho = r0r;
+        rho = fma(-omega, d[3], d[2]);
+        rTr = fma(omega * omega, d[6], fma(-2.0 * omega, d[5], d[4]));
         ++iter;
+        pending = true;
         if (rTr < crit) {
-            done = 1;
+            done = true;
         } else if (iter > A.max_iter) {
             status = rTr < crit * 100.0 ? 1 : -1;
-            done = 1;
+            done = true;
         }
     }
-    if (tid == 0) {
+    if (ok && pending) {  // the last update of x, and (r, r) of the final residual
+        double q[1] = {0.0};
+        for (long k = tid; k < n; k += gthreads) {
+            A.x[k] += alpha * __ldcg(A.y + k) + omega * __ldcg(A.z + k);
+            const double rk = __ldcg(A.s + k) - omega * __ldcg(A.t + k);
+            A.r[k] = rk;
+            q[0] += rk * rk;
+        }
+        put_bp<1>(bpA, q);
+        ok = grid_barrier(A.sync);
+        if (ok) {
+            sum_bp<1>(bpA, nb, q);
+            rTr = q[0];
+        }
+    }
+    if (threadIdx.x == 0) {
+        if (!ok) atomicCAS(&A.sync->error, 0, 2);
+        ring.drain();
+    }
+    if (ok && tid == 0) {
         ss->bTb = bTb;
         ss->crit = crit;
         ss->rTr = rTr;
@@ -431,9 +676,16 @@ __global__ void __launch_bounds__(kBlock) k_bicgstab_coop(CoopArgs A)
     }
 }
 
+template <typename T>
+size_t ring_bytes()
+{
+    return (size_t)Ring<T>::Stages * kTileElems * sizeof(T);
+}
+
 }  // namespace
 
-size_t coop_barrier_bytes() { return sizeof(CoopBarrier); }
+size_t coop_barrier_bytes() { return sizeof(CoopSync); }
+size_t coop_partial_doubles(int grid) { return (size_t)2 * kBp * grid; }
 
 // Launch the persistent solver; returns the status as bicgstab_core does.
 int bicgstab_coop(capac_ctx *c, const double *b, double *x, double tol, double skip)
@@ -460,49 +712,57 @@ int bicgstab_coop(capac_ctx *c, const double *b, double *x, double tol, double s
     A.b = b;
     A.diag = c->diag;
     A.x = x;
-    // work vectors: slots of bw (Ax slot reused for t's start value)
-    A.r0 = W(1); A.r = W(2); A.p = W(3); A.v = W(4); A.s = W(5); A.t = W(6); A.y = W(7); A.z = W(8);
-    A.K = W(10);
+    // work vectors in the slots of bw; the second p and v buffers take the
+    // slots the per-step solver uses for A x0 and K t
+    A.r0 = W(1); A.r = W(2); A.p[0] = W(3); A.v[0] = W(4); A.s = W(5); A.t = W(6); A.y = W(7); A.z = W(8);
+    A.v[1] = W(9); A.K = W(10); A.p[1] = W(0);
     A.tol = tol;
     A.skip = skip;
     A.ss = c->ss;
-    A.bar = reinterpret_cast<CoopBarrier *>(c->coop_bar);
-    CAPAC_CUDA(cudaMemsetAsync(c->coop_bar, 0, sizeof(CoopBarrier), c->stream));
+    A.sync = reinterpret_cast<CoopSync *>(c->coop_bar);
+    CAPAC_CUDA(cudaMemsetAsync(c->coop_bar, 0, sizeof(CoopSync), c->stream));
     void *args[] = {&A};
+    const bool mixed = c->opt.precision == CAPAC_PREC_MIXED;
     {
         ProfScope ps(c, K_SOLVE);
-        if (c->opt.precision == CAPAC_PREC_MIXED)
+        if (mixed)
             CAPAC_CUDA(cudaLaunchCooperativeKernel((const void *)k_bicgstab_coop<float>, dim3(c->coop_grid),
-                                                   dim3(kBlock), args, 0, c->stream));
+                                                   dim3(kBlock), args, ring_bytes<float>(), c->stream));
         else
             CAPAC_CUDA(cudaLaunchCooperativeKernel((const void *)k_bicgstab_coop<double>, dim3(c->coop_grid),
-                                                   dim3(kBlock), args, 0, c->stream));
+                                                   dim3(kBlock), args, ring_bytes<double>(), c->stream));
     }
     ++c->launches;
     CAPAC_CUDA(cudaMemcpyAsync(c->h_ss, c->ss, sizeof(SolverScalars), cudaMemcpyDeviceToHost, c->stream));
-    CoopBarrier hb;
-    CAPAC_CUDA(cudaMemcpyAsync(&hb, c->coop_bar, sizeof hb, cudaMemcpyDeviceToHost, c->stream));
+    CoopSync hs;
+    CAPAC_CUDA(cudaMemcpyAsync(&hs, c->coop_bar, sizeof hs, cudaMemcpyDeviceToHost, c->stream));
     CAPAC_CUDA(cudaStreamSynchronize(c->stream));
-    if (hb.error) throw Error(CAPAC_ERR_CUDA, "solver grid barrier timed out");
+    if (hs.error) throw Error(CAPAC_ERR_CUDA, "persistent solver: a bounded wait timed out");
     if (c->prof.on && c->h_ss->bTb >= skip) c->prof.spmv_effective += 1 + 2L * c->h_ss->iter;
     if (c->h_ss->status < 0) return CAPAC_ERR_NOT_CONVERGED;
     return c->h_ss->status == 1 ? 1 : CAPAC_OK;
 }
 
-// Largest co-resident grid for the persistent solver (0 if unsupported).
+// Blocks of the persistent solver (one per SM), 0 if the device cannot run
+// it (no cooperative launch, or the ring does not fit in shared memory).
 int coop_grid_size(int device, bool mixed)
 {
     int coop = 0;
     if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device) != cudaSuccess || !coop) return 0;
     int sms = 0;
     CAPAC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    const void *fn = mixed ? (const void *)k_bicgstab_coop<float> : (const void *)k_bicgstab_coop<double>;
+    const size_t dyn = mixed ? ring_bytes<float>() : ring_bytes<double>();
+    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
     int per_sm = 0;
-    if (mixed)
-        CAPAC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bicgstab_coop<float>, kBlock, 0));
-    else
-        CAPAC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bicgstab_coop<double>, kBlock, 0));
-    if (per_sm <= 0) return 0;
-    return sms * std::min(per_sm, 2);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kBlock, dyn) != cudaSuccess || per_sm < 1) {
+        cudaGetLastError();
+        return 0;
+    }
+    return sms;
 }
 
 }  // namespace capac

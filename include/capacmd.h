@@ -149,7 +149,8 @@ typedef struct capac_options {
                                1e-10 asked of the refinement, with room for ill-conditioned metal
                                clusters, where 1e-10 leaves charge errors near 1e-8) */
     int matrix_layout;      /* CPIM matrix: 0 symmetric packed 4x4 blocks (default), 1 full 4x4 blocks */
-    int predictor;          /* mixed path warm start: 0 last solution, 1 linear extrapolation (default) */
+    int predictor;          /* mixed path warm start: polynomial extrapolation of the last solutions of
+                               order 0 (last solution), 1 (linear), 2 (quadratic, default) or 3 */
     int solver_kernel;      /* BiCGSTAB on the symmetric layout: 0 one persistent cooperative launch per
                                solve when the device supports it (default), 1 a launch per vector step */
 } capac_options;
