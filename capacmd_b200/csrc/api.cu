@@ -295,6 +295,21 @@ int capac_create(const capac_desc *d, const capac_options *opt, capac_ctx **out)
             c->mol_type = dupload(d->mol_type, N, s);
             c->atom_in_mol = dupload(d->atom_in_mol, N, s);
             c->is_metal = dupload(d->is_metal, N, s);
+            {
+                // metal flag per type, when all atoms of a type agree
+                std::vector<int> tm(d->n_types, -1);
+                bool by_type = true;
+                for (int i = 0; i < N && by_type; ++i) {
+                    int &f = tm[d->atom_type[i]];
+                    const int m = d->is_metal[i] ? 1 : 0;
+                    if (f < 0) f = m;
+                    else if (f != m) by_type = false;
+                }
+                std::vector<unsigned char> tmb(d->n_types);
+                for (int t = 0; t < d->n_types; ++t) tmb[t] = tm[t] == 1 ? 1 : 0;
+                c->type_metal = dupload(tmb.data(), tmb.size(), s);
+                c->P.metal_by_type = by_type ? 1 : 0;
+            }
             c->charge = dupload(d->charge, N, s);
             c->mass = dupload(d->mass, N, s);
             c->inv_mass = dupload(d->inv_mass, N, s);
@@ -363,6 +378,7 @@ int capac_create(const capac_desc *d, const capac_options *opt, capac_ctx **out)
             P.mol_type = c->mol_type;
             P.atom_in_mol = c->atom_in_mol;
             P.is_metal = c->is_metal;
+            P.type_metal = c->type_metal;
             P.charge = c->charge;
             P.mass = c->mass;
             P.inv_mass = c->inv_mass;
@@ -475,7 +491,7 @@ int capac_destroy(capac_ctx *c)
     if (c->stream) cudaStreamSynchronize(c->stream);
     void *dev[] = {c->rx, c->ry, c->rz, c->vx, c->vy, c->vz, c->fx, c->fy, c->fz, c->ox, c->oy, c->oz,
                    c->rx0, c->ry0, c->rz0, c->pos4, c->pos4f, c->type, c->mol_id, c->mol_type,
-                   c->atom_in_mol, c->is_metal, c->charge, c->mass, c->inv_mass, c->mol_atoms,
+                   c->atom_in_mol, c->is_metal, c->type_metal, c->charge, c->mass, c->inv_mass, c->mol_atoms,
                    c->excl_offset, c->excl, c->nb_funct, c->nb_par, c->mol_first, c->mol_last, c->cstr_off,
                    c->cstr_cnt, c->cstr_i, c->cstr_j, c->cstr_r, c->np_start, c->np_end, c->np_charge,
                    c->nbr, c->nnb, c->cell_key, c->cell_key_sorted, c->atom_ids, c->cell_atoms,

@@ -51,6 +51,9 @@ struct DevParams {
     // nanoparticles
     const int *np_start, *np_end;
     const double *np_charge;
+    // per type: 1 metal, 0 not (valid when metal_by_type: every atom of a type agrees)
+    const unsigned char *type_metal;
+    int metal_by_type;
 };
 
 // Kernel classes for the event-based profiler.
@@ -111,6 +114,7 @@ struct capac_ctx {
     // topology
     int *type = nullptr, *mol_id = nullptr, *mol_type = nullptr, *atom_in_mol = nullptr;
     unsigned char *is_metal = nullptr;
+    unsigned char *type_metal = nullptr;  // [n_types]
     double *charge = nullptr, *mass = nullptr, *inv_mass = nullptr;
     int *mol_atoms = nullptr, *excl_offset = nullptr;
     unsigned char *excl = nullptr;

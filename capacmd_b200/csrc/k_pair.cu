@@ -32,9 +32,54 @@ constexpr int kPairWarps = 8;  // warps per block
 
 // FP32 constants of the run.
 struct PairConstsF {
-    float rc, inv_rc, inv_rc12, inv_rc6, alpha, a2_sqrtpi, w_const, w_erfc_arcut, fqq;
+    float rc, inv_rc, inv_rc12, inv_rc6, alpha, a2_sqrtpi, w_const, w_erfc_arcut, fqq, rc2;
     int use_vdw, use_coulomb;
 };
+
+// One type pair in FP32, with the shifted-force constants of funct 1
+// precomputed: fc = 12 c12 / rc^12 - 6 c6 / rc^6, es = c12 / rc^12 - c6 / rc^6.
+struct TypePairF {
+    float c6, c12, a, b, fc, es;
+    int fn, pad;
+};
+
+__device__ __forceinline__ TypePairF make_type_pair_f(const DevParams &P, const PairConstsF &K, int k)
+{
+    const double4 pd = P.nb_par[k];
+    TypePairF t;
+    t.c6 = (float)pd.x;
+    t.c12 = (float)pd.y;
+    t.a = (float)pd.z;
+    t.b = (float)pd.w;
+    t.fc = (float)(12.0 * pd.y * P.inv_rc12 - 6.0 * pd.x * P.inv_rc6);
+    t.es = (float)(pd.y * P.inv_rc12 - pd.x * P.inv_rc6);
+    t.fn = P.nb_funct[k];
+    t.pad = 0;
+    return t;
+}
+
+// erfc(x) for 0 <= x in FP32 as exp(-x^2) R(x), with R(x) = erfc(x) exp(x^2)
+// (the scaled complementary error function) fitted on [0, 5] by a degree-9
+// polynomial in t = 1 / (1 + x / 2), least squares in relative error
+// (relative error of R below 4e-8 in exact arithmetic, 3e-7 in FP32).  The
+// caller has exp(-x^2) already, for the Gaussian term of the same pair.
+// Beyond x = 5 the library erfcf.
+__device__ __forceinline__ float erfc_from_gauss_f(float x, float gauss)
+{
+    if (x >= 5.0f) return erfcf(x);
+    const float t = __frcp_rn(fmaf(0.5f, x, 1.0f));
+    float r = -3.71903017e-02f;
+    r = fmaf(r, t, 1.64898831e-01f);
+    r = fmaf(r, t, -2.03180485e-01f);
+    r = fmaf(r, t, -1.05265965e-01f);
+    r = fmaf(r, t, 2.97262422e-01f);
+    r = fmaf(r, t, 2.51787793e-02f);
+    r = fmaf(r, t, 3.06175054e-01f);
+    r = fmaf(r, t, 2.68365236e-01f);
+    r = fmaf(r, t, 2.83852814e-01f);
+    r = fmaf(r, t, -9.64172679e-05f);
+    return gauss * r;
+}
 
 // FP64 pair term (force on j = f * rvec), reference formulas with the
 // divisions by r, r^2, r^6, r^12 turned into products with 1/r.
@@ -91,13 +136,12 @@ __device__ __forceinline__ double pair_term(const DevParams &P, int k, double qi
     return f;
 }
 
-// The same terms in FP32.
-__device__ __forceinline__ float pair_term_f(const DevParams &P, const PairConstsF &K, int k, float qi, float qj,
-                                             float r2, float &e_qq, float &e_vdw)
+// The same terms in FP32, from the FP32 type pair.
+__device__ __forceinline__ float pair_term_f(const PairConstsF &K, const TypePairF &tp, float qi, float qj, float r2,
+                                             float &e_qq, float &e_vdw)
 {
-    const int fn = P.nb_funct[k];
-    const double4 pd = P.nb_par[k];
-    const float c6 = (float)pd.x, c12 = (float)pd.y, pa = (float)pd.z, pb = (float)pd.w;
+    const int fn = tp.fn;
+    const float c6 = tp.c6, c12 = tp.c12, pa = tp.a, pb = tp.b;
     const float rinv = rsqrtf(r2), r = r2 * rinv, r2inv = rinv * rinv;
     if (fn == 4) {
         if (c6 != 0.f || c12 != 0.f) {
@@ -124,9 +168,8 @@ __device__ __forceinline__ float pair_term_f(const DevParams &P, const PairConst
         const float r6inv = r2inv * r2inv * r2inv, r12inv = r6inv * r6inv;
         if (K.use_vdw == 1) {
             const float fr = 12.f * c12 * r12inv - 6.f * c6 * r6inv;
-            const float fc = 12.f * c12 * K.inv_rc12 - 6.f * c6 * K.inv_rc6;
-            f = (fr - fc) * r2inv;
-            e_vdw += (c12 * r12inv - c6 * r6inv) + (r - K.rc) * fc * K.inv_rc - (c12 * K.inv_rc12 - c6 * K.inv_rc6);
+            f = (fr - tp.fc) * r2inv;
+            e_vdw += (c12 * r12inv - c6 * r6inv) + (r - K.rc) * tp.fc * K.inv_rc - tp.es;
         } else {
             f = (c12 * 2.f * r12inv - c6 * r6inv) * 6.f * r2inv;
             e_vdw += c12 * r12inv - c6 * r6inv;
@@ -135,8 +178,8 @@ __device__ __forceinline__ float pair_term_f(const DevParams &P, const PairConst
     if (qi != 0.f && qj != 0.f) {
         const float qq = K.fqq * qi * qj;
         if (K.use_coulomb == 1) {
-            const float ar = K.alpha * r, ec = erfcf(ar);
-            f += qq * ((ec * r2inv + K.a2_sqrtpi * expf(-ar * ar) * rinv) - K.w_const) * rinv;
+            const float ar = K.alpha * r, eg = expf(-ar * ar), ec = erfc_from_gauss_f(ar, eg);
+            f += qq * ((ec * r2inv + K.a2_sqrtpi * eg * rinv) - K.w_const) * rinv;
             e_qq += qq * (ec * rinv - K.w_erfc_arcut + K.w_const * (r - K.rc));
         } else {
             f += qq * r2inv * rinv;
@@ -154,8 +197,9 @@ __device__ __forceinline__ void cpim_charge_pair_f(const PairConstsF &K, const f
     const float rinv = rsqrtf(r2), rr = r2 * rinv, r2inv = rinv * rinv;
     float a0, ec = 0.f, eg = 0.f;
     if (K.use_coulomb == 1) {
-        ec = erfcf(K.alpha * rr);
-        eg = expf(-K.alpha * K.alpha * r2);
+        const float ar = K.alpha * rr;
+        eg = expf(-ar * ar);
+        ec = erfc_from_gauss_f(ar, eg);
         a0 = (ec * r2inv + K.a2_sqrtpi * eg * rinv - K.w_const) * rinv;
     } else {
         a0 = r2inv * rinv;
@@ -203,29 +247,73 @@ struct Acc<float> {
     __device__ __forceinline__ double value() const { return (double)s - (double)c; }
 };
 
-// A candidate inside the cut-off, parked in the warp's queue.
-struct Cand {
+// A candidate inside the cut-off, parked in the warp's queue: FP64 record
+// (48 B) for the FP64 path, FP32 record (24 B) for the mixed path.
+template <typename Real>
+struct Cand;
+template <>
+struct Cand<double> {
     double dx, dy, dz, r2, qj;
     uint32_t e;
     int pad;
 };
+template <>
+struct Cand<float> {
+    float dx, dy, dz, r2, qj;
+    uint32_t e;
+};
 
+// Type-pair tables staged in shared memory when the type count allows.
+constexpr int kSmemTypes = 16;
+
+// Candidate chunks of 32 whose list entries and positions are loaded before
+// any is tested: more loads in flight per warp.
+template <typename Real>
+struct Batch {
+    static constexpr int N = 2;
+};
+
+// One warp per atom i (grid-stride); see the file comment.
 template <typename Real, bool NONBONDED, bool CPIM>
-__global__ void __launch_bounds__(kPairWarps * 32) k_pair(DevParams P, PairConstsF K, const double4 *__restrict__ pos4,
+__global__ void __launch_bounds__(kPairWarps * 32, sizeof(Real) == 4 ? 3 : 2) k_pair(DevParams P, PairConstsF K, const double4 *__restrict__ pos4,
                                                            const uint32_t *__restrict__ nbr,
                                                            const int *__restrict__ nnb, int cap,
                                                            const double *__restrict__ vec_pq, double *__restrict__ fx,
                                                            double *__restrict__ fy, double *__restrict__ fz,
                                                            double *__restrict__ partials)
 {
-    __shared__ Cand queue[kPairWarps][64];
+    constexpr int NB = Batch<Real>::N;
+    __shared__ Cand<Real> queue[kPairWarps][64];
     __shared__ double sh[32 * 11];
     __shared__ double wacc[kPairWarps][8];  // per warp: e_qq, e_vdw, virial xx xy xz yy yz zz
+    // type-pair table: double4 parameters (FP64) or TypePairF records (mixed), 32 B each
+    __shared__ __align__(16) unsigned char s_tab[kSmemTypes * kSmemTypes * 32];
+    __shared__ int s_fn[kSmemTypes * kSmemTypes];
+    __shared__ unsigned char s_metal[kSmemTypes];
+    double4 *s_par = reinterpret_cast<double4 *>(s_tab);
+    TypePairF *s_tpf = reinterpret_cast<TypePairF *>(s_tab);
     const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const unsigned lt_mask = (1u << lane) - 1u;
-    Cand *Q = queue[wib];
+    Cand<Real> *Q = queue[wib];
     if (lane < 8) wacc[wib][lane] = 0.0;
-    __syncwarp();
+    const bool smem_types = P.n_types <= kSmemTypes;
+    if (smem_types) {
+        const int nt2 = P.n_types * P.n_types;
+        for (int k = threadIdx.x; k < nt2; k += blockDim.x) {
+            if constexpr (sizeof(Real) == 8) s_par[k] = P.nb_par[k];
+            else s_tpf[k] = make_type_pair_f(P, K, k);
+            s_fn[k] = P.nb_funct[k];
+        }
+        for (int k = threadIdx.x; k < P.n_types; k += blockDim.x) s_metal[k] = P.type_metal[k];
+    }
+    __syncthreads();
+    // the type-pair table as the pair terms read it
+    DevParams Pt = P;
+    if (smem_types) {
+        Pt.nb_par = s_par;
+        Pt.nb_funct = s_fn;
+    }
+    const bool metal_by_type = smem_types && P.metal_by_type;
     const int stride = gridDim.x * kPairWarps;
     for (int i = blockIdx.x * kPairWarps + wib; i < P.N; i += stride) {
         const double4 pi = pos4[i];
@@ -239,14 +327,15 @@ __global__ void __launch_bounds__(kPairWarps * 32) k_pair(DevParams P, PairConst
 #pragma unroll
         for (int q = 0; q < 6; ++q) v[q] = 0;
 
-        auto process = [&](const Cand &c) {
-            const Real dx = (Real)c.dx, dy = (Real)c.dy, dz = (Real)c.dz;
+        auto process = [&](const Cand<Real> &c) {
+            const Real dx = c.dx, dy = c.dy, dz = c.dz;
             if (NONBONDED) {
                 Real f;
                 if constexpr (sizeof(Real) == 8)
-                    f = pair_term(P, trow + nb_type(c.e), pi.w, c.qj, c.r2, e_qq, e_vdw);
+                    f = pair_term(Pt, trow + nb_type(c.e), pi.w, c.qj, c.r2, e_qq, e_vdw);
                 else
-                    f = pair_term_f(P, K, trow + nb_type(c.e), (float)pi.w, (float)c.qj, (float)c.r2, e_qq, e_vdw);
+                    f = pair_term_f(K, smem_types ? s_tpf[trow + nb_type(c.e)] : make_type_pair_f(P, K, trow + nb_type(c.e)),
+                                    (float)pi.w, c.qj, c.r2, e_qq, e_vdw);
                 const Real gx = f * dx, gy = f * dy, gz = f * dz;
                 f0.add(-gx);
                 f1.add(-gy);
@@ -256,7 +345,8 @@ __global__ void __launch_bounds__(kPairWarps * 32) k_pair(DevParams P, PairConst
             }
             if (cpim_i) {
                 const int j = nb_index(c.e);
-                if (P.is_metal[j]) {
+                const bool mj = metal_by_type ? s_metal[nb_type(c.e)] != 0 : P.is_metal[j] != 0;
+                if (mj) {
                     const int jm = j - P.metal_min;
                     if constexpr (sizeof(Real) == 8) {
                         const double r[3] = {c.dx, c.dy, c.dz};  // metal - atom
@@ -267,11 +357,11 @@ __global__ void __launch_bounds__(kPairWarps * 32) k_pair(DevParams P, PairConst
                         f1.add(-g[1]);
                         f2.add(-g[2]);
                     } else {
-                        const float r[3] = {(float)c.dx, (float)c.dy, (float)c.dz};
+                        const float r[3] = {c.dx, c.dy, c.dz};
                         const float p[3] = {(float)vec_pq[3 * jm], (float)vec_pq[3 * jm + 1],
                                             (float)vec_pq[3 * jm + 2]};
                         float g[3];
-                        cpim_charge_pair_f(K, r, (float)c.r2, (float)pi.w, (float)vec_pq[3 * P.M + jm], p, g);
+                        cpim_charge_pair_f(K, r, c.r2, (float)pi.w, (float)vec_pq[3 * P.M + jm], p, g);
                         f0.add(-g[0]);
                         f1.add(-g[1]);
                         f2.add(-g[2]);
@@ -281,34 +371,66 @@ __global__ void __launch_bounds__(kPairWarps * 32) k_pair(DevParams P, PairConst
         };
 
         int qn = 0;  // queue fill, warp-uniform
-        for (int base = 0; base < n; base += 32) {
-            const int k = base + lane;
-            bool ok = false;
-            Cand c;
-            if (k < n) {
-                const uint32_t e = row[k];
-                const double4 pj = pos4[nb_index(e)];
-                double dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
-                image(dx, dy, dz, P.box);
-                const double r2 = norm2_exact(dx, dy, dz);
-                ok = r2 < P.rc2;
-                c.dx = dx;
-                c.dy = dy;
-                c.dz = dz;
-                c.r2 = r2;
-                c.qj = pj.w;
-                c.e = e;
+        // list entries are loaded one batch ahead (the list streams from
+        // HBM once per step, evict-first)
+        uint32_t nxt[NB];
+#pragma unroll
+        for (int u = 0; u < NB; ++u) {
+            const int k = u * 32 + lane;
+            nxt[u] = k < n ? __ldcs(row + k) : 0u;
+        }
+        for (int base = 0; base < n; base += 32 * NB) {
+            uint32_t ev[NB];
+            bool valid[NB];
+#pragma unroll
+            for (int u = 0; u < NB; ++u) {
+                valid[u] = base + u * 32 + lane < n;
+                ev[u] = nxt[u];
+                const int k = base + (NB + u) * 32 + lane;
+                nxt[u] = k < n ? __ldcs(row + k) : 0u;
             }
-            const unsigned ballot = __ballot_sync(0xffffffffu, ok);
-            if (ok) Q[qn + __popc(ballot & lt_mask)] = c;
-            qn += __popc(ballot);
-            __syncwarp();
-            if (qn >= 32) {
-                process(Q[lane]);
+            double4 pj[NB];
+#pragma unroll
+            for (int u = 0; u < NB; ++u)
+                if (valid[u]) pj[u] = pos4[nb_index(ev[u])];
+#pragma unroll
+            for (int u = 0; u < NB; ++u) {
+                bool ok = false;
+                Cand<Real> c;
+                if (valid[u]) {
+                    double dx = pj[u].x - pi.x, dy = pj[u].y - pi.y, dz = pj[u].z - pi.z;
+                    image(dx, dy, dz, P.box);
+                    if constexpr (sizeof(Real) == 8) {
+                        // the reference's rounding of r^2: the FP64 pair set is the reference's
+                        const double r2 = norm2_exact(dx, dy, dz);
+                        ok = r2 < P.rc2;
+                        c.r2 = r2;
+                    } else {
+                        // mixed: r^2 and the cut-off in FP32 from the FP64 minimum-image
+                        // difference; pairs within rounding of the cut-off contribute
+                        // nothing (shifted force and energy vanish there)
+                        const float fx = (float)dx, fy = (float)dy, fz = (float)dz;
+                        const float r2 = fmaf(fz, fz, fmaf(fy, fy, fx * fx));
+                        ok = r2 < K.rc2;
+                        c.r2 = r2;
+                    }
+                    c.dx = (Real)dx;
+                    c.dy = (Real)dy;
+                    c.dz = (Real)dz;
+                    c.qj = (Real)pj[u].w;
+                    c.e = ev[u];
+                }
+                const unsigned ballot = __ballot_sync(0xffffffffu, ok);
+                if (ok) Q[qn + __popc(ballot & lt_mask)] = c;
+                qn += __popc(ballot);
                 __syncwarp();
-                if (lane < qn - 32) Q[lane] = Q[lane + 32];
-                __syncwarp();
-                qn -= 32;
+                if (qn >= 32) {
+                    process(Q[lane]);
+                    __syncwarp();
+                    if (lane < qn - 32) Q[lane] = Q[lane + 32];
+                    __syncwarp();
+                    qn -= 32;
+                }
             }
         }
         if (lane < qn) process(Q[lane]);
@@ -358,6 +480,7 @@ PairConstsF pair_consts_f(const capac_ctx *c)
     K.w_const = (float)c->P.w_const;
     K.w_erfc_arcut = (float)c->P.w_erfc_arcut;
     K.fqq = (float)kFQQ;
+    K.rc2 = (float)c->P.rc2;
     K.use_vdw = c->P.use_vdw;
     K.use_coulomb = c->P.use_coulomb;
     return K;

@@ -3,11 +3,13 @@
 //
 // Same algorithm and stopping rules as bicgstab_core (bicg_stab.c:253-573,
 // with the breakdown guard); the host launches one kernel per solve instead
-// of about ten small kernels per iteration.  One block per SM.  Each block
-// owns the tiles t = blockIdx.x + k * gridDim.x and streams them from HBM
-// into a two-stage shared-memory ring with bulk asynchronous copies
-// (cp.async.bulk + mbarrier); the matrix does not change during a solve, so
-// the ring runs on across phases and iterations.
+// of about ten small kernels per iteration.  Two blocks per SM on the FP32
+// matrix, one on the FP64 matrix.  Each block owns the tiles t = blockIdx.x
+// + k * gridDim.x and streams them from HBM into a two-tile shared-memory
+// ring with bulk asynchronous copies (cp.async.bulk + mbarrier); the matrix
+// does not change during a solve, so the ring runs on across phases and
+// iterations.  A tile takes one block barrier: its row and column sums go
+// to one of two accumulator sets while the other set is written out.
 //
 // An iteration, with a grid barrier after each of its four phases:
 //   P  tile pass of y = K p, p = r + beta (p - omega v), r = s - omega t,
@@ -33,6 +35,7 @@
 // its own copies in flight and returns, the other blocks give up at their
 // next barrier, and the host reports the error.  The launch is cooperative,
 // so either all blocks are resident or the launch fails.
+#include <algorithm>
 #include <cstdint>
 
 #include "terms.cuh"
@@ -45,8 +48,21 @@ constexpr int kT = 32;
 constexpr int kPlanes = 10;
 constexpr int kTileElems = kPlanes * kT * kT;
 constexpr int kBlock = 256;
-constexpr int kRingBytes = 160 * 1024;  // 4 FP32 tiles or 2 FP64 tiles
-constexpr int kChunkTiles = 16;         // tiles whose inputs a pass gathers at once
+constexpr int kWarps = kBlock / 32;
+constexpr int kCols = kT / kWarps;  // tile columns per warp
+// Tile ring per block: two FP32 tiles (two blocks per SM) or two FP64 tiles
+// (one block per SM).
+template <typename T>
+__host__ __device__ constexpr int ring_tiles_bytes()
+{
+    return 2 * kTileElems * (int)sizeof(T);
+}
+// tiles whose inputs a pass gathers at once
+template <typename T>
+__host__ __device__ constexpr int chunk_tiles()
+{
+    return 8;
+}
 constexpr int kGroups = 4;              // partial-sum groups per output row in the reduce phases
 constexpr int kBatch = 16;              // partials one thread loads at once in the reduce phases
 constexpr long kSpinLimit = 1L << 24;
@@ -63,39 +79,48 @@ __device__ __forceinline__ int elem_offset(int p, int a, int b)
 {
     return ((p * (kT / 4) + (b >> 2)) * (kT * 4)) + a * 4 + (b & 3);
 }
-__device__ __forceinline__ void lds4(const float *p, float out[4])
+// The kCols consecutive columns of one plane row (kCols = 2 or 4).
+template <typename R>
+__device__ __forceinline__ void ldsc(const R *p, R (&out)[kCols])
 {
-    const float4 v = *reinterpret_cast<const float4 *>(p);
-    out[0] = v.x; out[1] = v.y; out[2] = v.z; out[3] = v.w;
-}
-__device__ __forceinline__ void lds4(const double *p, double out[4])
-{
-    const double2 u = *reinterpret_cast<const double2 *>(p);
-    const double2 v = *reinterpret_cast<const double2 *>(p + 2);
-    out[0] = u.x; out[1] = u.y; out[2] = v.x; out[3] = v.y;
+#pragma unroll
+    for (int k = 0; k < kCols; k += 2) {
+        if constexpr (sizeof(R) == 4) {
+            const float2 v = *reinterpret_cast<const float2 *>(p + k);
+            out[k] = v.x;
+            out[k + 1] = v.y;
+        } else {
+            const double2 v = *reinterpret_cast<const double2 *>(p + k);
+            out[k] = v.x;
+            out[k + 1] = v.y;
+        }
+    }
 }
 
-// Sums of 16 values over the 32 lanes of a warp by recursive halving: at
+// Sums of V values over the 32 lanes of a warp by recursive halving: at
 // each step a lane keeps half of its values and adds the partner's copy of
-// that half (8 + 4 + 2 + 1 exchanges), then one last exchange; 16 shuffles
-// instead of 80.  Lanes 2v and 2v + 1 return the sum of value v (v = 4 k + c
-// of cb[k][c]).  The order of additions is fixed.
-__device__ __forceinline__ double warp_sum16(double (&cb)[4][4], int lane)
+// that half (V/2 + V/4 + ... + 1 exchanges), then plain exchanges for the
+// remaining lane bits; V - 1 + 5 - log2 V shuffles instead of 5 V.  Lane l
+// returns the sum of value l >> (5 - log2 V).  The order of additions is
+// fixed.
+template <int V, typename R>
+__device__ __forceinline__ R warp_sum_halving(R (&v)[V], int lane)
 {
-    double v[16];
+    int m = 16;
 #pragma unroll
-    for (int i = 0; i < 16; ++i) v[i] = cb[i >> 2][i & 3];
-#pragma unroll
-    for (int half = 8, m = 16; half >= 1; half >>= 1, m >>= 1) {
+    for (int half = V / 2; half >= 1; half >>= 1, m >>= 1) {
         const bool upper = (lane & m) != 0;
 #pragma unroll
         for (int i = 0; i < half; ++i) {
-            const double send = upper ? v[i] : v[i + half];
-            const double keep = upper ? v[i + half] : v[i];
+            const R send = upper ? v[i] : v[i + half];
+            const R keep = upper ? v[i + half] : v[i];
             v[i] = keep + __shfl_xor_sync(0xffffffffu, send, m);
         }
     }
-    return v[0] + __shfl_xor_sync(0xffffffffu, v[0], 1);
+    R s = v[0];
+#pragma unroll
+    for (; m >= 1; m >>= 1) s += __shfl_xor_sync(0xffffffffu, s, m);
+    return s;
 }
 
 __device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
@@ -201,7 +226,7 @@ constexpr int kBp = 8;
 template <int K>
 __device__ void sum_bp(const double *bp, int nb, double (&out)[K])
 {
-    __shared__ double sh[8 * kBp];
+    __shared__ double sh[kWarps * kBp];
     __shared__ double res[kBp];
     double v[K];
 #pragma unroll
@@ -222,7 +247,7 @@ __device__ void sum_bp(const double *bp, int nb, double (&out)[K])
 template <int K>
 __device__ void put_bp(double *bp, double (&v)[K])
 {
-    __shared__ double sh[8 * kBp];
+    __shared__ double sh[kWarps * kBp];
     block_sum<K>(v, sh);
     if (threadIdx.x == 0)
 #pragma unroll
@@ -254,14 +279,14 @@ __device__ __forceinline__ double p_row(const CoopArgs &A, const PassScalars &S,
     return pn;
 }
 
-// The ring of tiles of one block: Stages = kRingBytes / tile bytes slots;
+// The ring of tiles of one block: Stages = ring bytes / tile bytes slots;
 // sequence number q -> slot q % Stages, whose k-th use waits for parity
 // k & 1; tile of q = blockIdx.x + (q mod n_my) * gridDim.x.  Every thread
 // counts `consumed`; thread 0 alone issues the copies and counts `issued`
 // (always consumed + Stages).
 template <typename T>
 struct Ring {
-    static constexpr int Stages = kRingBytes / (int)(kTileElems * sizeof(T));
+    static constexpr int Stages = ring_tiles_bytes<T>() / (int)(kTileElems * sizeof(T));
     T *buf;
     uint64_t *bar;  // Stages mbarriers
     long issued, consumed;
@@ -287,15 +312,14 @@ struct Ring {
 // FP32 matrix, and every sum across columns or tiles is in FP64.
 template <typename T>
 struct PassSmem {
-    T in[kChunkTiles][2][kT][4];  // pass inputs of the chunk's tiles: block rows I and J
-    double rowacc[8][kT][4];
-    double colacc[kT][4];
-    int tile_i[kChunkTiles], tile_j[kChunkTiles];
-    int wait_ok;
+    T in[chunk_tiles<T>()][2][kT][4];  // pass inputs of the chunk's tiles: block rows I and J
+    T rowacc[2][kWarps][kT][4];        // two sets: tile k + 1 fills one while tile k's is written out
+    double colacc[2][kT][4];
+    int tile_i[chunk_tiles<T>()], tile_j[chunk_tiles<T>()];
 };
 
 // Tile pass: partial products of the block's tiles with the pass input.
-// The inputs of up to kChunkTiles tiles are gathered in one batch of
+// The inputs of up to chunk_tiles<T>() tiles are gathered in one batch of
 // independent loads before the tiles are processed.  Returns false when a
 // ring wait timed out.
 template <typename T, int MODE>
@@ -304,7 +328,6 @@ __device__ bool tiles_pass(const CoopArgs &A, const PassScalars &S, Ring<T> &rin
     constexpr int Stages = Ring<T>::Stages;
     const int M = A.M;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int side = threadIdx.x >> 7, q4 = threadIdx.x & 127, at = q4 >> 2, comp = q4 & 3;
 
     // the Lagrange rows of the stored vectors (K = 1 there)
     if (MODE != MODE_X && threadIdx.x == 0) {
@@ -320,8 +343,9 @@ __device__ bool tiles_pass(const CoopArgs &A, const PassScalars &S, Ring<T> &rin
         }
     }
 
-    for (int c0 = 0; c0 < ring.n_my; c0 += kChunkTiles) {
-        const int nc = min(kChunkTiles, ring.n_my - c0);
+    constexpr int kChunk = chunk_tiles<T>();
+    for (int c0 = 0; c0 < ring.n_my; c0 += kChunk) {
+        const int nc = min(kChunk, ring.n_my - c0);
         if (threadIdx.x < nc) {
             const int t = blockIdx.x + (c0 + threadIdx.x) * gridDim.x;
             int I = 0;
@@ -330,9 +354,10 @@ __device__ bool tiles_pass(const CoopArgs &A, const PassScalars &S, Ring<T> &rin
             sm.tile_j[threadIdx.x] = I + (int)((size_t)t - tile_index(I, I, A.nT));
         }
         __syncthreads();
-        // gather: thread (side, atom, comp) of every tile of the chunk
+        // gather: element (tile, side, atom, comp) of the chunk's tiles
 #pragma unroll 4
-        for (int kk = 0; kk < nc; ++kk) {
+        for (int e = threadIdx.x; e < nc * 256; e += kBlock) {
+            const int kk = e >> 8, side = (e >> 7) & 1, q4 = e & 127, at = q4 >> 2, comp = q4 & 3;
             const int I = sm.tile_i[kk], J = sm.tile_j[kk];
             const int atom = (side ? J : I) * kT + at;
             double val = 0.0;
@@ -359,57 +384,55 @@ __device__ bool tiles_pass(const CoopArgs &A, const PassScalars &S, Ring<T> &rin
 
         for (int kk = 0; kk < nc; ++kk) {
             const int I = sm.tile_i[kk], J = sm.tile_j[kk];
+            const int set = kk & 1;
             const long q = ring.consumed;
             const int st = (int)(q % Stages);
             const unsigned parity = (unsigned)((q / Stages) & 1);
-            if (threadIdx.x == 0) sm.wait_ok = mbar_wait(ring.bar + st, parity) ? 1 : 0;
-            __syncthreads();
-            if (!sm.wait_ok) return false;
-            // every thread observes the completed phase before reading the stage
-            // (it has completed: this returns at the first poll)
-            mbar_wait(ring.bar + st, parity);
+            const bool landed = mbar_wait(ring.bar + st, parity);  // every thread, bounded
             const T *tile = ring.stage(st);
             const T(*xr)[4] = sm.in[kk][0];
             const T(*xc)[4] = sm.in[kk][1];
+            // thread (row a = lane, columns b = kCols w ...): row partials of
+            // a, column partials of b summed over the warp's 32 rows
             const int a = lane;
             T ra[4] = {0, 0, 0, 0};
-            T cb[4][4];
+            T cb[kCols * 4];
             const T xa0 = xr[a][0], xa1 = xr[a][1], xa2 = xr[a][2], xa3 = xr[a][3];
-            {
-                T vv[kPlanes][4];
+            if (landed) {
+                T vv[kPlanes][kCols];
 #pragma unroll
-                for (int pl = 0; pl < kPlanes; ++pl) lds4(tile + elem_offset(pl, a, 4 * w), vv[pl]);
+                for (int pl = 0; pl < kPlanes; ++pl) ldsc(tile + elem_offset(pl, a, kCols * w), vv[pl]);
 #pragma unroll
-                for (int k4 = 0; k4 < 4; ++k4) {
-                    const int b = 4 * w + k4;
-                    const T Axx = vv[0][k4], Axy = vv[1][k4], Axz = vv[2][k4], Ayy = vv[3][k4], Ayz = vv[4][k4],
-                            Azz = vv[5][k4], m0 = vv[6][k4], m1 = vv[7][k4], m2 = vv[8][k4], C = vv[9][k4];
+                for (int k = 0; k < kCols; ++k) {
+                    const int b = kCols * w + k;
+                    const T Axx = vv[0][k], Axy = vv[1][k], Axz = vv[2][k], Ayy = vv[3][k], Ayz = vv[4][k],
+                            Azz = vv[5][k], m0 = vv[6][k], m1 = vv[7][k], m2 = vv[8][k], C = vv[9][k];
                     const T xb0 = xc[b][0], xb1 = xc[b][1], xb2 = xc[b][2], xb3 = xc[b][3];
                     ra[0] += Axx * xb0 + Axy * xb1 + Axz * xb2 + m0 * xb3;
                     ra[1] += Axy * xb0 + Ayy * xb1 + Ayz * xb2 + m1 * xb3;
                     ra[2] += Axz * xb0 + Ayz * xb1 + Azz * xb2 + m2 * xb3;
                     ra[3] += -(m0 * xb0 + m1 * xb1 + m2 * xb2) + C * xb3;
-                    cb[k4][0] = Axx * xa0 + Axy * xa1 + Axz * xa2 - m0 * xa3;
-                    cb[k4][1] = Axy * xa0 + Ayy * xa1 + Ayz * xa2 - m1 * xa3;
-                    cb[k4][2] = Axz * xa0 + Ayz * xa1 + Azz * xa2 - m2 * xa3;
-                    cb[k4][3] = m0 * xa0 + m1 * xa1 + m2 * xa2 + C * xa3;
+                    cb[4 * k + 0] = Axx * xa0 + Axy * xa1 + Axz * xa2 - m0 * xa3;
+                    cb[4 * k + 1] = Axy * xa0 + Ayy * xa1 + Ayz * xa2 - m1 * xa3;
+                    cb[4 * k + 2] = Axz * xa0 + Ayz * xa1 + Azz * xa2 - m2 * xa3;
+                    cb[4 * k + 3] = m0 * xa0 + m1 * xa1 + m2 * xa2 + C * xa3;
                 }
+            } else {
+#pragma unroll
+                for (int k = 0; k < kCols * 4; ++k) cb[k] = 0;
             }
-            // column sums over the warp's 32 rows: lane 2v and 2v + 1 end
-            // with value v = 4 k + c
-            double cbd[4][4];
+            // lane l ends with value v = l >> (5 - log2(4 kCols)) (= 4 k + c) summed over the rows
+            const T colsum = warp_sum_halving<kCols * 4>(cb, lane);
 #pragma unroll
-            for (int k4 = 0; k4 < 4; ++k4)
-#pragma unroll
-                for (int c = 0; c < 4; ++c) cbd[k4][c] = (double)cb[k4][c];
-            const double colsum = warp_sum16(cbd, lane);
-#pragma unroll
-            for (int c = 0; c < 4; ++c) sm.rowacc[w][a][c] = (double)ra[c];
-            if ((lane & 1) == 0) {
-                const int v = lane >> 1;
-                sm.colacc[4 * w + (v >> 2)][v & 3] = colsum;
+            for (int c = 0; c < 4; ++c) sm.rowacc[set][w][a][c] = ra[c];
+            constexpr int kShift = 5 - (kCols == 1 ? 2 : kCols == 2 ? 3 : kCols == 4 ? 4 : 5);
+            if ((lane & ((1 << kShift) - 1)) == 0) {
+                const int v = lane >> kShift;
+                sm.colacc[set][kCols * w + (v >> 2)][v & 3] = (double)colsum;
             }
-            __syncthreads();  // the stage is free again
+            // one barrier per tile: the stage is free, this tile's sums are
+            // complete, and the previous tile's set has been written out
+            if (__syncthreads_or(!landed)) return false;
             ++ring.consumed;  // every thread keeps the same count
             if (threadIdx.x == 0) ring.issue(static_cast<const T *>(A.mat));  // the tile this slot holds next
             double *pr = A.part + ((size_t)I * A.nT + J) * (kT * 4);
@@ -418,11 +441,11 @@ __device__ bool tiles_pass(const CoopArgs &A, const PassScalars &S, Ring<T> &rin
                 const int aa = threadIdx.x >> 2, c = threadIdx.x & 3;
                 double s = 0.0;
 #pragma unroll
-                for (int ww = 0; ww < 8; ++ww) s += sm.rowacc[ww][aa][c];
-                pr[threadIdx.x] = I == J ? s + sm.colacc[aa][c] : s;
-            } else if (I != J) {
+                for (int ww = 0; ww < kWarps; ++ww) s += (double)sm.rowacc[set][ww][aa][c];
+                pr[threadIdx.x] = I == J ? s + sm.colacc[set][aa][c] : s;
+            } else if (threadIdx.x < 2 * kT * 4 && I != J) {
                 const int c = threadIdx.x - kT * 4;
-                pc[c] = sm.colacc[c >> 2][c & 3];
+                pc[c] = sm.colacc[set][c >> 2][c & 3];
             }
         }
         __syncthreads();  // rowacc, colacc and the chunk inputs are free again
@@ -531,12 +554,18 @@ __device__ void reduce_pass(const CoopArgs &A, const PassScalars &S, double *bp)
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kBlock, 1) k_bicgstab_coop(CoopArgs A)
+__host__ __device__ constexpr size_t ring_bytes()
+{
+    return (size_t)Ring<T>::Stages * kTileElems * sizeof(T);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? 2 : 1) k_bicgstab_coop(CoopArgs A)
 {
     extern __shared__ __align__(128) unsigned char ring_smem[];
     constexpr int Stages = Ring<T>::Stages;
     __shared__ __align__(8) uint64_t ring_bar[Stages];
-    __shared__ PassSmem<T> psm;
+    PassSmem<T> &psm = *reinterpret_cast<PassSmem<T> *>(ring_smem + ring_bytes<T>());
     SolverScalars *ss = A.ss;
     const int n = A.n;
     const long gthreads = (long)gridDim.x * blockDim.x;
@@ -677,9 +706,9 @@ __global__ void __launch_bounds__(kBlock, 1) k_bicgstab_coop(CoopArgs A)
 }
 
 template <typename T>
-size_t ring_bytes()
+size_t dyn_smem_bytes()
 {
-    return (size_t)Ring<T>::Stages * kTileElems * sizeof(T);
+    return ring_bytes<T>() + sizeof(PassSmem<T>);
 }
 
 }  // namespace
@@ -727,10 +756,10 @@ int bicgstab_coop(capac_ctx *c, const double *b, double *x, double tol, double s
         ProfScope ps(c, K_SOLVE);
         if (mixed)
             CAPAC_CUDA(cudaLaunchCooperativeKernel((const void *)k_bicgstab_coop<float>, dim3(c->coop_grid),
-                                                   dim3(kBlock), args, ring_bytes<float>(), c->stream));
+                                                   dim3(kBlock), args, dyn_smem_bytes<float>(), c->stream));
         else
             CAPAC_CUDA(cudaLaunchCooperativeKernel((const void *)k_bicgstab_coop<double>, dim3(c->coop_grid),
-                                                   dim3(kBlock), args, ring_bytes<double>(), c->stream));
+                                                   dim3(kBlock), args, dyn_smem_bytes<double>(), c->stream));
     }
     ++c->launches;
     CAPAC_CUDA(cudaMemcpyAsync(c->h_ss, c->ss, sizeof(SolverScalars), cudaMemcpyDeviceToHost, c->stream));
@@ -743,7 +772,8 @@ int bicgstab_coop(capac_ctx *c, const double *b, double *x, double tol, double s
     return c->h_ss->status == 1 ? 1 : CAPAC_OK;
 }
 
-// Blocks of the persistent solver (one per SM), 0 if the device cannot run
+// Blocks of the persistent solver (two per SM for the FP32 matrix, one for
+// the FP64 matrix), 0 if the device cannot run
 // it (no cooperative launch, or the ring does not fit in shared memory).
 int coop_grid_size(int device, bool mixed)
 {
@@ -752,7 +782,7 @@ int coop_grid_size(int device, bool mixed)
     int sms = 0;
     CAPAC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
     const void *fn = mixed ? (const void *)k_bicgstab_coop<float> : (const void *)k_bicgstab_coop<double>;
-    const size_t dyn = mixed ? ring_bytes<float>() : ring_bytes<double>();
+    const size_t dyn = mixed ? dyn_smem_bytes<float>() : dyn_smem_bytes<double>();
     if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn) != cudaSuccess) {
         cudaGetLastError();
         return 0;
@@ -762,7 +792,7 @@ int coop_grid_size(int device, bool mixed)
         cudaGetLastError();
         return 0;
     }
-    return sms;
+    return sms * std::min(per_sm, mixed ? 2 : 1);
 }
 
 }  // namespace capac

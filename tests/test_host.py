@@ -195,3 +195,26 @@ def test_oracle_tight_solve_matches_dense_solution():
     A = np.stack([o.matvec(e) for e in np.eye(n)], 1)
     x = np.linalg.solve(A, o.get("vec_ext"))
     assert np.abs(o.get("vec_pq") - x).max() / np.abs(x).max() < 1e-10
+
+
+def test_fp32_erfc_fit_error_bound():
+    """The mixed path's FP32 erfc (exp(-x^2) times a fitted polynomial in
+    t = 1 / (1 + x / 2)) against the exact erfc on [0, 5], evaluated with
+    FP32 rounding at every step as the kernel does."""
+    import math
+    import re
+    src = open(os.path.join(ROOT, "capacmd_b200", "csrc", "k_pair.cu")).read()
+    body = src[src.index("erfc_from_gauss_f(float x, float gauss)"):]
+    body = body[:body.index("return gauss * r;")]
+    coef = [float(c) for c in re.findall(r"([-+]?\d\.\d+e[-+]\d+)f", body)]
+    assert len(coef) == 10  # Horner order: highest degree first
+    x = np.linspace(0.0, 5.0, 200001).astype(np.float32)
+    t = (np.float32(1.0) / (np.float32(0.5) * x + np.float32(1.0))).astype(np.float32)
+    r = np.float32(coef[0]) * np.ones_like(x)
+    for c in coef[1:]:
+        r = (r * t + np.float32(c)).astype(np.float32)
+    gauss = np.exp(-(x.astype(np.float64) ** 2)).astype(np.float32)
+    approx = (gauss * r).astype(np.float64)
+    exact = np.array([math.erfc(float(v)) for v in x])
+    rel = np.abs(approx / exact - 1.0)
+    assert rel.max() < 6e-7  # a few FP32 ulp, as the library erfcf
