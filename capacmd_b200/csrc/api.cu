@@ -495,7 +495,7 @@ int capac_destroy(capac_ctx *c)
                    c->excl_offset, c->excl, c->nb_funct, c->nb_par, c->mol_first, c->mol_last, c->cstr_off,
                    c->cstr_cnt, c->cstr_i, c->cstr_j, c->cstr_r, c->np_start, c->np_end, c->np_charge,
                    c->nbr, c->nnb, c->cell_key, c->cell_key_sorted, c->atom_ids, c->cell_atoms,
-                   c->cell_start, c->cell_end, c->sort_tmp, c->flags, c->isd, c->vec_ext, c->vec_pq,
+                   c->cell_start, c->spos, c->sort_tmp, c->flags, c->isd, c->vec_ext, c->vec_pq,
                    c->diag, c->mat, c->matf, c->msym, c->sympart, c->coop_bp, c->coop_bar, c->rres, c->dcorr, c->xprev, c->bw, c->bwf, c->ss, c->partials, c->pot, c->vir, c->th};
     for (void *p : dev)
         if (p) cudaFree(p);

@@ -135,7 +135,8 @@ struct capac_ctx {
     double cell_len[3] = {0, 0, 0};
     int n_cells = 1;
     int *cell_key = nullptr, *cell_key_sorted = nullptr, *atom_ids = nullptr, *cell_atoms = nullptr;
-    int *cell_start = nullptr, *cell_end = nullptr;
+    int *cell_start = nullptr;   // [n_cells + 1] first sorted position of each cell
+    double4 *spos = nullptr;     // [N] positions in cell order, atom index in w
     void *sort_tmp = nullptr;
     size_t sort_tmp_bytes = 0;
     int *flags = nullptr;      // [0] rebuild needed, [1] list overflow max count, [2] rattle error

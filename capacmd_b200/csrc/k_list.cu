@@ -3,9 +3,13 @@
 // The reference has no neighbour structure: mpi_nonb_pair (force.c:1419-1473)
 // visits every j < i and keeps a pair when it is not excluded and
 // dist_2(pbc_12(r_j - r_i)) < rCut^2.  Here atoms are binned into cells of edge
-// >= rc + skin (wrapped coordinates), and each atom's full list holds every
+// >= (rc + skin) / 2 (wrapped coordinates) and sorted by cell, with a
+// cell-ordered copy of the positions; each atom's full list holds every
 // non-excluded j within rc + skin under the same pbc_12 metric on the
-// unwrapped coordinates.  The pair kernel re-applies the exact FP64 cut-off
+// unwrapped coordinates.  A warp scans the 5 x 5 cells around its atom in x
+// and y, each as one contiguous run of five z cells of the sorted copy
+// (coalesced loads), tests the distance first and the exclusions only for
+// the survivors.  The pair kernel re-applies the exact FP64 cut-off
 // every step, so the set of interacting pairs equals the reference's as long
 // as no atom has moved more than skin/2 since the build; a displacement check
 // every step triggers the rebuild.
@@ -47,13 +51,26 @@ __global__ void k_cell_keys(int N, const double *__restrict__ rx, const double *
     ids[i] = i;
 }
 
-__global__ void k_cell_bounds(int N, const int *__restrict__ key, int *start, int *end)
+// start[c] = first sorted position with key >= c, for c = 0 .. n_cells
+// (empty cells included), so the atoms of cells a..b are start[a] ..
+// start[b + 1] - 1.
+__global__ void k_cell_starts(int N, int n_cells, const int *__restrict__ key, int *start)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p > N) return;
+    const int prev = p > 0 ? key[p - 1] : -1;
+    const int cur = p < N ? key[p] : n_cells;
+    for (int c = prev + 1; c <= cur; ++c) start[c] = p;
+}
+
+// Positions in cell order, with the atom index in w.
+__global__ void k_sorted_positions(int N, const int *__restrict__ ids, const double *__restrict__ rx,
+                                   const double *__restrict__ ry, const double *__restrict__ rz, double4 *spos)
 {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= N) return;
-    const int k = key[p];
-    if (p == 0 || key[p - 1] != k) start[k] = p;
-    if (p == N - 1 || key[p + 1] != k) end[k] = p + 1;
+    const int j = ids[p];
+    spos[p] = make_double4(rx[j], ry[j], rz[j], (double)j);
 }
 
 __device__ __forceinline__ bool excluded(const DevParams &P, int i, int j)
@@ -63,13 +80,17 @@ __device__ __forceinline__ bool excluded(const DevParams &P, int i, int j)
     return P.excl[P.excl_offset[m] + P.atom_in_mol[i] * na + P.atom_in_mol[j]] != 0;
 }
 
-// One warp per atom i: scan the 27 (or fewer) neighbouring cells.
+// The k-th cell along one axis around cell c: c-2 .. c+2 (periodic) when
+// the axis has at least five cells, else the axis has one cell.
+__device__ __forceinline__ int axis_count(int n) { return n < 5 ? 1 : 5; }
+__device__ __forceinline__ int axis_cell(int c, int n, int k) { return n < 5 ? 0 : (c + k - 2 + n) % n; }
+
+// One warp per atom i.
 __global__ void __launch_bounds__(256) k_build_list(DevParams P, Grid g, const double *__restrict__ rx,
                                                     const double *__restrict__ ry,
                                                     const double *__restrict__ rz,
-                                                    const int *__restrict__ cell_atoms,
-                                                    const int *__restrict__ cell_start,
-                                                    const int *__restrict__ cell_end, int cap,
+                                                    const double4 *__restrict__ spos,
+                                                    const int *__restrict__ cell_start, int cap,
                                                     uint32_t *__restrict__ nbr, int *__restrict__ nnb,
                                                     double *rx0, double *ry0, double *rz0, int *flags)
 {
@@ -80,30 +101,41 @@ __global__ void __launch_bounds__(256) k_build_list(DevParams P, Grid g, const d
     const int c0[3] = {cell_coord(xi, P.box.L[0], g.inv_len[0], g.n[0]),
                        cell_coord(yi, P.box.L[1], g.inv_len[1], g.n[1]),
                        cell_coord(zi, P.box.L[2], g.inv_len[2], g.n[2])};
-    const int lo[3] = {g.n[0] >= 3 ? -1 : 0, g.n[1] >= 3 ? -1 : 0, g.n[2] >= 3 ? -1 : 0};
-    const int hi[3] = {g.n[0] >= 3 ? 1 : 0, g.n[1] >= 3 ? 1 : 0, g.n[2] >= 3 ? 1 : 0};
+    const int nxs = axis_count(g.n[0]), nys = axis_count(g.n[1]);
+    // the z window as one or two runs of consecutive cells
+    const int nz = g.n[2];
+    int za[2], zb[2], nzr;
+    if (nz < 5) {
+        za[0] = 0; zb[0] = nz - 1; nzr = 1;
+    } else {
+        const int lo = c0[2] - 2, hi = c0[2] + 2;
+        if (lo < 0) {
+            za[0] = lo + nz; zb[0] = nz - 1; za[1] = 0; zb[1] = hi; nzr = 2;
+        } else if (hi >= nz) {
+            za[0] = lo; zb[0] = nz - 1; za[1] = 0; zb[1] = hi - nz; nzr = 2;
+        } else {
+            za[0] = lo; zb[0] = hi; nzr = 1;
+        }
+    }
     const unsigned lt_mask = (1u << lane) - 1u;
     uint32_t *row = nbr + (size_t)i * cap;
     int count = 0;
-    for (int ox = lo[0]; ox <= hi[0]; ++ox) {
-        const int cx = (c0[0] + ox + g.n[0]) % g.n[0];
-        for (int oy = lo[1]; oy <= hi[1]; ++oy) {
-            const int cy = (c0[1] + oy + g.n[1]) % g.n[1];
-            for (int oz = lo[2]; oz <= hi[2]; ++oz) {
-                const int cz = (c0[2] + oz + g.n[2]) % g.n[2];
-                const int cell = (cx * g.n[1] + cy) * g.n[2] + cz;
-                const int s = cell_start[cell], e = cell_end[cell];
+    for (int ix = 0; ix < nxs; ++ix) {
+        for (int iy = 0; iy < nys; ++iy) {
+            const int col = (axis_cell(c0[0], g.n[0], ix) * g.n[1] + axis_cell(c0[1], g.n[1], iy)) * nz;
+            for (int r = 0; r < nzr; ++r) {
+                const int s = cell_start[col + (r ? za[1] : za[0])], e = cell_start[col + (r ? zb[1] : zb[0]) + 1];
                 for (int base = s; base < e; base += 32) {
                     const int p = base + lane;
                     bool ok = false;
                     int j = 0;
                     if (p < e) {
-                        j = cell_atoms[p];
-                        if (j != i && !excluded(P, i, j)) {
-                            double dx = rx[j] - xi, dy = ry[j] - yi, dz = rz[j] - zi;
-                            image(dx, dy, dz, P.box);
-                            ok = norm2_exact(dx, dy, dz) < P.list_r2;
-                        }
+                        const double4 q = spos[p];
+                        j = (int)q.w;
+                        double dx = q.x - xi, dy = q.y - yi, dz = q.z - zi;
+                        image(dx, dy, dz, P.box);
+                        ok = j != i && norm2_exact(dx, dy, dz) < P.list_r2;
+                        if (ok) ok = !excluded(P, i, j);
                     }
                     const unsigned ballot = __ballot_sync(0xffffffffu, ok);
                     const int pos = count + __popc(ballot & lt_mask);
@@ -209,10 +241,10 @@ __global__ void k_pack(int N, const double *__restrict__ rx, const double *__res
 Grid make_grid(const capac_ctx *c)
 {
     Grid g;
-    const double len = c->P.rc + c->opt.skin;
+    const double len = 0.5 * (c->P.rc + c->opt.skin);
     for (int a = 0; a < 3; ++a) {
         int n = (int)floor(c->P.box.L[a] / len);
-        if (n < 3) n = 1;
+        if (n < 5) n = 1;
         g.n[a] = n;
         g.inv_len[a] = n / c->P.box.L[a];
     }
@@ -226,11 +258,11 @@ void build_list(capac_ctx *c)
     const int n_cells = g.n[0] * g.n[1] * g.n[2];
     if (n_cells != c->n_cells || !c->cell_start) {
         cudaFree(c->cell_start);
-        cudaFree(c->cell_end);
-        CAPAC_CUDA(cudaMalloc(&c->cell_start, sizeof(int) * n_cells));
-        CAPAC_CUDA(cudaMalloc(&c->cell_end, sizeof(int) * n_cells));
+        c->cell_start = nullptr;
+        CAPAC_CUDA(cudaMalloc(&c->cell_start, sizeof(int) * (n_cells + 1)));
         c->n_cells = n_cells;
     }
+    if (!c->spos) CAPAC_CUDA(cudaMalloc(&c->spos, sizeof(double4) * N));
     for (int a = 0; a < 3; ++a) c->ncell[a] = g.n[a];
     cudaStream_t s = c->stream;
     k_cell_keys<<<grid_for(N, 256), 256, 0, s>>>(N, c->rx, c->ry, c->rz, c->P.box, g, c->cell_key, c->atom_ids);
@@ -247,17 +279,16 @@ void build_list(capac_ctx *c)
     }
     CAPAC_CUDA(cub::DeviceRadixSort::SortPairs(c->sort_tmp, need, c->cell_key, c->cell_key_sorted,
                                                c->atom_ids, c->cell_atoms, N, 0, end_bit, s));
-    CAPAC_CUDA(cudaMemsetAsync(c->cell_start, 0, sizeof(int) * n_cells, s));
-    CAPAC_CUDA(cudaMemsetAsync(c->cell_end, 0, sizeof(int) * n_cells, s));
-    k_cell_bounds<<<grid_for(N, 256), 256, 0, s>>>(N, c->cell_key_sorted, c->cell_start, c->cell_end);
-    ++c->launches;
+    k_cell_starts<<<grid_for(N + 1, 256), 256, 0, s>>>(N, n_cells, c->cell_key_sorted, c->cell_start);
+    k_sorted_positions<<<grid_for(N, 256), 256, 0, s>>>(N, c->cell_atoms, c->rx, c->ry, c->rz, c->spos);
+    c->launches += 2;
     for (int attempt = 0; attempt < 4; ++attempt) {
         CAPAC_CUDA(cudaMemsetAsync(c->flags + 1, 0, sizeof(int), s));
         {
             ProfScope ps(c, K_LIST);
             k_build_list<<<grid_for((long)N * 32, 256), 256, 0, s>>>(
-                c->P, g, c->rx, c->ry, c->rz, c->cell_atoms, c->cell_start, c->cell_end, c->cap, c->nbr,
-                c->nnb, c->rx0, c->ry0, c->rz0, c->flags);
+                c->P, g, c->rx, c->ry, c->rz, c->spos, c->cell_start, c->cap, c->nbr, c->nnb, c->rx0,
+                c->ry0, c->rz0, c->flags);
         }
         ++c->launches;
         CAPAC_CUDA(cudaMemcpyAsync(c->h_flags, c->flags, sizeof(int) * 4, cudaMemcpyDeviceToHost, s));

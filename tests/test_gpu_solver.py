@@ -57,8 +57,10 @@ def test_persistent_solver_meets_reference_rule(case):
     # rTr < 1e-8 bTb (bicg_stab.c:303, 523)
     assert st_c.solver_rel_residual < 1e-4
     assert st_s.solver_rel_residual < 1e-4
-    # same algorithm: the iteration counts differ by rounding only
-    assert abs(st_c.solver_iterations - st_s.solver_iterations) <= max(3, st_s.solver_iterations // 5)
+    # same algorithm; the iterate under the 1e-4 rule is sensitive to the
+    # order of floating-point sums, so counts agree only roughly
+    assert st_c.solver_iterations <= 1.5 * st_s.solver_iterations + 5
+    assert st_s.solver_iterations <= 1.5 * st_c.solver_iterations + 5
     # the answer is the reference's up to the 1e-4 stopping rule
     assert rel_err(coop.get("vec_pq"), step.get("vec_pq")) < 1e-2
 
