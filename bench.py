@@ -1,6 +1,6 @@
 """Throughput of CapacMD's per-timestep force-and-solve path on B200.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c5] [--precision fp64|mixed]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c5] [--precision mixed|fp64]
     python bench.py --impl reference ...      # the reference's own CPU code, same workload
 
 Metric: atom-steps/s -- atoms x MD steps per second of device time, one MD
@@ -13,6 +13,13 @@ seeded synthetic inputs written in the reference's file formats).
 Multi-GPU runs (torchrun) are independent replicas: every rank integrates its
 own copy and nothing is exchanged per step (the path does not shard); value is
 the sum over ranks, timed as the slowest rank.
+
+The headline arm is the mixed-precision form (FP32 pair terms, FP32 matrix
+and SpMV, FP64 refinement to relative residual 1e-10).  Beside it the plain
+FP64 path (the reference's algorithm and 1e-4 solver rule) runs the same
+steps, the FP64 path also at the mixed path's residual target, and an
+accuracy block compares the arms, at the final state, with an FP64 solve to
+rTr < 1e-24 bTb.
 
 Printed: one JSON line with value, e2e (the drop-in mpi_force call with host
 buffers, copies included), the roofline of the dominant kernel from CUDA-event
@@ -198,10 +205,11 @@ def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=100)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="c5", choices=sorted(WORKLOAD_DESC))
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
+    ap.add_argument("--no-compare", action="store_true", help="skip the comparison arms and the accuracy block")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--e2e-calls", type=int, default=20)
@@ -289,6 +297,13 @@ def main() -> int:
                 "kernel": dom, "algorithmic_bytes_per_launch": bytes_launch, "avg_launch_ms": avg_s * 1e3,
                 "launches": n_launch, "peak_kind": peak_kind}
 
+    # the other precision on the same workload and step count, the FP64 path
+    # also at the mixed path's residual target, and the accuracy of the arms
+    # against a tight FP64 solve at the final state
+    compare, accuracy = None, None
+    if not args.no_compare and world == 1:
+        compare, accuracy = compare_arms(args, cm, desc, sim, prec, local)
+
     # end to end through the drop-in mpi_force with pinned host buffers
     e2e = None
     if not args.no_e2e:
@@ -327,12 +342,69 @@ def main() -> int:
             "phase_ms_last_force": {"list": ps[10], "qsc": ps[1], "cpim_vec": ps[6], "cpim_matrix": ps[5],
                                     "cpim_solve": ps[7], "nonbonded": ps[4], "cpim_force": ps[8]},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "gpu_launches": launches,
+            "compare": compare, "accuracy": accuracy,
         }
         print(json.dumps(line))
     sim.close()
     if world > 1:
         dist.destroy_process_group()
     return 0
+
+
+def compare_arms(args, cm, desc, sim, prec, device) -> tuple[dict, dict]:
+    """Time the other precision (and FP64 at the mixed residual target) over
+    the same steps, then measure errors at the headline arm's final state."""
+    N = desc.n_atoms
+    arms = {}
+    other = cm.PREC_FP64 if prec == cm.PREC_MIXED else cm.PREC_MIXED
+    specs = [("fp64_plain" if other == cm.PREC_FP64 else "mixed", other, 0.0)]
+    if desc.n_mat > 0:
+        # rTr < 1e-20 bTb: relative residual 1e-10, the mixed path's target
+        specs.append(("fp64_equal_residual", cm.PREC_FP64, 1e-20))
+    for name, p, tol in specs:
+        s2 = cm.Simulation(desc, precision=p, device=device, solver_tol=tol, solver_kernel=args.solver_kernel,
+                           predictor=args.predictor)
+        s2.md_init()
+        s2.md_steps(args.warmup)
+        ms2 = ctypes_time(s2, args.steps)
+        st2 = s2.stats()
+        arms[name] = {"value": N * args.steps / (ms2 / 1e3), "unit": "atom-steps/s",
+                      "ms_per_step": ms2 / args.steps, "solver_iterations_last": st2.solver_iterations,
+                      "solver_rel_residual_last": st2.solver_rel_residual}
+        s2.close()
+
+    def rel(a, b):
+        nb = float(np.linalg.norm(b))
+        return float(np.linalg.norm(a - b) / nb) if nb > 0 else 0.0
+
+    def state_errors(x, ref):
+        M = desc.n_metal
+        ex, er = x.get("potential")[1:], ref.get("potential")[1:]
+        out = {"force": rel(x.forces(), ref.forces()),
+               "energy_vs_sum_abs_terms": float(abs(ex.sum() - er.sum()) / max(np.abs(er).sum(), 1e-300))}
+        if desc.n_mat > 0:
+            qx, qr = x.get("vec_pq"), ref.get("vec_pq")
+            out["charges"] = rel(qx[3 * M:4 * M], qr[3 * M:4 * M])
+            out["dipoles"] = rel(qx[:3 * M], qr[:3 * M])
+        return out
+
+    def same_state(x):
+        for a in ("rx", "ry", "rz") + (("vec_pq",) if desc.n_mat > 0 else ()):
+            x.set(a, sim.get(a))
+        x.force()
+
+    # the reference state: an FP64 solve to rTr < 1e-24 bTb at the final positions
+    sim.force()
+    ref = cm.Simulation(desc, precision=cm.PREC_FP64, device=device, solver_tol=1e-24)
+    same_state(ref)
+    acc = {"reference": "FP64 path at the same positions, solve to rTr < 1e-24 bTb",
+           "headline": state_errors(sim, ref)}
+    plain = cm.Simulation(desc, precision=other, device=device)
+    same_state(plain)
+    acc["fp64_plain" if other == cm.PREC_FP64 else "mixed"] = state_errors(plain, ref)
+    plain.close()
+    ref.close()
+    return arms, acc
 
 
 def ctypes_time(sim, steps: int) -> float:

@@ -154,7 +154,7 @@ class Simulation:
     """Device-resident state of one system on one B200."""
 
     def __init__(self, desc: Desc, precision: int = PREC_FP64, device: int = 0, skin: float = 0.2,
-                 solver_tol: float = 0.0, refine_tol: float = 1e-11, max_neighbors: int = 0,
+                 solver_tol: float = 0.0, refine_tol: float = 1e-10, max_neighbors: int = 0,
                  matrix_layout: int = 0, predictor: int = 2, solver_kernel: int = 0):
         self.desc = desc
         o = Options()

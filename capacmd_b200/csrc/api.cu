@@ -218,7 +218,7 @@ void capac_options_default(capac_options *o)
     o->list_every = 0;
     o->max_neighbors = 0;
     o->solver_tol = 0.0;
-    o->refine_tol = 1.0e-11;
+    o->refine_tol = 1.0e-10;
     o->matrix_layout = 0;
     o->predictor = 2;
     o->solver_kernel = 0;

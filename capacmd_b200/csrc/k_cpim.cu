@@ -744,7 +744,7 @@ int run_refined_solve(capac_ctx *c)
     const int n = c->n_mat;
     const int nbv = (int)grid_for(n, 256);
     cudaStream_t s = c->stream;
-    const double rtol = c->opt.refine_tol > 0.0 ? c->opt.refine_tol : 1.0e-11;
+    const double rtol = c->opt.refine_tol > 0.0 ? c->opt.refine_tol : 1.0e-10;
     const int max_sweeps = 12;
 
     k_vec_dot<<<nbv, 256, 0, s>>>(n, c->vec_ext, c->vec_ext, c->partials);

@@ -145,9 +145,9 @@ typedef struct capac_options {
     int list_every;         /* forced list rebuild interval in steps, 0 = displacement only */
     int max_neighbors;      /* 0 = estimate from density */
     double solver_tol;      /* rTr < solver_tol * bTb; 0 = reference 1e-8 (bicg_stab.c:303) */
-    double refine_tol;      /* mixed path: FP64 relative residual target (default 1e-11: within the
-                               1e-10 asked of the refinement, with room for ill-conditioned metal
-                               clusters, where 1e-10 leaves charge errors near 1e-8) */
+    double refine_tol;      /* mixed path: FP64 relative residual target (default 1e-10; an
+                               ill-conditioned metal cluster may need 1e-11 to keep the induced
+                               charges within 1e-8 of the FP64 solution) */
     int matrix_layout;      /* CPIM matrix: 0 symmetric packed 4x4 blocks (default), 1 full 4x4 blocks */
     int predictor;          /* mixed path warm start: polynomial extrapolation of the last solutions of
                                order 0 (last solution), 1 (linear), 2 (quadratic, default) or 3 */

@@ -22,10 +22,16 @@ def _need_gpu(gpu_available):
         pytest.fail("no sm_100 GPU: GPU tests must run on a B200")
 
 
-def _both(paths):
+# Au147 in vacuum under a field is ill-conditioned: the default FP64 residual
+# target of 1e-10 leaves the induced charges 1.6e-8 from the FP64 solution,
+# so it is refined to 1e-11 (the 452k-atom system meets 6e-10 at 1e-10)
+REFINE = {"c1_field": 1e-11}
+
+
+def _both(paths, case=None):
     d = cm.Desc.from_paths(paths)
     f64 = cm.Simulation(d, precision=cm.PREC_FP64, solver_tol=1e-24)
-    mix = cm.Simulation(d, precision=cm.PREC_MIXED)
+    mix = cm.Simulation(d, precision=cm.PREC_MIXED, refine_tol=REFINE.get(case, 1e-10))
     f64.force()
     mix.force()
     return d, f64, mix
@@ -33,7 +39,7 @@ def _both(paths):
 
 @pytest.mark.parametrize("case", ["t_au55w", "t_2np", "c1_field", "t_water", "c1"])
 def test_mixed_forces_and_charges(case):
-    d, f64, mix = _both(golden_paths(case))
+    d, f64, mix = _both(golden_paths(case), case)
     assert rel_err(mix.forces(), f64.forces()) < 1e-5
     if d.n_mat > 0:
         assert rel_err(mix.get("vec_pq"), f64.get("vec_pq")) < 1e-8
@@ -74,7 +80,7 @@ def test_mixed_medium_system():
 def test_mixed_md_runs_and_conserves_energy_nve():
     # c1 field variant: NVE, CPIM active in vacuum
     d = cm.Desc.from_paths(golden_paths("c1_field"))
-    mix = cm.Simulation(d, precision=cm.PREC_MIXED)
+    mix = cm.Simulation(d, precision=cm.PREC_MIXED, refine_tol=REFINE["c1_field"])
     mix.md_init()
     e = []
     for _ in range(50):
