@@ -293,9 +293,13 @@ def main() -> int:
         bytes_launch = algorithmic_bytes(sim, dom, N, M, args.precision)
     achieved = bytes_launch / avg_s / 1e9 if avg_s > 0 else None
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak if achieved else None, "traffic": _traffic(args.workload, dom),
+                "frac": achieved / peak if achieved else None, "traffic": _traffic(args.workload, args.precision, dom),
                 "kernel": dom, "algorithmic_bytes_per_launch": bytes_launch, "avg_launch_ms": avg_s * 1e3,
                 "launches": n_launch, "peak_kind": peak_kind}
+    if roofline["traffic"] and roofline["traffic"] < 0.5 * bytes_launch:
+        roofline["note"] = (f"operands stay in the 126 MB L2 across the launch: measured DRAM traffic is "
+                            f"{roofline['traffic'] / bytes_launch:.0%} of the algorithmic bytes, so the launch is "
+                            f"bound by L2 and latency, not HBM")
 
     # the other precision on the same workload and step count, the FP64 path
     # also at the mixed path's residual target, and the accuracy of the arms
@@ -431,12 +435,12 @@ def spmv_effective(sim, launched: int) -> int:
     return n if n > 0 else launched
 
 
-def _traffic(workload: str, kernel: str):
-    """DRAM bytes per launch measured by ncu for this kernel and workload, if a
-    capture summary is committed (profiles/ncu_traffic.json)."""
+def _traffic(workload: str, precision: str, kernel: str):
+    """DRAM bytes per launch measured by ncu for this kernel, workload and
+    precision, if a capture summary is committed (profiles/ncu_traffic.json)."""
     try:
         with open(os.path.join(ROOT, "profiles", "ncu_traffic.json")) as f:
-            return json.load(f).get(workload, {}).get(kernel)
+            return json.load(f).get(workload, {}).get(precision, {}).get(kernel)
     except Exception:
         return None
 

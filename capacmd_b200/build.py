@@ -70,6 +70,9 @@ def build_oracle(verbose: bool = False) -> None:
     subprocess.run(["make", "-s", "-C", odir], check=True)
     if os.path.isdir(REF_SRC):
         subprocess.run(["make", "-s", "-C", odir, "ref", f"REF={REF_SRC}"], check=True)
+        if os.path.exists(LIB):
+            # the reference driver with its mpi_force calls sent to this library
+            subprocess.run(["make", "-s", "-C", odir, "dropin", f"REF={REF_SRC}"], check=True)
 
 
 def main() -> int:
