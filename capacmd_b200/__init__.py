@@ -46,7 +46,8 @@ class Options(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int), ("device", ctypes.c_int), ("skin", ctypes.c_double),
                 ("list_every", ctypes.c_int), ("max_neighbors", ctypes.c_int),
                 ("solver_tol", ctypes.c_double), ("refine_tol", ctypes.c_double),
-                ("matrix_layout", ctypes.c_int), ("predictor", ctypes.c_int), ("solver_kernel", ctypes.c_int)]
+                ("matrix_layout", ctypes.c_int), ("predictor", ctypes.c_int), ("solver_kernel", ctypes.c_int),
+                ("inner_precond", ctypes.c_int)]
 
 
 class Stats(ctypes.Structure):
@@ -155,13 +156,14 @@ class Simulation:
 
     def __init__(self, desc: Desc, precision: int = PREC_FP64, device: int = 0, skin: float = 0.2,
                  solver_tol: float = 0.0, refine_tol: float = 1e-10, max_neighbors: int = 0,
-                 matrix_layout: int = 0, predictor: int = 2, solver_kernel: int = 0):
+                 matrix_layout: int = 0, predictor: int = 2, solver_kernel: int = 0, inner_precond: int = 1):
         self.desc = desc
         o = Options()
         lib().capac_options_default(ctypes.byref(o))
         o.precision, o.device, o.skin = precision, device, skin
         o.solver_tol, o.refine_tol, o.max_neighbors = solver_tol, refine_tol, max_neighbors
         o.matrix_layout, o.predictor, o.solver_kernel = matrix_layout, predictor, solver_kernel
+        o.inner_precond = inner_precond
         self._p = ctypes.c_void_p()
         _check(lib().capac_create(desc.ptr, ctypes.byref(o), ctypes.byref(self._p)))
         self.n_atoms = desc.n_atoms

@@ -20,7 +20,8 @@ OBJ = os.path.join(ROOT, "build", "obj")
 LIB = os.path.join(PKG, "libcapacmd_gpu.so")
 REF_SRC = "/root/reference"
 
-SOURCES = ["io.cpp", "api.cu", "k_list.cu", "k_pair.cu", "k_cpim.cu", "k_md.cu", "k_cpim_sym.cu", "k_solve_static.cu", "k_solve_coop.cu"]
+SOURCES = ["io.cpp", "api.cu", "k_list.cu", "k_pair.cu", "k_cpim.cu", "k_md.cu", "k_cpim_sym.cu", "k_solve_static.cu", "k_solve_coop.cu",
+           "k_precond.cu"]
 
 
 def nvcc() -> str:

@@ -222,6 +222,7 @@ void capac_options_default(capac_options *o)
     o->matrix_layout = 0;
     o->predictor = 2;
     o->solver_kernel = 0;
+    o->inner_precond = 1;
 }
 
 int capac_create(const capac_desc *d, const capac_options *opt, capac_ctx **out)
@@ -439,6 +440,12 @@ int capac_create(const capac_desc *d, const capac_options *opt, capac_ctx **out)
                         if (c->coop_grid > 0) {
                             c->coop_bp = dalloc<double>(coop_partial_doubles(c->coop_grid));
                             c->coop_bar = dalloc<unsigned char>(coop_barrier_bytes());
+                            if (mixed && o.inner_precond == 1) {
+                                const std::vector<int> g =
+                                    precond_group_atoms(M, d->metal_min, d->rx, d->ry, d->rz);
+                                c->g_atoms = dupload(g.data(), g.size(), s);
+                                c->dinv = dalloc<float>(precond_inverse_floats(M));
+                            }
                         }
                     } else if (mixed) {
                         c->matf = dalloc<float>((size_t)M * 16 * c->Mp);
@@ -496,7 +503,7 @@ int capac_destroy(capac_ctx *c)
                    c->cstr_cnt, c->cstr_i, c->cstr_j, c->cstr_r, c->np_start, c->np_end, c->np_charge,
                    c->nbr, c->nnb, c->cell_key, c->cell_key_sorted, c->atom_ids, c->cell_atoms,
                    c->cell_start, c->spos, c->sort_tmp, c->flags, c->isd, c->vec_ext, c->vec_pq,
-                   c->diag, c->mat, c->matf, c->msym, c->sympart, c->coop_bp, c->coop_bar, c->rres, c->dcorr, c->xprev, c->bw, c->bwf, c->ss, c->partials, c->pot, c->vir, c->th};
+                   c->diag, c->mat, c->matf, c->msym, c->sympart, c->coop_bp, c->coop_bar, c->g_atoms, c->dinv, c->rres, c->dcorr, c->xprev, c->bw, c->bwf, c->ss, c->partials, c->pot, c->vir, c->th};
     for (void *p : dev)
         if (p) cudaFree(p);
     if (c->h_flags) cudaFreeHost(c->h_flags);
@@ -737,6 +744,7 @@ int capac_set(capac_ctx *c, const char *name, const double *in)
         if (cnt > 0) CAPAC_CUDA(cudaMemcpy(p, in, sizeof(double) * cnt, cudaMemcpyHostToDevice));
         if (n == "rx" || n == "ry" || n == "rz") c->list_valid = false;
         if (n == "vec_pq") c->n_solves = 0;  // a new warm start restarts the predictor history
+        if (n == "rx" || n == "ry" || n == "rz") c->precond_age = 0;  // new positions: fresh preconditioner
         count = cnt;
     });
     return st == CAPAC_OK ? count : st;

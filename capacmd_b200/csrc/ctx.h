@@ -152,6 +152,9 @@ struct capac_ctx {
     void *msym = nullptr;        // symmetric packed tiles (float on the mixed path, else double)
     double *sympart = nullptr;   // per-tile partial sums of the symmetric SpMV
     int coop_grid = 0;           // blocks of the persistent solver (0: per-step launches)
+    int *g_atoms = nullptr;      // block-Jacobi groups of 32 metal atoms (mixed path inner solver)
+    float *dinv = nullptr;       // their inverse diagonal blocks, 128 x 128 each
+    long precond_age = 0;        // matrix builds since the inverse blocks were computed
     double *coop_bp = nullptr;   // its per-block dot partials
     void *coop_bar = nullptr;    // its grid barrier
     double *bw = nullptr;        // BiCGSTAB work vectors, 11 * n_mat
@@ -204,6 +207,12 @@ void launch_sym_assemble(capac_ctx *c);
 int sym_reduce_blocks(const capac_ctx *c);
 void launch_sym_spmv(capac_ctx *c, int dot, const double *x, double *y, const double *d1, const double *d2,
                      const SolverScalars *ss);
+void launch_sym_spmv_free(capac_ctx *c, const double *x, double *y);  // FP64, blocks from positions
+// block-Jacobi preconditioner of the mixed path's inner solves (k_precond.cu)
+int precond_groups(int M);
+size_t precond_inverse_floats(int M);
+std::vector<int> precond_group_atoms(int M, int metal_min, const double *rx, const double *ry, const double *rz);
+void launch_block_inverse(capac_ctx *c);
 constexpr int W_Y_SLOT = 7, W_V_SLOT = 4;  // BiCGSTAB work-vector slots used as scratch
 // persistent cooperative solver (k_solve_coop.cu)
 int coop_grid_size(int device, bool mixed);

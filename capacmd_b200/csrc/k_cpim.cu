@@ -217,10 +217,16 @@ __global__ void __launch_bounds__(128) k_cpim_matrix(DevParams P, const double4 
     for (int k = 0; k < 16; ++k) base[(size_t)k * Mp] = (T)e[k];
 }
 
+constexpr long kPrecondEvery = 10;
+
 void launch_cpim_matrix(capac_ctx *c)
 {
     if (c->msym) {
         launch_sym_assemble(c);
+        // the preconditioner only steers the inner solves (the FP64 residual
+        // defines the answer), so its inverse blocks are refreshed every
+        // kPrecondEvery matrix builds, not every step
+        if (c->dinv && c->precond_age++ % kPrecondEvery == 0) launch_block_inverse(c);
         return;
     }
     dim3 grid(grid_for(c->Mp, 128), c->M);
@@ -564,6 +570,10 @@ void launch_cpim_spmv(capac_ctx *c, const double *x, double *y)
 // y = A x with every block recomputed in FP64 from the positions.
 void spmv_free(capac_ctx *c, const double *x, double *y)
 {
+    if (c->sympart) {  // symmetric tiles: every unordered pair once
+        launch_sym_spmv_free(c, x, y);
+        return;
+    }
     const int nb = c->M + c->n_nps;
     ProfScope ps(c, K_RESID);
     k_spmv<DOT_NONE, double, true><<<nb, 256, 0, c->stream>>>(c->P, c->Mp, nullptr, c->pos4, x, y, nullptr, nullptr,

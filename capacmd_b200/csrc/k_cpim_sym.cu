@@ -191,6 +191,88 @@ __global__ void __launch_bounds__(256) k_sym_tiles(int M, int nT, const T *__res
     }
 }
 
+// Matrix-free tile product in FP64 (the mixed path's residual): the same
+// partials as k_sym_tiles with every unordered pair's block recomputed from
+// the positions by cpim_block, so each pair is evaluated once, not twice as in
+// the row-wise matrix-free product.  Thread (a = lane, b = 4 w + k).
+__global__ void __launch_bounds__(256) k_sym_free_tiles(DevParams P, const double4 *__restrict__ pos4, int nT,
+                                                        const double *__restrict__ x, double *__restrict__ part)
+{
+    __shared__ double xr[kT][4], xc[kT][4];
+    __shared__ double4 pr4[kT], pc4[kT];
+    __shared__ double rowacc[8][kT][4];
+    __shared__ double colacc[kT][4];
+    const int M = P.M;
+    const size_t t = blockIdx.x;
+    int I = 0;
+    while (tile_index(I + 1, I + 1, nT) <= t && I + 1 < nT) ++I;
+    const int J = I + (int)(t - tile_index(I, I, nT));
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (threadIdx.x < 2 * kT) {
+        const int side = threadIdx.x >> 5, at = threadIdx.x & 31;
+        const int i = (side ? J : I) * kT + at;
+        const bool in = i < M;
+        double *xv = side ? xc[at] : xr[at];
+        xv[0] = in ? x[3 * i] : 0.0;
+        xv[1] = in ? x[3 * i + 1] : 0.0;
+        xv[2] = in ? x[3 * i + 2] : 0.0;
+        xv[3] = in ? x[3 * M + i] : 0.0;
+        const double4 p = in ? pos4[P.metal_min + i] : make_double4(0, 0, 0, 0);
+        if (side) pc4[at] = p;
+        else pr4[at] = p;
+    }
+    __syncthreads();
+    const int a = lane, i = I * kT + a;
+    double ra[4] = {0.0, 0.0, 0.0, 0.0};
+    double cb[4][4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int b = 4 * w + k, j = J * kT + b;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) cb[k][c] = 0.0;
+        if (i < M && j < M && (I != J || a < b)) {
+            double e[16];
+            cpim_block(P, pr4[a], pc4[b], false, e);
+            const double A[3][3] = {{e[0], e[1], e[2]}, {e[4], e[5], e[6]}, {e[8], e[9], e[10]}};
+            const double m[3] = {e[3], e[7], e[11]};
+            const double C = e[15];
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+                ra[r] += A[r][0] * xc[b][0] + A[r][1] * xc[b][1] + A[r][2] * xc[b][2] + m[r] * xc[b][3];
+            ra[3] += -(m[0] * xc[b][0] + m[1] * xc[b][1] + m[2] * xc[b][2]) + C * xc[b][3];
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+                cb[k][r] = A[r][0] * xr[a][0] + A[r][1] * xr[a][1] + A[r][2] * xr[a][2] - m[r] * xr[a][3];
+            cb[k][3] = m[0] * xr[a][0] + m[1] * xr[a][1] + m[2] * xr[a][2] + C * xr[a][3];
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) cb[k][c] = warp_sum(cb[k][c]);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) rowacc[w][a][c] = ra[c];
+    if (lane == 0) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) colacc[4 * w + k][c] = cb[k][c];
+    }
+    __syncthreads();
+    double *pr = part + ((size_t)I * nT + J) * (kT * 4);
+    double *pc = part + ((size_t)J * nT + I) * (kT * 4);
+    if (threadIdx.x < kT * 4) {
+        const int aa = threadIdx.x >> 2, c = threadIdx.x & 3;
+        double s = 0.0;
+#pragma unroll
+        for (int ww = 0; ww < 8; ++ww) s += rowacc[ww][aa][c];
+        pr[threadIdx.x] = I == J ? s + colacc[aa][c] : s;
+    } else if (I != J) {
+        const int q = threadIdx.x - kT * 4;
+        pc[q] = colacc[q >> 2][q & 3];
+    }
+}
+
 // y = sum of partials + diagonal + neutrality terms; dot epilogue as k_spmv.
 // 512 threads per block row: four groups each add every fourth partial
 // (coalesced 1 KB rows), then the groups are added in a fixed order.
@@ -319,6 +401,17 @@ void launch_sym_spmv(capac_ctx *c, int dot, const double *x, double *y, const do
         k_sym_reduce<2><<<nb, 128 * kReduceGroups, 0, c->stream>>>(c->P, nT, c->sympart, x, y, d1, d2, c->partials, ss);
     else
         k_sym_reduce<0><<<nb, 128 * kReduceGroups, 0, c->stream>>>(c->P, nT, c->sympart, x, y, d1, d2, c->partials, ss);
+    c->launches += 2;
+}
+
+void launch_sym_spmv_free(capac_ctx *c, const double *x, double *y)
+{
+    const int nT = sym_tiles(c->M);
+    const unsigned tiles = (unsigned)(nT * (nT + 1) / 2);
+    ProfScope ps(c, K_RESID);
+    k_sym_free_tiles<<<tiles, 256, 0, c->stream>>>(c->P, c->pos4, nT, x, c->sympart);
+    k_sym_reduce<0><<<(unsigned)(nT + c->n_nps), 128 * kReduceGroups, 0, c->stream>>>(
+        c->P, nT, c->sympart, x, y, nullptr, nullptr, c->partials, nullptr);
     c->launches += 2;
 }
 

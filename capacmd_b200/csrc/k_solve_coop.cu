@@ -178,13 +178,21 @@ struct CoopArgs {
     const int *np_start, *np_end;
     const void *mat;
     double *part;  // nT * nT * 128 tile partials
-    double *bp;    // dot partials: 2 sets of 2 doubles per block
+    double *bp;    // dot partials: 3 sets of kBp doubles per block
     const double *b, *diag;
     double *x, *r0, *r, *s, *t, *y, *z, *K;
     double *p[2], *v[2];
     double tol, skip;
     SolverScalars *ss;
     CoopSync *sync;
+    // block-Jacobi mode (bj != 0): K is the inverse of the diagonal blocks of
+    // nG groups of 32 metal atoms; K r, K v, K t are carried as vectors and
+    // y = K p, z = K s follow from them elementwise (see the kernel)
+    int bj, nG;
+    const int *g_atoms;
+    const float *dinv;
+    double *Kr, *Kv, *Kt;
+    double *yb[2];
 };
 
 namespace {
@@ -307,6 +315,26 @@ struct Ring {
     }
 };
 
+// Block-Jacobi MODE_P, one row: with K r = z - omega K t (K r itself on the
+// first iteration), y = K r + beta (y_old - omega K v); on `store` the row's
+// deferred updates: r = s - omega t, K r, and x += alpha y_old + omega z of
+// the previous iteration.  Returns the new y.
+__device__ __forceinline__ double bj_p_row(const CoopArgs &A, const PassScalars &S, int row, bool store)
+{
+    const double y_old = __ldcg(A.yb[S.cur] + row);
+    const double kr = S.first ? __ldcg(A.Kr + row) : fma(-S.omega, __ldcg(A.Kt + row), __ldcg(A.z + row));
+    const double yn = fma(S.beta, fma(-S.omega, __ldcg(A.Kv + row), y_old), kr);
+    if (store) {
+        if (!S.first) {
+            A.r[row] = fma(-S.omega, __ldcg(A.t + row), __ldcg(A.s + row));
+            A.Kr[row] = kr;
+            A.x[row] += S.alpha * y_old + S.omega * __ldcg(A.z + row);
+        }
+        A.yb[S.cur ^ 1][row] = yn;
+    }
+    return yn;
+}
+
 // Shared arrays of a tile pass (one copy for all pass kinds).  The pass
 // inputs are held in the matrix's type: the products run in FP32 on the
 // FP32 matrix, and every sum across columns or tiles is in FP64.
@@ -334,11 +362,12 @@ __device__ bool tiles_pass(const CoopArgs &A, const PassScalars &S, Ring<T> &rin
         for (int k = blockIdx.x; k < A.n_nps; k += gridDim.x) {
             const int row = A.n4 + k;
             if (MODE == MODE_P) {
-                A.y[row] = p_row(A, S, row, true);
+                if (A.bj) bj_p_row(A, S, row, true);  // K = 1 on the Lagrange rows
+                else A.y[row] = p_row(A, S, row, true);
             } else {
                 const double sn = fma(-S.alpha, __ldcg(A.v[S.cur] + row), __ldcg(A.r + row));
                 A.s[row] = sn;
-                A.z[row] = sn;
+                A.z[row] = A.bj ? fma(-S.alpha, __ldcg(A.Kv + row), __ldcg(A.Kr + row)) : sn;
             }
         }
     }
@@ -367,11 +396,16 @@ __device__ bool tiles_pass(const CoopArgs &A, const PassScalars &S, Ring<T> &rin
                     val = __ldcg(A.x + row);
                 } else if (MODE == MODE_P) {
                     const bool owner = I == J && side == 0;  // the diagonal-tile owner stores block row I
-                    val = __dmul_rn(__ldcg(A.K + row), p_row(A, S, row, owner));
-                    if (owner) A.y[row] = val;
+                    if (A.bj) {
+                        val = bj_p_row(A, S, row, owner);
+                    } else {
+                        val = __dmul_rn(__ldcg(A.K + row), p_row(A, S, row, owner));
+                        if (owner) A.y[row] = val;
+                    }
                 } else {
                     const double sn = fma(-S.alpha, __ldcg(A.v[S.cur] + row), __ldcg(A.r + row));
-                    val = __dmul_rn(__ldcg(A.K + row), sn);
+                    val = A.bj ? fma(-S.alpha, __ldcg(A.Kv + row), __ldcg(A.Kr + row))
+                               : __dmul_rn(__ldcg(A.K + row), sn);
                     if (I == J && side == 0) {
                         A.s[row] = sn;
                         A.z[row] = val;
@@ -471,8 +505,10 @@ __device__ __forceinline__ void reduce_row(const CoopArgs &A, const PassScalars 
     } else {
         A.t[row] = out;
         const double kt = Krow * out, sr = __ldcg(A.s + row), r0 = __ldcg(A.r0 + row);
-        d[0] += kt * in;  // (K t, z)
-        d[1] += kt * kt;
+        if (!A.bj) {  // block-Jacobi: (K t, z), (K t, K t) come from the preconditioner pass
+            d[0] += kt * in;  // (K t, z)
+            d[1] += kt * kt;
+        }
         d[2] += r0 * sr;
         d[3] += r0 * out;
         d[4] += sr * sr;
@@ -491,7 +527,8 @@ template <int RED>
 __device__ void reduce_pass(const CoopArgs &A, const PassScalars &S, double *bp)
 {
     const int M = A.M;
-    const double *in = RED == RED_START ? A.x : (RED == RED_V ? A.y : A.z);
+    // RED_V in block-Jacobi mode: the tile pass just stored y in yb[cur ^ 1]
+    const double *in = RED == RED_START ? A.x : (RED == RED_V ? (A.bj ? A.yb[S.cur ^ 1] : A.y) : A.z);
     double d[7] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
     const long nwork = (long)A.nT * 128 * kGroups;
     const long gthreads = (long)gridDim.x * blockDim.x;
@@ -553,6 +590,60 @@ __device__ void reduce_pass(const CoopArgs &A, const PassScalars &S, double *bp)
     }
 }
 
+// Block-Jacobi application out = K in.  Work item w = (group G, quarter h):
+// rows 32 h .. 32 h + 31 of the group's 128; thread (row, part) sums 16 of
+// the 128 columns (FP32 inverse entries, FP64 products), the 8 parts of a row
+// are combined by shuffles in a fixed order; 4 nG items spread over the grid.
+// The Lagrange rows copy (K = 1).  WITH_DOTS: partials of (out, z),
+// (out, out), i.e. (K t, z) and (K t, K t).
+template <bool WITH_DOTS>
+__device__ void prec_pass(const CoopArgs &A, const double *in, double *out, double *bp)
+{
+    __shared__ double xin[128];
+    const int M = A.M, tid = threadIdx.x;
+    double d[2] = {0.0, 0.0};
+    for (int w = blockIdx.x; w < 4 * A.nG; w += gridDim.x) {
+        const int G = w >> 2, h = w & 3;
+        if (tid < 128) {
+            const int atom = A.g_atoms[G * 32 + (tid >> 2)], comp = tid & 3;
+            xin[tid] = atom >= 0 ? __ldcg(in + (comp < 3 ? 3 * atom + comp : 3 * M + atom)) : 0.0;
+        }
+        __syncthreads();
+        const int o = 32 * h + (tid >> 3), part = tid & 7;
+        const float *col = A.dinv + (size_t)G * 128 * 128 + (size_t)(16 * part) * 128 + o;
+        float m[16];
+#pragma unroll
+        for (int c = 0; c < 16; ++c) m[c] = __ldg(col + (size_t)c * 128);
+        double acc = 0.0;
+#pragma unroll
+        for (int c = 0; c < 16; ++c) acc = fma((double)m[c], xin[16 * part + c], acc);
+        acc += __shfl_xor_sync(0xffffffffu, acc, 1);
+        acc += __shfl_xor_sync(0xffffffffu, acc, 2);
+        acc += __shfl_xor_sync(0xffffffffu, acc, 4);
+        const int atom = A.g_atoms[G * 32 + (o >> 2)], comp = o & 3;
+        if (part == 0 && atom >= 0) {
+            const int row = comp < 3 ? 3 * atom + comp : 3 * M + atom;
+            out[row] = acc;
+            if (WITH_DOTS) {
+                d[0] += acc * __ldcg(A.z + row);
+                d[1] += acc * acc;
+            }
+        }
+        __syncthreads();  // xin free again
+    }
+    if (blockIdx.x == gridDim.x - 1)
+        for (int k = tid; k < A.n_nps; k += blockDim.x) {
+            const int row = A.n4 + k;
+            const double v = __ldcg(in + row);
+            out[row] = v;
+            if (WITH_DOTS) {
+                d[0] += v * __ldcg(A.z + row);
+                d[1] += v * v;
+            }
+        }
+    if (WITH_DOTS) put_bp<2>(bp, d);
+}
+
 template <typename T>
 __host__ __device__ constexpr size_t ring_bytes()
 {
@@ -571,7 +662,7 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? 2 : 1) k_bicgstab_coo
     const long gthreads = (long)gridDim.x * blockDim.x;
     const long tid = (long)blockIdx.x * blockDim.x + threadIdx.x;
     const int nb = gridDim.x;
-    double *bpA = A.bp, *bpB = A.bp + (size_t)kBp * nb;
+    double *bpA = A.bp, *bpB = A.bp + (size_t)kBp * nb, *bpC = A.bp + (size_t)2 * kBp * nb;
 
     Ring<T> ring;
     ring.buf = reinterpret_cast<T *>(ring_smem);
@@ -598,8 +689,9 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? 2 : 1) k_bicgstab_coo
             const double bk = A.b[k];
             pb[0] += bk * bk;
             A.K[k] = k < A.n4 ? 1.0 / A.diag[k] : 1.0;
-            A.p[0][k] = 0.0;
+            A.p[0][k] = 0.0;  // block-Jacobi: the first y buffer
             A.v[0][k] = 0.0;
+            if (A.bj) A.Kv[k] = 0.0;
         }
         put_bp<1>(bpA, pb);
     }
@@ -615,6 +707,10 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? 2 : 1) k_bicgstab_coo
         ok = tiles_pass<T, MODE_X>(A, S, ring, psm) && grid_barrier(A.sync);
         if (ok) reduce_pass<RED_START>(A, S, bpB);
         ok = ok && grid_barrier(A.sync);
+        if (ok && A.bj) {  // K r of the start residual; y = K r on the first iteration
+            prec_pass<false>(A, A.r, A.Kr, nullptr);
+            ok = grid_barrier(A.sync);
+        }
         done = !ok;
     }
     double rho = 0.0, rho_old = 1.0, alpha = 1.0, omega = 1.0;
@@ -637,6 +733,13 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? 2 : 1) k_bicgstab_coo
             ok = false;
             break;
         }
+        if (A.bj) {  // K v
+            prec_pass<false>(A, A.v[0], A.Kv, nullptr);
+            if (!grid_barrier(A.sync)) {
+                ok = false;
+                break;
+            }
+        }
         double r0v[1];
         sum_bp<1>(bpA, nb, r0v);
         const double al = rho / r0v[0];
@@ -654,8 +757,21 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? 2 : 1) k_bicgstab_coo
             ok = false;
             break;
         }
+        if (A.bj) {  // K t with (K t, z), (K t, K t)
+            prec_pass<true>(A, A.t, A.Kt, bpC);
+            if (!grid_barrier(A.sync)) {
+                ok = false;
+                break;
+            }
+        }
         double d[7];
         sum_bp<7>(bpB, nb, d);
+        if (A.bj) {
+            double k2[2];
+            sum_bp<2>(bpC, nb, k2);
+            d[0] = k2[0];
+            d[1] = k2[1];
+        }
         const double om = d[0] / d[1];
         if (!isfinite(om) || om == 0.0) {
             status = rTr < crit * 100.0 ? 1 : -2;
@@ -678,7 +794,7 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? 2 : 1) k_bicgstab_coo
     if (ok && pending) {  // the last update of x, and (r, r) of the final residual
         double q[1] = {0.0};
         for (long k = tid; k < n; k += gthreads) {
-            A.x[k] += alpha * __ldcg(A.y + k) + omega * __ldcg(A.z + k);
+            A.x[k] += alpha * __ldcg((A.bj ? A.yb[S.cur] : A.y) + k) + omega * __ldcg(A.z + k);
             const double rk = __ldcg(A.s + k) - omega * __ldcg(A.t + k);
             A.r[k] = rk;
             q[0] += rk * rk;
@@ -714,7 +830,7 @@ size_t dyn_smem_bytes()
 }  // namespace
 
 size_t coop_barrier_bytes() { return sizeof(CoopSync); }
-size_t coop_partial_doubles(int grid) { return (size_t)2 * kBp * grid; }
+size_t coop_partial_doubles(int grid) { return (size_t)3 * kBp * grid; }
 
 // Launch the persistent solver; returns the status as bicgstab_core does.
 int bicgstab_coop(capac_ctx *c, const double *b, double *x, double tol, double skip)
@@ -745,6 +861,23 @@ int bicgstab_coop(capac_ctx *c, const double *b, double *x, double tol, double s
     // slots the per-step solver uses for A x0 and K t
     A.r0 = W(1); A.r = W(2); A.p[0] = W(3); A.v[0] = W(4); A.s = W(5); A.t = W(6); A.y = W(7); A.z = W(8);
     A.v[1] = W(9); A.K = W(10); A.p[1] = W(0);
+    A.bj = c->dinv != nullptr;
+    A.nG = c->dinv ? precond_groups(c->M) : 0;
+    A.g_atoms = c->g_atoms;
+    A.dinv = c->dinv;
+    A.Kr = A.Kv = A.Kt = nullptr;
+    A.yb[0] = A.yb[1] = nullptr;
+    if (A.bj) {
+        // y double-buffered in the p slots; one v buffer; K v, K t, K r in
+        // the second v slot, the K slot (K is not read) and slot 0
+        A.yb[0] = W(3);
+        A.yb[1] = W(7);
+        A.y = W(7);
+        A.v[1] = A.v[0];
+        A.Kv = W(9);
+        A.Kt = W(10);
+        A.Kr = W(0);
+    }
     A.tol = tol;
     A.skip = skip;
     A.ss = c->ss;

@@ -153,6 +153,8 @@ typedef struct capac_options {
                                order 0 (last solution), 1 (linear), 2 (quadratic, default) or 3 */
     int solver_kernel;      /* BiCGSTAB on the symmetric layout: 0 one persistent cooperative launch per
                                solve when the device supports it (default), 1 a launch per vector step */
+    int inner_precond;      /* mixed path, persistent solver: preconditioner of the inner solves,
+                               0 the reference's Jacobi, 1 block-Jacobi on 32-atom groups (default) */
 } capac_options;
 
 void capac_options_default(capac_options *o);
