@@ -35,6 +35,9 @@ ERR_NO_DEVICE = -8
 PREC_FP64 = 0
 PREC_MIXED = 1
 
+# Metal parameters of capac_param_get/set, in the order of capac_energy_param_grad.
+PARAMS = ("cpff_capac", "cpff_polar", "cpim_rq", "cpim_rp", "qsc_eps", "qsc_c", "qsc_a", "qsc_n", "qsc_m")
+
 
 class CapacError(RuntimeError):
     def __init__(self, code: int, msg: str):
@@ -103,6 +106,10 @@ def lib() -> ctypes.CDLL:
     L.capac_phase_times.argtypes = [vp, dp]
     L.capac_kernel_launches.argtypes = [vp]
     L.capac_kernel_launches.restype = ctypes.c_long
+    L.capac_param_get.argtypes = [vp, cp, dp]
+    L.capac_param_set.argtypes = [vp, cp, ctypes.c_double]
+    L.capac_energy_grad.argtypes = [vp, dp, dp, dp, dp]
+    L.capac_force_match_grad.argtypes = [vp, dp, dp, dp, dp, dp]
     _lib = L
     return L
 
@@ -261,6 +268,37 @@ class Simulation:
 
     def kernel_launches(self) -> int:
         return int(lib().capac_kernel_launches(self._p))
+
+    def param_get(self, name: str) -> float:
+        """A metal parameter by its name in PARAMS (capac_param_get)."""
+        v = ctypes.c_double(0.0)
+        _check(lib().capac_param_get(self._p, name.encode(), ctypes.byref(v)))
+        return v.value
+
+    def param_set(self, name: str, value: float) -> None:
+        """Set a metal parameter; the next force call uses it (capac_param_set)."""
+        _check(lib().capac_param_set(self._p, name.encode(), float(value)))
+
+    def energy_grad(self, positions: bool = True) -> tuple[dict, Optional[np.ndarray]]:
+        """Total dE/dθ (dict over PARAMS, kJ/mol per unit) and dE/dr ((N, 3)
+        kJ/mol/nm, or None) of the last force call (capac_energy_grad)."""
+        g = np.zeros(len(PARAMS))
+        n = self.desc.n_atoms
+        xyz = [np.zeros(n) for _ in range(3)] if positions else [None] * 3
+        ptr = [a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) if a is not None else None for a in xyz]
+        _check(lib().capac_energy_grad(self._p, g.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), *ptr))
+        return dict(zip(PARAMS, g.tolist())), (np.stack(xyz, 1) if positions else None)
+
+    def force_match_grad(self, target: np.ndarray) -> tuple[float, dict]:
+        """Force-matching loss mean((F - target)^2) over atoms and axes and its
+        gradient over PARAMS (capac_force_match_grad); target is (N, 3)."""
+        t = np.ascontiguousarray(np.asarray(target, dtype=np.float64).T)
+        g = np.zeros(len(PARAMS))
+        loss = ctypes.c_double(0.0)
+        dpt = ctypes.POINTER(ctypes.c_double)
+        _check(lib().capac_force_match_grad(self._p, t[0].ctypes.data_as(dpt), t[1].ctypes.data_as(dpt),
+                                            t[2].ctypes.data_as(dpt), ctypes.byref(loss), g.ctypes.data_as(dpt)))
+        return loss.value, dict(zip(PARAMS, g.tolist()))
 
 
 def load(paths: dict) -> Desc:

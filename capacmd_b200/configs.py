@@ -58,6 +58,8 @@ WORKLOADS = {
     "c1_field": Workload("c1_field", [3], 0, 6.0, seed=0, ensemble="nve", steps=1000,
                          efield_vnm=(0.0, 0.0, 0.5)),
     "c2": Workload("c2", [4], 3000, 4.5, seed=1, steps=5000),
+    # the same system without thermostat, for energy-drift measurements
+    "c2_nve": Workload("c2_nve", [4], 3000, 4.5, seed=1, ensemble="nve", steps=5000),
     "c3": Workload("c3", [5, 5], 30000, 9.65, seed=2, steps=2000, efield_vnm=(0.0, 0.0, 0.5),
                    gap_z=1.5),
     "c4": Workload("c4", [3], 1000, 3.1, seed=3, steps=6400),

@@ -54,6 +54,7 @@ void record(capac_ctx *c, int k) { CAPAC_CUDA(cudaEventRecord(c->ev[k], c->strea
 void force(capac_ctx *c, bool solve = true)
 {
     cudaStream_t s = c->stream;
+    c->grad_ready = false;
     record(c, 0);
     launch_list_maintenance(c, false);
     launch_pack_positions(c);
@@ -83,6 +84,7 @@ void force(capac_ctx *c, bool solve = true)
         snprintf(msg, sizeof msg, "Error: bicg_stab not converged. rTr= %e, bTb= %e", c->h_ss->rTr, c->h_ss->bTb);
         throw Error(st, msg);
     }
+    c->grad_ready = solve;
 }
 
 void md_step(capac_ctx *c)
@@ -121,6 +123,11 @@ double *state_array(capac_ctx *c, const std::string &n, int *count)
         {"potential", c->pot, 15}, {"virial", c->vir, 9},
         {"vec_pq", c->vec_pq, c->M > 0 ? c->n_mat : 0}, {"vec_ext", c->vec_ext, c->M > 0 ? c->n_mat : 0},
         {"diag_relay", c->diag, c->M > 0 ? c->n_mat : 0}, {"inv_sqrt_dens", c->isd, c->M},
+        // gradient workspace (k_grad.cu): dE/dx, dPsi/dx, mu, nu of the last gradient call
+        {"adjoint_dedx", c->gw, c->gw ? c->n_mat : 0},
+        {"adjoint_dpsidx", c->gw ? c->gw + c->n_mat : nullptr, c->gw ? c->n_mat : 0},
+        {"adjoint_mu", c->gw ? c->gw + 2 * (size_t)c->n_mat : nullptr, c->gw ? c->n_mat : 0},
+        {"adjoint_nu", c->gw ? c->gw + 3 * (size_t)c->n_mat : nullptr, c->gw ? c->n_mat : 0},
     };
     for (auto &e : tab) {
         if (n == e.nm) {
@@ -373,6 +380,7 @@ int capac_create(const capac_desc *d, const capac_options *opt, capac_ctx **out)
             P.qsc_a = d->qsc_a;
             P.qsc_n = d->qsc_n;
             P.qsc_m = d->qsc_m;
+            if (d->n_metal > 0) param_defaults(c, d);
             for (int a = 0; a < 3; ++a) P.efield[a] = d->efield[a];
             P.type = c->type;
             P.mol_id = c->mol_id;
@@ -503,7 +511,7 @@ int capac_destroy(capac_ctx *c)
                    c->cstr_cnt, c->cstr_i, c->cstr_j, c->cstr_r, c->np_start, c->np_end, c->np_charge,
                    c->nbr, c->nnb, c->cell_key, c->cell_key_sorted, c->atom_ids, c->cell_atoms,
                    c->cell_start, c->spos, c->sort_tmp, c->flags, c->isd, c->vec_ext, c->vec_pq,
-                   c->diag, c->mat, c->matf, c->msym, c->sympart, c->coop_bp, c->coop_bar, c->g_atoms, c->dinv, c->rres, c->dcorr, c->xprev, c->bw, c->bwf, c->ss, c->partials, c->pot, c->vir, c->th};
+                   c->diag, c->mat, c->matf, c->msym, c->sympart, c->coop_bp, c->coop_bar, c->g_atoms, c->dinv, c->gw, c->rres, c->dcorr, c->xprev, c->bw, c->bwf, c->ss, c->partials, c->pot, c->vir, c->th};
     for (void *p : dev)
         if (p) cudaFree(p);
     if (c->h_flags) cudaFreeHost(c->h_flags);
@@ -739,9 +747,11 @@ int capac_set(capac_ctx *c, const char *name, const double *in)
         CAPAC_CUDA(cudaStreamSynchronize(c->stream));
         int cnt = 0;
         double *p = state_array(c, n, &cnt);
-        if (!p || n == "potential" || n == "virial" || n == "inv_sqrt_dens" || n == "diag_relay")
+        if (!p || n == "potential" || n == "virial" || n == "inv_sqrt_dens" || n == "diag_relay" ||
+            n.rfind("adjoint_", 0) == 0)
             throw Error(CAPAC_ERR_INVALID, "array " + n + " cannot be set");
         if (cnt > 0) CAPAC_CUDA(cudaMemcpy(p, in, sizeof(double) * cnt, cudaMemcpyHostToDevice));
+        if (n == "rx" || n == "ry" || n == "rz" || n == "vec_pq") c->grad_ready = false;
         if (n == "rx" || n == "ry" || n == "rz") c->list_valid = false;
         if (n == "vec_pq") c->n_solves = 0;  // a new warm start restarts the predictor history
         if (n == "rx" || n == "ry" || n == "rz") c->precond_age = 0;  // new positions: fresh preconditioner

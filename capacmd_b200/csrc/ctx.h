@@ -37,7 +37,7 @@ struct DevParams {
     double inv_rc12, inv_rc6, w_alpha, w_a2_sqrtpi, w_const, w_erfc_arcut;
     double inv_polar, inv_capac, inv_r_qq, inv_r_pq, inv_r_pp;
     double qsc_eps, qsc_c, qsc_a;
-    int qsc_n, qsc_m;
+    double qsc_n, qsc_m;  // integers in the reference's input; reals for parameter gradients
     double efield[3];
     // per atom
     const int *type, *mol_id, *mol_type, *atom_in_mol;
@@ -155,6 +155,12 @@ struct capac_ctx {
     int *g_atoms = nullptr;      // block-Jacobi groups of 32 metal atoms (mixed path inner solver)
     float *dinv = nullptr;       // their inverse diagonal blocks, 128 x 128 each
     long precond_age = 0;        // matrix builds since the inverse blocks were computed
+    // the metal's CPIM parameters (a.u.) and Gaussian widths (Bohr), which the
+    // widths follow unless set on their own (k_grad.cu)
+    double capac = 0.0, polar = 0.0, rq = 0.0, rp = 0.0;
+    bool rq_tied = true, rp_tied = true;  // widths derived from capac / polar
+    bool grad_ready = false;              // the state is that of a force call with a solve
+    double *gw = nullptr;                 // gradient workspace (k_grad.cu), allocated on first use
     double *coop_bp = nullptr;   // its per-block dot partials
     void *coop_bar = nullptr;    // its grid barrier
     double *bw = nullptr;        // BiCGSTAB work vectors, 11 * n_mat
@@ -213,6 +219,9 @@ int precond_groups(int M);
 size_t precond_inverse_floats(int M);
 std::vector<int> precond_group_atoms(int M, int metal_min, const double *rx, const double *ry, const double *rz);
 void launch_block_inverse(capac_ctx *c);
+void param_defaults(capac_ctx *c, const capac_desc *d);  // k_grad.cu
+void spmv_free(capac_ctx *c, const double *x, double *y);  // FP64 A x with blocks from positions
+int bicgstab_core(capac_ctx *c, const double *b, double *x, double tol, double skip);
 constexpr int W_Y_SLOT = 7, W_V_SLOT = 4;  // BiCGSTAB work-vector slots used as scratch
 // persistent cooperative solver (k_solve_coop.cu)
 int coop_grid_size(int device, bool mixed);

@@ -66,7 +66,7 @@ __global__ void __launch_bounds__(256) k_qsc_density(DevParams P, const double4 
         double dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
         image(dx, dy, dz, P.box);
         const double r2 = norm2_exact(dx, dy, dz);
-        if (r2 < P.rc2) rho += pow(P.qsc_a / sqrt(r2), (double)P.qsc_m);
+        if (r2 < P.rc2) rho += pow(P.qsc_a / sqrt(r2), P.qsc_m);
     }
     rho = warp_sum(rho);
     if (lane == 0) isd[i] = 1.0 / sqrt(rho);
@@ -93,7 +93,7 @@ __global__ void __launch_bounds__(256) k_qsc_force(DevParams P, const double4 *_
             const double r2 = norm2_exact(dx, dy, dz);
             if (r2 >= P.rc2) continue;
             const double r = sqrt(r2), ar = P.qsc_a / r;
-            const double an = pow(ar, (double)P.qsc_n), am = pow(ar, (double)P.qsc_m);
+            const double an = pow(ar, P.qsc_n), am = pow(ar, P.qsc_m);
             const double f = P.qsc_eps * (P.qsc_n * an - cm2 * (isd[i] + isd[j]) * am) / r2;
             const double gx = f * dx, gy = f * dy, gz = f * dz;
             f0 -= gx; f1 -= gy; f2 -= gz;
@@ -998,6 +998,7 @@ size_t partials_needed(const capac_ctx *c)
     need = std::max(need, (size_t)(c->M + c->n_nps + 8) * 16);
     need = std::max(need, (size_t)grid_for((long)c->n_mols, 256) * 16);
     need = std::max(need, (size_t)grid_for((long)c->n_mat, 256) * 4);
+    need = std::max(need, (size_t)c->M * 20);  // gradient sums (k_grad.cu)
     return need + 64;
 }
 

@@ -230,7 +230,10 @@ int capac_md_init(capac_ctx *ctx);
 /* State transfer.  Names for per-atom arrays (n_atoms doubles):
  * rx ry rz vx vy vz fx fy fz.  Others: potential(15) virial(9) vec_pq vec_ext
  * diag_relay (n_mat) inv_sqrt_dens(n_metal) vQ(10) thermo(4: eKsum inst_temp
- * ref_temp ndf) box(6).  capac_get returns the count written, <0 on error. */
+ * ref_temp ndf) box(6); after a gradient call (read only, n_mat each):
+ * adjoint_dedx (dE/dx), adjoint_dpsidx (dPsi/dx of the force matching),
+ * adjoint_mu, adjoint_nu (the adjoint solutions).  capac_get returns the
+ * count written, <0 on error. */
 int capac_get(capac_ctx *ctx, const char *name, double *out);
 int capac_set(capac_ctx *ctx, const char *name, const double *in);
 
@@ -277,6 +280,37 @@ int capac_time_md_steps(capac_ctx *ctx, int n_steps, double *ms);
  * total_ms 0). */
 int capac_profile_enable(capac_ctx *ctx, int on);
 int capac_profile_get(capac_ctx *ctx, const char *cls, long *launches, double *total_ms);
+
+/* Metal parameters for fitting (no counterpart in the reference, which reads
+ * them once from param.txt: file.c:533-549).  Names: "cpff_capac",
+ * "cpff_polar" (a.u.), "cpim_rq", "cpim_rp" (the Gaussian widths in Bohr;
+ * each follows its parameter the way the reference derives it,
+ * mpi-main.c:315-323, until it is set on its own; setting it to 0 ties it
+ * again), "qsc_eps", "qsc_c", "qsc_a",
+ * "qsc_n", "qsc_m" (Sutton-Chen, force.c:385-542; n and m may be real).
+ * A change takes effect at the next force call. */
+int capac_param_get(capac_ctx *ctx, const char *name, double *value);
+int capac_param_set(capac_ctx *ctx, const char *name, double value);
+
+/* Gradients of the state of the last force call (which must have solved the
+ * CPIM system, with no change of positions, induced vector or parameters
+ * since).  E is the sum of the energy terms potential[1..14] (force.c
+ * sum_potential); x the induced vector.  The reference's forces are -dE/dr
+ * at fixed x (cpff.c:526-950), and E is not stationary in x at the solution,
+ * so the total derivatives below include the response of the CPIM solve,
+ * computed with the adjoint system A mu = dE/dx (one extra solve).
+ *
+ * capac_energy_grad: dE/dtheta for the nine parameters above, in that order
+ * (kJ/mol per unit), and dE/dr (kJ/mol/nm, n_atoms each); pass NULL for
+ * what is not wanted.  For a system without CPIM dE/dr = -F.
+ *
+ * capac_force_match_grad: L = sum over atoms and axes of
+ * (F - F_target)^2 / (3 n_atoms) for the given target forces (host arrays,
+ * n_atoms each), and dL/dtheta for the nine parameters (second-order
+ * adjoint: one extra solve, Hessian-vector products by dual numbers). */
+int capac_energy_grad(capac_ctx *ctx, double grad[9], double *gx, double *gy, double *gz);
+int capac_force_match_grad(capac_ctx *ctx, const double *tfx, const double *tfy, const double *tfz,
+                           double *loss, double grad[9]);
 
 #ifdef __cplusplus
 }
