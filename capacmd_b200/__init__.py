@@ -109,7 +109,7 @@ def lib() -> ctypes.CDLL:
     L.capac_param_get.argtypes = [vp, cp, dp]
     L.capac_param_set.argtypes = [vp, cp, ctypes.c_double]
     L.capac_energy_grad.argtypes = [vp, dp, dp, dp, dp]
-    L.capac_force_match_grad.argtypes = [vp, dp, dp, dp, dp, dp]
+    L.capac_force_match_grad.argtypes = [vp, dp, dp, dp, dp, dp, dp, dp, dp]
     _lib = L
     return L
 
@@ -289,15 +289,22 @@ class Simulation:
         _check(lib().capac_energy_grad(self._p, g.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), *ptr))
         return dict(zip(PARAMS, g.tolist())), (np.stack(xyz, 1) if positions else None)
 
-    def force_match_grad(self, target: np.ndarray) -> tuple[float, dict]:
-        """Force-matching loss mean((F - target)^2) over atoms and axes and its
-        gradient over PARAMS (capac_force_match_grad); target is (N, 3)."""
+    def force_match_grad(self, target: np.ndarray, positions: bool = False):
+        """Force-matching loss mean((F - target)^2) over atoms and axes, its
+        gradient over PARAMS and, with positions=True, dL/dr as (N, 3)
+        (capac_force_match_grad); target is (N, 3)."""
         t = np.ascontiguousarray(np.asarray(target, dtype=np.float64).T)
         g = np.zeros(len(PARAMS))
         loss = ctypes.c_double(0.0)
         dpt = ctypes.POINTER(ctypes.c_double)
+        n = self.desc.n_atoms
+        xyz = [np.zeros(n) for _ in range(3)] if positions else [None] * 3
+        ptr = [a.ctypes.data_as(dpt) if a is not None else None for a in xyz]
         _check(lib().capac_force_match_grad(self._p, t[0].ctypes.data_as(dpt), t[1].ctypes.data_as(dpt),
-                                            t[2].ctypes.data_as(dpt), ctypes.byref(loss), g.ctypes.data_as(dpt)))
+                                            t[2].ctypes.data_as(dpt), ctypes.byref(loss), g.ctypes.data_as(dpt),
+                                            *ptr))
+        if positions:
+            return loss.value, dict(zip(PARAMS, g.tolist())), np.stack(xyz, 1)
         return loss.value, dict(zip(PARAMS, g.tolist()))
 
 

@@ -222,6 +222,8 @@ void launch_block_inverse(capac_ctx *c);
 void param_defaults(capac_ctx *c, const capac_desc *d);  // k_grad.cu
 void spmv_free(capac_ctx *c, const double *x, double *y);  // FP64 A x with blocks from positions
 int bicgstab_core(capac_ctx *c, const double *b, double *x, double tol, double skip);
+void launch_force_derivative(capac_ctx *c, const double *wdir, double *dfx, double *dfy, double *dfz, double *isd_v,
+                             double *isd_d);  // k_grad_forces.cu
 constexpr int W_Y_SLOT = 7, W_V_SLOT = 4;  // BiCGSTAB work-vector slots used as scratch
 // persistent cooperative solver (k_solve_coop.cu)
 int coop_grid_size(int device, bool mixed);

@@ -97,6 +97,33 @@ __host__ __device__ constexpr int width() { return std::is_same<T, Dual>::value 
 
 // Minimum image of a difference: the shift is decided on the values, as in
 // the force kernels, and does not change the derivative.
+template <class T>
+__device__ __forceinline__ T zero() { return lift<T>(0.0, 0.0); }
+
+template <class T>
+__device__ __forceinline__ T warp_sum_t(T v)
+{
+    if constexpr (std::is_same<T, Dual>::value) return Dual{warp_sum(v.v), warp_sum(v.d)};
+    else return warp_sum(v);
+}
+
+// Position of atom a; for Dual, with derivative wdir[3a .. 3a+2].
+template <class T>
+__device__ __forceinline__ void load_pos(const double4 *__restrict__ pos4, const double *__restrict__ wdir, int a,
+                                         T (&r)[3])
+{
+    const double4 p = pos4[a];
+    if constexpr (std::is_same<T, Dual>::value) {
+        r[0] = Dual{p.x, wdir[3 * a]};
+        r[1] = Dual{p.y, wdir[3 * a + 1]};
+        r[2] = Dual{p.z, wdir[3 * a + 2]};
+    } else {
+        r[0] = p.x;
+        r[1] = p.y;
+        r[2] = p.z;
+    }
+}
+
 __device__ __forceinline__ void set_val(double &a, double v) { a = v; }
 __device__ __forceinline__ void set_val(Dual &a, double v) { a.v = v; }
 

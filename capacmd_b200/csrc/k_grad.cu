@@ -52,32 +52,6 @@ constexpr double kPi = 3.14159265358979323846;
 constexpr double kAdjointTol = 1.0e-12;
 constexpr int kAdjointSweeps = 24;
 
-template <class T>
-__device__ __forceinline__ T zero() { return lift<T>(0.0, 0.0); }
-
-template <class T>
-__device__ __forceinline__ void load_pos(const double4 *__restrict__ pos4, const double *__restrict__ wdir, int a,
-                                         T (&r)[3])
-{
-    const double4 p = pos4[a];
-    if constexpr (std::is_same<T, Dual>::value) {
-        r[0] = Dual{p.x, wdir[3 * a]};
-        r[1] = Dual{p.y, wdir[3 * a + 1]};
-        r[2] = Dual{p.z, wdir[3 * a + 2]};
-    } else {
-        r[0] = p.x;
-        r[1] = p.y;
-        r[2] = p.z;
-    }
-}
-
-template <class T>
-__device__ __forceinline__ T warp_sum_t(T v)
-{
-    if constexpr (std::is_same<T, Dual>::value) return Dual{warp_sum(v.v), warp_sum(v.d)};
-    else return warp_sum(v);
-}
-
 // block_sum over T values; `sh` needs 32 * K * width<T>() doubles.
 template <class T, int K>
 __device__ __forceinline__ void block_sum_t(T (&v)[K], double *sh)
@@ -375,15 +349,15 @@ __device__ __forceinline__ void grad_block_form(const DevParams &P, const double
     }
 }
 
-// Adds -d/dr [mu^T (A(r) x - b(r))] to (gx, gy, gz): block per metal atom i;
+// Adds -scale d/dr [mu^T (A(r) x - b(r))] to (gx, gy, gz): block per metal atom i;
 // the metal atom's own entry is written by its block, the permanent charges
 // within its cut-off receive theirs by atomic adds.
 __global__ void __launch_bounds__(256) k_cpim_adjoint_positions(DevParams P, const double4 *__restrict__ pos4,
                                                                 const uint32_t *__restrict__ nbr,
                                                                 const int *__restrict__ nnb, int cap,
                                                                 const double *__restrict__ x,
-                                                                const double *__restrict__ mu, double *gx,
-                                                                double *gy, double *gz)
+                                                                const double *__restrict__ mu, double scale,
+                                                                double *gx, double *gy, double *gz)
 {
     __shared__ double sh[32 * 3];
     const int i = blockIdx.x, M = P.M, im = P.metal_min + i;
@@ -427,18 +401,18 @@ __global__ void __launch_bounds__(256) k_cpim_adjoint_positions(DevParams P, con
 #pragma unroll
         for (int a = 0; a < 3; ++a) acc[a] -= kConvV * f[a];
         // dPhi/dr_j = +kConvV f; the gradient takes -dPhi/dr_j
-        atomicAdd(gx + j, -kConvV * f[0]);
-        atomicAdd(gy + j, -kConvV * f[1]);
-        atomicAdd(gz + j, -kConvV * f[2]);
+        atomicAdd(gx + j, -scale * kConvV * f[0]);
+        atomicAdd(gy + j, -scale * kConvV * f[1]);
+        atomicAdd(gz + j, -scale * kConvV * f[2]);
     }
     block_sum<3>(acc, sh);
     if (threadIdx.x == 0) {
         // b_q includes -E_ext . r_i (cpff.c:176-183)
 #pragma unroll
         for (int a = 0; a < 3; ++a) acc[a] += kConvV * mqi * P.efield[a];
-        gx[im] -= acc[0];
-        gy[im] -= acc[1];
-        gz[im] -= acc[2];
+        gx[im] -= scale * acc[0];
+        gy[im] -= scale * acc[1];
+        gz[im] -= scale * acc[2];
     }
 }
 
@@ -699,6 +673,8 @@ int capac_param_get(capac_ctx *c, const char *name, double *value)
         else if (n == "cpff_polar") *value = c->polar;
         else if (n == "cpim_rq") *value = c->rq;
         else if (n == "cpim_rp") *value = c->rp;
+        else if (n == "cpim_rq_tied") *value = c->rq_tied ? 1.0 : 0.0;
+        else if (n == "cpim_rp_tied") *value = c->rp_tied ? 1.0 : 0.0;
         else if (n == "qsc_eps") *value = c->P.qsc_eps;
         else if (n == "qsc_c") *value = c->P.qsc_c;
         else if (n == "qsc_a") *value = c->P.qsc_a;
@@ -783,7 +759,7 @@ int capac_energy_grad(capac_ctx *c, double *grad, double *gx, double *gy, double
             }
             if (pos) {
                 k_cpim_adjoint_positions<<<c->M, 256, 0, s>>>(c->P, c->pos4, c->nbr, c->nnb, c->cap, c->vec_pq, mu,
-                                                              dgx, dgy, dgz);
+                                                              1.0, dgx, dgy, dgz);
                 ++c->launches;
             }
         }
@@ -800,12 +776,13 @@ int capac_energy_grad(capac_ctx *c, double *grad, double *gx, double *gy, double
 }
 
 int capac_force_match_grad(capac_ctx *c, const double *tfx, const double *tfy, const double *tfz, double *loss,
-                           double *grad)
+                           double *grad, double *gx, double *gy, double *gz)
 {
     return guard([&] {
         need_ctx(c);
         need_state(c);
-        if (!tfx || !tfy || !tfz || !loss || !grad) throw Error(CAPAC_ERR_INVALID, "null argument");
+        if (!tfx || !tfy || !tfz || !loss) throw Error(CAPAC_ERR_INVALID, "null argument");
+        const bool pos = gx && gy && gz;
         ensure_workspace(c);
         cudaStream_t s = c->stream;
         const int N = c->N;
@@ -820,15 +797,18 @@ int capac_force_match_grad(capac_ctx *c, const double *tfx, const double *tfy, c
         ++c->launches;
         *loss = host_sums(c->partials, (int)nb, 1, s)[0] / (3.0 * N);
         double out[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-        if (c->M > 0) {
+        if (grad && c->M > 0) {
             const std::vector<double> S = qsc_sums(c, true);  // [4..7]: derivatives along w
             qsc_grad(c, S.data() + 4, out + 4);
             for (int k = 4; k < 9; ++k) out[k] = -out[k];
         }
-        if (c->M > 0 && c->use_cpff) {
+        const bool cpim = c->M > 0 && c->use_cpff;
+        double *nu = gw_vec(c, GW_NU);
+        if (cpim) {
             launch_dx(c, true);  // GW_GD = dPsi/dx
-            double *nu = gw_vec(c, GW_NU);
             adjoint_solve(c, gw_vec(c, GW_GD), nu);
+        }
+        if (grad && cpim) {
             const std::vector<double> v = cpim_sums(c, nu, true);  // [0..9] values with nu, [10..19] derivatives
             // dPsi/dphi = dPsi/dphi|_x - nu^T (dA/dphi) x; dL/dphi = -dPsi/dphi
             const double dpsi[5] = {kFqqAu1 * v[10] - v[3], kFqqAu1 * v[11] - v[4], kFqqAu1 * v[12] - v[5], v[8],
@@ -837,7 +817,24 @@ int capac_force_match_grad(capac_ctx *c, const double *tfx, const double *tfy, c
             for (int k = 0; k < 5; ++k) prim[k] = -dpsi[k];
             chain_cpim(c, prim, out);
         }
-        for (int k = 0; k < 9; ++k) grad[k] = out[k];
+        if (grad)
+            for (int k = 0; k < 9; ++k) grad[k] = out[k];
+        if (pos) {
+            // dL/dr = -dPsi/dr|_x + d/dr [nu^T (A x - b)] = dF/de (along w) + dPhi_nu/dr;
+            // the targets are no longer needed: their planes take the gradient
+            double *dgx = tf, *dgy = tf + N, *dgz = tf + 2 * (size_t)N;
+            CAPAC_CUDA(cudaMemsetAsync(tf, 0, sizeof(double) * 3 * (size_t)N, s));
+            launch_force_derivative(c, gw_dir(c), dgx, dgy, dgz, gw_vec(c, GW_R), gw_vec(c, GW_D));
+            if (cpim) {
+                k_cpim_adjoint_positions<<<c->M, 256, 0, s>>>(c->P, c->pos4, c->nbr, c->nnb, c->cap, c->vec_pq, nu,
+                                                              -1.0, dgx, dgy, dgz);
+                ++c->launches;
+            }
+            CAPAC_CUDA(cudaMemcpyAsync(gx, dgx, bytes, cudaMemcpyDeviceToHost, s));
+            CAPAC_CUDA(cudaMemcpyAsync(gy, dgy, bytes, cudaMemcpyDeviceToHost, s));
+            CAPAC_CUDA(cudaMemcpyAsync(gz, dgz, bytes, cudaMemcpyDeviceToHost, s));
+            CAPAC_CUDA(cudaStreamSynchronize(s));
+        }
     });
 }
 

@@ -286,7 +286,8 @@ int capac_profile_get(capac_ctx *ctx, const char *cls, long *launches, double *t
  * "cpff_polar" (a.u.), "cpim_rq", "cpim_rp" (the Gaussian widths in Bohr;
  * each follows its parameter the way the reference derives it,
  * mpi-main.c:315-323, until it is set on its own; setting it to 0 ties it
- * again), "qsc_eps", "qsc_c", "qsc_a",
+ * again; "cpim_rq_tied" and "cpim_rp_tied" read 1 while tied), "qsc_eps",
+ * "qsc_c", "qsc_a",
  * "qsc_n", "qsc_m" (Sutton-Chen, force.c:385-542; n and m may be real).
  * A change takes effect at the next force call. */
 int capac_param_get(capac_ctx *ctx, const char *name, double *value);
@@ -306,11 +307,13 @@ int capac_param_set(capac_ctx *ctx, const char *name, double value);
  *
  * capac_force_match_grad: L = sum over atoms and axes of
  * (F - F_target)^2 / (3 n_atoms) for the given target forces (host arrays,
- * n_atoms each), and dL/dtheta for the nine parameters (second-order
- * adjoint: one extra solve, Hessian-vector products by dual numbers). */
+ * n_atoms each), dL/dtheta for the nine parameters and dL/dr (n_atoms each);
+ * grad or the position arrays may be NULL.  Second-order adjoint: one extra
+ * solve, and Hessian-vector products of every force term recomputed on dual
+ * numbers from the neighbour list. */
 int capac_energy_grad(capac_ctx *ctx, double grad[9], double *gx, double *gy, double *gz);
 int capac_force_match_grad(capac_ctx *ctx, const double *tfx, const double *tfy, const double *tfz,
-                           double *loss, double grad[9]);
+                           double *loss, double grad[9], double *gx, double *gy, double *gz);
 
 #ifdef __cplusplus
 }
