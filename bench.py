@@ -311,6 +311,7 @@ def main() -> int:
         compare, accuracy = compare_arms(args, cm, desc, sim, prec, local)
         if args.drift_steps > 0:
             accuracy["nve_drift"] = nve_drift(cm, configs, args.drift_steps, local)
+        accuracy["gradients"] = gradient_timing(cm, configs, local)
 
     # end to end through the drop-in mpi_force with pinned host buffers
     e2e = None
@@ -440,6 +441,45 @@ def nve_drift(cm, configs, steps: int, device: int, every: int = 10) -> dict:
                      "rms_fluctuation": float(np.std(np.array(e) - np.polyval(np.polyfit(t, e, 1), t))),
                      "e_start": float(e[0])}
         s.close()
+    return out
+
+
+def gradient_timing(cm, configs, device: int, calls: int = 10) -> dict:
+    """Wall time per gradient call on the 3.1k-atom system (Au147 + 1,000
+    waters): one mixed-precision force evaluation with a solve from zero,
+    then capac_energy_grad (parameters and positions) or
+    capac_force_match_grad (parameters and positions); each call includes its
+    adjoint solve and the host copies of its results."""
+    d = cm.Desc.from_paths(configs.cached("c4"))
+    s = cm.Simulation(d, precision=cm.PREC_MIXED, device=device)
+    zero = np.zeros(d.n_mat)
+
+    def fresh():
+        s.set("vec_pq", zero)
+        s.force()
+
+    fresh()
+    target = s.forces() * 1.05
+    out = {"workload": f"Au147 + 1,000 waters ({d.n_atoms:,} atoms), mixed forward", "unit": "ms per call"}
+    for name, fn in (("force", lambda: None), ("energy_grad", lambda: s.energy_grad()),
+                     ("force_match_grad", lambda: s.force_match_grad(target, positions=True))):
+        fresh()
+        fn()  # warm-up (workspace, graphs)
+        t = []
+        for _ in range(calls):
+            fresh()
+            t0 = time.perf_counter()
+            fn()
+            t.append(time.perf_counter() - t0)
+        out[name] = statistics.median(t) * 1e3
+    t = []
+    for _ in range(calls):
+        s.set("vec_pq", zero)
+        t0 = time.perf_counter()
+        s.force()
+        t.append(time.perf_counter() - t0)
+    out["force"] = statistics.median(t) * 1e3
+    s.close()
     return out
 
 
