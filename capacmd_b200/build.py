@@ -18,6 +18,7 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 OBJ = os.path.join(ROOT, "build", "obj")
 LIB = os.path.join(PKG, "libcapacmd_gpu.so")
+DRIVER = os.path.join(PKG, "capacmd-gpu")
 REF_SRC = "/root/reference"
 
 SOURCES = ["io.cpp", "api.cu", "k_list.cu", "k_pair.cu", "k_cpim.cu", "k_md.cu", "k_cpim_sym.cu", "k_solve_static.cu", "k_solve_coop.cu",
@@ -65,6 +66,20 @@ def build_library(verbose: bool = False) -> str:
     return LIB
 
 
+def build_driver(verbose: bool = False) -> str:
+    """The resident driver (reference command line and files, run on the GPU)."""
+    src = os.path.join(PKG, "driver", "capacmd_gpu.cpp")
+    deps = [src, LIB, os.path.join(ROOT, "include", "capacmd.h")]
+    if os.path.exists(DRIVER) and os.path.getmtime(DRIVER) >= max(os.path.getmtime(d) for d in deps):
+        return DRIVER
+    cmd = ["g++", "-O2", "-std=c++17", "-Wall", f"-I{os.path.join(ROOT, 'include')}", src, "-o", DRIVER,
+           f"-L{PKG}", "-lcapacmd_gpu", "-Wl,-rpath,$ORIGIN"]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+    return DRIVER
+
+
 def build_oracle(verbose: bool = False) -> None:
     """Compile the C restatement and, where its sources exist, the reference."""
     odir = os.path.join(ROOT, "oracle")
@@ -79,6 +94,7 @@ def build_oracle(verbose: bool = False) -> None:
 def main() -> int:
     verbose = "-v" in sys.argv
     build_library(verbose)
+    build_driver(verbose)
     build_oracle(verbose)
     print(LIB)
     return 0

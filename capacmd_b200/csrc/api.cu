@@ -282,6 +282,9 @@ int capac_create(const capac_desc *d, const capac_options *opt, capac_ctx **out)
             c->n_save = d->n_save > 0 ? d->n_save : 1;
             c->n_heating = d->n_heating;
             c->dt = d->dt;
+            c->run_type = d->run_type;
+            c->em_length = d->em_length;
+            c->em_tol = d->em_tol;
             c->metal_min = d->metal_min;
             c->has_cstr = d->n_cstr_total > 0;
             CAPAC_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
@@ -511,7 +514,7 @@ int capac_destroy(capac_ctx *c)
                    c->cstr_cnt, c->cstr_i, c->cstr_j, c->cstr_r, c->np_start, c->np_end, c->np_charge,
                    c->nbr, c->nnb, c->cell_key, c->cell_key_sorted, c->atom_ids, c->cell_atoms,
                    c->cell_start, c->spos, c->sort_tmp, c->flags, c->isd, c->vec_ext, c->vec_pq,
-                   c->diag, c->mat, c->matf, c->msym, c->sympart, c->coop_bp, c->coop_bar, c->g_atoms, c->dinv, c->gw, c->rres, c->dcorr, c->xprev, c->bw, c->bwf, c->ss, c->partials, c->pot, c->vir, c->th};
+                   c->diag, c->mat, c->matf, c->msym, c->sympart, c->coop_bp, c->coop_bar, c->g_atoms, c->dinv, c->gw, c->em_buf, c->rres, c->dcorr, c->xprev, c->bw, c->bwf, c->ss, c->partials, c->pot, c->vir, c->th};
     for (void *p : dev)
         if (p) cudaFree(p);
     if (c->h_flags) cudaFreeHost(c->h_flags);
@@ -677,6 +680,193 @@ int capac_md_init(capac_ctx *c)
         launch_fmax_rms(c);
         CAPAC_CUDA(cudaStreamSynchronize(c->stream));
         c->md_step = 0;
+    });
+}
+
+int capac_em_init(capac_ctx *c)
+{
+    return guard([&] {
+        check_ctx(c);
+        const size_t N = c->N;
+        if (!c->em_buf) c->em_buf = dalloc<double>(6 * N);
+        // s = F, old F = F (mpi-main.c:716-727); thermostat velocities zero
+        CAPAC_CUDA(cudaMemcpyAsync(c->em_buf, c->fx, sizeof(double) * N, cudaMemcpyDeviceToDevice, c->stream));
+        CAPAC_CUDA(cudaMemcpyAsync(c->em_buf + N, c->fy, sizeof(double) * N, cudaMemcpyDeviceToDevice, c->stream));
+        CAPAC_CUDA(cudaMemcpyAsync(c->em_buf + 2 * N, c->fz, sizeof(double) * N, cudaMemcpyDeviceToDevice,
+                                   c->stream));
+        CAPAC_CUDA(cudaMemcpyAsync(c->em_buf + 3 * N, c->em_buf, sizeof(double) * 3 * N, cudaMemcpyDeviceToDevice,
+                                   c->stream));
+        CAPAC_CUDA(cudaMemcpyAsync(c->h_th, c->th, sizeof(ThermoState), cudaMemcpyDeviceToHost, c->stream));
+        CAPAC_CUDA(cudaStreamSynchronize(c->stream));
+        for (double &v : c->h_th->vQ) v = 0.0;
+        CAPAC_CUDA(cudaMemcpyAsync(c->th, c->h_th, sizeof(ThermoState), cudaMemcpyHostToDevice, c->stream));
+        CAPAC_CUDA(cudaStreamSynchronize(c->stream));
+        c->em_step = 0;
+    });
+}
+
+int capac_em_step(capac_ctx *c, capac_em_status *out)
+{
+    return guard([&] {
+        check_ctx(c);
+        if (!c->em_buf) throw Error(CAPAC_ERR_INVALID, "capac_em_init has not been called");
+        cudaStream_t s = c->stream;
+        double old_pot = 0.0;
+        CAPAC_CUDA(cudaMemcpy(&old_pot, c->pot, sizeof(double), cudaMemcpyDeviceToHost));
+        // move along s, constrain, zero the velocities (mpi-main.c:730-763)
+        launch_em_move(c);
+        launch_rattle(c, 0);
+        CAPAC_CUDA(cudaMemsetAsync(c->vx, 0, sizeof(double) * c->N, s));
+        CAPAC_CUDA(cudaMemsetAsync(c->vy, 0, sizeof(double) * c->N, s));
+        CAPAC_CUDA(cudaMemsetAsync(c->vz, 0, sizeof(double) * c->N, s));
+        force(c);
+        check_flags(c);
+        launch_sum_potential(c);
+        launch_fmax_rms(c);
+        double pot0 = 0.0;
+        CAPAC_CUDA(cudaMemcpyAsync(&pot0, c->pot, sizeof(double), cudaMemcpyDeviceToHost, s));
+        CAPAC_CUDA(cudaMemcpyAsync(c->h_th, c->th, sizeof(ThermoState), cudaMemcpyDeviceToHost, s));
+        CAPAC_CUDA(cudaStreamSynchronize(s));
+        const double fmax = c->h_th->fmax, frms = c->h_th->frms;
+        // step length and convergence (mpi-main.c:770-816)
+        const double delta = pot0 - old_pot;
+        c->em_length *= delta <= 0.0 ? 1.2 : 0.2;
+        const bool converged = fmax < c->em_tol && frms < c->em_tol * 0.5 && fabs(delta) < c->em_tol * 0.1;
+        ++c->em_step;
+        if (!converged) {
+            double gamma = 0.0;  // steepest descent
+            if (c->run_type == CAPAC_RUN_CG) {
+                const unsigned nb = grid_for(c->N, 256);
+                launch_em_dots(c);
+                std::vector<double> h((size_t)nb * 3);
+                CAPAC_CUDA(cudaMemcpyAsync(h.data(), c->partials, sizeof(double) * h.size(), cudaMemcpyDeviceToHost,
+                                           s));
+                CAPAC_CUDA(cudaStreamSynchronize(s));
+                double g22 = 0.0, g12 = 0.0, g11 = 0.0;
+                for (unsigned b = 0; b < nb; ++b) {
+                    g22 += h[3 * b];
+                    g12 += h[3 * b + 1];
+                    g11 += h[3 * b + 2];
+                }
+                gamma = (g22 - g12) / g11;
+            }
+            launch_em_direction(c, gamma);
+            CAPAC_CUDA(cudaStreamSynchronize(s));
+        }
+        if (out) {
+            out->step = (int)c->em_step;
+            out->converged = converged ? 1 : 0;
+            out->f_max = fmax;
+            out->f_rms = frms;
+            out->energy = pot0;
+            out->delta_pot = delta;
+            out->em_length = c->em_length;
+        }
+    });
+}
+
+namespace {
+
+// Checkpoint file: magic, version, sizes, step counters, then the arrays.
+constexpr char kCkptMagic[8] = {'C', 'A', 'P', 'A', 'C', 'K', 'P', '1'};
+struct CkptHeader {
+    char magic[8];
+    int version, N, n_mat, has_hist;
+    long md_step, em_step;
+    int n_solves, pad;
+    double em_length;
+    double box[3];
+};
+
+}  // namespace
+
+int capac_checkpoint_save(capac_ctx *c, const char *path)
+{
+    return guard([&] {
+        check_ctx(c);
+        if (!path) throw Error(CAPAC_ERR_INVALID, "null path");
+        CAPAC_CUDA(cudaStreamSynchronize(c->stream));
+        CkptHeader h{};
+        memcpy(h.magic, kCkptMagic, 8);
+        h.version = 1;
+        h.N = c->N;
+        h.n_mat = c->M > 0 ? c->n_mat : 0;
+        h.has_hist = c->xprev != nullptr;
+        h.md_step = c->md_step;
+        h.em_step = c->em_step;
+        h.n_solves = c->n_solves;
+        h.em_length = c->em_length;
+        for (int a = 0; a < 3; ++a) h.box[a] = c->P.box.L[a];
+        FILE *f = fopen(path, "wb");
+        if (!f) throw Error(CAPAC_ERR_IO, std::string("cannot write ") + path);
+        std::vector<double> buf;
+        auto put = [&](const double *d, size_t n) {
+            buf.resize(n);
+            if (n) CAPAC_CUDA(cudaMemcpy(buf.data(), d, sizeof(double) * n, cudaMemcpyDeviceToHost));
+            if (fwrite(buf.data(), sizeof(double), n, f) != n) throw Error(CAPAC_ERR_IO, "short write");
+        };
+        bool ok = fwrite(&h, sizeof h, 1, f) == 1;
+        ThermoState th;
+        CAPAC_CUDA(cudaMemcpy(&th, c->th, sizeof th, cudaMemcpyDeviceToHost));
+        ok = ok && fwrite(&th, sizeof th, 1, f) == 1;
+        if (!ok) {
+            fclose(f);
+            throw Error(CAPAC_ERR_IO, "short write");
+        }
+        const size_t N = c->N;
+        for (const double *p : {c->rx, c->ry, c->rz, c->vx, c->vy, c->vz, c->fx, c->fy, c->fz}) put(p, N);
+        put(c->pot, 15);
+        put(c->vir, 9);
+        if (h.n_mat) put(c->vec_pq, h.n_mat);
+        if (h.has_hist) put(c->xprev, (size_t)3 * c->n_mat);
+        if (fclose(f) != 0) throw Error(CAPAC_ERR_IO, "close failed");
+    });
+}
+
+int capac_checkpoint_load(capac_ctx *c, const char *path)
+{
+    return guard([&] {
+        check_ctx(c);
+        if (!path) throw Error(CAPAC_ERR_INVALID, "null path");
+        FILE *f = fopen(path, "rb");
+        if (!f) throw Error(CAPAC_ERR_IO, std::string("cannot read ") + path);
+        CkptHeader h{};
+        ThermoState th;
+        const bool head = fread(&h, sizeof h, 1, f) == 1 && fread(&th, sizeof th, 1, f) == 1;
+        if (!head || memcmp(h.magic, kCkptMagic, 8) != 0 || h.version != 1) {
+            fclose(f);
+            throw Error(CAPAC_ERR_IO, "not a checkpoint of this library");
+        }
+        if (h.N != c->N || h.n_mat != (c->M > 0 ? c->n_mat : 0) || (h.has_hist && !c->xprev)) {
+            fclose(f);
+            throw Error(CAPAC_ERR_INVALID, "checkpoint is of a different system or precision");
+        }
+        std::vector<double> buf;
+        auto get = [&](double *d, size_t n) {
+            buf.resize(n);
+            if (fread(buf.data(), sizeof(double), n, f) != n) throw Error(CAPAC_ERR_IO, "truncated checkpoint");
+            if (n) CAPAC_CUDA(cudaMemcpy(d, buf.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+        };
+        try {
+            const size_t N = c->N;
+            for (double *p : {c->rx, c->ry, c->rz, c->vx, c->vy, c->vz, c->fx, c->fy, c->fz}) get(p, N);
+            get(c->pot, 15);
+            get(c->vir, 9);
+            if (h.n_mat) get(c->vec_pq, h.n_mat);
+            if (h.has_hist) get(c->xprev, (size_t)3 * c->n_mat);
+        } catch (...) {
+            fclose(f);
+            throw;
+        }
+        fclose(f);
+        CAPAC_CUDA(cudaMemcpy(c->th, &th, sizeof th, cudaMemcpyHostToDevice));
+        c->md_step = h.md_step;
+        c->em_step = h.em_step;
+        c->em_length = h.em_length;
+        c->n_solves = h.has_hist ? h.n_solves : 0;
+        c->list_valid = false;   // the list is rebuilt from the restored positions
+        c->precond_age = 0;
+        c->grad_ready = false;
     });
 }
 

@@ -95,6 +95,11 @@ struct capac_ctx {
     int ensemble = 0, fix_metal = 0, use_cpff = 0, n_save = 1, n_heating = 0;
     int metal_min = 0;
     double dt = 0.0;
+    // energy minimisation (mpi-main.c:700-865): run type, step length, tolerance
+    int run_type = 0;
+    double em_length = 0.0, em_tol = 0.0;
+    double *em_buf = nullptr;     // [6N]: direction s and previous forces, allocated by capac_em_init
+    long em_step = 0;
     bool has_cstr = false;
     cudaStream_t stream = nullptr;
     long launches = 0;
@@ -247,6 +252,9 @@ void launch_apply_pbc(capac_ctx *c);
 void launch_fmax_rms(capac_ctx *c);
 void launch_heating(capac_ctx *c, long step);
 void launch_sum_potential(capac_ctx *c);
+void launch_em_move(capac_ctx *c);                 // old_r = r; r += s / f_max * em_length
+void launch_em_direction(capac_ctx *c, double gamma);  // s = F + gamma s; old F = F
+void launch_em_dots(capac_ctx *c);                 // partials of (F,F), (F_old,F), (F_old,F_old)
 
 size_t partials_needed(const capac_ctx *c);
 

@@ -349,6 +349,58 @@ __global__ void k_fmax_final(const double *partials, int nb, int N, ThermoState 
     }
 }
 
+// Energy minimisation step (mpi-main.c:730-756): old_r = r for every atom;
+// r += s / f_max * em_length except for fixed metal atoms.
+__global__ void k_em_move(MdParams m, const unsigned char *is_metal, const ThermoState *th, double em_length,
+                          const double *__restrict__ sx, const double *__restrict__ sy,
+                          const double *__restrict__ sz, double *rx, double *ry, double *rz, double *ox, double *oy,
+                          double *oz)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.N) return;
+    ox[i] = rx[i];
+    oy[i] = ry[i];
+    oz[i] = rz[i];
+    if (m.fix_metal == 1 && is_metal[i]) return;
+    const double fmax = th->fmax;
+    rx[i] += sx[i] / fmax * em_length;
+    ry[i] += sy[i] / fmax * em_length;
+    rz[i] += sz[i] / fmax * em_length;
+}
+
+// s = F + gamma s, old F = F (mpi-main.c:843-852).
+__global__ void k_em_direction(int N, double gamma, const double *__restrict__ fx, const double *__restrict__ fy,
+                               const double *__restrict__ fz, double *sx, double *sy, double *sz, double *gx,
+                               double *gy, double *gz)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    sx[i] = fx[i] + gamma * sx[i];
+    sy[i] = fy[i] + gamma * sy[i];
+    sz[i] = fz[i] + gamma * sz[i];
+    gx[i] = fx[i];
+    gy[i] = fy[i];
+    gz[i] = fz[i];
+}
+
+// Partials of g22 = (F, F), g12 = (F_old, F), g11 = (F_old, F_old) for the
+// conjugate-gradient gamma (mpi-main.c:823-840).
+__global__ void __launch_bounds__(256) k_em_dots(int N, const double *__restrict__ fx, const double *__restrict__ fy,
+                                                 const double *__restrict__ fz, const double *__restrict__ gx,
+                                                 const double *__restrict__ gy, const double *__restrict__ gz,
+                                                 double *partials)
+{
+    __shared__ double sh[32 * 3];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double acc[3] = {0.0, 0.0, 0.0};
+    if (i < N) {
+        acc[0] = fx[i] * fx[i] + fy[i] * fy[i] + fz[i] * fz[i];
+        acc[1] = gx[i] * fx[i] + gy[i] * fy[i] + gz[i] * fz[i];
+        acc[2] = gx[i] * gx[i] + gy[i] * gy[i] + gz[i] * gz[i];
+    }
+    block_partials<3>(acc, sh, partials);
+}
+
 __global__ void k_sum_potential(double *pot)
 {
     double s = 0.0;
@@ -458,6 +510,34 @@ void launch_fmax_rms(capac_ctx *c)
 void launch_sum_potential(capac_ctx *c)
 {
     k_sum_potential<<<1, 1, 0, c->stream>>>(c->pot);
+    ++c->launches;
+}
+
+// em_buf layout: sx sy sz | old fx fy fz, N each
+void launch_em_move(capac_ctx *c)
+{
+    const size_t N = c->N;
+    k_em_move<<<grid_for(c->N, 256), 256, 0, c->stream>>>(md_params(c), c->is_metal, c->th, c->em_length, c->em_buf,
+                                                         c->em_buf + N, c->em_buf + 2 * N, c->rx, c->ry, c->rz,
+                                                         c->ox, c->oy, c->oz);
+    ++c->launches;
+}
+
+void launch_em_direction(capac_ctx *c, double gamma)
+{
+    const size_t N = c->N;
+    double *b = c->em_buf;
+    k_em_direction<<<grid_for(c->N, 256), 256, 0, c->stream>>>(c->N, gamma, c->fx, c->fy, c->fz, b, b + N,
+                                                              b + 2 * N, b + 3 * N, b + 4 * N, b + 5 * N);
+    ++c->launches;
+}
+
+void launch_em_dots(capac_ctx *c)
+{
+    const size_t N = c->N;
+    const double *b = c->em_buf;
+    k_em_dots<<<grid_for(c->N, 256), 256, 0, c->stream>>>(c->N, c->fx, c->fy, c->fz, b + 3 * N, b + 4 * N,
+                                                         b + 5 * N, c->partials);
     ++c->launches;
 }
 

@@ -227,6 +227,31 @@ int capac_md_steps(capac_ctx *ctx, int n_steps);
  * sum_potential, remove_comm, kinetic_energy, first/ext temperature. */
 int capac_md_init(capac_ctx *ctx);
 
+/* Energy minimisation, steepest descent ("em") or conjugate gradient ("cg")
+ * as run_type in mdset.txt selects (mpi-main.c:700-865).  capac_em_init
+ * (after capac_md_init) sets the direction to the forces; each
+ * capac_em_step moves the atoms by s / F_max * em_length, applies RATTLE and
+ * zeroes the velocities, evaluates the forces, scales em_length by 1.2 or
+ * 0.2 by the sign of the energy change, tests the reference's three
+ * convergence criteria and, unless converged, updates the direction
+ * (Polak-Ribiere gamma for "cg", 0 for "em"). */
+typedef struct capac_em_status {
+    int step;         /* steps taken since capac_em_init */
+    int converged;    /* F_max < tol, F_rms < tol / 2 and |dE| < tol / 10 */
+    double f_max, f_rms, energy, delta_pot, em_length;
+} capac_em_status;
+int capac_em_init(capac_ctx *ctx);
+int capac_em_step(capac_ctx *ctx, capac_em_status *out);
+
+/* Checkpoint of the whole dynamic state (no counterpart in the reference,
+ * whose restart is the .gro file with vQ[0] in its title line, file.c:156-160):
+ * positions, velocities, forces, energies, virial, the induced vector, the
+ * mixed path's warm-start history, the full thermostat chain and step
+ * counters.  A loaded state continues the run as if uninterrupted, up to the
+ * summation order of the neighbour list, which is rebuilt at load. */
+int capac_checkpoint_save(capac_ctx *ctx, const char *path);
+int capac_checkpoint_load(capac_ctx *ctx, const char *path);
+
 /* State transfer.  Names for per-atom arrays (n_atoms doubles):
  * rx ry rz vx vy vz fx fy fz.  Others: potential(15) virial(9) vec_pq vec_ext
  * diag_relay (n_mat) inv_sqrt_dens(n_metal) vQ(10) thermo(4: eKsum inst_temp
