@@ -269,6 +269,7 @@ int capac_create(const capac_desc *d, const capac_options *opt, capac_ctx **out)
             c->device = o.device;
             c->num_sms = prop.multiProcessorCount;
             c->use_graphs = getenv("CAPAC_NO_GRAPHS") == nullptr;
+            c->phase_timer = getenv("CAPAC_SOLVER_PHASES") != nullptr;
             derive(d, &c->c);
             c->N = d->n_atoms;
             c->M = d->n_metal;
@@ -514,7 +515,7 @@ int capac_destroy(capac_ctx *c)
                    c->cstr_cnt, c->cstr_i, c->cstr_j, c->cstr_r, c->np_start, c->np_end, c->np_charge,
                    c->nbr, c->nnb, c->cell_key, c->cell_key_sorted, c->atom_ids, c->cell_atoms,
                    c->cell_start, c->spos, c->sort_tmp, c->flags, c->isd, c->vec_ext, c->vec_pq,
-                   c->diag, c->mat, c->matf, c->msym, c->sympart, c->coop_bp, c->coop_bar, c->g_atoms, c->dinv, c->gw, c->em_buf, c->rres, c->dcorr, c->xprev, c->bw, c->bwf, c->ss, c->partials, c->pot, c->vir, c->th};
+                   c->diag, c->mat, c->matf, c->msym, c->sympart, c->coop_bp, c->coop_bar, c->g_atoms, c->dinv, c->gw, c->em_buf, c->phase_buf, c->rres, c->dcorr, c->xprev, c->bw, c->bwf, c->ss, c->partials, c->pot, c->vir, c->th};
     for (void *p : dev)
         if (p) cudaFree(p);
     if (c->h_flags) cudaFreeHost(c->h_flags);
@@ -912,6 +913,12 @@ int capac_get(capac_ctx *c, const char *name, double *out)
                 out[1] = th.frms;
                 count = 2;
             }
+            return;
+        }
+        if (n == "solver_phases") {  // mean ns per iteration of each phase, then the iteration count
+            for (int k = 0; k < 8; ++k) out[k] = c->phase_iters ? c->phase_ns[k] / c->phase_iters : 0.0;
+            out[8] = (double)c->phase_iters;
+            count = 9;
             return;
         }
         if (n == "box") {

@@ -165,6 +165,11 @@ struct capac_ctx {
     double capac = 0.0, polar = 0.0, rq = 0.0, rp = 0.0;
     bool rq_tied = true, rp_tied = true;  // widths derived from capac / polar
     bool grad_ready = false;              // the state is that of a force call with a solve
+    // persistent-solver phase timer (CAPAC_SOLVER_PHASES set at create)
+    bool phase_timer = false;
+    void *phase_buf = nullptr;
+    double phase_ns[8] = {};
+    long phase_iters = 0;
     double *gw = nullptr;                 // gradient workspace (k_grad.cu), allocated on first use
     double *coop_bp = nullptr;   // its per-block dot partials
     void *coop_bar = nullptr;    // its grid barrier

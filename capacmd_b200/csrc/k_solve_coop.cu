@@ -37,6 +37,7 @@
 // so either all blocks are resident or the launch fails.
 #include <algorithm>
 #include <cstdint>
+#include <vector>
 
 #include "terms.cuh"
 
@@ -193,9 +194,24 @@ struct CoopArgs {
     const float *dinv;
     double *Kr, *Kv, *Kt;
     double *yb[2];
+    // phase timer (null: off): block 0 records %globaltimer at the end of
+    // each phase of the first kPhaseIters iterations, kPhases per iteration
+    unsigned long long *ptime;
 };
 
+constexpr int kPhases = 8;
+constexpr int kPhaseIters = 256;
+
 namespace {
+
+__device__ __forceinline__ void phase_mark(const CoopArgs &A, int iter, int k)
+{
+    if (A.ptime && blockIdx.x == 0 && threadIdx.x == 0 && iter < kPhaseIters) {
+        unsigned long long t;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+        A.ptime[iter * kPhases + k] = t;
+    }
+}
 
 // Bounded grid barrier; false if any block gave up.
 __device__ bool grid_barrier(CoopSync *bar)
@@ -722,17 +738,22 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? 2 : 1) k_bicgstab_coo
     }
     bool pending = false;  // x += alpha y + omega z of the last iteration not yet applied
     while (!done) {
+        phase_mark(A, iter, 0);
         S.beta = (rho / rho_old) * (alpha / omega);
         S.omega = omega;
         S.alpha = alpha;
-        ok = tiles_pass<T, MODE_P>(A, S, ring, psm) && grid_barrier(A.sync);
+        ok = tiles_pass<T, MODE_P>(A, S, ring, psm);
+        phase_mark(A, iter, 1);
+        ok = ok && grid_barrier(A.sync);
         if (!ok) break;
+        phase_mark(A, iter, 2);
         S.first = 0;
         reduce_pass<RED_V>(A, S, bpA);
         if (!grid_barrier(A.sync)) {
             ok = false;
             break;
         }
+        phase_mark(A, iter, 3);
         if (A.bj) {  // K v
             prec_pass<false>(A, A.v[0], A.Kv, nullptr);
             if (!grid_barrier(A.sync)) {
@@ -740,6 +761,7 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? 2 : 1) k_bicgstab_coo
                 break;
             }
         }
+        phase_mark(A, iter, 4);
         double r0v[1];
         sum_bp<1>(bpA, nb, r0v);
         const double al = rho / r0v[0];
@@ -752,11 +774,13 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? 2 : 1) k_bicgstab_coo
         S.alpha = alpha;
         ok = tiles_pass<T, MODE_S>(A, S, ring, psm) && grid_barrier(A.sync);
         if (!ok) break;
+        phase_mark(A, iter, 5);
         reduce_pass<RED_T>(A, S, bpB);
         if (!grid_barrier(A.sync)) {
             ok = false;
             break;
         }
+        phase_mark(A, iter, 6);
         if (A.bj) {  // K t with (K t, z), (K t, K t)
             prec_pass<true>(A, A.t, A.Kt, bpC);
             if (!grid_barrier(A.sync)) {
@@ -764,6 +788,7 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? 2 : 1) k_bicgstab_coo
                 break;
             }
         }
+        phase_mark(A, iter, 7);
         double d[7];
         sum_bp<7>(bpB, nb, d);
         if (A.bj) {
@@ -882,6 +907,11 @@ int bicgstab_coop(capac_ctx *c, const double *b, double *x, double tol, double s
     A.skip = skip;
     A.ss = c->ss;
     A.sync = reinterpret_cast<CoopSync *>(c->coop_bar);
+    A.ptime = nullptr;
+    if (c->phase_timer) {
+        if (!c->phase_buf) CAPAC_CUDA(cudaMalloc(&c->phase_buf, sizeof(unsigned long long) * kPhases * kPhaseIters));
+        A.ptime = static_cast<unsigned long long *>(c->phase_buf);
+    }
     CAPAC_CUDA(cudaMemsetAsync(c->coop_bar, 0, sizeof(CoopSync), c->stream));
     void *args[] = {&A};
     const bool mixed = c->opt.precision == CAPAC_PREC_MIXED;
@@ -900,6 +930,20 @@ int bicgstab_coop(capac_ctx *c, const double *b, double *x, double tol, double s
     CAPAC_CUDA(cudaMemcpyAsync(&hs, c->coop_bar, sizeof hs, cudaMemcpyDeviceToHost, c->stream));
     CAPAC_CUDA(cudaStreamSynchronize(c->stream));
     if (hs.error) throw Error(CAPAC_ERR_CUDA, "persistent solver: a bounded wait timed out");
+    if (A.ptime && c->h_ss->iter > 1) {
+        // phase k of an iteration ends at mark k + 1 (the last at the next iteration's mark 0)
+        const int it = std::min(c->h_ss->iter, kPhaseIters);
+        std::vector<unsigned long long> t((size_t)kPhases * it);
+        CAPAC_CUDA(cudaMemcpy(t.data(), A.ptime, sizeof(unsigned long long) * t.size(), cudaMemcpyDeviceToHost));
+        for (int i = 0; i + 1 < it; ++i) {
+            for (int k = 0; k < kPhases; ++k) {
+                const unsigned long long a = t[(size_t)i * kPhases + k];
+                const unsigned long long b = k + 1 < kPhases ? t[(size_t)i * kPhases + k + 1] : t[(size_t)(i + 1) * kPhases];
+                c->phase_ns[k] += (double)(b - a);
+            }
+            ++c->phase_iters;
+        }
+    }
     if (c->prof.on && c->h_ss->bTb >= skip) c->prof.spmv_effective += 1 + 2L * c->h_ss->iter;
     if (c->h_ss->status < 0) return CAPAC_ERR_NOT_CONVERGED;
     return c->h_ss->status == 1 ? 1 : CAPAC_OK;
