@@ -179,7 +179,7 @@ struct CoopArgs {
     const int *np_start, *np_end;
     const void *mat;
     double *part;  // nT * nT * 128 tile partials
-    double *bp;    // dot partials: 3 sets of kBp doubles per block
+    double *bp;    // dot partials: 2 sets of kBp doubles per block
     const double *b, *diag;
     double *x, *r0, *r, *s, *t, *y, *z, *K;
     double *p[2], *v[2];
@@ -246,7 +246,7 @@ __device__ bool grid_barrier(CoopSync *bar)
 
 // Dot partials: kBp doubles per block.  sum_bp sums them over the blocks
 // in one fixed order, so every block gets the same K sums.
-constexpr int kBp = 8;
+constexpr int kBp = 16;
 template <int K>
 __device__ void sum_bp(const double *bp, int nb, double (&out)[K])
 {
@@ -678,7 +678,9 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? 2 : 1) k_bicgstab_coo
     const long gthreads = (long)gridDim.x * blockDim.x;
     const long tid = (long)blockIdx.x * blockDim.x + threadIdx.x;
     const int nb = gridDim.x;
-    double *bpA = A.bp, *bpB = A.bp + (size_t)kBp * nb, *bpC = A.bp + (size_t)2 * kBp * nb;
+    // bpB holds the 7 dots of the T phase and, in block-Jacobi mode, the 2 of
+    // the K t phase behind them, so one summation serves both
+    double *bpA = A.bp, *bpB = A.bp + (size_t)kBp * nb;
 
     Ring<T> ring;
     ring.buf = reinterpret_cast<T *>(ring_smem);
@@ -782,20 +784,22 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? 2 : 1) k_bicgstab_coo
         }
         phase_mark(A, iter, 6);
         if (A.bj) {  // K t with (K t, z), (K t, K t)
-            prec_pass<true>(A, A.t, A.Kt, bpC);
+            prec_pass<true>(A, A.t, A.Kt, bpB + 7);
             if (!grid_barrier(A.sync)) {
                 ok = false;
                 break;
             }
         }
         phase_mark(A, iter, 7);
-        double d[7];
-        sum_bp<7>(bpB, nb, d);
+        double d[9];
         if (A.bj) {
-            double k2[2];
-            sum_bp<2>(bpC, nb, k2);
-            d[0] = k2[0];
-            d[1] = k2[1];
+            sum_bp<9>(bpB, nb, d);
+            d[0] = d[7];  // (K t, z), (K t, K t) of the preconditioner pass
+            d[1] = d[8];
+        } else {
+            double d7[7];
+            sum_bp<7>(bpB, nb, d7);
+            for (int q = 0; q < 7; ++q) d[q] = d7[q];
         }
         const double om = d[0] / d[1];
         if (!isfinite(om) || om == 0.0) {
@@ -855,7 +859,7 @@ size_t dyn_smem_bytes()
 }  // namespace
 
 size_t coop_barrier_bytes() { return sizeof(CoopSync); }
-size_t coop_partial_doubles(int grid) { return (size_t)3 * kBp * grid; }
+size_t coop_partial_doubles(int grid) { return (size_t)2 * kBp * grid; }
 
 // Launch the persistent solver; returns the status as bicgstab_core does.
 int bicgstab_coop(capac_ctx *c, const double *b, double *x, double tol, double skip)
