@@ -35,6 +35,10 @@ ERR_NO_DEVICE = -8
 PREC_FP64 = 0
 PREC_MIXED = 1
 
+# bonded term kinds (CAPAC_BT_* of capacmd.h)
+BT_BOND_HARMONIC, BT_BOND_MORSE, BT_PAIR_14, BT_PAIR_USER = 1, 2, 3, 4
+BT_ANGLE_HARMONIC, BT_ANGLE_UB, BT_DIHEDRAL_RB = 5, 6, 7
+
 # Metal parameters of capac_param_get/set, in the order of capac_energy_param_grad.
 PARAMS = ("cpff_capac", "cpff_polar", "cpim_rq", "cpim_rp", "qsc_eps", "qsc_c", "qsc_a", "qsc_n", "qsc_m")
 

@@ -22,7 +22,7 @@ DRIVER = os.path.join(PKG, "capacmd-gpu")
 REF_SRC = "/root/reference"
 
 SOURCES = ["io.cpp", "api.cu", "k_list.cu", "k_pair.cu", "k_cpim.cu", "k_md.cu", "k_cpim_sym.cu", "k_solve_static.cu", "k_solve_coop.cu",
-           "k_precond.cu", "k_grad.cu", "k_grad_forces.cu"]
+           "k_precond.cu", "k_grad.cu", "k_grad_forces.cu", "k_bonded.cu"]
 
 
 def nvcc() -> str:

@@ -317,8 +317,197 @@ def gro_text(pos: np.ndarray, vel: np.ndarray, n_metal: int, box: float) -> str:
     return "\n".join(out) + "\n"
 
 
+# ------------------------------------------------------------------------------
+# A test system with every bonded term and a virtual site: Au13 (CPIM on),
+# 5-atom chains (harmonic and Morse bonds, 1-4 pairs of
+# both kinds, harmonic and Urey-Bradley angles, RB and periodic dihedrals of
+# multiplicity 1 to 4), rigid 4-site waters whose charge site is a funct-4
+# virtual site with an out-of-plane part, and flexible 3-site waters.
+
+BONDED_BOX = 3.5
+_CHAIN = dict(n=20, q=[0.2, -0.1, 0.0, -0.1, 0.0], m=12.011, t=3)
+_T4P = dict(n=30, q=[0.0, 0.52, 0.52, -1.04], m=[16.0, 1.008, 1.008, 0.0], t=[1, 2, 2, 4])
+_FLW = dict(n=10, q=[-0.82, 0.41, 0.41], m=[16.0, 1.008, 1.008], t=[1, 2, 2])
+_VS = (0.128, 0.128, 1.5)
+
+
+def _chain_local() -> np.ndarray:
+    """Zig-zag chain, bonds 0.153 nm, angles 111 degrees, torsions +-60 degrees."""
+    b, ang = 0.153, np.deg2rad(111.0)
+    pts = [np.zeros(3), np.array([b, 0.0, 0.0])]
+    pts.append(pts[1] + b * np.array([-np.cos(ang), np.sin(ang), 0.0]))
+    for tors in (np.deg2rad(60.0), np.deg2rad(-65.0)):
+        a, b_, c = pts[-3], pts[-2], pts[-1]
+        bc = (c - b_) / np.linalg.norm(c - b_)
+        n = np.cross(b_ - a, bc)
+        n /= np.linalg.norm(n)
+        m = np.cross(n, bc)
+        d = np.array([-b * np.cos(ang), b * np.sin(ang) * np.cos(tors), b * np.sin(ang) * np.sin(tors)])
+        pts.append(c + d[0] * bc + d[1] * m + d[2] * n)
+    return np.array(pts)
+
+
+def _t4p_local() -> np.ndarray:
+    half = np.deg2rad(104.52) / 2.0
+    oh = 0.09572
+    o, h1, h2 = np.zeros(3), np.array([oh * np.sin(half), 0.0, oh * np.cos(half)]), \
+        np.array([-oh * np.sin(half), 0.0, oh * np.cos(half)])
+    a, b, c = _VS
+    s = o + a * (h1 - o) + b * (h2 - o) + c * np.cross(h1 - o, h2 - o)
+    return np.array([o, h1, h2, s])
+
+
+def _flw_local() -> np.ndarray:
+    half = np.deg2rad(107.0) / 2.0
+    return np.array([[0.0, 0.0, 0.0], [0.101 * np.sin(half), 0.0, 0.101 * np.cos(half)],
+                     [-0.099 * np.sin(half), 0.0, 0.099 * np.cos(half)]])
+
+
+def build_bonded(seed: int = 11):
+    rng = np.random.default_rng(seed)
+    L = BONDED_BOX
+    metal = icosahedron(1) + L / 2
+    placed = [metal]
+    mols = []
+    for spec, local in ((_CHAIN, _chain_local()), (_T4P, _t4p_local()), (_FLW, _flw_local())):
+        for _ in range(spec["n"]):
+            for _attempt in range(10000):
+                rot = _random_rotations(rng, 1)[0]
+                x = (local - local.mean(0)) @ rot.T + rng.uniform(0.0, L, 3)
+                allp = np.concatenate(placed)
+                if _min_dist_to(x, allp, L).min() > 0.28:
+                    break
+            placed.append(x)
+            mols.append(x)
+    pos = np.concatenate(placed)
+    masses = np.concatenate([np.full(13, M_AU), np.full(_CHAIN["n"] * 5, _CHAIN["m"]),
+                             np.tile(_T4P["m"], _T4P["n"]), np.tile(_FLW["m"], _FLW["n"])])
+    vel = rng.normal(size=pos.shape) * np.sqrt(K_BOLTZ * 300.0 / np.where(masses > 0, masses, 1.0))[:, None]
+    vel[masses == 0] = 0.0
+    # rigid 4-site waters: remove the velocity components along their constraints
+    s0 = 13 + _CHAIN["n"] * 5
+    mw = np.array(_T4P["m"][:3])
+    for k in range(_T4P["n"]):
+        r = pos[s0 + 4 * k:s0 + 4 * k + 3]
+        v = vel[s0 + 4 * k:s0 + 4 * k + 3]
+        for _ in range(200):
+            for (i, j) in ((0, 1), (0, 2), (1, 2)):
+                rij, vij = r[i] - r[j], v[i] - v[j]
+                g = -(rij @ vij) / ((1 / mw[i] + 1 / mw[j]) * (rij @ rij))
+                v[i] += g * rij / mw[i]
+                v[j] -= g * rij / mw[j]
+    real = masses > 0
+    vel[real] -= (vel[real] * masses[real, None]).sum(0) / masses[real].sum()
+    return pos, vel
+
+
+def bonded_param_text() -> str:
+    eps = 0.012793 * EV2KJMOL
+    hh = 0.15139
+    L = ["SCALE_LJ_QQ    0.50000000     0.83333333", "", "MOLECULES      4",
+         "gold           13", f"CHN            {_CHAIN['n']}", f"T4P            {_T4P['n']}",
+         f"FLW            {_FLW['n']}", "",
+         "gold_ATOMS          1", f"     0.000000   {M_AU:.6f}       0", "",
+         "CHN_ATOMS           5"]
+    L += [f"    {q:.6f}    {_CHAIN['m']:.6f}       {_CHAIN['t']}" for q in _CHAIN["q"]]
+    L += ["", "T4P_ATOMS           4"]
+    L += [f"    {q:.6f}    {m:.6f}       {t}" for q, m, t in zip(_T4P["q"], _T4P["m"], _T4P["t"])]
+    L += ["", "FLW_ATOMS           3"]
+    L += [f"    {q:.6f}    {m:.6f}       {t}" for q, m, t in zip(_FLW["q"], _FLW["m"], _FLW["t"])]
+    L += ["", "NONBONDED      5         15",
+          " 1    0.00000000e+00      0.00000000e+00",   # Au Au
+          " 4  0.002522219544  3.624859037184e-06  2.25",  # Au O
+          " 4  0.001028707002  1.45541995368e-06   2.25",  # Au H
+          " 1    3.00000000e-03      5.00000000e-06",   # Au C
+          " 1    0.00000000e+00      0.00000000e+00",   # Au M
+          " 1    2.48970844e-03      2.43509761e-06",   # O O
+          " 1    0.00000000e+00      0.00000000e+00",   # O H
+          " 1    2.00000000e-03      3.00000000e-06",   # O C
+          " 1    0.00000000e+00      0.00000000e+00",   # O M
+          " 1    0.00000000e+00      0.00000000e+00",   # H H
+          " 1    5.00000000e-04      5.00000000e-07",   # H C
+          " 1    0.00000000e+00      0.00000000e+00",   # H M
+          " 1    4.00000000e-03      8.00000000e-06",   # C C
+          " 1    0.00000000e+00      0.00000000e+00",   # C M
+          " 1    0.00000000e+00      0.00000000e+00",   # M M
+          ""]
+    L += ["gold_BONDS          0", "gold_PAIRS          0", "gold_ANGLES         0", "gold_DIHEDRALS      0",
+          "gold_VSITES         0", "gold_CSTRS          0", ""]
+    # no funct-5 (exclusion-only) bond: the reference leaves its BondParam
+    # unset and mpi_bonded still applies it (undefined behaviour)
+    L += ["CHN_BONDS           3",
+          "0 1 1   0.153  250000.0",
+          "1 2 3   0.153  350.0  20.0",
+          "2 3 1   0.153  250000.0",
+          "CHN_PAIRS           2",
+          "0 3 1",
+          "1 4 2   0.5  0.1  -0.1  3.0e-01  4.0e-01",
+          "CHN_ANGLES          3",
+          "0 1 2 1   111.0  400.0",
+          "1 2 3 5   112.0  450.0  0.25  5000.0",
+          "2 3 4 1   110.0  420.0",
+          "CHN_DIHEDRALS       5",
+          "0 1 2 3 3   9.28  12.16  -13.12  -3.06  26.24  -31.5",
+          "1 2 3 4 9   0.0  5.92  3",
+          "1 2 3 4 1   180.0  2.0  1",
+          "0 1 2 3 4   0.0  1.0  2",
+          "0 1 2 3 9   180.0  0.5  4",
+          "CHN_VSITES          0",
+          "CHN_CSTRS           0", ""]
+    a, b, c = _VS
+    L += ["T4P_BONDS           0", "T4P_PAIRS           0", "T4P_ANGLES          0", "T4P_DIHEDRALS       0",
+          "T4P_VSITES          1", f"0 1 2 3 4   {a}  {b}  {c}",
+          "T4P_CSTRS           3", "0 1   0.09572", "0 2   0.09572", f"1 2   {hh}", ""]
+    L += ["FLW_BONDS           2", "0 1 1   0.1  345000.0", "0 2 1   0.1  345000.0",
+          "FLW_PAIRS           0", "FLW_ANGLES          1", "1 0 2 5   109.47  383.0  0.1633  2000.0",
+          "FLW_DIHEDRALS       0", "FLW_VSITES          0", "FLW_CSTRS           0", ""]
+    L += ["MM_METAL  0  12", f"QSC_METAL  10  8  {eps:.9f}  34.408000  0.408000",
+          "CPFF_METAL  39.529700  1.215900   ;  Note: atomic unit", "", "NANOPARTICLES   1",
+          "START_END_CHG   0  12   0.0"]
+    return "\n".join(L) + "\n"
+
+
+def bonded_gro_text(pos: np.ndarray, vel: np.ndarray) -> str:
+    out = ["step  0  vQ  0.000000  vP  0.000000", f"{len(pos):5d}"]
+    rows = [(k + 1, "AU", "Au") for k in range(13)]
+    res = 14
+    for _ in range(_CHAIN["n"]):
+        rows += [(res, "CHN", f"C{a + 1}") for a in range(5)]
+        res += 1
+    for _ in range(_T4P["n"]):
+        rows += [(res, "T4P", n) for n in ("OW", "HW1", "HW2", "MW")]
+        res += 1
+    for _ in range(_FLW["n"]):
+        rows += [(res, "FLW", n) for n in ("OW", "HW1", "HW2")]
+        res += 1
+    for i, ((r, rn, an), x, v) in enumerate(zip(rows, pos, vel)):
+        out.append(f"{r % 100000:5d}{rn:<5s}{an:>5s}{(i + 1) % 100000:5d}"
+                   f" {x[0]:.12f} {x[1]:.12f} {x[2]:.12f} {v[0]:.12f} {v[1]:.12f} {v[2]:.12f}")
+    out.append(f"{BONDED_BOX:10.5f}{BONDED_BOX:10.5f}{BONDED_BOX:10.5f}")
+    return "\n".join(out) + "\n"
+
+
+def write_bonded(out_dir: str, steps: int | None = None) -> dict:
+    os.makedirs(out_dir, exist_ok=True)
+    pos, vel = build_bonded()
+    w = Workload("t_bonded", [1], 0, BONDED_BOX, seed=11, ensemble="nvt", steps=steps or 20)
+    paths = {k: os.path.join(out_dir, f) for k, f in
+             (("gro", "init.gro"), ("par", "param.txt"), ("mds", "mdset.txt"))}
+    with open(paths["gro"], "w") as f:
+        f.write(bonded_gro_text(pos, vel))
+    with open(paths["par"], "w") as f:
+        f.write(bonded_param_text())
+    with open(paths["mds"], "w") as f:
+        f.write(mdset_text(w, steps))
+    paths["n_atoms"] = len(pos)
+    paths["n_metal"] = 13
+    return paths
+
+
 def write(name: str, out_dir: str, steps: int | None = None) -> dict:
     """Write one workload's three input files; returns their paths."""
+    if name == "t_bonded":
+        return write_bonded(out_dir, steps)
     w = WORKLOADS[name]
     os.makedirs(out_dir, exist_ok=True)
     s = build(w)

@@ -56,6 +56,7 @@ void force(capac_ctx *c, bool solve = true)
     cudaStream_t s = c->stream;
     c->grad_ready = false;
     record(c, 0);
+    launch_build_vsites(c);  // build_vsites before everything (force.c:2124-2129)
     launch_list_maintenance(c, false);
     launch_pack_positions(c);
     CAPAC_CUDA(cudaMemsetAsync(c->fx, 0, sizeof(double) * c->N, s));
@@ -65,6 +66,7 @@ void force(capac_ctx *c, bool solve = true)
     CAPAC_CUDA(cudaMemsetAsync(c->vir, 0, sizeof(double) * 9, s));
     record(c, 1);
     const bool cpim = c->M > 0 && c->use_cpff;
+    launch_bonded(c);
     if (c->M > 0) launch_qsc(c);
     record(c, 2);
     if (cpim) launch_cpim_rhs(c);
@@ -78,6 +80,7 @@ void force(capac_ctx *c, bool solve = true)
     record(c, 6);
     if (cpim) launch_cpim_metal_forces(c);
     launch_external_field(c);
+    launch_vsite_forces(c);  // mpi_vsites after all force terms (force.c:2290-2296)
     record(c, 7);
     if (st != CAPAC_OK) {
         char msg[160];
@@ -237,8 +240,8 @@ int capac_create(const capac_desc *d, const capac_options *opt, capac_ctx **out)
     return guard([&] {
         if (!d || !out) throw Error(CAPAC_ERR_INVALID, "null argument");
         *out = nullptr;
-        if (d->n_bonded_terms > 0 || d->n_vsites_total > 0)
-            throw Error(CAPAC_ERR_UNSUPPORTED, "bonded terms and virtual sites are outside this path");
+        if ((d->n_bonded_terms > 0 && !d->bt_offset) || (d->n_vsites_total > 0 && !d->vs_offset))
+            throw Error(CAPAC_ERR_INVALID, "bonded terms or virtual sites counted but not described");
         if (d->n_atoms <= 1 || d->n_atoms >= (1 << kIdxBits))
             throw Error(CAPAC_ERR_INVALID, "atom count out of range");
         if (d->n_types <= 0 || d->n_types > 255) throw Error(CAPAC_ERR_INVALID, "type count out of range");
@@ -337,6 +340,37 @@ int capac_create(const capac_desc *d, const capac_options *opt, capac_ctx **out)
             c->nb_funct = dupload(d->nb_funct, (size_t)NT * NT, s);
             c->nb_par = dupload(par.data(), par.size(), s);
             c->mol_first = dupload(d->mol_first, d->n_mols, s);
+            // bonded terms and virtual sites per molecule type
+            c->has_bonded = d->n_bonded_terms > 0;
+            c->has_vsites = d->n_vsites_total > 0;
+            if (c->has_bonded || c->has_vsites) {
+                const int T = d->mol_types;
+                size_t nt = 0, nv = 0;
+                for (int m = 0; m < T; ++m) {
+                    if (d->bt_offset) nt = std::max(nt, (size_t)(d->bt_offset[m] + d->bt_count[m]));
+                    if (d->vs_offset) nv = std::max(nv, (size_t)(d->vs_offset[m] + d->vs_count[m]));
+                }
+                auto keep = [&](void *p) {
+                    c->bonded_buffers.push_back(p);
+                    return p;
+                };
+                const std::vector<int> zeros(T, 0);
+                BondedView &B = c->bview;
+                B.n_mols = d->n_mols;
+                B.mol_first = c->mol_first;
+                B.scale_lj = d->scale_lj;
+                B.scale_qq = d->scale_qq;
+                B.bt_offset = (int *)keep(dupload(d->bt_offset ? d->bt_offset : zeros.data(), T, s));
+                B.bt_count = (int *)keep(dupload(d->bt_count ? d->bt_count : zeros.data(), T, s));
+                B.bt_kind = (int *)keep(dupload(d->bt_kind, std::max<size_t>(nt, 1), s));
+                B.bt_atoms = (int *)keep(dupload(d->bt_atoms, 4 * std::max<size_t>(nt, 1), s));
+                B.bt_par = (double *)keep(dupload(d->bt_par, 6 * std::max<size_t>(nt, 1), s));
+                B.vs_offset = (int *)keep(dupload(d->vs_offset ? d->vs_offset : zeros.data(), T, s));
+                B.vs_count = (int *)keep(dupload(d->vs_count ? d->vs_count : zeros.data(), T, s));
+                B.vs_atoms = (int *)keep(dupload(d->vs_atoms, 4 * std::max<size_t>(nv, 1), s));
+                B.vs_par = (double *)keep(dupload(d->vs_par, 3 * std::max<size_t>(nv, 1), s));
+                CAPAC_CUDA(cudaStreamSynchronize(s));
+            }
             c->mol_last = dupload(d->mol_last, d->n_mols, s);
             c->cstr_off = dupload(d->cstr_offset, T, s);
             c->cstr_cnt = dupload(d->cstr_count, T, s);
@@ -517,6 +551,8 @@ int capac_destroy(capac_ctx *c)
                    c->cell_start, c->spos, c->sort_tmp, c->flags, c->isd, c->vec_ext, c->vec_pq,
                    c->diag, c->mat, c->matf, c->msym, c->sympart, c->coop_bp, c->coop_bar, c->g_atoms, c->dinv, c->gw, c->em_buf, c->phase_buf, c->rres, c->dcorr, c->xprev, c->bw, c->bwf, c->ss, c->partials, c->pot, c->vir, c->th};
     for (void *p : dev)
+        if (p) cudaFree(p);
+    for (void *p : c->bonded_buffers)
         if (p) cudaFree(p);
     if (c->h_flags) cudaFreeHost(c->h_flags);
     if (c->h_ss) cudaFreeHost(c->h_ss);

@@ -56,6 +56,17 @@ struct DevParams {
     int metal_by_type;
 };
 
+// Bonded terms and virtual sites per molecule type (capac_desc bt_*, vs_*).
+struct BondedView {
+    int n_mols;
+    const int *mol_first;
+    const int *bt_offset, *bt_count, *bt_kind, *bt_atoms;
+    const double *bt_par;
+    const int *vs_offset, *vs_count, *vs_atoms;
+    const double *vs_par;
+    double scale_lj, scale_qq;
+};
+
 // Kernel classes for the event-based profiler.
 enum KClass {
     K_PAIR = 0, K_SPMV, K_MATRIX, K_CPIM_METAL, K_CPIM_RHS, K_QSC, K_LIST, K_SOLVER_VEC, K_INTEGRATE, K_RESID,
@@ -101,6 +112,9 @@ struct capac_ctx {
     double *em_buf = nullptr;     // [6N]: direction s and previous forces, allocated by capac_em_init
     long em_step = 0;
     bool has_cstr = false;
+    bool has_bonded = false, has_vsites = false;
+    capac::BondedView bview{};
+    std::vector<void *> bonded_buffers;  // device arrays behind bview
     cudaStream_t stream = nullptr;
     long launches = 0;
     long md_step = 0;
@@ -257,6 +271,9 @@ void launch_apply_pbc(capac_ctx *c);
 void launch_fmax_rms(capac_ctx *c);
 void launch_heating(capac_ctx *c, long step);
 void launch_sum_potential(capac_ctx *c);
+void launch_build_vsites(capac_ctx *c);   // k_bonded.cu
+void launch_bonded(capac_ctx *c);
+void launch_vsite_forces(capac_ctx *c);
 void launch_em_move(capac_ctx *c);                 // old_r = r; r += s / f_max * em_length
 void launch_em_direction(capac_ctx *c, double gamma);  // s = F + gamma s; old F = F
 void launch_em_dots(capac_ctx *c);                 // partials of (F,F), (F_old,F), (F_old,F_old)

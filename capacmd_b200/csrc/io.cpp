@@ -7,10 +7,12 @@
 //   param.txt  sections in a fixed order              (file.c:286-562, 569-1023)
 // followed by the per-atom bookkeeping of assign_indices (file.c:1031-1099) and
 // the constants derived in the driver (mpi-main.c:170-203, 315-323, 548-552).
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <initializer_list>
 #include <string>
 #include <vector>
 
@@ -195,6 +197,21 @@ void read_param(const char *path, capac_desc *d)
         d->excl = alloc_array<unsigned char>(excl_total);
         std::vector<int> ci, cj;
         std::vector<double> cr;
+        std::vector<int> bkind, batoms, vatoms;
+        std::vector<double> bpar, vpar;
+        d->bt_offset = alloc_array<int>(T);
+        d->bt_count = alloc_array<int>(T);
+        d->vs_offset = alloc_array<int>(T);
+        d->vs_count = alloc_array<int>(T);
+        auto add_term = [&](int kind, std::initializer_list<int> at, std::initializer_list<double> par) {
+            bkind.push_back(kind);
+            int k = 0;
+            for (int a : at) batoms.push_back(a), ++k;
+            for (; k < 4; ++k) batoms.push_back(0);
+            k = 0;
+            for (double v : par) bpar.push_back(v), ++k;
+            for (; k < 6; ++k) bpar.push_back(0.0);
+        };
         auto exclude = [&](int m, int a, int b) {
             const int na = d->mol_atoms[m];
             if (a < 0 || b < 0 || a >= na || b >= na)
@@ -202,55 +219,114 @@ void read_param(const char *path, capac_desc *d)
             d->excl[d->excl_offset[m] + a * na + b] = 1;
             d->excl[d->excl_offset[m] + b * na + a] = 1;
         };
+        auto bad = [&](const char *what) {
+            throw Error(CAPAC_ERR_UNSUPPORTED, std::string("unsupported ") + what + " in line: " + r.line);
+        };
         for (int m = 0; m < T; ++m) {
             int n = 0;
-            // bonds: every listed bond excludes its pair (file.c:720-770)
+            d->bt_offset[m] = (int)bkind.size();
+            // bonds (file.c:715-765); every listed bond excludes its pair
             r.expect(names[m] + "_BONDS");
             sscanf(r.line, "%*s%d", &n);
-            d->n_bonded_terms += n;
             for (int k = 0; k < n; ++k) {
                 r.next();
-                int a, b;
-                sscanf(r.line, "%d%d", &a, &b);
+                int a = 0, b = 0, fn = 0;
+                double p0 = 0, p1 = 0, p2 = 0;
+                sscanf(r.line, "%d%d%d", &a, &b, &fn);
+                if (fn == 1) {
+                    sscanf(r.line, "%*d%*d%*d%le%le", &p0, &p1);
+                    add_term(CAPAC_BT_BOND_HARMONIC, {a, b}, {p0, p1});
+                } else if (fn == 3) {
+                    sscanf(r.line, "%*d%*d%*d%le%le%le", &p0, &p1, &p2);
+                    add_term(CAPAC_BT_BOND_MORSE, {a, b}, {p0, p1, p2});
+                } else if (fn != 5) {  // 5: exclusion only
+                    bad("bond function type");
+                }
                 exclude(m, a, b);
             }
+            // 1-4 pairs (file.c:767-811)
             r.expect(names[m] + "_PAIRS");
             sscanf(r.line, "%*s%d", &n);
-            d->n_bonded_terms += n;
             for (int k = 0; k < n; ++k) {
                 r.next();
-                int a, b;
-                sscanf(r.line, "%d%d", &a, &b);
+                int a = 0, b = 0, fn = 0;
+                sscanf(r.line, "%d%d%d", &a, &b, &fn);
+                if (fn == 1) {
+                    add_term(CAPAC_BT_PAIR_14, {a, b}, {});
+                } else if (fn == 2) {
+                    double sq = 0, qa = 0, qb = 0, V = 0, W = 0;
+                    sscanf(r.line, "%*d%*d%*d%lf%lf%lf%le%le", &sq, &qa, &qb, &V, &W);
+                    // sigma, epsilon -> C6, C12 as force.c:1783-1786
+                    const double sig_6 = pow(V, 6.0), eps_4 = 4.0 * W;
+                    const double c6 = eps_4 * sig_6, c12 = c6 * sig_6;
+                    add_term(CAPAC_BT_PAIR_USER, {a, b}, {sq, qa, qb, c6, c12});
+                } else {
+                    bad("pair function type");
+                }
                 exclude(m, a, b);
             }
+            // angles (file.c:813-864)
             r.expect(names[m] + "_ANGLES");
             sscanf(r.line, "%*s%d", &n);
-            d->n_bonded_terms += n;
             for (int k = 0; k < n; ++k) {
                 r.next();
-                int a, b, c;
-                sscanf(r.line, "%d%d%d", &a, &b, &c);
+                int a = 0, b = 0, c = 0, fn = 0;
+                double p0 = 0, p1 = 0, p2 = 0, p3 = 0;
+                sscanf(r.line, "%d%d%d%d", &a, &b, &c, &fn);
+                if (fn == 1) {
+                    sscanf(r.line, "%*d%*d%*d%*d%le%le", &p0, &p1);
+                    add_term(CAPAC_BT_ANGLE_HARMONIC, {a, b, c}, {p0, p1});
+                } else if (fn == 5) {
+                    sscanf(r.line, "%*d%*d%*d%*d%le%le%le%le", &p0, &p1, &p2, &p3);
+                    add_term(CAPAC_BT_ANGLE_UB, {a, b, c}, {p0, p1, p2, p3});
+                } else {
+                    bad("angle function type");
+                }
                 exclude(m, a, b);
                 exclude(m, a, c);
                 exclude(m, b, c);
             }
+            // dihedrals (file.c:866-928); the periodic form becomes the RB
+            // coefficients compute_dihedral_9 derives (force.c:1236-1347)
             r.expect(names[m] + "_DIHEDRALS");
             sscanf(r.line, "%*s%d", &n);
-            d->n_bonded_terms += n;
             for (int k = 0; k < n; ++k) {
                 r.next();
-                int a, b, c, e;
-                sscanf(r.line, "%d%d%d%d", &a, &b, &c, &e);
+                int a = 0, b = 0, c = 0, e = 0, fn = 0;
+                sscanf(r.line, "%d%d%d%d%d", &a, &b, &c, &e, &fn);
+                double cc[6] = {0, 0, 0, 0, 0, 0};
+                if (fn == 3) {
+                    sscanf(r.line, "%*d%*d%*d%*d%*d%lf%lf%lf%lf%lf%lf", &cc[0], &cc[1], &cc[2], &cc[3], &cc[4],
+                           &cc[5]);
+                } else if (fn == 1 || fn == 4 || fn == 9) {
+                    double phi0 = 0, kphi = 0;
+                    int mult = 0;
+                    sscanf(r.line, "%*d%*d%*d%*d%*d%lf%lf%d", &phi0, &kphi, &mult);
+                    if (capac_dihedral_periodic_to_rb(phi0, kphi, mult, cc) != CAPAC_OK)
+                        bad("periodic dihedral (phi0 0 or 180, multiplicity 1 to 4)");
+                } else {
+                    bad("dihedral function type");
+                }
+                add_term(CAPAC_BT_DIHEDRAL_RB, {a, b, c, e}, {cc[0], cc[1], cc[2], cc[3], cc[4], cc[5]});
                 exclude(m, a, b); exclude(m, a, c); exclude(m, a, e);
                 exclude(m, b, c); exclude(m, b, e); exclude(m, c, e);
             }
+            d->bt_count[m] = (int)bkind.size() - d->bt_offset[m];
+            d->n_bonded_terms += d->bt_count[m] * d->mol_num[m];
+            // virtual sites (file.c:931-969)
             r.expect(names[m] + "_VSITES");
             sscanf(r.line, "%*s%d", &n);
+            d->vs_offset[m] = (int)(vatoms.size() / 4);
+            d->vs_count[m] = n;
             d->n_vsites_total += n * d->mol_num[m];
             for (int k = 0; k < n; ++k) {
                 r.next();
-                int a, b, c, s;
-                sscanf(r.line, "%d%d%d%d", &a, &b, &c, &s);
+                int a = 0, b = 0, c = 0, s = 0, fn = 0;
+                double va = 0, vb = 0, vc = 0;
+                sscanf(r.line, "%d%d%d%d%d%lf%lf%lf", &a, &b, &c, &s, &fn, &va, &vb, &vc);
+                if (fn != 4) bad("virtual_sites function type");
+                for (int x : {a, b, c, s}) vatoms.push_back(x);
+                for (double v : {va, vb, vc}) vpar.push_back(v);
                 exclude(m, s, a); exclude(m, s, b); exclude(m, s, c);
             }
             r.expect(names[m] + "_CSTRS");
@@ -270,6 +346,16 @@ void read_param(const char *path, capac_desc *d)
                 cr.push_back(len);
             }
         }
+        d->bt_kind = alloc_array<int>(bkind.size());
+        d->bt_atoms = alloc_array<int>(batoms.size());
+        d->bt_par = alloc_array<double>(bpar.size());
+        d->vs_atoms = alloc_array<int>(vatoms.size());
+        d->vs_par = alloc_array<double>(vpar.size());
+        std::copy(bkind.begin(), bkind.end(), d->bt_kind);
+        std::copy(batoms.begin(), batoms.end(), d->bt_atoms);
+        std::copy(bpar.begin(), bpar.end(), d->bt_par);
+        std::copy(vatoms.begin(), vatoms.end(), d->vs_atoms);
+        std::copy(vpar.begin(), vpar.end(), d->vs_par);
         d->cstr_i = alloc_array<int>(ci.size());
         d->cstr_j = alloc_array<int>(ci.size());
         d->cstr_r = alloc_array<double>(ci.size());
@@ -427,7 +513,9 @@ void desc_free(capac_desc *d)
                       d->excl_offset, d->excl, d->cstr_offset, d->cstr_count, d->cstr_i, d->cstr_j,
                       d->cstr_r, d->np_start, d->np_end, d->np_charge, d->atom_type, d->mol_id,
                       d->mol_type, d->atom_in_mol, d->is_metal, d->charge, d->mass, d->inv_mass,
-                      d->mol_first, d->mol_last, d->rx, d->ry, d->rz, d->vx, d->vy, d->vz};
+                      d->mol_first, d->mol_last, d->rx, d->ry, d->rz, d->vx, d->vy, d->vz,
+                      d->bt_offset, d->bt_count, d->bt_kind, d->bt_atoms, d->bt_par, d->vs_offset,
+                      d->vs_count, d->vs_atoms, d->vs_par};
     for (void *p : arrays) free(p);
     free(d);
 }
@@ -462,6 +550,44 @@ int capac_desc_load(const char *gro_path, const char *param_path, const char *md
 }
 
 void capac_desc_free(capac_desc *d) { capac::desc_free(d); }
+
+int capac_dihedral_periodic_to_rb(double phi0, double kphi, int n, double c[6])
+{
+    if (!c) return CAPAC_ERR_INVALID;
+    for (int k = 0; k < 6; ++k) c[k] = 0.0;
+    const bool zero = phi0 == 0.0, pi = phi0 == 180.0;
+    if (!zero && !pi) return CAPAC_ERR_UNSUPPORTED;
+    if (n == 1) {
+        c[0] = kphi;
+        c[1] = zero ? kphi : kphi * (-1.0);
+    } else if (n == 2) {
+        if (zero) {
+            c[2] = kphi * 2.0;
+        } else {
+            c[0] = kphi * 2.0;
+            c[2] = kphi * (-2.0);
+        }
+    } else if (n == 3) {
+        c[0] = kphi;
+        c[1] = zero ? kphi * (-3.0) : kphi * 3.0;
+        c[3] = zero ? kphi * 4.0 : kphi * (-4.0);
+    } else if (n == 4) {
+        if (zero) {
+            c[0] = kphi * 2.0;
+            c[2] = kphi * (-8.0);
+            c[4] = kphi * 8.0;
+        } else {
+            c[2] = kphi * 8.0;
+            c[4] = kphi * (-8.0);
+        }
+    } else {
+        return CAPAC_ERR_UNSUPPORTED;
+    }
+    c[1] *= -1.0;
+    c[3] *= -1.0;
+    c[5] *= -1.0;
+    return CAPAC_OK;
+}
 
 int capac_desc_derive(const capac_desc *d, capac_consts *out)
 {
@@ -504,6 +630,20 @@ int capac_desc_get(const capac_desc *d, const char *name, double *out)
     if (0 == strcmp(name, "atom_type")) {
         for (int i = 0; i < n; ++i) out[i] = d->atom_type[i];
         return n;
+    }
+    if (0 == strcmp(name, "bonded_counts")) {  // terms in the system, virtual sites, constraints
+        out[0] = d->n_bonded_terms;
+        out[1] = d->n_vsites_total;
+        out[2] = d->n_cstr_total;
+        return 3;
+    }
+    if (0 == strcmp(name, "bonded_kinds")) {  // terms of each CAPAC_BT_* kind (1..7) in the system
+        for (int k = 0; k < 8; ++k) out[k] = 0.0;
+        if (d->bt_offset)
+            for (int m = 0; m < d->mol_types; ++m)
+                for (int t = d->bt_offset[m]; t < d->bt_offset[m] + d->bt_count[m]; ++t)
+                    if (d->bt_kind[t] >= 0 && d->bt_kind[t] < 8) out[d->bt_kind[t]] += d->mol_num[m];
+        return 8;
     }
     return CAPAC_ERR_INVALID;
 }

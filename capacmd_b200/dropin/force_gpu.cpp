@@ -18,13 +18,20 @@
 // Compiled as C++ against the reference's headers (typedef.h pulls in
 // std::vector): the `dropin` target of oracle/Makefile links it with the
 // reference's objects into oracle/_ref/mpi-main-gpu.
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <initializer_list>
 #include <string>
 #include <vector>
 
 #include "capacmd.h"
 #include "typedef.h"
+
+// build_vsites is defined in the reference's force.c (force.c:1582), which the
+// drop-in binary links; it has no header declaration there
+void build_vsites(int mol_start, int mol_end, Mol_Info *mol_info, Atom_Info *atom_info, int *nVSites,
+                  int **vsite_funct, VSite_4 **vsite_4, double *rx, double *ry, double *rz, double *box);
 
 namespace {
 
@@ -36,6 +43,65 @@ std::vector<int> v_mol_num, v_mol_atoms, v_nb_funct, v_excl_offset, v_cstr_offse
     v_cstr_j, v_atom_type, v_mol_id, v_mol_type, v_atom_in_mol, v_mol_first, v_mol_last;
 std::vector<double> v_nb_c6, v_nb_c12, v_nb_a, v_nb_b, v_cstr_r, v_charge, v_mass, v_inv_mass;
 std::vector<unsigned char> v_excl, v_is_metal;
+std::vector<int> v_bt_offset, v_bt_count, v_bt_kind, v_bt_atoms, v_vs_offset, v_vs_count, v_vs_atoms;
+std::vector<double> v_bt_par, v_vs_par;
+
+void add_term(int kind, std::initializer_list<int> at, std::initializer_list<double> par)
+{
+    v_bt_kind.push_back(kind);
+    int k = 0;
+    for (int a : at) v_bt_atoms.push_back(a), ++k;
+    for (; k < 4; ++k) v_bt_atoms.push_back(0);
+    k = 0;
+    for (double v : par) v_bt_par.push_back(v), ++k;
+    for (; k < 6; ++k) v_bt_par.push_back(0.0);
+}
+
+// Bonded terms and virtual sites of molecule type mt in the order
+// mpi_bonded (force.c:1694-1900) and build_vsites (force.c:1582-1629) use.
+void add_bonded(const Topol *t, int mt)
+{
+    v_bt_offset[mt] = (int)v_bt_kind.size();
+    for (int k = 0; k < t->n_bonds[mt]; ++k) {
+        const BondParam &b = t->bond_param[mt][k];
+        if (b.funct == 1) add_term(CAPAC_BT_BOND_HARMONIC, {b.atom_i, b.atom_j}, {b.b0, b.kb});
+        else if (b.funct == 3) add_term(CAPAC_BT_BOND_MORSE, {b.atom_i, b.atom_j}, {b.b0, b.D, b.beta});
+    }
+    for (int k = 0; k < t->n_pairs[mt]; ++k) {
+        const PairParam &p = t->pair_param[mt][k];
+        if (p.funct == 1) {
+            add_term(CAPAC_BT_PAIR_14, {p.atom_i, p.atom_j}, {});
+        } else if (p.funct == 2) {
+            const double sig_6 = pow(p.V, 6.0), eps_4 = 4.0 * p.W;
+            const double c6 = eps_4 * sig_6, c12 = c6 * sig_6;
+            add_term(CAPAC_BT_PAIR_USER, {p.atom_i, p.atom_j}, {p.scaleQQ, p.q_i, p.q_j, c6, c12});
+        }
+    }
+    for (int k = 0; k < t->n_angles[mt]; ++k) {
+        const AngleParam &a = t->angle_param[mt][k];
+        if (a.funct == 1)
+            add_term(CAPAC_BT_ANGLE_HARMONIC, {a.atom_i, a.atom_j, a.atom_k}, {a.a0, a.ka});
+        else if (a.funct == 5)
+            add_term(CAPAC_BT_ANGLE_UB, {a.atom_i, a.atom_j, a.atom_k}, {a.a0, a.ka, a.b0_ub, a.kb_ub});
+    }
+    for (int k = 0; k < t->n_dihedrals[mt]; ++k) {
+        const DihedralParam &q = t->dihedral_param[mt][k];
+        double c[6] = {q.c0, q.c1, q.c2, q.c3, q.c4, q.c5};
+        if (q.funct != 3 && capac_dihedral_periodic_to_rb(q.phi0, q.kphi, q.n, c) != CAPAC_OK) {
+            printf("<> Error: phi0 is not equal to 0 or pi, or n is not 1 to 4\n");
+            exit(1);
+        }
+        add_term(CAPAC_BT_DIHEDRAL_RB, {q.atom_i, q.atom_j, q.atom_k, q.atom_l}, {c[0], c[1], c[2], c[3], c[4], c[5]});
+    }
+    v_bt_count[mt] = (int)v_bt_kind.size() - v_bt_offset[mt];
+    v_vs_offset[mt] = (int)(v_vs_atoms.size() / 4);
+    v_vs_count[mt] = t->n_vsites[mt];
+    for (int k = 0; k < t->n_vsites[mt]; ++k) {
+        const VSite_4 &v = t->vsite_4[mt][k];
+        for (int a : {v.atom_i, v.atom_j, v.atom_k, v.atom_s}) v_vs_atoms.push_back(a);
+        for (double x : {v.a, v.b, v.c}) v_vs_par.push_back(x);
+    }
+}
 
 void fail(const char *what)
 {
@@ -114,6 +180,15 @@ void build_desc(const Topol *t, const Atom_Info *ai, const Mol_Info *mi, const R
     d.n_cstr_total = 0;
     d.n_bonded_terms = 0;
     d.n_vsites_total = 0;
+    v_bt_offset.assign(T, 0);
+    v_bt_count.assign(T, 0);
+    v_vs_offset.assign(T, 0);
+    v_vs_count.assign(T, 0);
+    v_bt_kind.clear();
+    v_bt_atoms.clear();
+    v_bt_par.clear();
+    v_vs_atoms.clear();
+    v_vs_par.clear();
     for (int mt = 0; mt < T; ++mt) {
         const int na = t->atom_num[mt];
         v_excl_offset[mt] = (int)v_excl.size();
@@ -127,9 +202,19 @@ void build_desc(const Topol *t, const Atom_Info *ai, const Mol_Info *mi, const R
             v_cstr_r.push_back(t->constraint[mt][k].r);
         }
         d.n_cstr_total += t->n_constraints[mt] * t->mol_num[mt];
-        d.n_bonded_terms += t->n_bonds[mt] + t->n_pairs[mt] + t->n_angles[mt] + t->n_dihedrals[mt];
+        add_bonded(t, mt);
+        d.n_bonded_terms += v_bt_count[mt] * t->mol_num[mt];
         d.n_vsites_total += t->n_vsites[mt] * t->mol_num[mt];
     }
+    d.bt_offset = v_bt_offset.data();
+    d.bt_count = v_bt_count.data();
+    d.bt_kind = v_bt_kind.data();
+    d.bt_atoms = v_bt_atoms.data();
+    d.bt_par = v_bt_par.data();
+    d.vs_offset = v_vs_offset.data();
+    d.vs_count = v_vs_count.data();
+    d.vs_atoms = v_vs_atoms.data();
+    d.vs_par = v_vs_par.data();
     d.excl_offset = v_excl_offset.data();
     d.excl = v_excl.data();
     d.cstr_offset = v_cstr_offset.data();
@@ -217,6 +302,11 @@ extern "C" void __wrap__Z9mpi_forceP4TaskP5TopolP9Atom_InfoP8Mol_InfoP6RunSetP5M
         if (const char *dev = getenv("CAPAC_DEVICE")) o.device = atoi(dev);
         if (capac_create(&g_desc, &o, &g_ctx)) fail("create");
     }
+    // the reference's mpi_force places the virtual sites in the caller's
+    // positions first (force.c:2124-2129); the driver's own build_vsites does
+    // the same here, and the GPU rebuilds them identically
+    if (g_desc.n_vsites_total > 0)
+        build_vsites(0, t->n_mols - 1, mi, ai, t->n_vsites, t->vsite_funct, t->vsite_4, s->rx, s->ry, s->rz, s->box);
     double vir[9];
     // the driver allocates the CPIM vectors whenever there are metal atoms
     // (mpi-main.c:576-591) and inv_sqrt_dens with them (mpi-main.c:290)

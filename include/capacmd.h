@@ -47,7 +47,7 @@ extern "C" {
 #define CAPAC_ERR_CUDA (-3)           /* CUDA runtime failure */
 #define CAPAC_ERR_NOT_CONVERGED (-4)  /* BiCGSTAB above 100x tolerance after MAX_ITER (bicg_stab.c:561-570) */
 #define CAPAC_ERR_RATTLE (-5)         /* RATTLE did not converge (force.c:1990-1994, 2083-2087) */
-#define CAPAC_ERR_UNSUPPORTED (-6)    /* input uses a term outside this path (bonded terms, vsites) */
+#define CAPAC_ERR_UNSUPPORTED (-6)    /* input uses a function type the reference does not support either */
 #define CAPAC_ERR_CAPACITY (-7)       /* a fixed-capacity buffer is too small for this input */
 #define CAPAC_ERR_NO_DEVICE (-8)      /* no usable sm_100 device */
 
@@ -57,6 +57,14 @@ const char *capac_last_error(void);
 #define CAPAC_RUN_MD 0
 #define CAPAC_RUN_EM 1
 #define CAPAC_RUN_CG 2
+/* bonded term kinds (force.c:822-1347 as mpi_bonded dispatches them, force.c:1694-1900) */
+#define CAPAC_BT_BOND_HARMONIC 1  /* par: b0, kb                              (bond funct 1) */
+#define CAPAC_BT_BOND_MORSE 2     /* par: b0, D, beta                         (bond funct 3) */
+#define CAPAC_BT_PAIR_14 3        /* types, charges, SCALE_LJ_QQ of the atoms (pair funct 1) */
+#define CAPAC_BT_PAIR_USER 4      /* par: scaleQQ, q_i, q_j, c6, c12          (pair funct 2) */
+#define CAPAC_BT_ANGLE_HARMONIC 5 /* par: a0 (degrees), ka                    (angle funct 1) */
+#define CAPAC_BT_ANGLE_UB 6       /* par: a0, ka, b0_ub, kb_ub                (angle funct 5) */
+#define CAPAC_BT_DIHEDRAL_RB 7    /* par: c0..c5 (periodic funct 1/4/9 are given as their RB form) */
 #define CAPAC_NVE 0
 #define CAPAC_NVT 1
 
@@ -114,7 +122,25 @@ typedef struct capac_desc {
     double box[3];
     double *rx, *ry, *rz, *vx, *vy, *vz;
     double vq0, vp;                /* thermostat velocities from the title line */
+
+    /* bonded terms per molecule type, in the reference's order within a
+     * molecule (bonds, pairs, angles, dihedrals; file.c:715-930) */
+    int *bt_offset, *bt_count;     /* [mol_types] */
+    int *bt_kind;                  /* [terms] CAPAC_BT_* */
+    int *bt_atoms;                 /* [4 * terms] atom indices within the molecule */
+    double *bt_par;                /* [6 * terms] */
+    /* virtual sites per molecule type (funct 4, file.c:931-969):
+     * r_s = r_i + a r_ij + b r_ik + c (r_ij x r_ik) */
+    int *vs_offset, *vs_count;     /* [mol_types] */
+    int *vs_atoms;                 /* [4 * sites] i, j, k, s */
+    double *vs_par;                /* [3 * sites] a, b, c */
 } capac_desc;
+
+/* The RB coefficients compute_dihedral_9 (force.c:1236-1347) derives from a
+ * periodic dihedral (phi0 0 or 180 degrees, multiplicity 1 to 4), signs of
+ * c1, c3, c5 already flipped for the polymer convention; CAPAC_ERR_UNSUPPORTED
+ * otherwise (where the reference exits). */
+int capac_dihedral_periodic_to_rb(double phi0, double kphi, int n, double c[6]);
 
 /* Constants the reference derives at start-up. */
 typedef struct capac_consts {
@@ -134,6 +160,9 @@ int capac_desc_derive(const capac_desc *d, capac_consts *out);
 /* Copy a named per-system array of a description into out (doubles).  Names:
  * rx ry rz vx vy vz charge mass box.  Returns the count written or <0. */
 int capac_desc_get(const capac_desc *d, const char *name, double *out);
+/* capac_desc_get names: rx ry rz vx vy vz charge mass is_metal atom_type
+ * (n_atoms), box (3), bonded_counts (3: terms, virtual sites, constraints in
+ * the system), bonded_kinds (8: terms of each CAPAC_BT_* kind). */
 /* Sizes of a description: atoms, molecules, metal atoms, NPs, n_mat. */
 int capac_desc_info(const capac_desc *d, int *n_atoms, int *n_mols, int *n_metal, int *n_nps, int *n_mat);
 

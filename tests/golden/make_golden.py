@@ -30,7 +30,7 @@ sys.path.insert(0, ROOT)
 from capacmd_b200 import configs  # noqa: E402
 from oracle.oracle import RefSim  # noqa: E402
 
-CASES = ["t_au13", "t_au55w", "t_2np", "t_water", "c1", "c1_field"]
+CASES = ["t_au13", "t_au55w", "t_2np", "t_water", "c1", "c1_field", "t_bonded"]
 MD_STEPS = 10
 
 

@@ -79,7 +79,7 @@ def _vec_pq(path):
     return np.array(vals)
 
 
-@pytest.mark.parametrize("case", ["t_water", "t_au13", "t_au55w", "t_2np"])
+@pytest.mark.parametrize("case", ["t_water", "t_au13", "t_au55w", "t_2np", "t_bonded"])
 def test_reference_driver_with_gpu_force(case, tmp_path):
     out_c = _run(CPU, case, str(tmp_path / "cpu"))
     out_g = _run(GPU, case, str(tmp_path / "gpu"))

@@ -102,7 +102,7 @@ def _compare(tmp_path, out_c, out_g, cpim):
     assert open(tmp_path / "ref" / "traj.gro").read().count("step") == open(tmp_path / "gpu" / "traj.gro").read().count("step")
 
 
-@pytest.mark.parametrize("case", ["t_water", "t_au55w", "t_2np"])
+@pytest.mark.parametrize("case", ["t_water", "t_au55w", "t_2np", "t_bonded"])
 def test_md_run_matches_reference(case, tmp_path):
     keys = dict(run_type="md", number_of_steps=20, save_step=2)
     _setup(case, str(tmp_path / "ref"), **keys)
@@ -119,7 +119,7 @@ def test_md_run_matches_reference(case, tmp_path):
 
 
 @pytest.mark.parametrize("run_type", ["em", "cg"])
-@pytest.mark.parametrize("case", ["t_water", "t_au55w"])
+@pytest.mark.parametrize("case", ["t_water", "t_au55w", "t_bonded"])
 def test_minimisation_matches_reference(case, run_type, tmp_path):
     keys = dict(run_type=run_type, em_steps=8)
     _setup(case, str(tmp_path / "ref"), **keys)

@@ -85,14 +85,18 @@ def test_parser_errors(tmp_path):
     assert e.value.code == cm.ERR_IO
 
 
-def test_bonded_terms_are_refused(tmp_path):
+@pytest.mark.parametrize("section,line", [("SOL_BONDS", "0 1 7 0.1 1000.0"),
+                                          ("SOL_DIHEDRALS", "0 1 2 0 9 90.0 1.0 2")])
+def test_unsupported_bonded_function_types_are_refused(tmp_path, section, line):
+    """Function types the reference rejects (file.c:755-760, force.c:1260-1340)."""
     p = golden_paths("t_water")
-    txt = open(p["par"]).read().replace("SOL_BONDS          0", "SOL_BONDS          1\n0 1 1 0.1 1000.0")
+    txt = open(p["par"]).read()
+    old = re.search(rf"(?m)^{section}\s+0$", txt).group(0)
+    txt = txt.replace(old, f"{section}   1\n{line}")
     par = tmp_path / "param.txt"
     par.write_text(txt)
-    d = cm.Desc(p["gro"], str(par), p["mds"])
     with pytest.raises(cm.CapacError) as e:
-        cm.Simulation(d)
+        cm.Desc(p["gro"], str(par), p["mds"])
     assert e.value.code == cm.ERR_UNSUPPORTED
 
 
