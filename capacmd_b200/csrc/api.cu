@@ -233,6 +233,7 @@ void capac_options_default(capac_options *o)
     o->predictor = 2;
     o->solver_kernel = 0;
     o->inner_precond = 1;
+    o->pair_list = 0;
 }
 
 int capac_create(const capac_desc *d, const capac_options *opt, capac_ctx **out)
@@ -455,9 +456,9 @@ int capac_create(const capac_desc *d, const capac_options *opt, capac_ctx **out)
             c->cell_key_sorted = dalloc<int>(N);
             c->atom_ids = dalloc<int>(N);
             c->cell_atoms = dalloc<int>(N);
-            c->flags = dalloc<int>(4);
-            CAPAC_CUDA(cudaMemsetAsync(c->flags, 0, sizeof(int) * 4, s));
-            CAPAC_CUDA(cudaMallocHost(&c->h_flags, sizeof(int) * 4));
+            c->flags = dalloc<int>(8);
+            CAPAC_CUDA(cudaMemsetAsync(c->flags, 0, sizeof(int) * 8, s));
+            CAPAC_CUDA(cudaMallocHost(&c->h_flags, sizeof(int) * 8));
 
             // metal / CPIM
             if (c->M > 0) {
@@ -548,7 +549,8 @@ int capac_destroy(capac_ctx *c)
                    c->excl_offset, c->excl, c->nb_funct, c->nb_par, c->mol_first, c->mol_last, c->cstr_off,
                    c->cstr_cnt, c->cstr_i, c->cstr_j, c->cstr_r, c->np_start, c->np_end, c->np_charge,
                    c->nbr, c->nnb, c->cell_key, c->cell_key_sorted, c->atom_ids, c->cell_atoms,
-                   c->cell_start, c->spos, c->sort_tmp, c->flags, c->isd, c->vec_ext, c->vec_pq,
+                   c->cell_start, c->spos, c->sort_tmp, c->flags, c->cl_atoms, c->cl_cell_start, c->cl_counts,
+                   c->cl_nbr, c->cl_nnb, c->cl_metal, c->scan_tmp, c->isd, c->vec_ext, c->vec_pq,
                    c->diag, c->mat, c->matf, c->msym, c->sympart, c->coop_bp, c->coop_bar, c->g_atoms, c->dinv, c->gw, c->em_buf, c->phase_buf, c->rres, c->dcorr, c->xprev, c->bw, c->bwf, c->ss, c->partials, c->pot, c->vir, c->th};
     for (void *p : dev)
         if (p) cudaFree(p);
@@ -951,6 +953,12 @@ int capac_get(capac_ctx *c, const char *name, double *out)
             }
             return;
         }
+        if (n == "pair_list") {  // 1 when the pair kernel walks the cluster list, then the cluster count
+            out[0] = c->clusters ? 1.0 : 0.0;
+            out[1] = (double)c->n_clusters;
+            count = 2;
+            return;
+        }
         if (n == "solver_phases") {  // mean ns per iteration of each phase, then the iteration count
             for (int k = 0; k < 8; ++k) out[k] = c->phase_iters ? c->phase_ns[k] / c->phase_iters : 0.0;
             out[8] = (double)c->phase_iters;
@@ -1004,12 +1012,15 @@ int capac_get_stats(capac_ctx *c, capac_stats *out)
         out->solver_rel_residual = c->last_rel_res;
         out->solver_initial_rel_residual = c->last_init_res;
         out->list_builds = c->list_builds;
-        out->list_capacity = c->cap;
+        out->list_capacity = c->clusters ? c->cl_cap : c->cap;
         out->md_step = c->md_step;
         if (c->list_valid) {
-            std::vector<int> nn(c->N);
+            // entries of the list the pair kernel walks: per cluster or per atom
+            const int rows = c->clusters ? c->n_clusters : c->N;
+            std::vector<int> nn(rows);
             CAPAC_CUDA(cudaStreamSynchronize(c->stream));
-            CAPAC_CUDA(cudaMemcpy(nn.data(), c->nnb, sizeof(int) * c->N, cudaMemcpyDeviceToHost));
+            CAPAC_CUDA(cudaMemcpy(nn.data(), c->clusters ? c->cl_nnb : c->nnb, sizeof(int) * rows,
+                                  cudaMemcpyDeviceToHost));
             long tot = 0, mx = 0;
             for (int v : nn) {
                 tot += v;

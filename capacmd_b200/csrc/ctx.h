@@ -158,9 +158,30 @@ struct capac_ctx {
     double4 *spos = nullptr;     // [N] positions in cell order, atom index in w
     void *sort_tmp = nullptr;
     size_t sort_tmp_bytes = 0;
-    int *flags = nullptr;      // [0] rebuild needed, [1] list overflow max count, [2] rattle error
+    int *flags = nullptr;      // [0] rebuild needed, [1] list overflow max count, [2] rattle error,
+                               // [4] cluster-list overflow max count, [5] cluster extent (float bits)
     int *h_flags = nullptr;    // pinned mirror
     bool list_valid = false;
+    int cell_sub_bits = 0;     // sub-cell Morton bits below the cell index in cell_key
+
+    // cluster-pair list (mixed path): clusters of up to four atoms, consecutive
+    // in the sub-cell order of one cell; per cluster the j atoms with a mask of
+    // the members each is a list neighbour of (see k_list.cu)
+    bool clusters = false;        // the pair kernel runs on the cluster list (decided at each build)
+    bool atom_list_full = true;   // atom-list rows exist for every atom (else metal rows only)
+    bool need_full_list = false;  // a caller (the gradients) needs every atom-list row
+    int cl_cap = 0;               // entries per cluster
+    int cl_max = 0;               // cluster slots allocated (N / 4 + cells + 1)
+    int cl_cells = 0;             // cell count cl_cell_start was sized for
+    int n_clusters = 0;
+    int4 *cl_atoms = nullptr;          // [cl_max] member atoms, -1 padding at the end
+    int *cl_cell_start = nullptr;      // [cells + 1] first cluster of each cell; [cells] = count
+    int *cl_counts = nullptr;          // [cells + 1] scratch: clusters per cell
+    uint32_t *cl_nbr = nullptr;        // [cl_max * cl_cap]
+    int *cl_nnb = nullptr;             // [cl_max]
+    unsigned char *cl_metal = nullptr; // [cl_max] the cluster has a metal neighbour
+    void *scan_tmp = nullptr;
+    size_t scan_tmp_bytes = 0;
 
     // metal / CPIM
     int Mp = 0;                  // M padded to a multiple of 32
@@ -222,6 +243,9 @@ void cuda_check(cudaError_t e, const char *what);
 // Kernel launchers (one stream; every launch is counted).
 void launch_pack_positions(capac_ctx *c);
 void launch_list_maintenance(capac_ctx *c, bool force_rebuild);
+// Rebuild the lists with an atom-list row for every atom, now and at every
+// later build (the gradient kernels walk all rows).
+void ensure_full_atom_list(capac_ctx *c);
 void launch_pair_forces(capac_ctx *c, int mode);  // mode: 0 full, 1 CPIM water side only
 void launch_qsc(capac_ctx *c);
 void launch_cpim_rhs(capac_ctx *c);

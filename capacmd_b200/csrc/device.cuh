@@ -113,4 +113,18 @@ __host__ __device__ __forceinline__ uint32_t pack_nb(int j, int t) { return (uin
 __host__ __device__ __forceinline__ int nb_index(uint32_t e) { return (int)(e & kIdxMask); }
 __host__ __device__ __forceinline__ int nb_type(uint32_t e) { return (int)(e >> kIdxBits); }
 
+// Cluster-list entries: the j atom in the low 22 bits, in bits 22-25 the mask
+// of the cluster members j is a list neighbour of, the j type in bits 26-31.
+// In the pair kernel's queue bits 22-23 carry the member instead of the mask.
+constexpr int kClIdxBits = 22, kClMaskShift = 22, kClTypeShift = 26;
+constexpr uint32_t kClIdxMask = (1u << kClIdxBits) - 1u;
+constexpr int kClMaxTypes = 64;
+__host__ __device__ __forceinline__ uint32_t pack_cl(int j, unsigned mask, int t)
+{
+    return (uint32_t)j | (mask << kClMaskShift) | ((uint32_t)t << kClTypeShift);
+}
+
+// Minimum image by rounding (any number of box lengths apart).
+__device__ __forceinline__ double min_image(double d, double L, double inv_L) { return d - L * rint(d * inv_L); }
+
 }  // namespace capac

@@ -323,6 +323,7 @@ __global__ void __launch_bounds__(256) k_cpim_metal_dual(DevParams P, const doub
 void launch_force_derivative(capac_ctx *c, const double *wdir, double *dfx, double *dfy, double *dfz, double *isd_v,
                              double *isd_d)
 {
+    ensure_full_atom_list(c);  // the dual pair kernel walks every atom's row
     cudaStream_t s = c->stream;
     const bool cpim = c->M > 0 && c->use_cpff;
     const unsigned pair_blocks = grid_for((long)c->N * 32, 256);

@@ -15,11 +15,29 @@
 // every step triggers the rebuild.
 //
 // The atom order within a cell comes from a stable radix sort on the cell key,
-// so lists (and hence force summation order) are identical run to run.
+// so lists (and hence force summation order) are identical run to run.  The
+// key carries, below the cell index, a Morton code of the atom's position on
+// an 8 x 8 x 8 grid inside its cell, so consecutive atoms of a cell are
+// close together.
+//
+// Mixed path, cluster list: the atoms of each cell are cut, in that order,
+// into clusters of up to four.  Per cluster a warp scans the same 5 x 5 x 5
+// cell window; a candidate j within rc + skin + (cluster radius) of the
+// cluster's centroid is tested against each member k exactly as the atom
+// list tests it (pbc_12 image, the reference's r^2 rounding, exclusions), and
+// kept with the mask of the members that pass.  The pair set per member is
+// therefore the atom list's.  The pair kernel rounds j's minimum-image
+// difference from the centroid and the members' offsets from it to FP32; the
+// composite is the pair's minimum image whenever rc + (largest member offset
+// at the build) + skin < half the shortest box edge, which each build checks,
+// falling back to the atom list otherwise.  Metal atoms keep atom-list rows
+// (the CPIM kernels walk them); the gradients ask for every atom's row.
 #include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
 
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 
 #include "ctx.h"
 
@@ -39,27 +57,45 @@ struct Grid {
     double inv_len[3];
 };
 
+// Cell coordinate and, in sub, the position inside the cell on a grid of
+// 2^sub_per cells per axis.
+__device__ __forceinline__ int cell_coord_sub(double x, double L, double inv_len, int n, int sub_per, int &sub)
+{
+    const double u = (x - L * floor(x / L)) * inv_len;
+    int c = (int)u;
+    c = c < 0 ? 0 : (c >= n ? n - 1 : c);
+    const int ns = 1 << sub_per;
+    int s = (int)((u - c) * ns);
+    sub = s < 0 ? 0 : (s >= ns ? ns - 1 : s);
+    return c;
+}
+
 __global__ void k_cell_keys(int N, const double *__restrict__ rx, const double *__restrict__ ry,
-                            const double *__restrict__ rz, Box box, Grid g, int *key, int *ids)
+                            const double *__restrict__ rz, Box box, Grid g, int sub_bits, int *key, int *ids)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
-    const int cx = cell_coord(rx[i], box.L[0], g.inv_len[0], g.n[0]);
-    const int cy = cell_coord(ry[i], box.L[1], g.inv_len[1], g.n[1]);
-    const int cz = cell_coord(rz[i], box.L[2], g.inv_len[2], g.n[2]);
-    key[i] = (cx * g.n[1] + cy) * g.n[2] + cz;
+    const int per = sub_bits / 3;
+    int sx, sy, sz;
+    const int cx = cell_coord_sub(rx[i], box.L[0], g.inv_len[0], g.n[0], per, sx);
+    const int cy = cell_coord_sub(ry[i], box.L[1], g.inv_len[1], g.n[1], per, sy);
+    const int cz = cell_coord_sub(rz[i], box.L[2], g.inv_len[2], g.n[2], per, sz);
+    int sub = 0;
+    for (int b = 0; b < per; ++b)
+        sub |= (((sx >> b) & 1) << (3 * b + 2)) | (((sy >> b) & 1) << (3 * b + 1)) | (((sz >> b) & 1) << (3 * b));
+    key[i] = (((cx * g.n[1] + cy) * g.n[2] + cz) << sub_bits) | sub;
     ids[i] = i;
 }
 
 // start[c] = first sorted position with key >= c, for c = 0 .. n_cells
 // (empty cells included), so the atoms of cells a..b are start[a] ..
 // start[b + 1] - 1.
-__global__ void k_cell_starts(int N, int n_cells, const int *__restrict__ key, int *start)
+__global__ void k_cell_starts(int N, int n_cells, int sub_bits, const int *__restrict__ key, int *start)
 {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p > N) return;
-    const int prev = p > 0 ? key[p - 1] : -1;
-    const int cur = p < N ? key[p] : n_cells;
+    const int prev = p > 0 ? key[p - 1] >> sub_bits : -1;
+    const int cur = p < N ? key[p] >> sub_bits : n_cells;
     for (int c = prev + 1; c <= cur; ++c) start[c] = p;
 }
 
@@ -85,8 +121,31 @@ __device__ __forceinline__ bool excluded(const DevParams &P, int i, int j)
 __device__ __forceinline__ int axis_count(int n) { return n < 5 ? 1 : 5; }
 __device__ __forceinline__ int axis_cell(int c, int n, int k) { return n < 5 ? 0 : (c + k - 2 + n) % n; }
 
-// One warp per atom i.
-__global__ void __launch_bounds__(256) k_build_list(DevParams P, Grid g, const double *__restrict__ rx,
+// The z window c-2 .. c+2 as one or two runs of consecutive cells.
+struct ZRuns {
+    int a[2], b[2], n;
+};
+__device__ __forceinline__ ZRuns z_runs(int cz, int nz)
+{
+    ZRuns z;
+    if (nz < 5) {
+        z.a[0] = 0; z.b[0] = nz - 1; z.n = 1;
+    } else {
+        const int lo = cz - 2, hi = cz + 2;
+        if (lo < 0) {
+            z.a[0] = lo + nz; z.b[0] = nz - 1; z.a[1] = 0; z.b[1] = hi; z.n = 2;
+        } else if (hi >= nz) {
+            z.a[0] = lo; z.b[0] = nz - 1; z.a[1] = 0; z.b[1] = hi - nz; z.n = 2;
+        } else {
+            z.a[0] = lo; z.b[0] = hi; z.n = 1;
+        }
+    }
+    return z;
+}
+
+// One warp per atom i, for the rows i0 .. i0 + rows - 1.
+__global__ void __launch_bounds__(256) k_build_list(DevParams P, Grid g, int i0, int rows,
+                                                    const double *__restrict__ rx,
                                                     const double *__restrict__ ry,
                                                     const double *__restrict__ rz,
                                                     const double4 *__restrict__ spos,
@@ -94,37 +153,25 @@ __global__ void __launch_bounds__(256) k_build_list(DevParams P, Grid g, const d
                                                     uint32_t *__restrict__ nbr, int *__restrict__ nnb,
                                                     double *rx0, double *ry0, double *rz0, int *flags)
 {
-    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
-    if (i >= P.N) return;
+    if (w >= rows) return;
+    const int i = i0 + w;
     const double xi = rx[i], yi = ry[i], zi = rz[i];
     const int c0[3] = {cell_coord(xi, P.box.L[0], g.inv_len[0], g.n[0]),
                        cell_coord(yi, P.box.L[1], g.inv_len[1], g.n[1]),
                        cell_coord(zi, P.box.L[2], g.inv_len[2], g.n[2])};
     const int nxs = axis_count(g.n[0]), nys = axis_count(g.n[1]);
-    // the z window as one or two runs of consecutive cells
     const int nz = g.n[2];
-    int za[2], zb[2], nzr;
-    if (nz < 5) {
-        za[0] = 0; zb[0] = nz - 1; nzr = 1;
-    } else {
-        const int lo = c0[2] - 2, hi = c0[2] + 2;
-        if (lo < 0) {
-            za[0] = lo + nz; zb[0] = nz - 1; za[1] = 0; zb[1] = hi; nzr = 2;
-        } else if (hi >= nz) {
-            za[0] = lo; zb[0] = nz - 1; za[1] = 0; zb[1] = hi - nz; nzr = 2;
-        } else {
-            za[0] = lo; zb[0] = hi; nzr = 1;
-        }
-    }
+    const ZRuns zr = z_runs(c0[2], nz);
     const unsigned lt_mask = (1u << lane) - 1u;
     uint32_t *row = nbr + (size_t)i * cap;
     int count = 0;
     for (int ix = 0; ix < nxs; ++ix) {
         for (int iy = 0; iy < nys; ++iy) {
             const int col = (axis_cell(c0[0], g.n[0], ix) * g.n[1] + axis_cell(c0[1], g.n[1], iy)) * nz;
-            for (int r = 0; r < nzr; ++r) {
-                const int s = cell_start[col + (r ? za[1] : za[0])], e = cell_start[col + (r ? zb[1] : zb[0]) + 1];
+            for (int r = 0; r < zr.n; ++r) {
+                const int s = cell_start[col + zr.a[r]], e = cell_start[col + zr.b[r] + 1];
                 for (int base = s; base < e; base += 32) {
                     const int p = base + lane;
                     bool ok = false;
@@ -151,6 +198,210 @@ __global__ void __launch_bounds__(256) k_build_list(DevParams P, Grid g, const d
         rx0[i] = xi;
         ry0[i] = yi;
         rz0[i] = zi;
+    }
+}
+
+// ------------------------------------------------------------ clusters
+
+// Clusters per cell, ceil(atoms / 4); counts[n_cells] = 0 so that the
+// exclusive scan's last element is the total.
+__global__ void k_cluster_counts(int n_cells, const int *__restrict__ cell_start, int *counts)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c > n_cells) return;
+    counts[c] = c < n_cells ? (cell_start[c + 1] - cell_start[c] + 3) / 4 : 0;
+}
+
+struct InvBox {
+    double L[3], inv[3];
+};
+
+// Member offsets from the centroid of a cluster (minimum image from the
+// first member); returns the number of members.
+__device__ __forceinline__ int cluster_offsets(const int m[4], const double *__restrict__ rx,
+                                               const double *__restrict__ ry, const double *__restrict__ rz,
+                                               const InvBox &B, double o[4][3], double c[3])
+{
+    const double *r[3] = {rx, ry, rz};
+    int nk = 0;
+    double s[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        if (m[k] < 0) break;
+        ++nk;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            o[k][a] = min_image(r[a][m[k]] - r[a][m[0]], B.L[a], B.inv[a]);
+            s[a] += o[k][a];
+        }
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const double mean = s[a] / nk;
+        c[a] = r[a][m[0]] + mean;
+        for (int k = 0; k < nk; ++k) o[k][a] -= mean;
+    }
+    return nk;
+}
+
+// The clusters of one cell (a thread per cell), and in flags[5] the largest
+// component of a member's offset from its cluster's centroid (float bits,
+// rounded up).
+__global__ void k_make_clusters(int n_cells, const int *__restrict__ cell_start, const int *__restrict__ cl_start,
+                                const int *__restrict__ cell_atoms, const double *__restrict__ rx,
+                                const double *__restrict__ ry, const double *__restrict__ rz, InvBox B,
+                                int4 *cl_atoms, int *flags)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n_cells) return;
+    const int s = cell_start[c], e = cell_start[c + 1];
+    int cl = cl_start[c];
+    double emax = 0.0;
+    for (int p = s; p < e; p += 4, ++cl) {
+        int m[4];
+#pragma unroll
+        for (int t = 0; t < 4; ++t) m[t] = p + t < e ? cell_atoms[p + t] : -1;
+        cl_atoms[cl] = make_int4(m[0], m[1], m[2], m[3]);
+        double o[4][3], cc[3];
+        const int nk = cluster_offsets(m, rx, ry, rz, B, o, cc);
+        for (int k = 0; k < nk; ++k)
+            for (int a = 0; a < 3; ++a) emax = fmax(emax, fabs(o[k][a]));
+    }
+    if (emax > 0.0) atomicMax(&flags[5], __float_as_int(__double2float_ru(emax)));
+}
+
+// One warp per cluster: the cluster list (see the file comment).
+__global__ void __launch_bounds__(256) k_build_cluster_list(DevParams P, Grid g, InvBox B,
+                                                            const double *__restrict__ rx,
+                                                            const double *__restrict__ ry,
+                                                            const double *__restrict__ rz,
+                                                            const double4 *__restrict__ spos,
+                                                            const int *__restrict__ cell_start,
+                                                            const int4 *__restrict__ cl_atoms,
+                                                            const int *__restrict__ n_cl, int cap,
+                                                            uint32_t *__restrict__ nbr, int *__restrict__ nnb,
+                                                            unsigned char *__restrict__ cl_metal, double *rx0,
+                                                            double *ry0, double *rz0, int *flags)
+{
+    const int cl = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (cl >= *n_cl) return;
+    const int4 A = cl_atoms[cl];
+    const int m[4] = {A.x, A.y, A.z, A.w};
+    double o[4][3], cc[3];
+    const int nk = cluster_offsets(m, rx, ry, rz, B, o, cc);
+    double xm[4], ym[4], zm[4], R2 = 0.0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int a = k < nk ? m[k] : m[0];
+        xm[k] = rx[a];
+        ym[k] = ry[a];
+        zm[k] = rz[a];
+        if (k < nk) R2 = fmax(R2, o[k][0] * o[k][0] + o[k][1] * o[k][1] + o[k][2] * o[k][2]);
+    }
+    // prefilter radius, widened by a relative 1e-12 against rounding
+    const double pre = (sqrt(P.list_r2) + sqrt(R2)) * (1.0 + 1e-12);
+    const double pre2 = pre * pre;
+    // all members are in the cell of the first one (the cells were assigned
+    // from the same positions)
+    const int c0[3] = {cell_coord(xm[0], P.box.L[0], g.inv_len[0], g.n[0]),
+                       cell_coord(ym[0], P.box.L[1], g.inv_len[1], g.n[1]),
+                       cell_coord(zm[0], P.box.L[2], g.inv_len[2], g.n[2])};
+    const int nxs = axis_count(g.n[0]), nys = axis_count(g.n[1]);
+    const int nz = g.n[2];
+    const ZRuns zr = z_runs(c0[2], nz);
+    const unsigned lt_mask = (1u << lane) - 1u;
+    uint32_t *row = nbr + (size_t)cl * cap;
+    int count = 0;
+    bool metal = false;
+    for (int ix = 0; ix < nxs; ++ix) {
+        for (int iy = 0; iy < nys; ++iy) {
+            const int col = (axis_cell(c0[0], g.n[0], ix) * g.n[1] + axis_cell(c0[1], g.n[1], iy)) * nz;
+            for (int r = 0; r < zr.n; ++r) {
+                const int s = cell_start[col + zr.a[r]], e = cell_start[col + zr.b[r] + 1];
+                for (int base = s; base < e; base += 32) {
+                    const int p = base + lane;
+                    unsigned mask = 0;
+                    int j = 0;
+                    if (p < e) {
+                        const double4 q = spos[p];
+                        j = (int)q.w;
+                        const double ex = min_image(q.x - cc[0], B.L[0], B.inv[0]);
+                        const double ey = min_image(q.y - cc[1], B.L[1], B.inv[1]);
+                        const double ez = min_image(q.z - cc[2], B.L[2], B.inv[2]);
+                        if (ex * ex + ey * ey + ez * ez < pre2) {
+#pragma unroll
+                            for (int k = 0; k < 4; ++k) {
+                                if (k >= nk || j == m[k]) continue;
+                                double dx = q.x - xm[k], dy = q.y - ym[k], dz = q.z - zm[k];
+                                image(dx, dy, dz, P.box);
+                                if (norm2_exact(dx, dy, dz) < P.list_r2 && !excluded(P, m[k], j)) mask |= 1u << k;
+                            }
+                        }
+                    }
+                    const bool ok = mask != 0;
+                    const unsigned ballot = __ballot_sync(0xffffffffu, ok);
+                    const int pos = count + __popc(ballot & lt_mask);
+                    if (ok) {
+                        if (pos < cap) row[pos] = pack_cl(j, mask, P.type[j]);
+                        metal |= P.is_metal[j] != 0;
+                    }
+                    count += __popc(ballot);
+                }
+            }
+        }
+    }
+    metal = __any_sync(0xffffffffu, metal);
+    if (lane == 0) {
+        nnb[cl] = count < cap ? count : cap;
+        if (count > cap) atomicMax(&flags[4], count);
+        cl_metal[cl] = metal ? 1 : 0;
+    }
+    if (lane < nk) {
+        rx0[m[lane]] = lane == 0 ? xm[0] : lane == 1 ? xm[1] : lane == 2 ? xm[2] : xm[3];
+        ry0[m[lane]] = lane == 0 ? ym[0] : lane == 1 ? ym[1] : lane == 2 ? ym[2] : ym[3];
+        rz0[m[lane]] = lane == 0 ? zm[0] : lane == 1 ? zm[1] : lane == 2 ? zm[2] : zm[3];
+    }
+}
+
+// Pair-set fingerprint over the cluster list: per member i the j < i
+// entries of its mask inside the cut-off.
+__global__ void k_fingerprint_clusters(DevParams P, const double *__restrict__ rx, const double *__restrict__ ry,
+                                       const double *__restrict__ rz, const int4 *__restrict__ cl_atoms,
+                                       const int *__restrict__ n_cl, const uint32_t *__restrict__ nbr,
+                                       const int *__restrict__ nnb, int cap, unsigned long long *out)
+{
+    const int cl = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (cl >= *n_cl) return;
+    const int4 A = cl_atoms[cl];
+    const int m[4] = {A.x, A.y, A.z, A.w};
+    unsigned long long cnt = 0, h = 0;
+    for (int k = lane; k < nnb[cl]; k += 32) {
+        const uint32_t e = nbr[(size_t)cl * cap + k];
+        const int j = (int)(e & kClIdxMask);
+        const unsigned mask = (e >> kClMaskShift) & 15u;
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+            if (!((mask >> t) & 1u)) continue;
+            const int i = m[t];
+            if (j >= i) continue;
+            double dx = rx[j] - rx[i], dy = ry[j] - ry[i], dz = rz[j] - rz[i];
+            image(dx, dy, dz, P.box);
+            if (norm2_exact(dx, dy, dz) < P.rc2) {
+                ++cnt;
+                h += mix64(((uint64_t)(uint32_t)i << 32) | (uint32_t)j);
+            }
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+        h += __shfl_xor_sync(0xffffffffu, h, o);
+    }
+    if (lane == 0 && cnt) {
+        atomicAdd(&out[0], cnt);
+        atomicAdd(&out[1], h);
     }
 }
 
@@ -251,43 +502,138 @@ Grid make_grid(const capac_ctx *c)
     return g;
 }
 
-void build_list(capac_ctx *c)
+// Sub-cell Morton bits below the cell index: three per axis, as many as fit
+// a non-negative int key (at most 9).
+int sub_cell_bits(int n_cells)
+{
+    int b = 1;
+    while ((1L << b) < n_cells) ++b;
+    return std::max(0, std::min(9, (31 - b) / 3 * 3));
+}
+
+InvBox inv_box(const capac_ctx *c)
+{
+    InvBox B;
+    for (int a = 0; a < 3; ++a) {
+        B.L[a] = c->P.box.L[a];
+        B.inv[a] = 1.0 / c->P.box.L[a];
+    }
+    return B;
+}
+
+bool cluster_list_allowed(const capac_ctx *c)
+{
+    return c->opt.precision == CAPAC_PREC_MIXED && c->opt.pair_list == 0 && c->N < (1 << kClIdxBits) &&
+           c->P.n_types <= kClMaxTypes;
+}
+
+// Cluster slots and the first per-cluster capacity, from the densest
+// plausible environment of a cluster (radius rc + skin + 0.5 nm).
+void ensure_cluster_buffers(capac_ctx *c, int n_cells)
 {
     const int N = c->N;
-    const Grid g = make_grid(c);
-    const int n_cells = g.n[0] * g.n[1] * g.n[2];
-    if (n_cells != c->n_cells || !c->cell_start) {
-        cudaFree(c->cell_start);
-        c->cell_start = nullptr;
-        CAPAC_CUDA(cudaMalloc(&c->cell_start, sizeof(int) * (n_cells + 1)));
-        c->n_cells = n_cells;
+    if (n_cells != c->cl_cells) {
+        cudaFree(c->cl_cell_start);
+        cudaFree(c->cl_counts);
+        c->cl_cell_start = c->cl_counts = nullptr;
+        CAPAC_CUDA(cudaMalloc(&c->cl_cell_start, sizeof(int) * (n_cells + 1)));
+        CAPAC_CUDA(cudaMalloc(&c->cl_counts, sizeof(int) * (n_cells + 1)));
+        c->cl_cells = n_cells;
     }
-    if (!c->spos) CAPAC_CUDA(cudaMalloc(&c->spos, sizeof(double4) * N));
-    for (int a = 0; a < 3; ++a) c->ncell[a] = g.n[a];
+    const int need = N / 4 + n_cells + 1;
+    if (need > c->cl_max || !c->cl_nbr) {
+        if (c->cl_cap == 0) {
+            const double V = c->P.box.L[0] * c->P.box.L[1] * c->P.box.L[2];
+            const double rl = c->P.rc + c->opt.skin + 0.5;
+            const double dens = std::max((double)N / V, 60.0);
+            long est = (long)(1.25 * dens * 4.0 / 3.0 * M_PI * rl * rl * rl) + 64;
+            est = std::min<long>(est, (long)N);
+            c->cl_cap = (int)((est + 31) & ~31L);
+        }
+        cudaFree(c->cl_atoms);
+        cudaFree(c->cl_nbr);
+        cudaFree(c->cl_nnb);
+        cudaFree(c->cl_metal);
+        c->cl_atoms = nullptr;
+        c->cl_nbr = nullptr;
+        c->cl_nnb = nullptr;
+        c->cl_metal = nullptr;
+        CAPAC_CUDA(cudaMalloc(&c->cl_atoms, sizeof(int4) * need));
+        CAPAC_CUDA(cudaMalloc(&c->cl_nbr, sizeof(uint32_t) * (size_t)need * c->cl_cap));
+        CAPAC_CUDA(cudaMalloc(&c->cl_nnb, sizeof(int) * need));
+        CAPAC_CUDA(cudaMalloc(&c->cl_metal, need));
+        c->cl_max = need;
+    }
+}
+
+// Clusters of the sorted cells; returns false when the largest member offset
+// breaks the minimum-image condition (see the file comment).
+bool make_clusters(capac_ctx *c, int n_cells)
+{
     cudaStream_t s = c->stream;
-    k_cell_keys<<<grid_for(N, 256), 256, 0, s>>>(N, c->rx, c->ry, c->rz, c->P.box, g, c->cell_key, c->atom_ids);
-    ++c->launches;
-    int end_bit = 1;
-    while ((1 << end_bit) < n_cells) ++end_bit;
+    ensure_cluster_buffers(c, n_cells);
+    k_cluster_counts<<<grid_for(n_cells + 1, 256), 256, 0, s>>>(n_cells, c->cell_start, c->cl_counts);
     size_t need = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, need, c->cell_key, c->cell_key_sorted, c->atom_ids,
-                                    c->cell_atoms, N, 0, end_bit, s);
-    if (need > c->sort_tmp_bytes) {
-        cudaFree(c->sort_tmp);
-        CAPAC_CUDA(cudaMalloc(&c->sort_tmp, need));
-        c->sort_tmp_bytes = need;
+    cub::DeviceScan::ExclusiveSum(nullptr, need, c->cl_counts, c->cl_cell_start, n_cells + 1, s);
+    if (need > c->scan_tmp_bytes) {
+        cudaFree(c->scan_tmp);
+        c->scan_tmp = nullptr;
+        CAPAC_CUDA(cudaMalloc(&c->scan_tmp, need));
+        c->scan_tmp_bytes = need;
     }
-    CAPAC_CUDA(cub::DeviceRadixSort::SortPairs(c->sort_tmp, need, c->cell_key, c->cell_key_sorted,
-                                               c->atom_ids, c->cell_atoms, N, 0, end_bit, s));
-    k_cell_starts<<<grid_for(N + 1, 256), 256, 0, s>>>(N, n_cells, c->cell_key_sorted, c->cell_start);
-    k_sorted_positions<<<grid_for(N, 256), 256, 0, s>>>(N, c->cell_atoms, c->rx, c->ry, c->rz, c->spos);
-    c->launches += 2;
+    CAPAC_CUDA(cub::DeviceScan::ExclusiveSum(c->scan_tmp, need, c->cl_counts, c->cl_cell_start, n_cells + 1, s));
+    CAPAC_CUDA(cudaMemsetAsync(c->flags + 5, 0, sizeof(int), s));
+    k_make_clusters<<<grid_for(n_cells, 128), 128, 0, s>>>(n_cells, c->cell_start, c->cl_cell_start, c->cell_atoms,
+                                                           c->rx, c->ry, c->rz, inv_box(c), c->cl_atoms, c->flags);
+    c->launches += 3;
+    CAPAC_CUDA(cudaMemcpyAsync(c->h_flags + 6, c->cl_cell_start + n_cells, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CAPAC_CUDA(cudaMemcpyAsync(c->h_flags + 5, c->flags + 5, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CAPAC_CUDA(cudaStreamSynchronize(s));
+    c->n_clusters = c->h_flags[6];
+    float ext;
+    memcpy(&ext, &c->h_flags[5], sizeof ext);
+    const double half = 0.5 * std::min(c->P.box.L[0], std::min(c->P.box.L[1], c->P.box.L[2]));
+    return c->P.rc + (double)ext + c->opt.skin < half;
+}
+
+void build_cluster_list(capac_ctx *c, const Grid &g, int n_cells)
+{
+    cudaStream_t s = c->stream;
+    const int *n_cl = c->cl_cell_start + n_cells;
+    for (int attempt = 0; attempt < 4; ++attempt) {
+        CAPAC_CUDA(cudaMemsetAsync(c->flags + 4, 0, sizeof(int), s));
+        {
+            ProfScope ps(c, K_LIST);
+            k_build_cluster_list<<<grid_for((long)c->n_clusters * 32, 256), 256, 0, s>>>(
+                c->P, g, inv_box(c), c->rx, c->ry, c->rz, c->spos, c->cell_start, c->cl_atoms, n_cl, c->cl_cap,
+                c->cl_nbr, c->cl_nnb, c->cl_metal, c->rx0, c->ry0, c->rz0, c->flags);
+        }
+        ++c->launches;
+        CAPAC_CUDA(cudaMemcpyAsync(c->h_flags + 4, c->flags + 4, sizeof(int), cudaMemcpyDeviceToHost, s));
+        CAPAC_CUDA(cudaStreamSynchronize(s));
+        const int need_cap = c->h_flags[4];
+        if (need_cap <= c->cl_cap) return;
+        if (attempt == 3) throw Error(CAPAC_ERR_CAPACITY, "cluster list capacity could not be met");
+        int new_cap = (int)std::min<long>((long)(need_cap * 1.25) + 32, 1L << 20);
+        new_cap = (new_cap + 31) & ~31;
+        cudaFree(c->cl_nbr);
+        c->cl_nbr = nullptr;
+        CAPAC_CUDA(cudaMalloc(&c->cl_nbr, sizeof(uint32_t) * (size_t)c->cl_max * new_cap));
+        c->cl_cap = new_cap;
+    }
+}
+
+// Atom-list rows i0 .. i0 + rows - 1, growing the per-atom capacity as needed.
+void build_atom_rows(capac_ctx *c, const Grid &g, int i0, int rows)
+{
+    const int N = c->N;
+    cudaStream_t s = c->stream;
     for (int attempt = 0; attempt < 4; ++attempt) {
         CAPAC_CUDA(cudaMemsetAsync(c->flags + 1, 0, sizeof(int), s));
         {
             ProfScope ps(c, K_LIST);
-            k_build_list<<<grid_for((long)N * 32, 256), 256, 0, s>>>(
-                c->P, g, c->rx, c->ry, c->rz, c->spos, c->cell_start, c->cap, c->nbr, c->nnb, c->rx0,
+            k_build_list<<<grid_for((long)rows * 32, 256), 256, 0, s>>>(
+                c->P, g, i0, rows, c->rx, c->ry, c->rz, c->spos, c->cell_start, c->cap, c->nbr, c->nnb, c->rx0,
                 c->ry0, c->rz0, c->flags);
         }
         ++c->launches;
@@ -304,6 +650,54 @@ void build_list(capac_ctx *c)
         c->cap = new_cap;
         if (attempt == 3) throw Error(CAPAC_ERR_CAPACITY, "neighbour list capacity could not be met");
     }
+}
+
+void build_list(capac_ctx *c)
+{
+    const int N = c->N;
+    const Grid g = make_grid(c);
+    const int n_cells = g.n[0] * g.n[1] * g.n[2];
+    if (n_cells != c->n_cells || !c->cell_start) {
+        cudaFree(c->cell_start);
+        c->cell_start = nullptr;
+        CAPAC_CUDA(cudaMalloc(&c->cell_start, sizeof(int) * (n_cells + 1)));
+        c->n_cells = n_cells;
+    }
+    if (!c->spos) CAPAC_CUDA(cudaMalloc(&c->spos, sizeof(double4) * N));
+    for (int a = 0; a < 3; ++a) c->ncell[a] = g.n[a];
+    const int sub_bits = sub_cell_bits(n_cells);
+    c->cell_sub_bits = sub_bits;
+    cudaStream_t s = c->stream;
+    k_cell_keys<<<grid_for(N, 256), 256, 0, s>>>(N, c->rx, c->ry, c->rz, c->P.box, g, sub_bits, c->cell_key,
+                                                 c->atom_ids);
+    ++c->launches;
+    int end_bit = 1;
+    while ((1 << end_bit) < n_cells) ++end_bit;
+    end_bit += sub_bits;
+    size_t need = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, need, c->cell_key, c->cell_key_sorted, c->atom_ids,
+                                    c->cell_atoms, N, 0, end_bit, s);
+    if (need > c->sort_tmp_bytes) {
+        cudaFree(c->sort_tmp);
+        CAPAC_CUDA(cudaMalloc(&c->sort_tmp, need));
+        c->sort_tmp_bytes = need;
+    }
+    CAPAC_CUDA(cub::DeviceRadixSort::SortPairs(c->sort_tmp, need, c->cell_key, c->cell_key_sorted,
+                                               c->atom_ids, c->cell_atoms, N, 0, end_bit, s));
+    k_cell_starts<<<grid_for(N + 1, 256), 256, 0, s>>>(N, n_cells, sub_bits, c->cell_key_sorted, c->cell_start);
+    k_sorted_positions<<<grid_for(N, 256), 256, 0, s>>>(N, c->cell_atoms, c->rx, c->ry, c->rz, c->spos);
+    c->launches += 2;
+
+    bool use_cl = cluster_list_allowed(c) && make_clusters(c, n_cells);
+    if (use_cl) build_cluster_list(c, g, n_cells);
+    // atom-list rows: every atom on the atom path or when asked for, else
+    // the metal atoms (the CPIM kernels walk their rows)
+    if (!use_cl || c->need_full_list)
+        build_atom_rows(c, g, 0, N);
+    else if (c->M > 0)
+        build_atom_rows(c, g, c->metal_min, c->M);
+    c->clusters = use_cl;
+    c->atom_list_full = !use_cl || c->need_full_list;
     c->list_valid = true;
     ++c->list_builds;
 }
@@ -315,6 +709,12 @@ void launch_pack_positions(capac_ctx *c)
     k_pack<<<grid_for(c->N, 256), 256, 0, c->stream>>>(c->N, c->rx, c->ry, c->rz, c->charge, c->pos4,
                                                        c->pos4f);
     ++c->launches;
+}
+
+void ensure_full_atom_list(capac_ctx *c)
+{
+    c->need_full_list = true;
+    if (!c->list_valid || !c->atom_list_full) build_list(c);
 }
 
 void launch_list_maintenance(capac_ctx *c, bool force_rebuild)
@@ -339,8 +739,13 @@ void launch_pair_fingerprint(capac_ctx *c, int from_list, long *count, unsigned 
     CAPAC_CUDA(cudaMemsetAsync(d, 0, 2 * sizeof(unsigned long long), c->stream));
     if (from_list) {
         launch_list_maintenance(c, false);
-        k_fingerprint_list<<<grid_for((long)c->N * 32, 256), 256, 0, c->stream>>>(
-            c->P, c->rx, c->ry, c->rz, c->nbr, c->nnb, c->cap, d);
+        if (c->clusters)
+            k_fingerprint_clusters<<<grid_for((long)c->n_clusters * 32, 256), 256, 0, c->stream>>>(
+                c->P, c->rx, c->ry, c->rz, c->cl_atoms, c->cl_cell_start + c->n_cells, c->cl_nbr, c->cl_nnb,
+                c->cl_cap, d);
+        else
+            k_fingerprint_list<<<grid_for((long)c->N * 32, 256), 256, 0, c->stream>>>(
+                c->P, c->rx, c->ry, c->rz, c->nbr, c->nnb, c->cap, d);
     } else {
         k_fingerprint_all<<<grid_for((long)c->N * 32, 256), 256, 0, c->stream>>>(c->P, c->rx, c->ry, c->rz, d);
     }

@@ -468,6 +468,251 @@ __global__ void __launch_bounds__(kPairWarps * 32, sizeof(Real) == 4 ? 3 : 2) k_
     }
 }
 
+// Mixed path on the cluster list (k_list.cu): one warp per cluster of up to
+// four atoms.  Each entry (a j atom, its type, the mask of members it is a
+// list neighbour of) is loaded once; j's minimum-image difference from the
+// cluster centroid is formed in FP64 and rounded once, and the members' FP32
+// offsets from the centroid give each member's difference and r^2 in FP32,
+// cut as in k_pair.  The survivors go through the same per-warp queue and
+// pair terms as k_pair, tagged with their member.  Each lane adds its pair's
+// force in FP64 to its own slot of a shared-memory accumulator per member
+// and axis; at the end of the cluster the 32 slots are summed in a fixed
+// order, so the FP32 pair forces are summed without loss and run to run
+// identically.  Pair energies are summed per lane in FP64 too.  The member
+// tests run in a rolled loop with one flush site, which keeps the pair terms
+// in the code once.
+template <bool NONBONDED, bool CPIM>
+__global__ void __launch_bounds__(kPairWarps * 32, 3) k_pair_cl(DevParams P, PairConstsF K, const double4 *__restrict__ pos4,
+                                                              const int4 *__restrict__ cl_atoms,
+                                                              const int *__restrict__ n_cl,
+                                                              const uint32_t *__restrict__ nbr,
+                                                              const int *__restrict__ nnb,
+                                                              const unsigned char *__restrict__ cl_metal, int cap,
+                                                              const double *__restrict__ vec_pq,
+                                                              double *__restrict__ fx, double *__restrict__ fy,
+                                                              double *__restrict__ fz, double *__restrict__ partials)
+{
+    constexpr int NB = 2;
+    __shared__ Cand<float> queue[kPairWarps][64];
+    __shared__ float4 s_mem[kPairWarps][4];  // member offset from the centroid, charge
+    __shared__ int s_trow[kPairWarps][4];    // member type * n_types
+    __shared__ unsigned char s_cpim[kPairWarps][4];  // the member takes the CPIM force of metal neighbours
+    __shared__ double s_acc[kPairWarps][12][32];  // force on (member, axis) per lane slot
+    __shared__ double sh[32 * 11];
+    __shared__ double wacc[kPairWarps][8];
+    __shared__ __align__(16) TypePairF s_tpf[kSmemTypes * kSmemTypes];
+    __shared__ unsigned char s_metal[kSmemTypes];
+    const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const unsigned lt_mask = (1u << lane) - 1u;
+    Cand<float> *Q = queue[wib];
+    if (lane < 8) wacc[wib][lane] = 0.0;
+    const bool smem_types = P.n_types <= kSmemTypes;
+    if (smem_types) {
+        const int nt2 = P.n_types * P.n_types;
+        for (int k = threadIdx.x; k < nt2; k += blockDim.x) s_tpf[k] = make_type_pair_f(P, K, k);
+        for (int k = threadIdx.x; k < P.n_types; k += blockDim.x) s_metal[k] = P.type_metal[k];
+    }
+    __syncthreads();
+    const bool metal_by_type = smem_types && P.metal_by_type;
+    const double L[3] = {P.box.L[0], P.box.L[1], P.box.L[2]};
+    const double iL[3] = {1.0 / L[0], 1.0 / L[1], 1.0 / L[2]};
+    const int ncl = *n_cl;
+    const int stride = gridDim.x * kPairWarps;
+    for (int cl = blockIdx.x * kPairWarps + wib; cl < ncl; cl += stride) {
+        const int4 A = cl_atoms[cl];
+        const int nk = 1 + (A.y >= 0) + (A.z >= 0) + (A.w >= 0);
+        const int mine = lane == 0 ? A.x : lane == 1 ? A.y : lane == 2 ? A.z : A.w;
+        double4 pm = make_double4(0.0, 0.0, 0.0, 0.0);
+        if (lane < nk) pm = pos4[mine];
+        const double x0 = __shfl_sync(0xffffffffu, pm.x, 0), y0 = __shfl_sync(0xffffffffu, pm.y, 0),
+                     z0 = __shfl_sync(0xffffffffu, pm.z, 0);
+        double ox = 0.0, oy = 0.0, oz = 0.0;
+        if (lane < nk) {
+            ox = min_image(pm.x - x0, L[0], iL[0]);
+            oy = min_image(pm.y - y0, L[1], iL[1]);
+            oz = min_image(pm.z - z0, L[2], iL[2]);
+        }
+        // member mean offset: lanes 0..3 hold the offsets, the others zero
+        double sx = ox, sy = oy, sz = oz;
+#pragma unroll
+        for (int o = 1; o <= 2; o <<= 1) {
+            sx += __shfl_xor_sync(0xffffffffu, sx, o);
+            sy += __shfl_xor_sync(0xffffffffu, sy, o);
+            sz += __shfl_xor_sync(0xffffffffu, sz, o);
+        }
+        const double inv_nk = 1.0 / nk;
+        const double mx = __shfl_sync(0xffffffffu, sx, 0) * inv_nk, my = __shfl_sync(0xffffffffu, sy, 0) * inv_nk,
+                     mz = __shfl_sync(0xffffffffu, sz, 0) * inv_nk;
+        const double cx = x0 + mx, cy = y0 + my, cz = z0 + mz;
+        if (lane < nk) {
+            s_mem[wib][lane] = make_float4((float)(ox - mx), (float)(oy - my), (float)(oz - mz), (float)pm.w);
+            s_trow[wib][lane] = P.type[mine] * P.n_types;
+            s_cpim[wib][lane] = CPIM && P.is_metal[mine] == 0 && pm.w != 0.0;
+        }
+#pragma unroll
+        for (int q = 0; q < 12; ++q) s_acc[wib][q][lane] = 0.0;
+        __syncwarp();
+        const bool cpim_cl = CPIM && cl_metal[cl] != 0;
+        const int n = nnb[cl];
+        const uint32_t *row = nbr + (size_t)cl * cap;
+        double e_qq = 0.0, e_vdw = 0.0;  // per pair in FP64: a cluster's lane sums ~100 pairs
+        float v[6];
+#pragma unroll
+        for (int q = 0; q < 6; ++q) v[q] = 0.f;
+
+        // pair terms of the first cnt queue entries into the lanes' slots
+        auto flush = [&](int cnt) {
+            if (lane < cnt) {
+                float g0 = 0.f, g1 = 0.f, g2 = 0.f;
+                const Cand<float> c = Q[lane];
+                const int k = (int)((c.e >> kClMaskShift) & 3u);
+                const int tj = (int)(c.e >> kClTypeShift);
+                const float4 mk = s_mem[wib][k];
+                if (NONBONDED) {
+                    const int tp = s_trow[wib][k] + tj;
+                    float eq = 0.f, ev = 0.f;
+                    const float f = pair_term_f(K, smem_types ? s_tpf[tp] : make_type_pair_f(P, K, tp), mk.w, c.qj,
+                                                c.r2, eq, ev);
+                    e_qq += (double)eq;
+                    e_vdw += (double)ev;
+                    const float gx = f * c.dx, gy = f * c.dy, gz = f * c.dz;
+                    g0 = -gx;
+                    g1 = -gy;
+                    g2 = -gz;
+                    v[0] -= c.dx * gx; v[1] -= c.dx * gy; v[2] -= c.dx * gz;
+                    v[3] -= c.dy * gy; v[4] -= c.dy * gz; v[5] -= c.dz * gz;
+                }
+                if (cpim_cl && s_cpim[wib][k]) {
+                    const int j = (int)(c.e & kClIdxMask);
+                    const bool mj = metal_by_type ? s_metal[tj] != 0 : P.is_metal[j] != 0;
+                    if (mj) {
+                        const int jm = j - P.metal_min;
+                        const float r[3] = {c.dx, c.dy, c.dz};  // metal - atom
+                        const float p[3] = {(float)vec_pq[3 * jm], (float)vec_pq[3 * jm + 1],
+                                            (float)vec_pq[3 * jm + 2]};
+                        float g[3];
+                        cpim_charge_pair_f(K, r, c.r2, mk.w, (float)vec_pq[3 * P.M + jm], p, g);
+                        g0 -= g[0];
+                        g1 -= g[1];
+                        g2 -= g[2];
+                    }
+                }
+                s_acc[wib][3 * k][lane] += (double)g0;
+                s_acc[wib][3 * k + 1][lane] += (double)g1;
+                s_acc[wib][3 * k + 2][lane] += (double)g2;
+            }
+        };
+
+        int qn = 0;  // queue fill, warp-uniform
+        uint32_t nxt[NB];
+#pragma unroll
+        for (int u = 0; u < NB; ++u) {
+            const int k = u * 32 + lane;
+            nxt[u] = k < n ? __ldcs(row + k) : 0u;
+        }
+        for (int base = 0; base < n; base += 32 * NB) {
+            uint32_t ev[NB];
+            bool valid[NB];
+#pragma unroll
+            for (int u = 0; u < NB; ++u) {
+                valid[u] = base + u * 32 + lane < n;
+                ev[u] = nxt[u];
+                const int k = base + (NB + u) * 32 + lane;
+                nxt[u] = k < n ? __ldcs(row + k) : 0u;
+            }
+            double4 pj[NB];
+#pragma unroll
+            for (int u = 0; u < NB; ++u)
+                if (valid[u]) pj[u] = pos4[ev[u] & kClIdxMask];
+            static_assert(NB == 2, "the member loop selects between two chunks");
+            float dxc[NB], dyc[NB], dzc[NB], qj[NB];
+            unsigned mask[NB];
+            uint32_t keep[NB];
+#pragma unroll
+            for (int u = 0; u < NB; ++u) {
+                dxc[u] = dyc[u] = dzc[u] = qj[u] = 0.f;
+                mask[u] = 0;
+                if (valid[u]) {
+                    dxc[u] = (float)min_image(pj[u].x - cx, L[0], iL[0]);
+                    dyc[u] = (float)min_image(pj[u].y - cy, L[1], iL[1]);
+                    dzc[u] = (float)min_image(pj[u].z - cz, L[2], iL[2]);
+                    qj[u] = (float)pj[u].w;
+                    mask[u] = (ev[u] >> kClMaskShift) & 15u;
+                }
+                keep[u] = ev[u] & ~(15u << kClMaskShift);
+            }
+            // (chunk, member) tests in a rolled loop: one flush site
+#pragma unroll 1
+            for (int t = 0; t < NB * nk; ++t) {
+                const bool hi = t >= nk;
+                const int kk = hi ? t - nk : t;
+                const float4 mk = s_mem[wib][kk];
+                const float dx = (hi ? dxc[1] : dxc[0]) - mk.x, dy = (hi ? dyc[1] : dyc[0]) - mk.y,
+                            dz = (hi ? dzc[1] : dzc[0]) - mk.z;
+                const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+                const bool ok = (((hi ? mask[1] : mask[0]) >> kk) & 1u) && r2 < K.rc2;
+                const unsigned ballot = __ballot_sync(0xffffffffu, ok);
+                if (ok) {
+                    Cand<float> c;
+                    c.dx = dx;
+                    c.dy = dy;
+                    c.dz = dz;
+                    c.r2 = r2;
+                    c.qj = hi ? qj[1] : qj[0];
+                    c.e = (hi ? keep[1] : keep[0]) | ((uint32_t)kk << kClMaskShift);
+                    Q[qn + __popc(ballot & lt_mask)] = c;
+                }
+                qn += __popc(ballot);
+                __syncwarp();
+                if (qn >= 32) {
+                    flush(32);
+                    __syncwarp();
+                    if (lane < qn - 32) Q[lane] = Q[lane + 32];
+                    __syncwarp();
+                    qn -= 32;
+                }
+            }
+        }
+        if (qn > 0) flush(qn);
+        __syncwarp();
+
+        // member forces: lane 3 k + a sums the 32 slots of (k, a), starting
+        // at its own slot (no bank conflicts), in a fixed order
+        if (lane < 3 * nk) {
+            const int k = lane / 3, a = lane - 3 * k;
+            double s = 0.0;
+#pragma unroll 8
+            for (int q = 0; q < 32; ++q) s += s_acc[wib][lane][(q + lane) & 31];
+            const int atom = k == 0 ? A.x : k == 1 ? A.y : k == 2 ? A.z : A.w;
+            double *f = a == 0 ? fx : (a == 1 ? fy : fz);
+            f[atom] += s;
+        }
+        if (NONBONDED) {
+            const double t[8] = {warp_sum(e_qq), warp_sum(e_vdw), warp_sum((double)v[0]),
+                                 warp_sum((double)v[1]), warp_sum((double)v[2]), warp_sum((double)v[3]),
+                                 warp_sum((double)v[4]), warp_sum((double)v[5])};
+            if (lane == 0) {
+#pragma unroll
+                for (int q = 0; q < 8; ++q) wacc[wib][q] += 0.5 * t[q];
+            }
+        }
+        __syncwarp();
+    }
+    if (NONBONDED) {
+        __syncthreads();
+        double acc[11] = {0.0};
+        if (threadIdx.x < kPairWarps) {
+            const double *w = wacc[threadIdx.x];
+            acc[0] = w[0];
+            acc[1] = w[1];
+            acc[2] = w[2]; acc[3] = w[3]; acc[4] = w[4];
+            acc[5] = w[3]; acc[6] = w[5]; acc[7] = w[6];
+            acc[8] = w[4]; acc[9] = w[6]; acc[10] = w[7];
+        }
+        block_partials<11>(acc, sh, partials);
+    }
+}
+
 PairConstsF pair_consts_f(const capac_ctx *c)
 {
     PairConstsF K;
@@ -504,11 +749,35 @@ void launch_pair_t(capac_ctx *c, int mode, unsigned grid)
     ++c->launches;
 }
 
+void launch_pair_clusters(capac_ctx *c, int mode, unsigned grid)
+{
+    const PairConstsF K = pair_consts_f(c);
+    const bool cpim = c->M > 0 && c->use_cpff;
+    const int *n_cl = c->cl_cell_start + c->n_cells;
+    ProfScope ps(c, K_PAIR);
+    if (mode == 0 && cpim)
+        k_pair_cl<true, true><<<grid, kPairWarps * 32, 0, c->stream>>>(c->P, K, c->pos4, c->cl_atoms, n_cl, c->cl_nbr,
+                                                                      c->cl_nnb, c->cl_metal, c->cl_cap, c->vec_pq,
+                                                                      c->fx, c->fy, c->fz, c->partials);
+    else if (mode == 0)
+        k_pair_cl<true, false><<<grid, kPairWarps * 32, 0, c->stream>>>(c->P, K, c->pos4, c->cl_atoms, n_cl, c->cl_nbr,
+                                                                       c->cl_nnb, c->cl_metal, c->cl_cap, c->vec_pq,
+                                                                       c->fx, c->fy, c->fz, c->partials);
+    else
+        k_pair_cl<false, true><<<grid, kPairWarps * 32, 0, c->stream>>>(c->P, K, c->pos4, c->cl_atoms, n_cl, c->cl_nbr,
+                                                                       c->cl_nnb, c->cl_metal, c->cl_cap, c->vec_pq,
+                                                                       c->fx, c->fy, c->fz, c->partials);
+    ++c->launches;
+}
+
 }  // namespace
 
+// Blocks of the pair launch: one warp per atom (or per cluster), at most 16
+// blocks per SM (grid-stride beyond).
 unsigned pair_grid(const capac_ctx *c)
 {
-    const long need = (c->N + kPairWarps - 1) / kPairWarps;
+    const long units = c->clusters ? c->n_clusters : c->N;
+    const long need = (units + kPairWarps - 1) / kPairWarps;
     const long cap = (long)c->num_sms * 16;
     return (unsigned)std::max(1L, std::min(need, cap));
 }
@@ -516,7 +785,9 @@ unsigned pair_grid(const capac_ctx *c)
 void launch_pair_forces(capac_ctx *c, int mode)
 {
     const unsigned grid = pair_grid(c);
-    if (c->opt.precision == CAPAC_PREC_MIXED)
+    if (c->clusters)
+        launch_pair_clusters(c, mode, grid);
+    else if (c->opt.precision == CAPAC_PREC_MIXED)
         launch_pair_t<float>(c, mode, grid);
     else
         launch_pair_t<double>(c, mode, grid);

@@ -184,6 +184,9 @@ typedef struct capac_options {
                                solve when the device supports it (default), 1 a launch per vector step */
     int inner_precond;      /* mixed path, persistent solver: preconditioner of the inner solves,
                                0 the reference's Jacobi, 1 block-Jacobi on 32-atom groups (default) */
+    int pair_list;          /* mixed path nonbonded list: 0 clusters of four atoms sharing each
+                               neighbour's load where the box is large enough (default), 1 one list
+                               per atom (the FP64 path always uses one list per atom) */
 } capac_options;
 
 void capac_options_default(capac_options *o);
@@ -286,13 +289,18 @@ int capac_checkpoint_load(capac_ctx *ctx, const char *path);
  * diag_relay (n_mat) inv_sqrt_dens(n_metal) vQ(10) thermo(4: eKsum inst_temp
  * ref_temp ndf) box(6); after a gradient call (read only, n_mat each):
  * adjoint_dedx (dE/dx), adjoint_dpsidx (dPsi/dx of the force matching),
- * adjoint_mu, adjoint_nu (the adjoint solutions).  capac_get returns the
- * count written, <0 on error. */
+ * adjoint_mu, adjoint_nu (the adjoint solutions).  Read-only diagnostics:
+ * pair_list(2: 1 when the pair kernel walks the cluster list, cluster count),
+ * solver_phases(9: mean ns per iteration of the persistent solver's phases
+ * when CAPAC_SOLVER_PHASES is set, then the iterations timed).  capac_get
+ * returns the count written, <0 on error. */
 int capac_get(capac_ctx *ctx, const char *name, double *out);
 int capac_set(capac_ctx *ctx, const char *name, const double *in);
 
 /* Statistics of the last force call: BiCGSTAB iterations, neighbour-list
- * rebuilds so far, list entries, pairs inside the cut-off. */
+ * rebuilds so far, list entries, pairs inside the cut-off.  list_entries,
+ * max_neighbors and list_capacity describe the list the pair kernel walks:
+ * per cluster of four atoms on the mixed path's cluster list, else per atom. */
 typedef struct capac_stats {
     int solver_iterations;
     int solver_outer;           /* refinement sweeps (mixed path) */

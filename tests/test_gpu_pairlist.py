@@ -1,0 +1,140 @@
+"""Cluster-pair list of the mixed path against the atom list and the reference.
+
+The mixed path walks a list per cluster of four atoms (k_list.cu, k_pair.cu)
+when the box is large enough for the cluster's shared minimum image; every
+member keeps exactly the atom list's pairs (the reference's r^2 rounding and
+exclusions at the build, the cut-off in FP32 every step).  Checked here: the
+pair set equals the reference's (count and hash of all pairs inside the
+cut-off, mpi_nonb_pair force.c:1419-1473), forces, energies and virial equal
+the atom-list kernel's within FP32 rounding and the FP64 path's within the
+mixed path's 1e-5 bar, through list rebuilds in MD, and the gradients that
+switch the build to full atom rows.
+"""
+import numpy as np
+import pytest
+
+import capacmd_b200 as cm
+from capacmd_b200 import configs
+from conftest import golden_paths, golden_ref, rel_err
+
+pytestmark = pytest.mark.gpu
+
+# boxes with rc + cluster extent + skin below half the shortest edge
+CLUSTER_CASES = ["t_au13", "t_2np", "c1", "c1_field"]
+ATOM_CASES = ["t_au55w", "t_water"]
+
+
+@pytest.fixture(autouse=True)
+def _need_gpu(gpu_available):
+    if not gpu_available:
+        pytest.fail("no sm_100 GPU: GPU tests must run on a B200")
+
+
+def _mixed(paths, **kw):
+    d = cm.Desc.from_paths(paths)
+    return d, cm.Simulation(d, precision=cm.PREC_MIXED, **kw)
+
+
+def _uses_clusters(sim) -> bool:
+    return sim.get("pair_list")[0] == 1.0
+
+
+@pytest.mark.parametrize("case", CLUSTER_CASES + ATOM_CASES)
+def test_path_choice_and_pair_set(case):
+    d, s = _mixed(golden_paths(case))
+    g = golden_ref(case)
+    ref = (int(g["pair_count"]), int(g["pair_hash"]))
+    assert s.pair_fingerprint(from_list=True) == ref
+    assert _uses_clusters(s) == (case in CLUSTER_CASES)
+    _, a = _mixed(golden_paths(case), pair_list=1)
+    assert a.pair_fingerprint(from_list=True) == ref
+    assert not _uses_clusters(a)
+
+
+def test_medium_system_pair_set():
+    p = configs.cached("c2")
+    d, s = _mixed(p)
+    fp = s.pair_fingerprint(from_list=True)
+    assert _uses_clusters(s)
+    assert fp == s.pair_fingerprint(from_list=False)
+    st = s.stats()
+    _, a = _mixed(p, pair_list=1)
+    a.force()
+    sa = a.stats()
+    # a cluster's list is shared by its members: fewer entries than the
+    # atom list
+    assert 0 < st.list_entries < sa.list_entries
+    assert st.max_neighbors <= st.list_capacity
+
+
+@pytest.mark.parametrize("case", ["t_2np", "c1_field", "c2"])
+def test_cluster_forces_match_atom_list_and_fp64(case):
+    paths = configs.cached(case) if case == "c2" else golden_paths(case)
+    d, cl = _mixed(paths, refine_tol=1e-11)
+    _, at = _mixed(paths, refine_tol=1e-11, pair_list=1)
+    f64 = cm.Simulation(d, precision=cm.PREC_FP64, solver_tol=1e-24)
+    for s in (cl, at, f64):
+        s.force()
+    assert _uses_clusters(cl) and not _uses_clusters(at)
+    # FP32 rounding of the differences: one more rounding than the atom kernel
+    assert rel_err(cl.forces(), at.forces()) < 2e-6
+    assert rel_err(cl.forces(), f64.forces()) < 1e-5
+    pc, pa, p64 = cl.get("potential"), at.get("potential"), f64.get("potential")
+    # the pair energies nearly cancel (FP32 terms of +-100 kJ/mol summing to
+    # tens): bars relative to the magnitude of the terms, as for the mixed path
+    scale = np.abs(p64[1:]).sum()
+    for k in (7, 8):  # Coulomb and van der Waals sums of the pair kernel
+        assert abs(pc[k] - p64[k]) <= 1e-5 * scale
+        assert abs(pa[k] - p64[k]) <= 1e-5 * scale
+    assert abs(pc[1:].sum() - p64[1:].sum()) <= 1e-5 * scale
+    assert rel_err(cl.get("virial"), at.get("virial")) < 1e-5
+    if d.n_mat:
+        assert rel_err(cl.get("vec_pq"), f64.get("vec_pq")) < 1e-8
+
+
+def test_cluster_md_through_rebuilds():
+    p = configs.cached("c2")
+    d, cl = _mixed(p)
+    _, at = _mixed(p, pair_list=1)
+    f64 = cm.Simulation(d, precision=cm.PREC_FP64)
+    for s in (cl, at, f64):
+        s.md_init()
+    e = {id(s): [] for s in (cl, at, f64)}
+    for _ in range(60):
+        for s in (cl, at, f64):
+            s.md_steps(1)
+            e[id(s)].append(s.get("potential")[0])
+    assert cl.stats().list_builds >= 2
+    assert _uses_clusters(cl)
+    ec, ea, e64 = (np.array(e[id(s)]) for s in (cl, at, f64))
+    scale = np.abs(e64).max()
+    assert np.abs(ec - ea).max() <= 1e-5 * scale
+    assert np.abs(ec - e64).max() <= 1e-5 * scale
+    # 60 fs of trajectories that differ by FP32 rounding from the first step
+    assert rel_err(cl.get("rx"), f64.get("rx")) < 1e-5
+    assert rel_err(at.get("rx"), f64.get("rx")) < 1e-5
+
+
+def test_gradients_on_the_cluster_path():
+    """The force-matching gradient walks every atom row: the build switches
+    to full atom rows and the pair kernel stays on the clusters."""
+    paths = golden_paths("t_2np")
+    d, cl = _mixed(paths, refine_tol=1e-11)
+    _, at = _mixed(paths, refine_tol=1e-11, pair_list=1)
+    for s in (cl, at):
+        s.set("vec_pq", np.zeros(d.n_mat))
+        s.force()
+    # residuals F - target of half the forces, so that the two paths' FP32
+    # force rounding (~1e-6 of the largest force) moves the loss little
+    target = at.forces() * 0.5
+    lc, gc, rc_ = cl.force_match_grad(target, positions=True)
+    la, ga, ra = at.force_match_grad(target, positions=True)
+    assert _uses_clusters(cl)
+    assert lc == pytest.approx(la, rel=1e-5)
+    for name in cm.PARAMS:
+        assert abs(gc[name] - ga[name]) <= 1e-5 * abs(ga[name]) + 1e-12, name
+    assert rel_err(rc_, ra) < 1e-5
+    # the pair kernel still runs on the clusters after the full rebuild
+    cl.md_init()
+    cl.md_steps(5)
+    assert _uses_clusters(cl)
