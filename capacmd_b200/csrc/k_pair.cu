@@ -478,11 +478,15 @@ __global__ void __launch_bounds__(kPairWarps * 32, sizeof(Real) == 4 ? 3 : 2) k_
 // force in FP64 to its own slot of a shared-memory accumulator per member
 // and axis; at the end of the cluster the 32 slots are summed in a fixed
 // order, so the FP32 pair forces are summed without loss and run to run
-// identically.  Pair energies are summed per lane in FP64 too.  The member
-// tests run in a rolled loop with one flush site, which keeps the pair terms
-// in the code once.
+// identically.  Pair energies are summed per lane in FP64 too.  Per chunk of
+// 32 entries the four member tests run in straight-line code and append up to
+// 128 pairs to the warp's queue (dynamic shared memory, kClQueue entries);
+// full flushes of 32 follow at one site, which keeps the pair terms in the
+// code once.
+constexpr int kClQueue = 160;  // < 32 left over + 4 x 32 appended
+constexpr size_t kClQueueBytes = (size_t)kPairWarps * kClQueue * sizeof(Cand<float>);
 template <bool NONBONDED, bool CPIM>
-__global__ void __launch_bounds__(kPairWarps * 32, 3) k_pair_cl(DevParams P, PairConstsF K, const double4 *__restrict__ pos4,
+__global__ void __launch_bounds__(kPairWarps * 32, 2) k_pair_cl(DevParams P, PairConstsF K, const double4 *__restrict__ pos4,
                                                               const int4 *__restrict__ cl_atoms,
                                                               const int *__restrict__ n_cl,
                                                               const uint32_t *__restrict__ nbr,
@@ -493,7 +497,7 @@ __global__ void __launch_bounds__(kPairWarps * 32, 3) k_pair_cl(DevParams P, Pai
                                                               double *__restrict__ fz, double *__restrict__ partials)
 {
     constexpr int NB = 2;
-    __shared__ Cand<float> queue[kPairWarps][64];
+    extern __shared__ __align__(16) unsigned char s_dyn[];  // the warps' queues
     __shared__ float4 s_mem[kPairWarps][4];  // member offset from the centroid, charge
     __shared__ int s_trow[kPairWarps][4];    // member type * n_types
     __shared__ unsigned char s_cpim[kPairWarps][4];  // the member takes the CPIM force of metal neighbours
@@ -504,7 +508,7 @@ __global__ void __launch_bounds__(kPairWarps * 32, 3) k_pair_cl(DevParams P, Pai
     __shared__ unsigned char s_metal[kSmemTypes];
     const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const unsigned lt_mask = (1u << lane) - 1u;
-    Cand<float> *Q = queue[wib];
+    Cand<float> *Q = reinterpret_cast<Cand<float> *>(s_dyn) + wib * kClQueue;
     if (lane < 8) wacc[wib][lane] = 0.0;
     const bool smem_types = P.n_types <= kSmemTypes;
     if (smem_types) {
@@ -560,11 +564,12 @@ __global__ void __launch_bounds__(kPairWarps * 32, 3) k_pair_cl(DevParams P, Pai
 #pragma unroll
         for (int q = 0; q < 6; ++q) v[q] = 0.f;
 
-        // pair terms of the first cnt queue entries into the lanes' slots
-        auto flush = [&](int cnt) {
+        // pair terms of the queue entries head .. head + cnt - 1 into the
+        // lanes' slots
+        auto flush = [&](int head, int cnt) {
             if (lane < cnt) {
                 float g0 = 0.f, g1 = 0.f, g2 = 0.f;
-                const Cand<float> c = Q[lane];
+                const Cand<float> c = Q[head + lane];
                 const int k = (int)((c.e >> kClMaskShift) & 3u);
                 const int tj = (int)(c.e >> kClTypeShift);
                 const float4 mk = s_mem[wib][k];
@@ -641,39 +646,53 @@ __global__ void __launch_bounds__(kPairWarps * 32, 3) k_pair_cl(DevParams P, Pai
                 }
                 keep[u] = ev[u] & ~(15u << kClMaskShift);
             }
-            // (chunk, member) tests in a rolled loop: one flush site
+            // per chunk: the member tests in straight-line code (mask bits
+            // exist only for members < nk), the survivors appended to the
+            // queue, then the full flushes and the remainder moved to the front
 #pragma unroll 1
-            for (int t = 0; t < NB * nk; ++t) {
-                const bool hi = t >= nk;
-                const int kk = hi ? t - nk : t;
-                const float4 mk = s_mem[wib][kk];
-                const float dx = (hi ? dxc[1] : dxc[0]) - mk.x, dy = (hi ? dyc[1] : dyc[0]) - mk.y,
-                            dz = (hi ? dzc[1] : dzc[0]) - mk.z;
-                const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-                const bool ok = (((hi ? mask[1] : mask[0]) >> kk) & 1u) && r2 < K.rc2;
-                const unsigned ballot = __ballot_sync(0xffffffffu, ok);
-                if (ok) {
-                    Cand<float> c;
-                    c.dx = dx;
-                    c.dy = dy;
-                    c.dz = dz;
-                    c.r2 = r2;
-                    c.qj = hi ? qj[1] : qj[0];
-                    c.e = (hi ? keep[1] : keep[0]) | ((uint32_t)kk << kClMaskShift);
-                    Q[qn + __popc(ballot & lt_mask)] = c;
+            for (int u = 0; u < NB; ++u) {
+                const bool hi = u == 1;
+                const float bx = hi ? dxc[1] : dxc[0], by = hi ? dyc[1] : dyc[0], bz = hi ? dzc[1] : dzc[0];
+                const float bq = hi ? qj[1] : qj[0];
+                const unsigned bm = hi ? mask[1] : mask[0];
+                const uint32_t bk = hi ? keep[1] : keep[0];
+#pragma unroll
+                for (int kk = 0; kk < 4; ++kk) {
+                    const float4 mk = s_mem[wib][kk];
+                    const float dx = bx - mk.x, dy = by - mk.y, dz = bz - mk.z;
+                    const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+                    const bool ok = ((bm >> kk) & 1u) && r2 < K.rc2;
+                    const unsigned ballot = __ballot_sync(0xffffffffu, ok);
+                    if (ok) {
+                        Cand<float> c;
+                        c.dx = dx;
+                        c.dy = dy;
+                        c.dz = dz;
+                        c.r2 = r2;
+                        c.qj = bq;
+                        c.e = bk | ((uint32_t)kk << kClMaskShift);
+                        Q[qn + __popc(ballot & lt_mask)] = c;
+                    }
+                    qn += __popc(ballot);
                 }
-                qn += __popc(ballot);
                 __syncwarp();
-                if (qn >= 32) {
-                    flush(32);
+                int head = 0;
+                while (qn - head >= 32) {
+                    flush(head, 32);
+                    head += 32;
+                }
+                if (head > 0) {
+                    const int rest = qn - head;
+                    Cand<float> tmp;
+                    if (lane < rest) tmp = Q[head + lane];
                     __syncwarp();
-                    if (lane < qn - 32) Q[lane] = Q[lane + 32];
+                    if (lane < rest) Q[lane] = tmp;
                     __syncwarp();
-                    qn -= 32;
+                    qn = rest;
                 }
             }
         }
-        if (qn > 0) flush(qn);
+        if (qn > 0) flush(0, qn);
         __syncwarp();
 
         // member forces: lane 3 k + a sums the 32 slots of (k, a), starting
@@ -749,24 +768,27 @@ void launch_pair_t(capac_ctx *c, int mode, unsigned grid)
     ++c->launches;
 }
 
+template <bool NONBONDED, bool CPIM>
+void launch_pair_cl_t(capac_ctx *c, unsigned grid)
+{
+    // the queues and the static arrays together exceed the default 48 KB
+    CAPAC_CUDA(cudaFuncSetAttribute(k_pair_cl<NONBONDED, CPIM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)kClQueueBytes));
+    k_pair_cl<NONBONDED, CPIM><<<grid, kPairWarps * 32, kClQueueBytes, c->stream>>>(
+        c->P, pair_consts_f(c), c->pos4, c->cl_atoms, c->cl_cell_start + c->n_cells, c->cl_nbr, c->cl_nnb,
+        c->cl_metal, c->cl_cap, c->vec_pq, c->fx, c->fy, c->fz, c->partials);
+}
+
 void launch_pair_clusters(capac_ctx *c, int mode, unsigned grid)
 {
-    const PairConstsF K = pair_consts_f(c);
     const bool cpim = c->M > 0 && c->use_cpff;
-    const int *n_cl = c->cl_cell_start + c->n_cells;
     ProfScope ps(c, K_PAIR);
     if (mode == 0 && cpim)
-        k_pair_cl<true, true><<<grid, kPairWarps * 32, 0, c->stream>>>(c->P, K, c->pos4, c->cl_atoms, n_cl, c->cl_nbr,
-                                                                      c->cl_nnb, c->cl_metal, c->cl_cap, c->vec_pq,
-                                                                      c->fx, c->fy, c->fz, c->partials);
+        launch_pair_cl_t<true, true>(c, grid);
     else if (mode == 0)
-        k_pair_cl<true, false><<<grid, kPairWarps * 32, 0, c->stream>>>(c->P, K, c->pos4, c->cl_atoms, n_cl, c->cl_nbr,
-                                                                       c->cl_nnb, c->cl_metal, c->cl_cap, c->vec_pq,
-                                                                       c->fx, c->fy, c->fz, c->partials);
+        launch_pair_cl_t<true, false>(c, grid);
     else
-        k_pair_cl<false, true><<<grid, kPairWarps * 32, 0, c->stream>>>(c->P, K, c->pos4, c->cl_atoms, n_cl, c->cl_nbr,
-                                                                       c->cl_nnb, c->cl_metal, c->cl_cap, c->vec_pq,
-                                                                       c->fx, c->fy, c->fz, c->partials);
+        launch_pair_cl_t<false, true>(c, grid);
     ++c->launches;
 }
 
