@@ -316,7 +316,7 @@ def main() -> int:
     # end to end through the drop-in mpi_force with pinned host buffers
     e2e = None
     if not args.no_e2e:
-        e2e = e2e_drop_in(sim, desc, args.e2e_calls, configs.WORKLOADS[args.workload].dt, torch)
+        e2e = e2e_drop_in(sim, desc, args.e2e_calls, prec, local, torch)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -521,50 +521,50 @@ def _traffic(workload: str, precision: str, kernel: str):
         return None
 
 
-def e2e_drop_in(sim, desc, calls: int, dt: float, torch) -> dict:
+def e2e_drop_in(sim, desc, calls: int, prec: int, device: int, torch) -> dict:
     """atom-steps/s through capac_mpi_force with pinned host buffers: positions
     (and the induced-vector warm start) copied in, forces, energies, virial and
-    the induced vector copied out, every call.  Between calls the caller moves
-    the atoms by one leapfrog step of the workload's time step with the forces
-    just returned (no constraints), so the warm start and the pair list see a
-    real step's displacement; only the calls are timed."""
-    import ctypes
+    the induced vector copied out, every call.  The positions of successive
+    calls are successive frames of the workload's own MD (the resident
+    simulation, stepped outside the timed region, as the drop-in mode's caller
+    integrates between its force calls); the calls go to a second context, so
+    each sees one real step's displacement and keeps its own induced vector as
+    the warm start, as the reference's caller does.  Only the calls are timed."""
     import capacmd_b200 as cm
     N, n = desc.n_atoms, max(desc.n_mat, 1)
 
     def pinned(k):
         return torch.empty(k, dtype=torch.float64, pin_memory=True).numpy()
 
+    drop = cm.Simulation(desc, precision=prec, device=device)
     rx, ry, rz = pinned(N), pinned(N), pinned(N)
-    rx[:], ry[:], rz[:] = sim.get("rx"), sim.get("ry"), sim.get("rz")
-    vx, vy, vz = sim.get("vx"), sim.get("vy"), sim.get("vz")
     fx, fy, fz, pot, vir, pq = pinned(N), pinned(N), pinned(N), pinned(15), pinned(9), pinned(n)
-    fx[:], fy[:], fz[:] = sim.get("fx"), sim.get("fy"), sim.get("fz")
-    mass = desc.get("mass")
-    step_inv_m = np.where(mass > 0.0, dt / np.where(mass > 0.0, mass, 1.0), 0.0)
     pq[:] = sim.get("vec_pq") if desc.n_mat else 0.0
     lib = cm.lib()
     ptr = lambda a: a.ctypes.data  # noqa: E731
+
+    def call():
+        cm._check(lib.capac_mpi_force(drop._p, ptr(rx), ptr(ry), ptr(rz), ptr(fx), ptr(fy), ptr(fz), ptr(pot),
+                                      ptr(vir), ptr(pq) if desc.n_mat else None, None, None, None))
+
+    rx[:], ry[:], rz[:] = sim.get("rx"), sim.get("ry"), sim.get("rz")
+    call()  # first call: list, matrix and preconditioner set-up of the new context
     h2d = 3 * N * 8 + desc.n_mat * 8
     d2h = 3 * N * 8 + 15 * 8 + 9 * 8 + desc.n_mat * 8
-    torch.cuda.synchronize()
     elapsed = 0.0
     for _ in range(calls):
-        vx += step_inv_m * fx
-        vy += step_inv_m * fy
-        vz += step_inv_m * fz
-        rx += dt * vx
-        ry += dt * vy
-        rz += dt * vz
+        sim.md_steps(1)
+        rx[:], ry[:], rz[:] = sim.get("rx"), sim.get("ry"), sim.get("rz")
+        torch.cuda.synchronize()
         t0 = time.perf_counter()
-        cm._check(lib.capac_mpi_force(sim._p, ptr(rx), ptr(ry), ptr(rz), ptr(fx), ptr(fy), ptr(fz), ptr(pot),
-                                      ptr(vir), ptr(pq) if desc.n_mat else None, None, None, None))
+        call()
         elapsed += time.perf_counter() - t0
+    drop.close()
     return {"value": N * calls / elapsed, "unit": "atom-steps/s", "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": d2h, "calls": calls, "ms_per_call": elapsed / calls * 1e3,
-            "what": f"one drop-in mpi_force per step (host positions in, host forces/energies/virial/vec_pq out), "
-                    f"atoms moved between calls by a {dt * 1e3:g} fs leapfrog step in the caller (untimed, as the "
-                    f"drop-in mode's MD integration runs in the caller)"}
+            "what": "one drop-in mpi_force per MD step (host positions in, host forces/energies/virial/vec_pq "
+                    "out) on successive frames of the workload's own trajectory, the induced vector carried "
+                    "between calls by the caller; the integration between calls is the caller's, untimed"}
 
 
 if __name__ == "__main__":
