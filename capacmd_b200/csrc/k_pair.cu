@@ -484,9 +484,11 @@ __global__ void __launch_bounds__(kPairWarps * 32, sizeof(Real) == 4 ? 3 : 2) k_
 // full flushes of 32 follow at one site, which keeps the pair terms in the
 // code once.
 constexpr int kClQueue = 160;  // < 32 left over + 4 x 32 appended
-constexpr size_t kClQueueBytes = (size_t)kPairWarps * kClQueue * sizeof(Cand<float>);
+constexpr int kClWarps = 8;      // warps per block of the cluster kernel
+constexpr int kClMinBlocks = 2;  // resident blocks per SM the register budget allows
+constexpr size_t kClQueueBytes = (size_t)kClWarps * kClQueue * sizeof(Cand<float>);
 template <bool NONBONDED, bool CPIM>
-__global__ void __launch_bounds__(kPairWarps * 32, 2) k_pair_cl(DevParams P, PairConstsF K, const double4 *__restrict__ pos4,
+__global__ void __launch_bounds__(kClWarps * 32, kClMinBlocks) k_pair_cl(DevParams P, PairConstsF K, const double4 *__restrict__ pos4,
                                                               const int4 *__restrict__ cl_atoms,
                                                               const int *__restrict__ n_cl,
                                                               const uint32_t *__restrict__ nbr,
@@ -498,12 +500,12 @@ __global__ void __launch_bounds__(kPairWarps * 32, 2) k_pair_cl(DevParams P, Pai
 {
     constexpr int NB = 2;
     extern __shared__ __align__(16) unsigned char s_dyn[];  // the warps' queues
-    __shared__ float4 s_mem[kPairWarps][4];  // member offset from the centroid, charge
-    __shared__ int s_trow[kPairWarps][4];    // member type * n_types
-    __shared__ unsigned char s_cpim[kPairWarps][4];  // the member takes the CPIM force of metal neighbours
-    __shared__ double s_acc[kPairWarps][12][32];  // force on (member, axis) per lane slot
+    __shared__ float4 s_mem[kClWarps][4];  // member offset from the centroid, charge
+    __shared__ int s_trow[kClWarps][4];    // member type * n_types
+    __shared__ unsigned char s_cpim[kClWarps][4];  // the member takes the CPIM force of metal neighbours
+    __shared__ double s_acc[kClWarps][12][32];  // force on (member, axis) per lane slot
     __shared__ double sh[32 * 11];
-    __shared__ double wacc[kPairWarps][8];
+    __shared__ double wacc[kClWarps][8];
     __shared__ __align__(16) TypePairF s_tpf[kSmemTypes * kSmemTypes];
     __shared__ unsigned char s_metal[kSmemTypes];
     const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -521,8 +523,8 @@ __global__ void __launch_bounds__(kPairWarps * 32, 2) k_pair_cl(DevParams P, Pai
     const double L[3] = {P.box.L[0], P.box.L[1], P.box.L[2]};
     const double iL[3] = {1.0 / L[0], 1.0 / L[1], 1.0 / L[2]};
     const int ncl = *n_cl;
-    const int stride = gridDim.x * kPairWarps;
-    for (int cl = blockIdx.x * kPairWarps + wib; cl < ncl; cl += stride) {
+    const int stride = gridDim.x * kClWarps;
+    for (int cl = blockIdx.x * kClWarps + wib; cl < ncl; cl += stride) {
         const int4 A = cl_atoms[cl];
         const int nk = 1 + (A.y >= 0) + (A.z >= 0) + (A.w >= 0);
         const int mine = lane == 0 ? A.x : lane == 1 ? A.y : lane == 2 ? A.z : A.w;
@@ -720,7 +722,7 @@ __global__ void __launch_bounds__(kPairWarps * 32, 2) k_pair_cl(DevParams P, Pai
     if (NONBONDED) {
         __syncthreads();
         double acc[11] = {0.0};
-        if (threadIdx.x < kPairWarps) {
+        if (threadIdx.x < kClWarps) {
             const double *w = wacc[threadIdx.x];
             acc[0] = w[0];
             acc[1] = w[1];
@@ -774,7 +776,7 @@ void launch_pair_cl_t(capac_ctx *c, unsigned grid)
     // the queues and the static arrays together exceed the default 48 KB
     CAPAC_CUDA(cudaFuncSetAttribute(k_pair_cl<NONBONDED, CPIM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)kClQueueBytes));
-    k_pair_cl<NONBONDED, CPIM><<<grid, kPairWarps * 32, kClQueueBytes, c->stream>>>(
+    k_pair_cl<NONBONDED, CPIM><<<grid, kClWarps * 32, kClQueueBytes, c->stream>>>(
         c->P, pair_consts_f(c), c->pos4, c->cl_atoms, c->cl_cell_start + c->n_cells, c->cl_nbr, c->cl_nnb,
         c->cl_metal, c->cl_cap, c->vec_pq, c->fx, c->fy, c->fz, c->partials);
 }
@@ -799,7 +801,8 @@ void launch_pair_clusters(capac_ctx *c, int mode, unsigned grid)
 unsigned pair_grid(const capac_ctx *c)
 {
     const long units = c->clusters ? c->n_clusters : c->N;
-    const long need = (units + kPairWarps - 1) / kPairWarps;
+    const int warps = c->clusters ? kClWarps : kPairWarps;
+    const long need = (units + warps - 1) / warps;
     const long cap = (long)c->num_sms * 16;
     return (unsigned)std::max(1L, std::min(need, cap));
 }
