@@ -119,6 +119,35 @@ struct CstrView {
     const int *mol_first, *mol_type, *off, *cnt, *ci, *cj;
     const double *len;
     const double *inv_mass;
+    const int *mol_atoms;  // atoms per molecule type
+};
+
+// Three-atom molecules with at most three constraints (the 3-site waters)
+// iterate on a copy of their atoms held in registers, written back once: the
+// same operations in the same order as on the global arrays, without a round
+// trip to L2 per constraint and iteration.  Mol3 reads and updates atom a of
+// a molecule with selects, so the values never leave registers.
+struct Mol3 {
+    double v0, v1, v2;
+    __device__ __forceinline__ double get(int a) const { return a == 0 ? v0 : (a == 1 ? v1 : v2); }
+    __device__ __forceinline__ void add(int a, double x)
+    {
+        if (a == 0) v0 += x;
+        else if (a == 1) v1 += x;
+        else v2 += x;
+    }
+    __device__ __forceinline__ void load(const double *p, int first)
+    {
+        v0 = p[first];
+        v1 = p[first + 1];
+        v2 = p[first + 2];
+    }
+    __device__ __forceinline__ void store(double *p, int first) const
+    {
+        p[first] = v0;
+        p[first + 1] = v1;
+        p[first + 2] = v2;
+    }
 };
 
 // rattle_1st, force.c:1907-1997: one thread per molecule.
@@ -132,6 +161,54 @@ __global__ void k_rattle1(MdParams m, CstrView cv, double *rx, double *ry, doubl
     if (nc == 0) return;
     const double tol2 = 2.0e-05;
     int iter = 0, done = 0;
+    if (cv.mol_atoms[mt] == 3 && nc <= 3) {
+        Mol3 X, Y, Z, VX, VY, VZ, OX, OY, OZ, IM;
+        X.load(rx, first); Y.load(ry, first); Z.load(rz, first);
+        VX.load(vx, first); VY.load(vy, first); VZ.load(vz, first);
+        OX.load(ox, first); OY.load(oy, first); OZ.load(oz, first);
+        IM.load(cv.inv_mass, first);
+        int ca[3] = {0, 0, 0}, cb[3] = {0, 0, 0};
+        double l2[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+            if (k < nc) {
+                ca[k] = cv.ci[c0 + k];
+                cb[k] = cv.cj[c0 + k];
+                l2[k] = cv.len[c0 + k] * cv.len[c0 + k];
+            }
+        while (!done) {
+            done = 1;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                if (k >= nc) continue;
+                const int a = ca[k], b = cb[k];
+                const double len2 = l2[k];
+                const double px = wrap1(X.get(a) - X.get(b), m.box.L[0]);
+                const double py = wrap1(Y.get(a) - Y.get(b), m.box.L[1]);
+                const double pz = wrap1(Z.get(a) - Z.get(b), m.box.L[2]);
+                const double diff = len2 - (px * px + py * py + pz * pz);
+                if (fabs(diff) > len2 * tol2) {
+                    const double qx = wrap1(OX.get(a) - OX.get(b), m.box.L[0]);
+                    const double qy = wrap1(OY.get(a) - OY.get(b), m.box.L[1]);
+                    const double qz = wrap1(OZ.get(a) - OZ.get(b), m.box.L[2]);
+                    const double ma = IM.get(a), mb = IM.get(b);
+                    const double g = diff / (2.0 * (ma + mb) * (qx * px + qy * py + qz * pz));
+                    double dx = qx * g, dy = qy * g, dz = qz * g;
+                    X.add(a, ma * dx); Y.add(a, ma * dy); Z.add(a, ma * dz);
+                    X.add(b, -(mb * dx)); Y.add(b, -(mb * dy)); Z.add(b, -(mb * dz));
+                    dx /= m.dt; dy /= m.dt; dz /= m.dt;
+                    VX.add(a, ma * dx); VY.add(a, ma * dy); VZ.add(a, ma * dz);
+                    VX.add(b, -(mb * dx)); VY.add(b, -(mb * dy)); VZ.add(b, -(mb * dz));
+                    done = 0;
+                }
+            }
+            if (++iter > kMaxIter) break;
+        }
+        X.store(rx, first); Y.store(ry, first); Z.store(rz, first);
+        VX.store(vx, first); VY.store(vy, first); VZ.store(vz, first);
+        if (!done) atomicOr(&flags[2], 1);
+        return;
+    }
     while (!done) {
         done = 1;
         for (int k = 0; k < nc; ++k) {
@@ -175,7 +252,50 @@ __global__ void __launch_bounds__(256) k_rattle2(MdParams m, CstrView cv, const 
         const int nc = cv.cnt[mt], c0 = cv.off[mt];
         const double tol = 1.0e-05, hdt = 0.5 * m.dt;
         int iter = 0, done = nc == 0;
-        while (!done) {
+        const bool fast = !done && cv.mol_atoms[mt] == 3 && nc <= 3;
+        if (fast) {
+            Mol3 X, Y, Z, VX, VY, VZ, IM;
+            X.load(rx, first); Y.load(ry, first); Z.load(rz, first);
+            VX.load(vx, first); VY.load(vy, first); VZ.load(vz, first);
+            IM.load(cv.inv_mass, first);
+            int ca[3] = {0, 0, 0}, cb[3] = {0, 0, 0};
+            double l2[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+            for (int k = 0; k < 3; ++k)
+                if (k < nc) {
+                    ca[k] = cv.ci[c0 + k];
+                    cb[k] = cv.cj[c0 + k];
+                    l2[k] = cv.len[c0 + k] * cv.len[c0 + k];
+                }
+            while (!done) {
+                done = 1;
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    if (k >= nc) continue;
+                    const int a = ca[k], b = cb[k];
+                    const double len2 = l2[k];
+                    const double ux = VX.get(a) - VX.get(b), uy = VY.get(a) - VY.get(b), uz = VZ.get(a) - VZ.get(b);
+                    const double px = wrap1(X.get(a) - X.get(b), m.box.L[0]);
+                    const double py = wrap1(Y.get(a) - Y.get(b), m.box.L[1]);
+                    const double pz = wrap1(Z.get(a) - Z.get(b), m.box.L[2]);
+                    const double ma = IM.get(a), mb = IM.get(b);
+                    const double g = -(px * ux + py * uy + pz * uz) / ((ma + mb) * len2);
+                    if (fabs(g) > tol) {
+                        double dx = px * g, dy = py * g, dz = pz * g;
+                        VX.add(a, ma * dx); VY.add(a, ma * dy); VZ.add(a, ma * dz);
+                        VX.add(b, -(mb * dx)); VY.add(b, -(mb * dy)); VZ.add(b, -(mb * dz));
+                        dx /= hdt; dy /= hdt; dz /= hdt;
+                        vir[0] -= px * dx; vir[1] -= px * dy; vir[2] -= px * dz;
+                        vir[3] -= py * dx; vir[4] -= py * dy; vir[5] -= py * dz;
+                        vir[6] -= pz * dx; vir[7] -= pz * dy; vir[8] -= pz * dz;
+                        done = 0;
+                    }
+                }
+                if (++iter > kMaxIter) break;
+            }
+            VX.store(vx, first); VY.store(vy, first); VZ.store(vz, first);
+        }
+        while (!fast && !done) {
             done = 1;
             for (int k = 0; k < nc; ++k) {
                 const int a = first + cv.ci[c0 + k], b = first + cv.cj[c0 + k];
@@ -419,6 +539,7 @@ CstrView cstr_view(const capac_ctx *c)
     v.cj = c->cstr_j;
     v.len = c->cstr_r;
     v.inv_mass = c->inv_mass;
+    v.mol_atoms = c->mol_atoms;
     return v;
 }
 
