@@ -217,7 +217,7 @@ def main() -> int:
     ap.add_argument("--e2e-calls", type=int, default=20)
     ap.add_argument("--solver-kernel", type=int, default=0, choices=[0, 1],
                     help="0: persistent cooperative BiCGSTAB launch per solve, 1: a launch per vector step")
-    ap.add_argument("--predictor", type=int, default=2, choices=[0, 1, 2, 3],
+    ap.add_argument("--predictor", type=int, default=3, choices=[0, 1, 2, 3],
                     help="mixed path warm start: order of the polynomial extrapolation of past solutions")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)

@@ -230,7 +230,7 @@ void capac_options_default(capac_options *o)
     o->solver_tol = 0.0;
     o->refine_tol = 1.0e-10;
     o->matrix_layout = 0;
-    o->predictor = 2;
+    o->predictor = 3;
     o->solver_kernel = 0;
     o->inner_precond = 1;
     o->pair_list = 0;

@@ -179,7 +179,7 @@ typedef struct capac_options {
                                charges within 1e-8 of the FP64 solution) */
     int matrix_layout;      /* CPIM matrix: 0 symmetric packed 4x4 blocks (default), 1 full 4x4 blocks */
     int predictor;          /* mixed path warm start: polynomial extrapolation of the last solutions of
-                               order 0 (last solution), 1 (linear), 2 (quadratic, default) or 3 */
+                               order 0 (last solution), 1 (linear), 2 (quadratic) or 3 (cubic, default) */
     int solver_kernel;      /* BiCGSTAB on the symmetric layout: 0 one persistent cooperative launch per
                                solve when the device supports it (default), 1 a launch per vector step */
     int inner_precond;      /* mixed path, persistent solver: preconditioner of the inner solves,
