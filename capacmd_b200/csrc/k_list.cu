@@ -23,10 +23,13 @@
 // Mixed path, cluster list: the atoms of each cell are cut, in that order,
 // into clusters of up to four.  Per cluster a warp scans the same 5 x 5 x 5
 // cell window; a candidate j within rc + skin + (cluster radius) of the
-// cluster's centroid is tested against each member k exactly as the atom
-// list tests it (pbc_12 image, the reference's r^2 rounding, exclusions), and
-// kept with the mask of the members that pass.  The pair set per member is
-// therefore the atom list's.  The pair kernel rounds j's minimum-image
+// cluster's centroid is tested against each member k in FP32 (j's FP64
+// minimum image from the centroid, rounded, minus the member's offset) with
+// the list radius widened by 1e-5 relative, far beyond the rounding, and
+// against the exclusions, and kept with the mask of the members that pass.
+// Each member's entries are thus a superset of its atom-list row; the pair
+// kernel's per-step cut-off decides the pair set, which the pair-set
+// fingerprint checks against the reference.  The pair kernel rounds j's minimum-image
 // difference from the centroid and the members' offsets from it to FP32; the
 // composite is the pair's minimum image whenever rc + (largest member offset
 // at the build) + skin < half the shortest box edge, which each build checks,
@@ -302,6 +305,16 @@ __global__ void __launch_bounds__(256) k_build_cluster_list(DevParams P, Grid g,
     // prefilter radius, widened by a relative 1e-12 against rounding
     const double pre = (sqrt(P.list_r2) + sqrt(R2)) * (1.0 + 1e-12);
     const double pre2 = pre * pre;
+    // FP32 member test: the list radius widened by 1e-5 relative; the
+    // members' offsets from the centroid (selected by member, in registers)
+    const float lr2f = (float)(P.list_r2 * (1.0 + 1e-5));
+    const float ofx0 = (float)o[0][0], ofy0 = (float)o[0][1], ofz0 = (float)o[0][2];
+    const float ofx1 = nk > 1 ? (float)o[1][0] : 0.f, ofy1 = nk > 1 ? (float)o[1][1] : 0.f,
+                ofz1 = nk > 1 ? (float)o[1][2] : 0.f;
+    const float ofx2 = nk > 2 ? (float)o[2][0] : 0.f, ofy2 = nk > 2 ? (float)o[2][1] : 0.f,
+                ofz2 = nk > 2 ? (float)o[2][2] : 0.f;
+    const float ofx3 = nk > 3 ? (float)o[3][0] : 0.f, ofy3 = nk > 3 ? (float)o[3][1] : 0.f,
+                ofz3 = nk > 3 ? (float)o[3][2] : 0.f;
     // all members are in the cell of the first one (the cells were assigned
     // from the same positions)
     const int c0[3] = {cell_coord(xm[0], P.box.L[0], g.inv_len[0], g.n[0]),
@@ -333,9 +346,12 @@ __global__ void __launch_bounds__(256) k_build_cluster_list(DevParams P, Grid g,
 #pragma unroll
                             for (int k = 0; k < 4; ++k) {
                                 if (k >= nk || j == m[k]) continue;
-                                double dx = q.x - xm[k], dy = q.y - ym[k], dz = q.z - zm[k];
-                                image(dx, dy, dz, P.box);
-                                if (norm2_exact(dx, dy, dz) < P.list_r2 && !excluded(P, m[k], j)) mask |= 1u << k;
+                                const float ox = k == 0 ? ofx0 : k == 1 ? ofx1 : k == 2 ? ofx2 : ofx3;
+                                const float oy = k == 0 ? ofy0 : k == 1 ? ofy1 : k == 2 ? ofy2 : ofy3;
+                                const float oz = k == 0 ? ofz0 : k == 1 ? ofz1 : k == 2 ? ofz2 : ofz3;
+                                const float sx = (float)ex - ox, sy = (float)ey - oy, sz = (float)ez - oz;
+                                if (fmaf(sz, sz, fmaf(sy, sy, sx * sx)) < lr2f && !excluded(P, m[k], j))
+                                    mask |= 1u << k;
                             }
                         }
                     }
