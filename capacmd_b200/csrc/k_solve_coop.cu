@@ -700,30 +700,44 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? 2 : 1) k_bicgstab_coo
     double bTb = 0.0, crit = 0.0, rTr = 0.0, rr0 = 0.0;
     bool ok = true;
 
-    // start: bTb, K, p = v = 0 (first buffers)
+    // start: bTb, the count of non-zero entries of x, K, p = v = 0 (first buffers)
     {
-        double pb[1] = {0.0};
+        double pb[2] = {0.0, 0.0};
         for (long k = tid; k < n; k += gthreads) {
             const double bk = A.b[k];
             pb[0] += bk * bk;
+            pb[1] += A.x[k] != 0.0 ? 1.0 : 0.0;
             A.K[k] = k < A.n4 ? 1.0 / A.diag[k] : 1.0;
             A.p[0][k] = 0.0;  // block-Jacobi: the first y buffer
             A.v[0][k] = 0.0;
             if (A.bj) A.Kv[k] = 0.0;
         }
-        put_bp<1>(bpA, pb);
+        put_bp<2>(bpA, pb);
     }
     ok = grid_barrier(A.sync);
+    bool x_zero = false;
     if (ok) {
-        double t1[1];
-        sum_bp<1>(bpA, nb, t1);
-        bTb = t1[0];
+        double t2[2];
+        sum_bp<2>(bpA, nb, t2);
+        bTb = t2[0];
+        x_zero = t2[1] == 0.0;  // the same in every block
         crit = bTb * A.tol;
     }
     bool done = !ok || bTb < A.skip;  // zero right-hand side: x stays (bicg_stab.c:303-307)
     if (!done) {
-        ok = tiles_pass<T, MODE_X>(A, S, ring, psm) && grid_barrier(A.sync);
-        if (ok) reduce_pass<RED_START>(A, S, bpB);
+        if (x_zero) {
+            // r0 = r = b - A 0 = b: no product pass (the refinement sweeps
+            // start their correction from zero); the tile ring is untouched,
+            // so the next pass starts on the same tiles
+            for (long k = tid; k < n; k += gthreads) {
+                const double bk = A.b[k];
+                A.r0[k] = bk;
+                A.r[k] = bk;
+            }
+        } else {
+            ok = tiles_pass<T, MODE_X>(A, S, ring, psm) && grid_barrier(A.sync);
+            if (ok) reduce_pass<RED_START>(A, S, bpB);
+        }
         ok = ok && grid_barrier(A.sync);
         if (ok && A.bj) {  // K r of the start residual; y = K r on the first iteration
             prec_pass<false>(A, A.r, A.Kr, nullptr);
@@ -733,9 +747,13 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? 2 : 1) k_bicgstab_coo
     }
     double rho = 0.0, rho_old = 1.0, alpha = 1.0, omega = 1.0;
     if (!done) {
-        double t1[1];
-        sum_bp<1>(bpB, nb, t1);
-        rho = rTr = rr0 = t1[0];
+        if (x_zero) {
+            rho = rTr = rr0 = bTb;
+        } else {
+            double t1[1];
+            sum_bp<1>(bpB, nb, t1);
+            rho = rTr = rr0 = t1[0];
+        }
         if (rho < A.skip) done = true;  // warm start already converged (bicg_stab.c:368)
     }
     bool pending = false;  // x += alpha y + omega z of the last iteration not yet applied
