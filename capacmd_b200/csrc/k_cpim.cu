@@ -810,11 +810,72 @@ int run_refined_solve(capac_ctx *c)
 
 // ------------------------------------------------- CPIM metal-side forces
 
+// One metal-metal pair of mpi_cpff_force (cpff.c:752-926) in the arithmetic
+// type R, atomic units, r = r_j - r_i in Bohr: f is the pair force the
+// reference subtracts from atom i, e the halves of the charge-charge,
+// charge-dipole and dipole-dipole energies (each pair is visited from both
+// atoms).
+template <typename R>
+__device__ __forceinline__ void metal_pair(const R r[3], R qi, const R pi[3], R qj, const R pj[3], R iqq, R ipq,
+                                           R ipp, R f[3], R e[3])
+{
+    const R isp = (R)kInvSqrtPi, fq2 = (R)kFqqAu2, fq1 = (R)kFqqAu1, half = (R)0.5;
+    const R ipq3 = ipq * ipq * ipq, ipp3 = ipp * ipp * ipp, ipp5 = ipp3 * ipp * ipp;
+    const R r2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2], rr = sqrt(r2);
+    const R ir3 = (R)1 / (r2 * rr), ir5 = ir3 / r2, ir7 = ir5 / r2;
+    f[0] = f[1] = f[2] = (R)0;
+    e[0] = e[1] = e[2] = (R)0;
+    // charge - charge
+    const R gqq = exp(-(r2 * iqq * iqq)), erq = erf(rr * iqq);
+    const R A0 = ir3 * (erq - (R)2 * isp * iqq * rr * gqq);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) f[a] += A0 * r[a] * fq2 * qi * qj;
+    e[0] += fq1 * qi * qj * erq / rr * half;
+    // charge - dipole
+    const R gpq = exp(-(r2 * ipq * ipq));
+    const R tpq = erf(rr * ipq) - (R)2 * isp * ipq * rr * gpq;
+    const R Apq0 = ir3 * tpq, A1 = ir5 * tpq, B1 = (R)4 * isp * ipq3 / r2 * gpq;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+#pragma unroll
+        for (int b = 0; b < 3; ++b) {
+            const R dab = a == b ? (R)1 : (R)0;
+            const R T = A1 * ((R)3 * r[a] * r[b] - dab * r2) - B1 * r[a] * r[b];
+            f[b] += -T * fq2 * qi * pj[a];
+            f[b] += T * fq2 * qj * pi[a];
+        }
+        e[1] += -fq1 * qi * pj[a] * r[a] * Apq0 * half;
+        e[1] += fq1 * qj * pi[a] * r[a] * Apq0 * half;
+    }
+    // dipole - dipole
+    const R gpp = exp(-(r2 * ipp * ipp)), erp = erf(rr * ipp);
+    const R App1 = ir5 * (erp - (R)2 * isp * ipp * rr * gpp);
+    const R Bpp1 = (R)4 * isp * ipp3 / r2 * gpp;
+    const R A2 = ir7 * ((R)3 * erp - (R)6 * isp * ipp * rr * gpp - (R)4 * (r2 * rr) * isp * ipp3 * gpp);
+    const R B2 = (R)8 * isp * ipp5 / r2 * gpp;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+#pragma unroll
+        for (int b = 0; b < 3; ++b) {
+            const R dab = a == b ? (R)1 : (R)0;
+#pragma unroll
+            for (int cc = 0; cc < 3; ++cc) {
+                const R dbc = b == cc ? (R)1 : (R)0, dca = cc == a ? (R)1 : (R)0;
+                f[cc] += -(A2 * ((R)5 * r[a] * r[b] * r[cc] - r2 * (r[a] * dbc + r[b] * dca + r[cc] * dab)) -
+                           B2 * r[a] * r[b] * r[cc]) * fq2 * pi[a] * pj[b];
+            }
+            e[2] += -fq1 * pi[a] * pj[b] * (((R)3 * r[a] * r[b] - dab * r2) * App1 - r[a] * r[b] * Bpp1) * half;
+        }
+    }
+}
+
 // mpi_cpff_force (cpff.c:526-950) for one metal atom per block: metal -
 // permanent-charge terms over its list, self terms, dense metal - metal
 // damped T0/T1/T2 terms (forces on i only, virial halved), external field on
 // the induced charge and dipole.  Energies [9..14] and the virial go to
-// per-block partials.
+// per-block partials.  The metal-metal pair terms are evaluated in R (FP32
+// on the mixed path, FP64 otherwise); every sum is FP64.
+template <typename R>
 __global__ void __launch_bounds__(256) k_cpim_metal(DevParams P, const double4 *__restrict__ pos4,
                                                     const uint32_t *__restrict__ nbr, const int *__restrict__ nnb,
                                                     int cap, const double *__restrict__ pq, double *fx, double *fy,
@@ -861,72 +922,30 @@ __global__ void __launch_bounds__(256) k_cpim_metal(DevParams P, const double4 *
             for (int b = 0; b < 3; ++b) acc[9 + 3 * a + b] += -r[a] * f[b];
     }
 
-    // metal - metal, atomic units (cpff.c:752-926)
-    const double iqq = P.inv_r_qq, ipq = P.inv_r_pq, ipp = P.inv_r_pp;
-    const double ipq3 = ipq * ipq * ipq, ipp3 = ipp * ipp * ipp, ipp5 = ipp3 * ipp * ipp;
+    // metal - metal, atomic units (cpff.c:752-926); the pair terms in R,
+    // their sums in FP64
+    const R iqq = (R)P.inv_r_qq, ipq = (R)P.inv_r_pq, ipp = (R)P.inv_r_pp;
+    const R qiR = (R)qi, piR[3] = {(R)pi[0], (R)pi[1], (R)pi[2]};
     for (int j = threadIdx.x; j < M; j += blockDim.x) {
         if (j == i) continue;
         const double4 pj4 = pos4[P.metal_min + j];
-        double r[3] = {pj4.x - pi4.x, pj4.y - pi4.y, pj4.z - pi4.z};
-        image(r[0], r[1], r[2], P.box);
-        r[0] *= kNm2Bohr;
-        r[1] *= kNm2Bohr;
-        r[2] *= kNm2Bohr;
-        const double r2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2], rr = sqrt(r2);
-        const double ir3 = 1.0 / (r2 * rr), ir5 = ir3 / r2, ir7 = ir5 / r2;
-        const double qj = pq[3 * M + j];
-        const double pj[3] = {pq[3 * j], pq[3 * j + 1], pq[3 * j + 2]};
-        double f[3] = {0.0, 0.0, 0.0};
-        // charge - charge
-        const double gqq = exp(-(r2 * iqq * iqq)), erq = erf(rr * iqq);
-        const double A0 = ir3 * (erq - 2.0 * kInvSqrtPi * iqq * rr * gqq);
-#pragma unroll
-        for (int a = 0; a < 3; ++a) f[a] += A0 * r[a] * kFqqAu2 * qi * qj;
-        acc[6] += kFqqAu1 * qi * qj * erq / rr * 0.5;
-        // charge - dipole
-        const double gpq = exp(-(r2 * ipq * ipq));
-        const double tpq = erf(rr * ipq) - 2.0 * kInvSqrtPi * ipq * rr * gpq;
-        const double Apq0 = ir3 * tpq, A1 = ir5 * tpq, B1 = 4.0 * kInvSqrtPi * ipq3 / r2 * gpq;
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-#pragma unroll
-            for (int b = 0; b < 3; ++b) {
-                const double dab = a == b ? 1.0 : 0.0;
-                const double T = A1 * (3.0 * r[a] * r[b] - dab * r2) - B1 * r[a] * r[b];
-                f[b] += -T * kFqqAu2 * qi * pj[a];
-                f[b] += T * kFqqAu2 * qj * pi[a];
-            }
-            acc[7] += -kFqqAu1 * qi * pj[a] * r[a] * Apq0 * 0.5;
-            acc[7] += kFqqAu1 * qj * pi[a] * r[a] * Apq0 * 0.5;
-        }
-        // dipole - dipole
-        const double gpp = exp(-(r2 * ipp * ipp)), erp = erf(rr * ipp);
-        const double App1 = ir5 * (erp - 2.0 * kInvSqrtPi * ipp * rr * gpp);
-        const double Bpp1 = 4.0 * kInvSqrtPi * ipp3 / r2 * gpp;
-        const double A2 = ir7 * (3.0 * erp - 6.0 * kInvSqrtPi * ipp * rr * gpp -
-                                 4.0 * (r2 * rr) * kInvSqrtPi * ipp3 * gpp);
-        const double B2 = 8.0 * kInvSqrtPi * ipp5 / r2 * gpp;
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-#pragma unroll
-            for (int b = 0; b < 3; ++b) {
-                const double dab = a == b ? 1.0 : 0.0;
-#pragma unroll
-                for (int cc = 0; cc < 3; ++cc) {
-                    const double dbc = b == cc ? 1.0 : 0.0, dca = cc == a ? 1.0 : 0.0;
-                    f[cc] += -(A2 * (5.0 * r[a] * r[b] * r[cc] - r2 * (r[a] * dbc + r[b] * dca + r[cc] * dab)) -
-                               B2 * r[a] * r[b] * r[cc]) * kFqqAu2 * pi[a] * pj[b];
-                }
-                acc[8] += -kFqqAu1 * pi[a] * pj[b] * ((3.0 * r[a] * r[b] - dab * r2) * App1 - r[a] * r[b] * Bpp1) * 0.5;
-            }
-        }
-        acc[0] -= f[0];
-        acc[1] -= f[1];
-        acc[2] -= f[2];
+        double rd[3] = {pj4.x - pi4.x, pj4.y - pi4.y, pj4.z - pi4.z};
+        image(rd[0], rd[1], rd[2], P.box);
+        const R r[3] = {(R)(rd[0] * kNm2Bohr), (R)(rd[1] * kNm2Bohr), (R)(rd[2] * kNm2Bohr)};
+        const R qj = (R)pq[3 * M + j];
+        const R pj[3] = {(R)pq[3 * j], (R)pq[3 * j + 1], (R)pq[3 * j + 2]};
+        R f[3], e[3];
+        metal_pair<R>(r, qiR, piR, qj, pj, iqq, ipq, ipp, f, e);
+        acc[6] += (double)e[0];
+        acc[7] += (double)e[1];
+        acc[8] += (double)e[2];
+        acc[0] -= (double)f[0];
+        acc[1] -= (double)f[1];
+        acc[2] -= (double)f[2];
 #pragma unroll
         for (int a = 0; a < 3; ++a)
 #pragma unroll
-            for (int b = 0; b < 3; ++b) acc[9 + 3 * a + b] += -r[a] * f[b] * 0.5;
+            for (int b = 0; b < 3; ++b) acc[9 + 3 * a + b] += -(double)r[a] * (double)f[b] * 0.5;
     }
     block_sum<18>(acc, sh);
     if (threadIdx.x == 0) {
@@ -950,8 +969,12 @@ void launch_cpim_metal_forces(capac_ctx *c)
 {
     {
         ProfScope ps(c, K_CPIM_METAL);
-        k_cpim_metal<<<c->M, 256, 0, c->stream>>>(c->P, c->pos4, c->nbr, c->nnb, c->cap, c->vec_pq, c->fx, c->fy,
-                                                   c->fz, c->partials);
+        if (c->opt.precision == CAPAC_PREC_MIXED)
+            k_cpim_metal<float><<<c->M, 256, 0, c->stream>>>(c->P, c->pos4, c->nbr, c->nnb, c->cap, c->vec_pq, c->fx,
+                                                             c->fy, c->fz, c->partials);
+        else
+            k_cpim_metal<double><<<c->M, 256, 0, c->stream>>>(c->P, c->pos4, c->nbr, c->nnb, c->cap, c->vec_pq, c->fx,
+                                                              c->fy, c->fz, c->partials);
     }
     ++c->launches;
     static const int pot_slots[15] = {9, 10, 11, 12, 13, 14, -1, -1, -1, -1, -1, -1, -1, -1, -1};
