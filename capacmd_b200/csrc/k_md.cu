@@ -46,19 +46,27 @@ __global__ void k_nhc(ThermoState *th, MdParams m)
     const double w1 = 0.41449077179437571194, w3 = -0.65796308717750284778;
     const double w[5] = {w1, w1, w3, w1, w1};
     const double Q = m.q_mass, kT = th->kT, NkT = kT * m.ndf, dt = m.dt, ek = th->eksum;
-    double *vQ = th->vQ, *aQ = th->aQ, scale = 1.0;
+    // the chain in registers (every index is fixed once the loops unroll),
+    // written back at the end
+    double vQ[kNhc], aQ[kNhc], scale = 1.0;
+#pragma unroll
+    for (int k = 0; k < L; ++k) vQ[k] = th->vQ[k];
     aQ[0] = (ek - NkT) / Q;
+#pragma unroll
     for (int k = 0; k < L - 1; ++k) aQ[k + 1] = (Q * vQ[k] * vQ[k] - kT) / Q;
     for (int c = 0; c < Nc; ++c) {
+#pragma unroll
         for (int y = 0; y < 5; ++y) {
             const double h4 = w[y] * dt / (4 * Nc), h8 = w[y] * dt / (8 * Nc), h2 = w[y] * dt / (2 * Nc);
             vQ[L - 1] += aQ[L - 1] * h4;
+#pragma unroll
             for (int k = 0; k < L - 1; ++k) {
                 const double e = exp(-h8 * vQ[L - (k + 1)]);
                 vQ[L - 1 - (k + 1)] = vQ[L - 1 - (k + 1)] * e * e + h4 * aQ[L - 1 - (k + 1)] * e;
             }
             scale *= exp(-h2 * vQ[0]);
             aQ[0] = (ek * scale * scale - NkT) / Q;
+#pragma unroll
             for (int k = 0; k < L - 1; ++k) {
                 const double e = exp(-h8 * vQ[k + 1]);
                 vQ[k] = vQ[k] * e * e + h4 * aQ[k] * e;
@@ -66,6 +74,11 @@ __global__ void k_nhc(ThermoState *th, MdParams m)
             }
             vQ[L - 1] += aQ[L - 1] * h4;
         }
+    }
+#pragma unroll
+    for (int k = 0; k < L; ++k) {
+        th->vQ[k] = vQ[k];
+        th->aQ[k] = aQ[k];
     }
     th->scale = scale;
     th->eksum = ek * (scale * scale);
