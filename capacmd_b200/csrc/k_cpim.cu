@@ -23,19 +23,21 @@ struct Slots {
     int vir[24];
 };
 
+// One block per value k (the slots of one launch are distinct, checked on
+// the host), each summing its column of the per-block partials in a fixed
+// order.
 __global__ void __launch_bounds__(256) k_finalize(const double *__restrict__ partials, int nblocks, int K,
                                                   Slots s, double *pot, double *vir)
 {
     __shared__ double sh[32];
-    for (int k = 0; k < K; ++k) {
-        double v = 0.0;
-        for (int b = threadIdx.x; b < nblocks; b += blockDim.x) v += partials[(size_t)b * K + k];
-        double t[1] = {v};
-        block_sum<1>(t, sh);
-        if (threadIdx.x == 0) {
-            if (s.pot[k] >= 0) pot[s.pot[k]] += t[0];
-            if (s.vir[k] >= 0) vir[s.vir[k]] += t[0];
-        }
+    const int k = blockIdx.x;
+    double v = 0.0;
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x) v += partials[(size_t)b * K + k];
+    double t[1] = {v};
+    block_sum<1>(t, sh);
+    if (threadIdx.x == 0) {
+        if (s.pot[k] >= 0) pot[s.pot[k]] += t[0];
+        if (s.vir[k] >= 0) vir[s.vir[k]] += t[0];
     }
 }
 
@@ -46,7 +48,12 @@ void launch_finalize(capac_ctx *c, int nblocks, int K, const int *slots_pot, con
         s.pot[k] = k < K ? slots_pot[k] : -1;
         s.vir[k] = k < K ? slots_vir[k] : -1;
     }
-    k_finalize<<<1, 256, 0, c->stream>>>(c->partials, nblocks, K, s, c->pot, c->vir);
+    // the values are summed by separate blocks: no two may share a slot
+    for (int a = 0; a < K; ++a)
+        for (int b = a + 1; b < K; ++b)
+            if ((s.pot[a] >= 0 && s.pot[a] == s.pot[b]) || (s.vir[a] >= 0 && s.vir[a] == s.vir[b]))
+                throw Error(CAPAC_ERR_INVALID, "finalize: two values share an energy or virial slot");
+    k_finalize<<<K, 256, 0, c->stream>>>(c->partials, nblocks, K, s, c->pot, c->vir);
     ++c->launches;
 }
 
