@@ -31,6 +31,20 @@ def test_library_exports_every_declared_symbol():
     assert not missing, missing
 
 
+def test_options_mirror_matches_library_defaults():
+    """The Python Options structure has the C layout: every field read back
+    from capac_options_default is the documented default."""
+    o = cm.Options()
+    cm.lib().capac_options_default(ctypes.byref(o))
+    assert (o.precision, o.device, o.skin) == (cm.PREC_FP64, 0, 0.2)
+    assert (o.list_every, o.max_neighbors, o.solver_tol, o.refine_tol) == (0, 0, 0.0, 1e-10)
+    assert (o.matrix_layout, o.predictor, o.solver_kernel, o.inner_precond, o.pair_list) == (0, 3, 0, 1, 0)
+    src = open(os.path.join(ROOT, "include", "capacmd.h")).read()
+    body = src[src.index("typedef struct capac_options {"):src.index("} capac_options;")]
+    fields = re.findall(r"^\s*(?:int|double)\s+(\w+);", body, flags=re.M)
+    assert fields == [f[0] for f in cm.Options._fields_]
+
+
 def test_library_reports_no_device_without_gpu(gpu_available):
     if gpu_available:
         pytest.skip("a GPU is present")
