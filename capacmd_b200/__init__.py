@@ -54,7 +54,8 @@ class Options(ctypes.Structure):
                 ("list_every", ctypes.c_int), ("max_neighbors", ctypes.c_int),
                 ("solver_tol", ctypes.c_double), ("refine_tol", ctypes.c_double),
                 ("matrix_layout", ctypes.c_int), ("predictor", ctypes.c_int), ("solver_kernel", ctypes.c_int),
-                ("inner_precond", ctypes.c_int), ("pair_list", ctypes.c_int)]
+                ("inner_precond", ctypes.c_int), ("pair_list", ctypes.c_int), ("max_iter", ctypes.c_int),
+                ("wait_polls", ctypes.c_int)]
 
 
 class Stats(ctypes.Structure):
@@ -168,7 +169,7 @@ class Simulation:
     def __init__(self, desc: Desc, precision: int = PREC_FP64, device: int = 0, skin: float = 0.2,
                  solver_tol: float = 0.0, refine_tol: float = 1e-10, max_neighbors: int = 0,
                  matrix_layout: int = 0, predictor: int = 3, solver_kernel: int = 0, inner_precond: int = 1,
-                 pair_list: int = 0):
+                 pair_list: int = 0, max_iter: int = 0, wait_polls: int = 0):
         self.desc = desc
         o = Options()
         lib().capac_options_default(ctypes.byref(o))
@@ -177,6 +178,7 @@ class Simulation:
         o.matrix_layout, o.predictor, o.solver_kernel = matrix_layout, predictor, solver_kernel
         o.inner_precond = inner_precond
         o.pair_list = pair_list
+        o.max_iter, o.wait_polls = max_iter, wait_polls
         self._p = ctypes.c_void_p()
         _check(lib().capac_create(desc.ptr, ctypes.byref(o), ctypes.byref(self._p)))
         self.n_atoms = desc.n_atoms

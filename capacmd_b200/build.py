@@ -1,6 +1,10 @@
 """Build the CUDA library in-tree (sm_100a) and the CPU oracles.
 
-    python -m capacmd_b200.build            # library + oracle (+ reference oracle if its sources exist)
+    python -m capacmd_b200.build [--reference DIR]
+
+builds the library, the resident driver and the C oracle; with the reference
+sources given (--reference, else the CAPAC_REFERENCE_SRC environment
+variable) also the reference compiled in place (oracle/_ref).
 
 The library is ``capacmd_b200/libcapacmd_gpu.so``: host C++ (input parsing,
 orchestration, C ABI) and the sm_100a kernels, linked against the CUDA runtime.
@@ -19,7 +23,6 @@ CSRC = os.path.join(PKG, "csrc")
 OBJ = os.path.join(ROOT, "build", "obj")
 LIB = os.path.join(PKG, "libcapacmd_gpu.so")
 DRIVER = os.path.join(PKG, "capacmd-gpu")
-REF_SRC = "/root/reference"
 
 SOURCES = ["io.cpp", "api.cu", "k_list.cu", "k_pair.cu", "k_cpim.cu", "k_md.cu", "k_cpim_sym.cu", "k_solve_static.cu", "k_solve_coop.cu",
            "k_precond.cu", "k_grad.cu", "k_grad_forces.cu", "k_bonded.cu"]
@@ -80,22 +83,32 @@ def build_driver(verbose: bool = False) -> str:
     return DRIVER
 
 
-def build_oracle(verbose: bool = False) -> None:
-    """Compile the C restatement and, where its sources exist, the reference."""
+def reference_dir(reference: str | None = None) -> str | None:
+    """The reference source folder: the argument, else $CAPAC_REFERENCE_SRC;
+    None when neither names an existing folder."""
+    ref = reference or os.environ.get("CAPAC_REFERENCE_SRC")
+    return ref if ref and os.path.isdir(ref) else None
+
+
+def build_oracle(verbose: bool = False, reference: str | None = None) -> None:
+    """Compile the C restatement and, where the reference sources are given,
+    the reference itself (oracle/_ref)."""
     odir = os.path.join(ROOT, "oracle")
     subprocess.run(["make", "-s", "-C", odir], check=True)
-    if os.path.isdir(REF_SRC):
-        subprocess.run(["make", "-s", "-C", odir, "ref", f"REF={REF_SRC}"], check=True)
+    ref = reference_dir(reference)
+    if ref:
+        subprocess.run(["make", "-s", "-C", odir, "ref", f"REF={ref}"], check=True)
         if os.path.exists(LIB):
             # the reference driver with its mpi_force calls sent to this library
-            subprocess.run(["make", "-s", "-C", odir, "dropin", f"REF={REF_SRC}"], check=True)
+            subprocess.run(["make", "-s", "-C", odir, "dropin", f"REF={ref}"], check=True)
 
 
 def main() -> int:
     verbose = "-v" in sys.argv
+    reference = sys.argv[sys.argv.index("--reference") + 1] if "--reference" in sys.argv[:-1] else None
     build_library(verbose)
     build_driver(verbose)
-    build_oracle(verbose)
+    build_oracle(verbose, reference)
     print(LIB)
     return 0
 

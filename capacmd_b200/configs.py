@@ -49,6 +49,9 @@ class Workload:
     temperature: float = 300.0
     save_step: int = 10
     use_cpff: int = 1
+    # NONBONDED lines replacing the default table, upper triangle of types
+    # (Au, O, H): Au-Au, Au-O, Au-H, O-O, O-H, H-H
+    nonbonded: tuple | None = None
 
 
 # The five measured workloads plus small systems for tests.  Sizes: c1 147
@@ -71,6 +74,16 @@ WORKLOADS = {
     "t_2np": Workload("t_2np", [2, 2], 400, 4.2, seed=7, steps=20, efield_vnm=(0.0, 0.0, 0.5),
                       gap_z=0.8),
     "t_water": Workload("t_water", [], 120, 1.7, seed=8, steps=20, use_cpff=0),
+    # Au-O as Buckingham (funct 2: A kJ/mol, B 1/nm, C6 kJ mol^-1 nm^6) and Au-H
+    # as Morse (funct 3: D kJ/mol, a 1/nm, R nm), the two nonbonded forms no
+    # other input uses (force.c:639-703); no CPIM, so a trace has no solver noise
+    "t_morse_buck": Workload("t_morse_buck", [2], 150, 2.9, seed=9, steps=20, use_cpff=0,
+                             nonbonded=(" 1    0.00000000e+00      0.00000000e+00",
+                                        " 2    1.0e+05    30.0    2.0e-03",
+                                        " 3    5.0    20.0    0.28",
+                                        " 1    2.48970844e-03      2.43509761e-06",
+                                        " 1    0.00000000e+00      0.00000000e+00",
+                                        " 1    0.00000000e+00      0.00000000e+00")),
 }
 
 
@@ -211,7 +224,7 @@ def build(w: Workload):
                            for k in range(len(nps))])
 
 
-def param_text(n_metal: int, n_waters: int, np_ranges, use_cpff: int = 1) -> str:
+def param_text(n_metal: int, n_waters: int, np_ranges, use_cpff: int = 1, nonbonded=None) -> str:
     eps = 0.012793 * EV2KJMOL
     lines = ["SCALE_LJ_QQ    0.50000000     0.83333333", ""]
     mols = []
@@ -229,16 +242,13 @@ def param_text(n_metal: int, n_waters: int, np_ranges, use_cpff: int = 1) -> str
         else:
             lines += ["SOL_ATOMS           3", f"    {Q_O:.6f}    {M_O:.6f}       1",
                       f"     {Q_H:.6f}     {M_H:.6f}       2", f"     {Q_H:.6f}     {M_H:.6f}       2", ""]
-    lines += [
-        "NONBONDED      3         6",
+    lines += ["NONBONDED      3         6"] + list(nonbonded or (
         " 1    0.00000000e+00      0.00000000e+00",
         " 4  0.002522219544  3.624859037184e-06  2.25",
         " 4  0.001028707002  1.45541995368e-06   2.25",
         " 1    2.48970844e-03      2.43509761e-06",
         " 1    0.00000000e+00      0.00000000e+00",
-        " 1    0.00000000e+00      0.00000000e+00",
-        "",
-    ]
+        " 1    0.00000000e+00      0.00000000e+00")) + [""]
     hh = 2.0 * OH * np.sin(np.deg2rad(HOH_DEG) / 2.0)
     for nm, _ in mols:
         for sec in ("BONDS", "PAIRS", "ANGLES", "DIHEDRALS", "VSITES"):
@@ -516,7 +526,7 @@ def write(name: str, out_dir: str, steps: int | None = None) -> dict:
     with open(paths["gro"], "w") as f:
         f.write(gro_text(s["pos"], s["vel"], s["n_metal"], w.box))
     with open(paths["par"], "w") as f:
-        f.write(param_text(s["n_metal"], s["n_waters"], s["np_ranges"], w.use_cpff))
+        f.write(param_text(s["n_metal"], s["n_waters"], s["np_ranges"], w.use_cpff, w.nonbonded))
     with open(paths["mds"], "w") as f:
         f.write(mdset_text(w, steps))
     paths["n_atoms"] = len(s["pos"])

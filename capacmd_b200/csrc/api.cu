@@ -470,8 +470,8 @@ int capac_create(const capac_desc *d, const capac_options *opt, capac_ctx **out)
                 c->diag = dalloc<double>(n);
                 CAPAC_CUDA(cudaMemsetAsync(c->vec_ext, 0, sizeof(double) * n, s));
                 CAPAC_CUDA(cudaMemsetAsync(c->vec_pq, 0, sizeof(double) * n, s));
-                std::vector<double> diag(n, 1.0);
-                for (int i = 0; i < M; ++i) {
+                std::vector<double> diag(n, 1.0);  // mpi-main.c:584-590: 1 until the matrix is built
+                for (int i = 0; i < M && c->use_cpff; ++i) {
                     diag[3 * i] = diag[3 * i + 1] = diag[3 * i + 2] = c->c.inv_polar;
                     diag[3 * M + i] = -c->c.inv_capac;
                 }
@@ -628,6 +628,10 @@ int capac_cpim_matvec(capac_ctx *c, const double *x, double *y)
     return guard([&] {
         check_ctx(c);
         if (!x || !y) throw Error(CAPAC_ERR_INVALID, "null argument");
+        if (c->M > 0 && !c->use_cpff) {  // use_cpff 0: the reference's COO matrix stays empty
+            std::fill(y, y + c->n_mat, 0.0);
+            return;
+        }
         if (c->M == 0 || (!c->mat && !c->matf && !c->msym)) throw Error(CAPAC_ERR_INVALID, "no CPIM matrix in this system");
         double *dx = c->bw + (size_t)W_Y_SLOT * c->n_mat, *dy = c->bw + (size_t)W_V_SLOT * c->n_mat;
         const size_t nb = sizeof(double) * c->n_mat;
@@ -819,6 +823,24 @@ struct CkptHeader {
 
 }  // namespace
 
+namespace {
+// Closes a FILE on every way out of a scope.
+struct FileGuard {
+    FILE *f;
+    explicit FileGuard(FILE *ff) : f(ff) {}
+    ~FileGuard()
+    {
+        if (f) fclose(f);
+    }
+    int close()
+    {
+        const int r = fclose(f);
+        f = nullptr;
+        return r;
+    }
+};
+}  // namespace
+
 int capac_checkpoint_save(capac_ctx *c, const char *path)
 {
     return guard([&] {
@@ -836,69 +858,70 @@ int capac_checkpoint_save(capac_ctx *c, const char *path)
         h.n_solves = c->n_solves;
         h.em_length = c->em_length;
         for (int a = 0; a < 3; ++a) h.box[a] = c->P.box.L[a];
-        FILE *f = fopen(path, "wb");
-        if (!f) throw Error(CAPAC_ERR_IO, std::string("cannot write ") + path);
+        ThermoState th;
+        CAPAC_CUDA(cudaMemcpy(&th, c->th, sizeof th, cudaMemcpyDeviceToHost));
+        FileGuard fg(fopen(path, "wb"));
+        if (!fg.f) throw Error(CAPAC_ERR_IO, std::string("cannot write ") + path);
         std::vector<double> buf;
         auto put = [&](const double *d, size_t n) {
             buf.resize(n);
             if (n) CAPAC_CUDA(cudaMemcpy(buf.data(), d, sizeof(double) * n, cudaMemcpyDeviceToHost));
-            if (fwrite(buf.data(), sizeof(double), n, f) != n) throw Error(CAPAC_ERR_IO, "short write");
+            if (fwrite(buf.data(), sizeof(double), n, fg.f) != n) throw Error(CAPAC_ERR_IO, "short write");
         };
-        bool ok = fwrite(&h, sizeof h, 1, f) == 1;
-        ThermoState th;
-        CAPAC_CUDA(cudaMemcpy(&th, c->th, sizeof th, cudaMemcpyDeviceToHost));
-        ok = ok && fwrite(&th, sizeof th, 1, f) == 1;
-        if (!ok) {
-            fclose(f);
+        if (fwrite(&h, sizeof h, 1, fg.f) != 1 || fwrite(&th, sizeof th, 1, fg.f) != 1)
             throw Error(CAPAC_ERR_IO, "short write");
-        }
         const size_t N = c->N;
         for (const double *p : {c->rx, c->ry, c->rz, c->vx, c->vy, c->vz, c->fx, c->fy, c->fz}) put(p, N);
         put(c->pot, 15);
         put(c->vir, 9);
         if (h.n_mat) put(c->vec_pq, h.n_mat);
         if (h.has_hist) put(c->xprev, (size_t)3 * c->n_mat);
-        if (fclose(f) != 0) throw Error(CAPAC_ERR_IO, "close failed");
+        if (fg.close() != 0) throw Error(CAPAC_ERR_IO, "close failed");
     });
 }
 
+// The whole file is read and checked before any device state changes: a
+// truncated or foreign file leaves the context as it was.
 int capac_checkpoint_load(capac_ctx *c, const char *path)
 {
     return guard([&] {
         check_ctx(c);
         if (!path) throw Error(CAPAC_ERR_INVALID, "null path");
-        FILE *f = fopen(path, "rb");
-        if (!f) throw Error(CAPAC_ERR_IO, std::string("cannot read ") + path);
         CkptHeader h{};
         ThermoState th;
-        const bool head = fread(&h, sizeof h, 1, f) == 1 && fread(&th, sizeof th, 1, f) == 1;
-        if (!head || memcmp(h.magic, kCkptMagic, 8) != 0 || h.version != 1) {
-            fclose(f);
-            throw Error(CAPAC_ERR_IO, "not a checkpoint of this library");
+        std::vector<double> data;
+        size_t n_hist = 0;
+        {
+            FileGuard fg(fopen(path, "rb"));
+            if (!fg.f) throw Error(CAPAC_ERR_IO, std::string("cannot read ") + path);
+            const bool head = fread(&h, sizeof h, 1, fg.f) == 1 && fread(&th, sizeof th, 1, fg.f) == 1;
+            if (!head || memcmp(h.magic, kCkptMagic, 8) != 0 || h.version != 1)
+                throw Error(CAPAC_ERR_IO, "not a checkpoint of this library");
+            if (h.N != c->N || h.n_mat != (c->M > 0 ? c->n_mat : 0) || (h.has_hist && !c->xprev))
+                throw Error(CAPAC_ERR_INVALID, "checkpoint is of a different system or precision");
+            for (int a = 0; a < 3; ++a)
+                if (h.box[a] != c->P.box.L[a]) throw Error(CAPAC_ERR_INVALID, "checkpoint is of a different box");
+            n_hist = h.has_hist ? (size_t)3 * c->n_mat : 0;
+            const size_t total = 9 * (size_t)c->N + 15 + 9 + (size_t)h.n_mat + n_hist;
+            data.resize(total);
+            if (fread(data.data(), sizeof(double), total, fg.f) != total)
+                throw Error(CAPAC_ERR_IO, "truncated checkpoint");
         }
-        if (h.N != c->N || h.n_mat != (c->M > 0 ? c->n_mat : 0) || (h.has_hist && !c->xprev)) {
-            fclose(f);
-            throw Error(CAPAC_ERR_INVALID, "checkpoint is of a different system or precision");
-        }
-        std::vector<double> buf;
-        auto get = [&](double *d, size_t n) {
-            buf.resize(n);
-            if (fread(buf.data(), sizeof(double), n, f) != n) throw Error(CAPAC_ERR_IO, "truncated checkpoint");
-            if (n) CAPAC_CUDA(cudaMemcpy(d, buf.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+        // the context's stream may still be using the arrays about to be replaced
+        CAPAC_CUDA(cudaStreamSynchronize(c->stream));
+        const double *src = data.data();
+        auto put = [&](double *d, size_t n) {
+            if (n) CAPAC_CUDA(cudaMemcpyAsync(d, src, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
+            src += n;
         };
-        try {
-            const size_t N = c->N;
-            for (double *p : {c->rx, c->ry, c->rz, c->vx, c->vy, c->vz, c->fx, c->fy, c->fz}) get(p, N);
-            get(c->pot, 15);
-            get(c->vir, 9);
-            if (h.n_mat) get(c->vec_pq, h.n_mat);
-            if (h.has_hist) get(c->xprev, (size_t)3 * c->n_mat);
-        } catch (...) {
-            fclose(f);
-            throw;
-        }
-        fclose(f);
-        CAPAC_CUDA(cudaMemcpy(c->th, &th, sizeof th, cudaMemcpyHostToDevice));
+        const size_t N = c->N;
+        for (double *p : {c->rx, c->ry, c->rz, c->vx, c->vy, c->vz, c->fx, c->fy, c->fz}) put(p, N);
+        put(c->pot, 15);
+        put(c->vir, 9);
+        if (h.n_mat) put(c->vec_pq, h.n_mat);
+        if (n_hist) put(c->xprev, n_hist);
+        CAPAC_CUDA(cudaMemcpyAsync(c->th, &th, sizeof th, cudaMemcpyHostToDevice, c->stream));
+        CAPAC_CUDA(cudaStreamSynchronize(c->stream));
         c->md_step = h.md_step;
         c->em_step = h.em_step;
         c->em_length = h.em_length;
@@ -986,6 +1009,12 @@ int capac_set(capac_ctx *c, const char *name, const double *in)
         if (!name || !in) throw Error(CAPAC_ERR_INVALID, "null argument");
         std::string n(name);
         CAPAC_CUDA(cudaStreamSynchronize(c->stream));
+        if (n == "wait_polls") {  // the persistent solver's grid-barrier poll limit (0: the default)
+            if (!(in[0] >= 0.0 && in[0] <= 2147483647.0)) throw Error(CAPAC_ERR_INVALID, "wait_polls out of range");
+            c->opt.wait_polls = (int)in[0];
+            count = 1;
+            return;
+        }
         int cnt = 0;
         double *p = state_array(c, n, &cnt);
         if (!p || n == "potential" || n == "virial" || n == "inv_sqrt_dens" || n == "diag_relay" ||

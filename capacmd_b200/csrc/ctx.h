@@ -17,7 +17,7 @@ struct SolverScalars {
     double bTb, crit, rho, rho_old, alpha, omega, rTr, skip;
     double res0;     // refinement: FP64 residual norm^2 at the sweep start
     double rr0;      // (r, r) of the warm start
-    int iter, done, status, pad;
+    int iter, done, status, max_iter;
 };
 
 // Thermostat and integrator scalars (System, typedef.h:353-401).
@@ -278,6 +278,8 @@ int coop_grid_size(int device, bool mixed);
 size_t coop_barrier_bytes();
 size_t coop_partial_doubles(int grid);
 int bicgstab_coop(capac_ctx *c, const double *b, double *x, double tol, double skip);
+// BiCGSTAB iteration limit of the context (the option, else MAX_ITER)
+inline int solver_max_iter(const capac_ctx *c);
 void launch_cpim_metal_forces(capac_ctx *c);
 void launch_external_field(capac_ctx *c);
 void launch_finalize(capac_ctx *c, int nblocks, int K, const int *slots_pot, const int *slots_vir);
@@ -316,5 +318,7 @@ struct ProfScope {
 };
 
 inline unsigned grid_for(long n, int block) { return (unsigned)((n + block - 1) / block); }
+
+inline int solver_max_iter(const capac_ctx *c) { return c->opt.max_iter > 0 ? c->opt.max_iter : kMaxIter; }
 
 }  // namespace capac

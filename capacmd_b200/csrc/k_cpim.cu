@@ -366,7 +366,8 @@ __global__ void __launch_bounds__(256) k_vec_dot(int n, const double *__restrict
 // absolute threshold of the reference's two early exits (bTb < 1e-10 and, on
 // the first iteration, rho < 1e-10); refinement sweeps, whose right-hand
 // sides are small residuals, pass a threshold that only catches exact zero.
-__global__ void k_bcg_start(const double *partials, int nb, double tol, double skip, SolverScalars *ss)
+__global__ void k_bcg_start(const double *partials, int nb, double tol, double skip, int max_iter,
+                            SolverScalars *ss)
 {
     __shared__ double sh[64];
     double s0, s1;
@@ -378,6 +379,7 @@ __global__ void k_bcg_start(const double *partials, int nb, double tol, double s
         ss->iter = 0;
         ss->status = 0;
         ss->skip = skip;
+        ss->max_iter = max_iter;
         ss->done = s0 < skip ? 1 : 0;
         ss->rTr = 0.0;
     }
@@ -530,7 +532,7 @@ __global__ void k_bcg_check(const double *partials, int nb, SolverScalars *ss)
         ss->iter += 1;
         if (rTr < ss->crit) {
             ss->done = 1;
-        } else if (ss->iter > kMaxIter) {
+        } else if (ss->iter > ss->max_iter) {
             ss->done = 1;
             ss->status = rTr < ss->crit * 100.0 ? 1 : -1;  // 1: loosened criterion accepted
         }
@@ -655,7 +657,7 @@ int bicgstab_core(capac_ctx *c, const double *b, double *x, double tol, double s
     auto W = [&](int k) { return bw + (size_t)k * n; };
 
     k_vec_dot<<<nbv, 256, 0, s>>>(n, b, b, c->partials);
-    k_bcg_start<<<1, 256, 0, s>>>(c->partials, nbv, tol, skip, c->ss);
+    k_bcg_start<<<1, 256, 0, s>>>(c->partials, nbv, tol, skip, solver_max_iter(c), c->ss);
     spmv(c, DOT_NONE, x, W(W_AX), nullptr, nullptr, c->ss);
     k_bcg_init<<<nbv, 256, 0, s>>>(n, n4, b, c->diag, bw, c->partials, c->ss);
     k_bcg_rho0<<<1, 256, 0, s>>>(c->partials, nbv, c->ss);
@@ -710,7 +712,7 @@ int bicgstab_core(capac_ctx *c, const double *b, double *x, double tol, double s
             c->launches = l0;
         }
     }
-    for (int it = 0; it <= kMaxIter + chunk; it += chunk) {
+    for (int it = 0; it <= solver_max_iter(c) + chunk; it += chunk) {
         if (g) {
             CAPAC_CUDA(cudaGraphLaunch(g->exec, s));
             c->launches += g->kernels;
@@ -767,7 +769,7 @@ int run_refined_solve(capac_ctx *c)
     const int max_sweeps = 12;
 
     k_vec_dot<<<nbv, 256, 0, s>>>(n, c->vec_ext, c->vec_ext, c->partials);
-    k_bcg_start<<<1, 256, 0, s>>>(c->partials, nbv, 1.0, 1.0e-10, c->ss);
+    k_bcg_start<<<1, 256, 0, s>>>(c->partials, nbv, 1.0, 1.0e-10, solver_max_iter(c), c->ss);
     c->launches += 2;
     CAPAC_CUDA(cudaMemcpyAsync(c->h_ss, c->ss, sizeof(SolverScalars), cudaMemcpyDeviceToHost, s));
     CAPAC_CUDA(cudaStreamSynchronize(s));

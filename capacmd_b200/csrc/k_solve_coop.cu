@@ -30,7 +30,8 @@
 // returned is summed directly from the final residual.
 //
 // Every wait is bounded.  The grid barrier (counter and generation word)
-// gives up after 2^24 polls, a ring-stage wait after 2^20 polls of at most
+// gives up after 2^24 polls (the context's wait_polls option when set), a
+// ring-stage wait after 2^20 polls of at most
 // 1 us each; either sets the error word, the block then waits (bounded) for
 // its own copies in flight and returns, the other blocks give up at their
 // next barrier, and the host reports the error.  The launch is cooperative,
@@ -175,6 +176,7 @@ struct CoopSync {
 
 struct CoopArgs {
     int M, n, n4, nT, ntiles, n_nps, metal_min, max_iter;
+    long spin_limit;  // polls of a grid barrier before it gives up
     double inv_polar, inv_capac;
     const int *np_start, *np_end;
     const void *mat;
@@ -213,8 +215,8 @@ __device__ __forceinline__ void phase_mark(const CoopArgs &A, int iter, int k)
     }
 }
 
-// Bounded grid barrier; false if any block gave up.
-__device__ bool grid_barrier(CoopSync *bar)
+// Bounded grid barrier (`limit` polls); false if any block gave up.
+__device__ bool grid_barrier(CoopSync *bar, long limit)
 {
     __shared__ int ok;
     __syncthreads();
@@ -230,7 +232,7 @@ __device__ bool grid_barrier(CoopSync *bar)
         } else {
             long spins = 0;
             while (*gen == g) {
-                if (++spins > kSpinLimit) {
+                if (++spins > limit) {
                     atomicCAS(&bar->error, 0, 1);
                     break;
                 }
@@ -714,7 +716,7 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? 2 : 1) k_bicgstab_coo
         }
         put_bp<2>(bpA, pb);
     }
-    ok = grid_barrier(A.sync);
+    ok = grid_barrier(A.sync, A.spin_limit);
     bool x_zero = false;
     if (ok) {
         double t2[2];
@@ -735,13 +737,13 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? 2 : 1) k_bicgstab_coo
                 A.r[k] = bk;
             }
         } else {
-            ok = tiles_pass<T, MODE_X>(A, S, ring, psm) && grid_barrier(A.sync);
+            ok = tiles_pass<T, MODE_X>(A, S, ring, psm) && grid_barrier(A.sync, A.spin_limit);
             if (ok) reduce_pass<RED_START>(A, S, bpB);
         }
-        ok = ok && grid_barrier(A.sync);
+        ok = ok && grid_barrier(A.sync, A.spin_limit);
         if (ok && A.bj) {  // K r of the start residual; y = K r on the first iteration
             prec_pass<false>(A, A.r, A.Kr, nullptr);
-            ok = grid_barrier(A.sync);
+            ok = grid_barrier(A.sync, A.spin_limit);
         }
         done = !ok;
     }
@@ -764,19 +766,19 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? 2 : 1) k_bicgstab_coo
         S.alpha = alpha;
         ok = tiles_pass<T, MODE_P>(A, S, ring, psm);
         phase_mark(A, iter, 1);
-        ok = ok && grid_barrier(A.sync);
+        ok = ok && grid_barrier(A.sync, A.spin_limit);
         if (!ok) break;
         phase_mark(A, iter, 2);
         S.first = 0;
         reduce_pass<RED_V>(A, S, bpA);
-        if (!grid_barrier(A.sync)) {
+        if (!grid_barrier(A.sync, A.spin_limit)) {
             ok = false;
             break;
         }
         phase_mark(A, iter, 3);
         if (A.bj) {  // K v
             prec_pass<false>(A, A.v[0], A.Kv, nullptr);
-            if (!grid_barrier(A.sync)) {
+            if (!grid_barrier(A.sync, A.spin_limit)) {
                 ok = false;
                 break;
             }
@@ -792,18 +794,18 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? 2 : 1) k_bicgstab_coo
         alpha = al;
         S.cur ^= 1;  // v[cur] and p[cur] are now the new ones
         S.alpha = alpha;
-        ok = tiles_pass<T, MODE_S>(A, S, ring, psm) && grid_barrier(A.sync);
+        ok = tiles_pass<T, MODE_S>(A, S, ring, psm) && grid_barrier(A.sync, A.spin_limit);
         if (!ok) break;
         phase_mark(A, iter, 5);
         reduce_pass<RED_T>(A, S, bpB);
-        if (!grid_barrier(A.sync)) {
+        if (!grid_barrier(A.sync, A.spin_limit)) {
             ok = false;
             break;
         }
         phase_mark(A, iter, 6);
         if (A.bj) {  // K t with (K t, z), (K t, K t)
             prec_pass<true>(A, A.t, A.Kt, bpB + 7);
-            if (!grid_barrier(A.sync)) {
+            if (!grid_barrier(A.sync, A.spin_limit)) {
                 ok = false;
                 break;
             }
@@ -847,7 +849,7 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? 2 : 1) k_bicgstab_coo
             q[0] += rk * rk;
         }
         put_bp<1>(bpA, q);
-        ok = grid_barrier(A.sync);
+        ok = grid_barrier(A.sync, A.spin_limit);
         if (ok) {
             sum_bp<1>(bpA, nb, q);
             rTr = q[0];
@@ -893,7 +895,8 @@ int bicgstab_coop(capac_ctx *c, const double *b, double *x, double tol, double s
     A.ntiles = A.nT * (A.nT + 1) / 2;
     A.n_nps = c->n_nps;
     A.metal_min = c->P.metal_min;
-    A.max_iter = kMaxIter;
+    A.max_iter = solver_max_iter(c);
+    A.spin_limit = c->opt.wait_polls > 0 ? c->opt.wait_polls : kSpinLimit;
     A.inv_polar = c->P.inv_polar;
     A.inv_capac = c->P.inv_capac;
     A.np_start = c->np_start;

@@ -187,6 +187,12 @@ typedef struct capac_options {
     int pair_list;          /* mixed path nonbonded list: 0 clusters of four atoms sharing each
                                neighbour's load where the box is large enough (default), 1 one list
                                per atom (the FP64 path always uses one list per atom) */
+    int max_iter;           /* BiCGSTAB iteration limit before the 100x fallback and
+                               CAPAC_ERR_NOT_CONVERGED; 0 = the reference's MAX_ITER, 1000
+                               (typedef.h:85, bicg_stab.c:546-570) */
+    int wait_polls;         /* persistent solver: polls of a grid barrier before it gives up and the
+                               call returns CAPAC_ERR_CUDA (the context stays usable); 0 = 2^24, about
+                               a second.  Also settable on a live context (capac_set "wait_polls") */
 } capac_options;
 
 void capac_options_default(capac_options *o);
@@ -232,14 +238,22 @@ int capac_force_given_pq(capac_ctx *ctx);
  * hands all device memory to its own pool at start-up and forbids later
  * allocations, or a per-time-step caller for which an allocation (which may
  * synchronise the device) is not acceptable.  Same Jacobi-preconditioned
- * BiCGSTAB as capac_bicgstab, on arrays the caller owns (device pointers):
+ * BiCGSTAB as capac_bicgstab, with the same breakdown guard (a zero or
+ * non-finite alpha or omega leaves x at its last finite value and restarts
+ * from there, up to eight starts) and the same acceptance of 100x the
+ * criterion after MAX_ITER iterations (CAPAC_OK, with the reference's
+ * "Loosen bicg_stab convergence criteria" note on stderr), on arrays the
+ * caller owns (device pointers):
  *   mat   the 4x4-block matrix, mat[(i*16 + 4*row + col)*mat_stride + j] for
  *         block row i and block column j of n_metal metal atoms, rows/cols of a
  *         block ordered (p_x, p_y, p_z, q);
  *   rhs, diag  n_mat = 4*n_metal + n_nps values, reference vector layout;
  *   x     in: warm start, out: solution.
  * np_start/np_end are HOST arrays of metal-local atom ranges.  tol: criterion
- * rTr < tol*bTb (0 = 1e-8).  stream: a cudaStream_t, NULL for the default.
+ * rTr < tol*bTb (0 = 1e-8).  stream: a cudaStream_t, NULL for the default;
+ * the call reads the convergence state back every four iterations and
+ * returns when the solve has ended on that stream.  iterations: summed over
+ * the starts.
  * Limits: n_mat <= 16384 and n_nps <= 16 (CAPAC_ERR_CAPACITY beyond).  The
  * work space is one static device array of about 1.2 MB that every device
  * loading the library holds until exit; the first call on a device looks up
@@ -292,7 +306,8 @@ int capac_checkpoint_load(capac_ctx *ctx, const char *path);
  * adjoint_mu, adjoint_nu (the adjoint solutions).  Read-only diagnostics:
  * pair_list(2: 1 when the pair kernel walks the cluster list, cluster count),
  * solver_phases(9: mean ns per iteration of the persistent solver's phases
- * when CAPAC_SOLVER_PHASES is set, then the iterations timed).  capac_get
+ * when CAPAC_SOLVER_PHASES is set, then the iterations timed).  Set only:
+ * wait_polls(1), the option of that name on the live context.  capac_get
  * returns the count written, <0 on error. */
 int capac_get(capac_ctx *ctx, const char *name, double *out);
 int capac_set(capac_ctx *ctx, const char *name, const double *in);

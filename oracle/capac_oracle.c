@@ -19,6 +19,8 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <pthread.h>
+#include <unistd.h>
 
 #include "capacmd.h"
 
@@ -49,6 +51,8 @@ typedef struct orc {
     int iterations;
     double f_max, f_rms;
     int error;
+    int *sample; /* atoms whose nonbonded forces are formed when set (orc_set_sample) */
+    int n_sample;
 } orc;
 
 /* ---------------------------------------------------------- geometry */
@@ -149,27 +153,214 @@ static int excluded(const capac_desc *d, int i, int j)
     return d->excl[d->excl_offset[m] + d->atom_in_mol[i] * na + d->atom_in_mol[j]] != 0;
 }
 
-/* mpi_nonb_pair, force.c:1402-1540, one rank, all j < i. */
+/* Cells of edge >= rc over the box, for traversals that must visit exactly
+ * the reference's pairs without its N(N-1)/2 loop.  Positions wrapped into the
+ * box pick a cell; two atoms that pbc_12 puts within rc are within rc of each
+ * other's minimum image, so they lie in neighbouring cells, and with three or
+ * more cells per edge the 27 cells around a cell are distinct, so each pair
+ * is met once.  cells_build returns 0 (nothing allocated) for boxes with
+ * fewer than three cells along an edge. */
+typedef struct cells {
+    int nc[3];
+    int *cell;  /* [N] cell of each atom */
+    int *start; /* [cells + 1] */
+    int *atoms; /* [N] atoms in cell order, ascending index within a cell */
+} cells;
+
+static int cells_build(const orc *o, cells *c)
+{
+    const int N = o->N;
+    for (int a = 0; a < 3; ++a) c->nc[a] = (int)floor(o->box[a] / o->d->r_cut);
+    if (c->nc[0] < 3 || c->nc[1] < 3 || c->nc[2] < 3) return 0;
+    const int ncell = c->nc[0] * c->nc[1] * c->nc[2];
+    c->cell = (int *)malloc(sizeof(int) * (size_t)N);
+    c->start = (int *)calloc((size_t)ncell + 1, sizeof(int));
+    c->atoms = (int *)malloc(sizeof(int) * (size_t)N);
+    int *fill = (int *)malloc(sizeof(int) * (size_t)ncell);
+    const double *r[3] = {o->rx, o->ry, o->rz};
+    for (int i = 0; i < N; ++i) {
+        int k3[3];
+        for (int a = 0; a < 3; ++a) {
+            const double L = o->box[a];
+            const double w = r[a][i] - L * floor(r[a][i] / L);
+            const int k = (int)(w / L * c->nc[a]);
+            k3[a] = k < 0 ? 0 : (k >= c->nc[a] ? c->nc[a] - 1 : k);
+        }
+        c->cell[i] = (k3[0] * c->nc[1] + k3[1]) * c->nc[2] + k3[2];
+        ++c->start[c->cell[i] + 1];
+    }
+    for (int k = 0; k < ncell; ++k) c->start[k + 1] += c->start[k];
+    memcpy(fill, c->start, sizeof(int) * (size_t)ncell);
+    for (int i = 0; i < N; ++i) c->atoms[fill[c->cell[i]]++] = i;
+    free(fill);
+    return 1;
+}
+
+static void cells_free(cells *c)
+{
+    free(c->cell); free(c->start); free(c->atoms);
+}
+
+/* The k-th (0..26) cell around atom i's cell. */
+static int cells_near(const cells *c, int i, int k)
+{
+    const int ci = c->cell[i], nz = c->nc[2], ny = c->nc[1];
+    const int cz = ci % nz, cy = (ci / nz) % ny, cx = ci / (ny * nz);
+    const int kx = (cx + k / 9 - 1 + c->nc[0]) % c->nc[0], ky = (cy + (k / 3) % 3 - 1 + ny) % ny,
+              kz = (cz + k % 3 - 1 + nz) % nz;
+    return (kx * ny + ky) * nz + kz;
+}
+
+/* Accumulators of the pair loop: forces (fx, fy, fz of N each), the
+ * Coulomb and van der Waals energies, the virial. */
+typedef struct nb_acc {
+    double *fx, *fy, *fz;
+    double e_qq, e_vdw;
+    double vir[9];
+} nb_acc;
+
+/* One pair of mpi_nonb_pair's loop (force.c:1440-1538): i > j, r = r_j - r_i. */
+static void nonbonded_pair(const orc *o, int i, int j, nb_acc *a)
+{
+    const capac_desc *d = o->d;
+    const double rc = d->r_cut;
+    if (excluded(d, i, j)) return;
+    double x = o->rx[j] - o->rx[i], y = o->ry[j] - o->ry[i], z = o->rz[j] - o->rz[i];
+    image(&x, &y, &z, o->box);
+    if (x >= rc && y >= rc && z >= rc) return;
+    const double r2 = norm2(x, y, z);
+    if (r2 >= o->c.r_cut2) return;
+    const double f = pair_term(o, d->atom_type[i], d->atom_type[j], d->charge[i], d->charge[j], r2, &a->e_qq,
+                               &a->e_vdw);
+    const double fjx = f * x, fjy = f * y, fjz = f * z;
+    a->fx[i] -= fjx; a->fy[i] -= fjy; a->fz[i] -= fjz;
+    a->fx[j] += fjx; a->fy[j] += fjy; a->fz[j] += fjz;
+    acc_vir(a->vir, x, y, z, fjx, fjy, fjz, 1.0);
+}
+
+/* All pairs j < i of rows i = first, first + stride, ..., through cells when
+ * c is set, else the reference's loop. */
+static void nonbonded_rows(const orc *o, const cells *c, int first, int stride, nb_acc *a)
+{
+    for (int i = first; i < o->N; i += stride) {
+        if (c) {
+            for (int k = 0; k < 27; ++k) {
+                const int cc = cells_near(c, i, k);
+                for (int t = c->start[cc]; t < c->start[cc + 1]; ++t)
+                    if (c->atoms[t] < i) nonbonded_pair(o, i, c->atoms[t], a);
+            }
+        } else {
+            for (int j = 0; j < i; ++j) nonbonded_pair(o, i, j, a);
+        }
+    }
+}
+
+/* Host threads for the large-system loops: the online cores, at most 64. */
+static int host_threads(void)
+{
+    const long n = sysconf(_SC_NPROCESSORS_ONLN);
+    return n < 1 ? 1 : (n > 64 ? 64 : (int)n);
+}
+
+typedef struct nb_job {
+    const orc *o;
+    const cells *c;
+    int first, stride;
+    nb_acc acc;
+} nb_job;
+
+static void *nb_thread(void *arg)
+{
+    nb_job *j = (nb_job *)arg;
+    nonbonded_rows(j->o, j->c, j->first, j->stride, &j->acc);
+    return NULL;
+}
+
+static void nonbonded_with(orc *o, const cells *c)
+{
+    const int N = o->N;
+    const int nt = N >= 2048 ? host_threads() : 1;
+    if (nt <= 1) {
+        nb_acc a = {o->fx, o->fy, o->fz, 0.0, 0.0, {0}};
+        nonbonded_rows(o, c, 0, 1, &a);
+        o->pot[7] += a.e_qq;
+        o->pot[8] += a.e_vdw;
+        for (int k = 0; k < 9; ++k) o->vir[k] += a.vir[k];
+        return;
+    }
+    nb_job *job = (nb_job *)calloc((size_t)nt, sizeof(nb_job));
+    double *buf = (double *)calloc((size_t)nt * 3 * N, sizeof(double));
+    pthread_t *th = (pthread_t *)malloc(sizeof(pthread_t) * (size_t)nt);
+    for (int t = 0; t < nt; ++t) {
+        job[t].o = o;
+        job[t].c = c;
+        job[t].first = t;
+        job[t].stride = nt;
+        job[t].acc.fx = buf + (size_t)t * 3 * N;
+        job[t].acc.fy = job[t].acc.fx + N;
+        job[t].acc.fz = job[t].acc.fy + N;
+        pthread_create(&th[t], NULL, nb_thread, &job[t]);
+    }
+    for (int t = 0; t < nt; ++t) pthread_join(th[t], NULL);
+    for (int t = 0; t < nt; ++t) { /* in thread order: a fixed summation order */
+        const nb_acc *a = &job[t].acc;
+        for (int i = 0; i < N; ++i) { o->fx[i] += a->fx[i]; o->fy[i] += a->fy[i]; o->fz[i] += a->fz[i]; }
+        o->pot[7] += a->e_qq;
+        o->pot[8] += a->e_vdw;
+        for (int k = 0; k < 9; ++k) o->vir[k] += a->vir[k];
+    }
+    free(th);
+    free(buf);
+    free(job);
+}
+
+/* mpi_nonb_pair, force.c:1402-1540, one rank, all j < i.  Systems of 2,048
+ * atoms or more in boxes of four or more cells per edge visit the same pairs
+ * through cells; systems of 2,048 atoms or more split the rows over the
+ * host threads, each with its own accumulators, added in thread order
+ * afterwards.  Both change only the order of the sums (rounding); smaller
+ * systems take the reference's loop literally. */
 static void nonbonded(orc *o)
+{
+    const int N = o->N;
+    cells c;
+    const int use_cells = N >= 2048 && cells_build(o, &c);
+    if (use_cells && (c.nc[0] < 4 || c.nc[1] < 4 || c.nc[2] < 4)) {
+        cells_free(&c);
+        return nonbonded_with(o, NULL);
+    }
+    nonbonded_with(o, use_cells ? &c : NULL);
+    if (use_cells) cells_free(&c);
+}
+/* Nonbonded forces on the atoms of a sample only: every pair that involves a
+ * sampled atom s, taken in the reference's orientation (the larger index is
+ * the outer atom i, r = r_j - r_i; force.c:1419-1473), so the cut-off decision
+ * is the reference's to the bit.  The pairs' energies and virial are not
+ * formed.  O(N) per sampled atom, for systems whose all-pairs loop is too slow
+ * for a test; force_terms() uses it while a sample is set. */
+static void nonbonded_sample(orc *o)
 {
     const capac_desc *d = o->d;
     const double rc = d->r_cut, rc2 = o->c.r_cut2;
-    for (int i = 0; i < o->N; ++i) {
-        const double xi = o->rx[i], yi = o->ry[i], zi = o->rz[i];
-        for (int j = 0; j < i; ++j) {
-            if (excluded(d, i, j)) continue;
-            double x = o->rx[j] - xi, y = o->ry[j] - yi, z = o->rz[j] - zi;
+    double e_qq = 0.0, e_vdw = 0.0;
+    for (int k = 0; k < o->n_sample; ++k) {
+        const int s = o->sample[k];
+        double fx = 0.0, fy = 0.0, fz = 0.0;
+        for (int j = 0; j < o->N; ++j) {
+            if (j == s) continue;
+            const int i = s > j ? s : j, jj = s > j ? j : s;
+            if (excluded(d, i, jj)) continue;
+            double x = o->rx[jj] - o->rx[i], y = o->ry[jj] - o->ry[i], z = o->rz[jj] - o->rz[i];
             image(&x, &y, &z, o->box);
             if (x >= rc && y >= rc && z >= rc) continue;
             const double r2 = norm2(x, y, z);
             if (r2 >= rc2) continue;
-            const double f = pair_term(o, d->atom_type[i], d->atom_type[j], d->charge[i], d->charge[j],
-                                       r2, &o->pot[7], &o->pot[8]);
-            const double fjx = f * x, fjy = f * y, fjz = f * z;
-            o->fx[i] -= fjx; o->fy[i] -= fjy; o->fz[i] -= fjz;
-            o->fx[j] += fjx; o->fy[j] += fjy; o->fz[j] += fjz;
-            acc_vir(o->vir, x, y, z, fjx, fjy, fjz, 1.0);
+            const double f = pair_term(o, d->atom_type[i], d->atom_type[jj], d->charge[i], d->charge[jj], r2,
+                                       &e_qq, &e_vdw);
+            if (s == i) { fx -= f * x; fy -= f * y; fz -= f * z; }
+            else { fx += f * x; fy += f * y; fz += f * z; }
         }
+        o->fx[s] += fx; o->fy[s] += fy; o->fz[s] += fz;
     }
 }
 
@@ -316,15 +507,53 @@ static void cpim_matrix(orc *o)
     for (int k = 0; k < d->n_nps; ++k) o->diag[4 * M + k] = 1.0;
 }
 
-static void matvec(const orc *o, const double *x, double *y)
+/* Rows r0 .. r1 - 1 of y = A x (one row's sum in column order). */
+static void matvec_rows(const orc *o, const double *x, double *y, int r0, int r1)
 {
     const int n = o->n_mat;
-    for (int r = 0; r < n; ++r) {
+    for (int r = r0; r < r1; ++r) {
         double s = 0.0;
         const double *row = o->A + (size_t)r * n;
         for (int c = 0; c < n; ++c) s += row[c] * x[c];
         y[r] = s;
     }
+}
+
+typedef struct mv_job {
+    const orc *o;
+    const double *x;
+    double *y;
+    int r0, r1;
+} mv_job;
+
+static void *mv_thread(void *arg)
+{
+    mv_job *j = (mv_job *)arg;
+    matvec_rows(j->o, j->x, j->y, j->r0, j->r1);
+    return NULL;
+}
+
+static void matvec(const orc *o, const double *x, double *y)
+{
+    const int n = o->n_mat;
+    if (!o->A) { /* use_cpff 0: the reference's COO matrix stays empty */
+        memset(y, 0, (size_t)n * sizeof(double));
+        return;
+    }
+    if (n >= 1024) {
+        const int nt = host_threads();
+        mv_job *job = (mv_job *)malloc(sizeof(mv_job) * (size_t)nt);
+        pthread_t *th = (pthread_t *)malloc(sizeof(pthread_t) * (size_t)nt);
+        for (int t = 0; t < nt; ++t) {
+            job[t] = (mv_job){o, x, y, (int)((long)n * t / nt), (int)((long)n * (t + 1) / nt)};
+            pthread_create(&th[t], NULL, mv_thread, &job[t]);
+        }
+        for (int t = 0; t < nt; ++t) pthread_join(th[t], NULL);
+        free(th);
+        free(job);
+        return;
+    }
+    matvec_rows(o, x, y, 0, n);
 }
 
 static double dot(int n, const double *a, const double *b)
@@ -528,7 +757,8 @@ static void force_terms(orc *o, int solve)
     memset(o->fz, 0, sizeof(double) * o->N);
     memset(o->pot, 0, sizeof o->pot);
     memset(o->vir, 0, sizeof o->vir);
-    nonbonded(o);
+    if (o->n_sample > 0) nonbonded_sample(o);
+    else nonbonded(o);
     if (o->M > 0) {
         sutton_chen(o);
         if (d->use_cpff) {
@@ -782,7 +1012,7 @@ void orc_destroy(orc *o)
 {
     if (!o) return;
     free(o->rx); free(o->inv_sqrt_dens); free(o->vec_ext); free(o->vec_pq); free(o->diag);
-    free(o->w); free(o->A); free(o);
+    free(o->w); free(o->A); free(o->sample); free(o);
 }
 
 int orc_force(orc *o)
@@ -898,6 +1128,59 @@ void orc_pair_fingerprint(orc *o, long *count, unsigned long long *hash)
     }
     *count = cnt;
     *hash = hs;
+}
+
+/* The same pair set as orc_pair_fingerprint, found through cells (see
+ * cells_build) instead of all N(N-1)/2 pairs: each atom i tests the j < i of
+ * the 27 cells around its own with the reference's image, early skip, r^2
+ * formula and exclusions.  Boxes with fewer than three cells along an edge
+ * take the all-pairs loop. */
+void orc_pair_fingerprint_cells(orc *o, long *count, unsigned long long *hash)
+{
+    const capac_desc *d = o->d;
+    const double rc = d->r_cut, rc2 = o->c.r_cut2;
+    cells c;
+    if (!cells_build(o, &c)) {
+        orc_pair_fingerprint(o, count, hash);
+        return;
+    }
+    long cnt = 0;
+    uint64_t hs = 0;
+    for (int i = 0; i < o->N; ++i)
+        for (int k = 0; k < 27; ++k) {
+            const int cc = cells_near(&c, i, k);
+            for (int t = c.start[cc]; t < c.start[cc + 1]; ++t) {
+                const int j = c.atoms[t];
+                if (j >= i || excluded(d, i, j)) continue;
+                double x = o->rx[j] - o->rx[i], y = o->ry[j] - o->ry[i], z = o->rz[j] - o->rz[i];
+                image(&x, &y, &z, o->box);
+                if (x >= rc && y >= rc && z >= rc) continue;
+                if (norm2(x, y, z) >= rc2) continue;
+                ++cnt;
+                hs += mix64(((uint64_t)(uint32_t)i << 32) | (uint32_t)j);
+            }
+        }
+    cells_free(&c);
+    *count = cnt;
+    *hash = hs;
+}
+
+/* Restrict the nonbonded pass of later force calls to the given atoms
+ * (nonbonded_sample); n = 0 restores the full pass. */
+int orc_set_sample(orc *o, const long *idx, int n)
+{
+    free(o->sample);
+    o->sample = NULL;
+    o->n_sample = 0;
+    if (n <= 0) return 0;
+    o->sample = (int *)malloc(sizeof(int) * (size_t)n);
+    if (!o->sample) return -1;
+    for (int k = 0; k < n; ++k) {
+        if (idx[k] < 0 || idx[k] >= o->N) return -1;
+        o->sample[k] = (int)idx[k];
+    }
+    o->n_sample = n;
+    return 0;
 }
 
 int orc_get(orc *o, const char *what, double *out)

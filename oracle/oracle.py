@@ -47,6 +47,9 @@ def _orc_lib():
         L.orc_matvec.restype = None
         L.orc_pair_fingerprint.argtypes = [vp, ctypes.POINTER(ctypes.c_long), ctypes.POINTER(ctypes.c_ulonglong)]
         L.orc_pair_fingerprint.restype = None
+        L.orc_pair_fingerprint_cells.argtypes = L.orc_pair_fingerprint.argtypes
+        L.orc_pair_fingerprint_cells.restype = None
+        L.orc_set_sample.argtypes = [vp, vp, ctypes.c_int]
         _orc = L
     return _orc
 
@@ -109,10 +112,20 @@ class Oracle:
     def forces(self) -> np.ndarray:
         return np.stack([self.get("fx"), self.get("fy"), self.get("fz")], 1)
 
-    def pair_fingerprint(self) -> tuple[int, int]:
+    def pair_fingerprint(self, cells: bool = False) -> tuple[int, int]:
+        """Count and hash of the reference's pair set: all-pairs loop, or
+        (cells=True) the same set found through a cell search."""
         c, h = ctypes.c_long(0), ctypes.c_ulonglong(0)
-        _orc_lib().orc_pair_fingerprint(self._p, ctypes.byref(c), ctypes.byref(h))
+        fn = _orc_lib().orc_pair_fingerprint_cells if cells else _orc_lib().orc_pair_fingerprint
+        fn(self._p, ctypes.byref(c), ctypes.byref(h))
         return c.value, h.value
+
+    def set_sample(self, atoms) -> None:
+        """Form nonbonded forces only on these atoms in later force calls
+        (all their pairs; no pair energies or virial); empty restores."""
+        self._sample = np.ascontiguousarray(atoms, dtype=np.int64)
+        if _orc_lib().orc_set_sample(self._p, self._sample.ctypes.data, len(self._sample)) != 0:
+            raise ValueError("sample index out of range")
 
 
 def ref_available() -> bool:

@@ -1,3 +1,4 @@
+import hashlib
 import os
 import sys
 
@@ -8,7 +9,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 sys.path.insert(0, ROOT)
 
 GOLDEN = os.path.join(ROOT, "tests", "golden")
-GOLDEN_CASES = ["t_au13", "t_au55w", "t_2np", "t_water", "c1", "c1_field"]
+GOLDEN_CASES = ["t_au13", "t_au55w", "t_2np", "t_water", "c1", "c1_field", "t_morse_buck"]
 
 
 def pytest_configure(config):
@@ -24,6 +25,26 @@ def golden_paths(case: str) -> dict:
 def golden_ref(case: str) -> dict:
     with np.load(os.path.join(GOLDEN, case, "ref.npz")) as z:
         return {k: z[k] for k in z.files}
+
+
+def input_digest(paths: dict) -> str:
+    """SHA-256 over the three input files, in the order gro, param, mdset."""
+    h = hashlib.sha256()
+    for k in ("gro", "par", "mds"):
+        with open(paths[k], "rb") as f:
+            h.update(f.read())
+    return h.hexdigest()
+
+
+def large_case(case: str) -> tuple[dict, dict]:
+    """Inputs of a large golden case, rebuilt by the seeded generator (their
+    files are not stored), with the reference's record of them; fails if the
+    generator no longer writes the inputs the record was made from."""
+    from capacmd_b200 import configs
+    paths = configs.cached(case)
+    g = golden_ref(case)
+    assert input_digest(paths) == str(g["input_sha256"]), f"{case}: generated inputs differ from the golden's"
+    return paths, g
 
 
 def rel_err(a, b) -> float:
@@ -53,3 +74,30 @@ def gpu_available() -> bool:
         return torch.cuda.get_device_capability(0)[0] == 10
     except Exception:
         return False
+
+
+def variant(case: str, out_dir: str, par=None, mds=None) -> dict:
+    """A golden case's three inputs written to out_dir under the reference
+    program's default names, with param.txt / mdset.txt text passed through
+    the given functions."""
+    src = golden_paths(case)
+    names = {"gro": "init.gro", "par": "param.txt", "mds": "mdset.txt"}
+    edit = {"par": par, "mds": mds}
+    out = {}
+    for k, p in src.items():
+        text = open(p).read()
+        if edit.get(k):
+            new = edit[k](text)
+            assert new != text, f"{k}: the edit changed nothing"
+            text = new
+        out[k] = os.path.join(str(out_dir), names[k])
+        with open(out[k], "w") as f:
+            f.write(text)
+    return out
+
+
+def impossible_constraints(text: str) -> str:
+    """t_water's param.txt with an H-H constraint longer than the two O-H
+    constraints together: no geometry satisfies it, so RATTLE cannot converge
+    (the reference stops with "RATTLE_1 not converged!", force.c:1990-1994)."""
+    return text.replace("1 2   0.163298", "1 2   0.300000")

@@ -37,7 +37,7 @@ def _both(paths, case=None):
     return d, f64, mix
 
 
-@pytest.mark.parametrize("case", ["t_au55w", "t_2np", "c1_field", "t_water", "c1"])
+@pytest.mark.parametrize("case", ["t_au55w", "t_2np", "c1_field", "t_water", "c1", "t_morse_buck"])
 def test_mixed_forces_and_charges(case):
     d, f64, mix = _both(golden_paths(case), case)
     assert rel_err(mix.forces(), f64.forces()) < 1e-5

@@ -130,9 +130,10 @@ def test_md_100_steps_energy_trace(case):
     assert rel_err(s.get("rx"), o.get("rx")) < 1e-8
 
 
-def test_reference_md_trace_without_solve_noise():
-    d, s, o = _pair("c1")
-    g = golden_ref("c1")
+@pytest.mark.parametrize("case", ["c1", "t_water", "t_morse_buck"])
+def test_reference_md_trace_without_solve_noise(case):
+    d, s, o = _pair(case)
+    g = golden_ref(case)
     s.md_init()
     pots = []
     for _ in range(len(g["md_potential"])):

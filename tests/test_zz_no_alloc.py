@@ -3,11 +3,14 @@
 capac_bicgstab_static serves callers that cannot call cudaMalloc (a host code
 that owns all device memory through its own pool, or a per-step caller that
 must not trigger an allocation): they pass device arrays they own, and the
-solver's work space is a fixed static device array.  This test hands it the
+solver's work space is a fixed static device array.  These tests hand it the
 same matrix, right-hand side and diagonal the context solver (capac_bicgstab)
-used, on two calls in a row, and checks both solutions against the context
-solver's at the tolerance of the tight-solve parity tests.  It sits in a file
-of its own that pytest collects last.
+used, on two calls in a row, and check both solutions against the context
+solver's at the tolerance of the tight-solve parity tests; then the branches
+a caller meets next: a system without nanoparticles (no neutrality rows), a
+warm start from the solution, a zero right-hand side (the reference's early
+exit), and a breakdown, which must leave the caller's x as it was.  The file
+sits on its own and pytest collects it last.
 """
 import ctypes
 import os
@@ -21,6 +24,12 @@ from conftest import golden_paths, rel_err
 pytestmark = pytest.mark.gpu
 
 TIGHT = 1e-26
+
+
+@pytest.fixture(autouse=True)
+def _need_gpu(gpu_available):
+    if not gpu_available:
+        pytest.fail("no sm_100 GPU: GPU tests must run on a B200")
 
 
 def _np_ranges(par_path):
@@ -41,25 +50,18 @@ def _bind():
     return L
 
 
-def test_static_solver_matches_context_solver(gpu_available):
-    if not gpu_available:
-        pytest.fail("no sm_100 GPU: GPU tests must run on a B200")
-    import torch
-
-    paths = golden_paths("t_2np")
+def _context_solution(paths):
+    """The context solver's tight solution from a zero start, and the
+    context's matrix in the static entry point's 4x4-block layout."""
     d = cm.Desc.from_paths(paths)
     M, n = d.n_metal, d.n_mat
     s = cm.Simulation(d, solver_tol=TIGHT)
     s.force()  # assembles the matrix, right-hand side and diagonal on the device
-
-    # the context solver from a zero start
     s.set("vec_pq", np.zeros(n))
     it_ctx = ctypes.c_int(0)
     assert cm.lib().capac_bicgstab(s._p, ctypes.byref(it_ctx)) == 0
-    x_ctx = s.get("vec_pq")
     assert it_ctx.value > 0
-
-    # the same matrix, column by column through the context's own SpMV
+    # the matrix, column by column through the context's own SpMV
     A = np.zeros((n, n))
     e = np.zeros(n)
     col = np.zeros(n)
@@ -74,29 +76,99 @@ def test_static_solver_matches_context_solver(gpu_available):
     for i in range(M):
         ri = rows(i)
         for j in range(M):
-            blk = A[np.ix_(ri, rows(j))]
-            planes[i, :, j] = blk.reshape(16)
-    starts, ends = _np_ranges(paths["par"])
+            planes[i, :, j] = A[np.ix_(ri, rows(j))].reshape(16)
+    return dict(x=s.get("vec_pq"), planes=planes, Mp=Mp, M=M, n=n, rhs=s.get("vec_ext"), diag=s.get("diag_relay"))
 
+
+def _static(L, case, ranges, x, tol=TIGHT):
+    import torch
+    starts, ends = ranges
     dev = torch.device("cuda", 0)
-    mat = torch.tensor(planes.reshape(-1), dtype=torch.float64, device=dev)
-    rhs = torch.tensor(s.get("vec_ext"), dtype=torch.float64, device=dev)
-    diag = torch.tensor(s.get("diag_relay"), dtype=torch.float64, device=dev)
+    mat = torch.tensor(case["planes"].reshape(-1), dtype=torch.float64, device=dev)
+    rhs = torch.tensor(case["rhs"], dtype=torch.float64, device=dev)
+    diag = torch.tensor(case["diag"], dtype=torch.float64, device=dev)
+    xd = torch.tensor(x, dtype=torch.float64, device=dev)
+    torch.cuda.synchronize()
+    it = ctypes.c_int(-1)
+    rc = L.capac_bicgstab_static(mat.data_ptr(), case["M"], case["Mp"], len(starts), starts.ctypes.data,
+                                 ends.ctypes.data, rhs.data_ptr(), diag.data_ptr(), xd.data_ptr(), tol,
+                                 ctypes.byref(it), None)
+    torch.cuda.synchronize()
+    return rc, it.value, xd.cpu().numpy()
+
+
+def test_static_solver_matches_context_solver():
+    paths = golden_paths("t_2np")
+    case = _context_solution(paths)
+    ranges = _np_ranges(paths["par"])
     L = _bind()
     results = []
     for call in range(2):
-        x = torch.zeros(n, dtype=torch.float64, device=dev)
-        torch.cuda.synchronize()
-        it = ctypes.c_int(0)
-        rc = L.capac_bicgstab_static(mat.data_ptr(), M, Mp, len(starts), starts.ctypes.data, ends.ctypes.data,
-                                     rhs.data_ptr(), diag.data_ptr(), x.data_ptr(), TIGHT, ctypes.byref(it), None)
+        rc, it, xs = _static(L, case, ranges, np.zeros(case["n"]))
         assert rc == 0, L.capac_last_error().decode()
-        torch.cuda.synchronize()
-        xs = x.cpu().numpy()
-        assert it.value > 0
-        assert rel_err(xs, x_ctx) < 1e-10, f"call {call}"
+        assert it > 0
+        assert rel_err(xs, case["x"]) < 1e-10, f"call {call}"
         results.append(xs)
     assert rel_err(results[1], results[0]) < 1e-10
+    # warm start from the solution: the reference's iteration-0 exit or a
+    # couple of iterations, and the same answer
+    rc, it, xw = _static(L, case, ranges, results[1])
+    assert rc == 0, L.capac_last_error().decode()
+    assert it <= 2
+    assert rel_err(xw, case["x"]) < 1e-10
+
+
+def test_static_solver_without_nanoparticles(tmp_path):
+    """NANOPARTICLES 0: no neutrality rows, the SpMV grid holds metal rows
+    only and the static call passes n_nps = 0 with null range pointers."""
+    src = golden_paths("t_au55w")
+    paths = {}
+    for k, p in src.items():
+        text = open(p).read()
+        if k == "par":
+            text = text[:text.index("NANOPARTICLES")] + "NANOPARTICLES   0\n"
+        paths[k] = os.path.join(tmp_path, os.path.basename(p))
+        with open(paths[k], "w") as f:
+            f.write(text)
+    case = _context_solution(paths)
+    assert case["n"] == 4 * case["M"]
+    L = _bind()
+    import torch
+    dev = torch.device("cuda", 0)
+    mat = torch.tensor(case["planes"].reshape(-1), dtype=torch.float64, device=dev)
+    rhs = torch.tensor(case["rhs"], dtype=torch.float64, device=dev)
+    diag = torch.tensor(case["diag"], dtype=torch.float64, device=dev)
+    x = torch.zeros(case["n"], dtype=torch.float64, device=dev)
+    torch.cuda.synchronize()
+    it = ctypes.c_int(0)
+    rc = L.capac_bicgstab_static(mat.data_ptr(), case["M"], case["Mp"], 0, None, None, rhs.data_ptr(),
+                                 diag.data_ptr(), x.data_ptr(), TIGHT, ctypes.byref(it), None)
+    torch.cuda.synchronize()
+    assert rc == 0, L.capac_last_error().decode()
+    assert it.value > 0
+    assert rel_err(x.cpu().numpy(), case["x"]) < 1e-10
+
+
+def test_static_solver_zero_rhs_and_breakdown():
+    """A zero right-hand side returns at once with x untouched (the
+    reference's bTb < 1e-10 exit); a system on which BiCGSTAB breaks down
+    (r0 orthogonal to A r0, so alpha = rho / 0) is reported as not converged
+    after the restarts, with the caller's warm start still in x."""
+    L = _bind()
+    M, n = 1, 4
+    # one metal atom, no nanoparticle: block [[0, 1], [-1, 0]] on (p_x, p_y)
+    blk = np.eye(4)
+    blk[0, 0] = blk[1, 1] = 0.0
+    blk[0, 1], blk[1, 0] = 1.0, -1.0
+    case = dict(planes=blk.reshape(1, 16, 1), Mp=1, M=M, n=n, diag=np.ones(n))
+    no_np = (np.zeros(0, dtype=np.int32), np.zeros(0, dtype=np.int32))
+    x0 = np.array([0.25, -0.5, 0.125, 2.0])
+    rc, it, x = _static(L, dict(case, rhs=np.zeros(n)), no_np, x0)
+    assert rc == 0 and it == 0
+    assert np.array_equal(x, x0)
+    rc, it, x = _static(L, dict(case, rhs=np.array([1.0, 0.0, 0.0, 0.0])), no_np, np.zeros(n))
+    assert rc == cm.ERR_NOT_CONVERGED
+    assert np.array_equal(x, np.zeros(n))
 
 
 def test_static_solver_rejects_oversized_systems():
