@@ -492,6 +492,27 @@ int capac_create(const capac_desc *d, const capac_options *opt, capac_ctx **out)
                                     precond_group_atoms(M, d->metal_min, d->rx, d->ry, d->rz);
                                 c->g_atoms = dupload(g.data(), g.size(), s);
                                 c->dinv = dalloc<float>(precond_inverse_floats(M));
+                                // the group-ordered solver (unless CAPAC_SOLVER_UNGROUPED is set)
+                                if (!getenv("CAPAC_SOLVER_UNGROUPED") && group_grid_size(c->device) == c->coop_grid) {
+                                    std::vector<int> slot_np(g.size(), -1), off(d->n_nps + 1, 0), rows;
+                                    for (int k = 0; k < d->n_nps; ++k) {
+                                        for (size_t q = 0; q < g.size(); ++q) {
+                                            const int atom = g[q] < 0 ? -1 : d->metal_min + g[q];
+                                            if (atom >= d->np_start[k] && atom <= d->np_end[k]) {
+                                                if (slot_np[q] < 0) slot_np[q] = k;
+                                                rows.push_back((int)(4 * q + 3));
+                                            }
+                                        }
+                                        off[k + 1] = (int)rows.size();
+                                    }
+                                    c->slot_np = dupload(slot_np.data(), slot_np.size(), s);
+                                    c->np_off = dupload(off.data(), off.size(), s);
+                                    c->np_rows = dupload(rows.data(), rows.size(), s);
+                                    const size_t nv = 12 * group_rows(M, d->n_nps);
+                                    c->gvec = dalloc<double>(nv);
+                                    CAPAC_CUDA(cudaMemsetAsync(c->gvec, 0, sizeof(double) * nv, s));
+                                    c->grouped = true;
+                                }
                             }
                         }
                     } else if (mixed) {
@@ -551,7 +572,7 @@ int capac_destroy(capac_ctx *c)
                    c->nbr, c->nnb, c->cell_key, c->cell_key_sorted, c->atom_ids, c->cell_atoms,
                    c->cell_start, c->spos, c->sort_tmp, c->flags, c->cl_atoms, c->cl_cell_start, c->cl_counts,
                    c->cl_nbr, c->cl_nnb, c->cl_metal, c->scan_tmp, c->isd, c->vec_ext, c->vec_pq,
-                   c->diag, c->mat, c->matf, c->msym, c->sympart, c->coop_bp, c->coop_bar, c->g_atoms, c->dinv, c->gw, c->em_buf, c->phase_buf, c->rres, c->dcorr, c->xprev, c->bw, c->bwf, c->ss, c->partials, c->pot, c->vir, c->th};
+                   c->diag, c->mat, c->matf, c->msym, c->sympart, c->coop_bp, c->coop_bar, c->g_atoms, c->dinv, c->slot_np, c->np_off, c->np_rows, c->gvec, c->gw, c->em_buf, c->phase_buf, c->rres, c->dcorr, c->xprev, c->bw, c->bwf, c->ss, c->partials, c->pot, c->vir, c->th};
     for (void *p : dev)
         if (p) cudaFree(p);
     for (void *p : c->bonded_buffers)
@@ -980,6 +1001,11 @@ int capac_get(capac_ctx *c, const char *name, double *out)
             out[0] = c->clusters ? 1.0 : 0.0;
             out[1] = (double)c->n_clusters;
             count = 2;
+            return;
+        }
+        if (n == "solver_layout") {  // 1 when the persistent solver runs in the block-Jacobi groups' order
+            out[0] = c->grouped ? 1.0 : 0.0;
+            count = 1;
             return;
         }
         if (n == "solver_phases") {  // mean ns per iteration of each phase, then the iteration count

@@ -194,6 +194,13 @@ struct capac_ctx {
     int coop_grid = 0;           // blocks of the persistent solver (0: per-step launches)
     int *g_atoms = nullptr;      // block-Jacobi groups of 32 metal atoms (mixed path inner solver)
     float *dinv = nullptr;       // their inverse diagonal blocks, 128 x 128 each
+    // group-ordered persistent solver (mixed path, block-Jacobi): the stored
+    // tiles follow the groups' atom order and the solver works in that order
+    bool grouped = false;
+    int *slot_np = nullptr;      // [32 nG] nanoparticle of each group slot's atom, -1 none
+    int *np_off = nullptr;       // [n_nps + 1] offsets into np_rows
+    int *np_rows = nullptr;      // [M] internal charge rows of each nanoparticle's atoms
+    double *gvec = nullptr;      // 12 internal vectors of group_rows() doubles
     long precond_age = 0;        // matrix builds since the inverse blocks were computed
     // the metal's CPIM parameters (a.u.) and Gaussian widths (Bohr), which the
     // widths follow unless set on their own (k_grad.cu)
@@ -278,8 +285,9 @@ int coop_grid_size(int device, bool mixed);
 size_t coop_barrier_bytes();
 size_t coop_partial_doubles(int grid);
 int bicgstab_coop(capac_ctx *c, const double *b, double *x, double tol, double skip);
-// BiCGSTAB iteration limit of the context (the option, else MAX_ITER)
-inline int solver_max_iter(const capac_ctx *c);
+// group-ordered solver (k_solve_coop.cu): internal vector length, blocks
+size_t group_rows(int M, int n_nps);
+int group_grid_size(int device);
 void launch_cpim_metal_forces(capac_ctx *c);
 void launch_external_field(capac_ctx *c);
 void launch_finalize(capac_ctx *c, int nblocks, int K, const int *slots_pot, const int *slots_vir);

@@ -62,8 +62,10 @@ __device__ __forceinline__ void load4(const double *p, double out[4])
 
 // Assembly: one block per tile, 256 threads, 4 pairs each.
 template <typename T>
+// slots: null for the metal atoms in index order, else the atom of each
+// tile slot (-1 for padding): the group order of the grouped solver.
 __global__ void __launch_bounds__(256) k_sym_assemble(DevParams P, const double4 *__restrict__ pos4, int nT,
-                                                      T *__restrict__ mat)
+                                                      const int *__restrict__ slots, T *__restrict__ mat)
 {
     // decode the tile from the linear index
     const size_t t = blockIdx.x;
@@ -73,11 +75,18 @@ __global__ void __launch_bounds__(256) k_sym_assemble(DevParams P, const double4
     T *tile = mat + t * kTileElems;
     for (int q = threadIdx.x; q < kT * kT; q += blockDim.x) {
         const int a = q & (kT - 1), b = q >> 5;
-        const int i = I * kT + a, j = J * kT + b;
+        int i = I * kT + a, j = J * kT + b;
+        if (slots) {
+            i = slots[i];
+            j = slots[j];
+        } else {
+            i = i < P.M ? i : -1;
+            j = j < P.M ? j : -1;
+        }
         double v[kPlanes];
 #pragma unroll
         for (int p = 0; p < kPlanes; ++p) v[p] = 0.0;
-        if (i < P.M && j < P.M && (I != J || a < b)) {
+        if (i >= 0 && j >= 0 && (I != J || a < b)) {
             double e[16];
             cpim_block(P, pos4[P.metal_min + i], pos4[P.metal_min + j], false, e);
             v[0] = e[0]; v[1] = e[1]; v[2] = e[2]; v[3] = e[5]; v[4] = e[6]; v[5] = e[10];
@@ -373,9 +382,11 @@ void launch_sym_assemble(capac_ctx *c)
     const unsigned tiles = (unsigned)(nT * (nT + 1) / 2);
     ProfScope ps(c, K_MATRIX);
     if (c->opt.precision == CAPAC_PREC_MIXED)
-        k_sym_assemble<float><<<tiles, 256, 0, c->stream>>>(c->P, c->pos4, nT, static_cast<float *>(c->msym));
+        k_sym_assemble<float><<<tiles, 256, 0, c->stream>>>(c->P, c->pos4, nT, c->grouped ? c->g_atoms : nullptr,
+                                                             static_cast<float *>(c->msym));
     else
-        k_sym_assemble<double><<<tiles, 256, 0, c->stream>>>(c->P, c->pos4, nT, static_cast<double *>(c->msym));
+        k_sym_assemble<double><<<tiles, 256, 0, c->stream>>>(c->P, c->pos4, nT, nullptr,
+                                                              static_cast<double *>(c->msym));
     ++c->launches;
 }
 

@@ -29,6 +29,10 @@
 // dots differs from the directly summed one by rounding only; the value
 // returned is summed directly from the final residual.
 //
+// The mixed path with the block-Jacobi preconditioner runs a variant in the
+// preconditioner's group order (k_bicgstab_group below): four grid barriers
+// per iteration instead of six.
+//
 // Every wait is bounded.  The grid barrier (counter and generation word)
 // gives up after 2^24 polls (the context's wait_polls option when set), a
 // ring-stage wait after 2^20 polls of at most
@@ -768,6 +772,7 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? 2 : 1) k_bicgstab_coo
         phase_mark(A, iter, 1);
         ok = ok && grid_barrier(A.sync, A.spin_limit);
         if (!ok) break;
+        pending = false;  // the P pass applied the previous iteration's x update
         phase_mark(A, iter, 2);
         S.first = 0;
         reduce_pass<RED_V>(A, S, bpA);
@@ -876,14 +881,516 @@ size_t dyn_smem_bytes()
     return ring_bytes<T>() + sizeof(PassSmem<T>);
 }
 
+// ---------------------------------------------------------------------------
+// Group-ordered solver (mixed path, block-Jacobi preconditioner).
+//
+// The metal atoms are numbered inside the solver by the preconditioner's
+// groups (32 atoms each, along a Morton curve): slot a of group G is
+// internal atom 32 G + a, and its four unknowns are the contiguous internal
+// rows 128 G + 4 a + c (c = 0..2 dipole, 3 charge); the Lagrange rows follow
+// at 128 nG + k.  The tiles are assembled in that order (tile (I, J) couples
+// groups I and J), so
+//   * a tile pass gathers its inputs as two contiguous runs of 128 rows, and
+//   * the rows a block reduces from the tile partials are exactly one group,
+//     so the same block applies the group's inverse diagonal block at once:
+//     the V and T reductions and the preconditioner applications K v, K t
+//     become one phase each, four grid barriers per iteration instead of six.
+// The right-hand side and the solution stay in the reference layout outside
+// the solver: b is gathered into the internal order at the start, x is read
+// at the start and written back at the end.
+struct GroupArgs {
+    int M, nG, ntiles, n_nps, ni, max_iter;
+    long spin_limit;
+    double inv_polar, inv_capac;
+    const int *g_atoms;          // [32 nG] metal-local atom of each slot, -1 padding
+    const int *slot_np;          // [32 nG] nanoparticle of the slot's atom, -1 none
+    const int *np_off, *np_rows; // internal charge rows of each nanoparticle's atoms
+    const float *mat;            // tiles of the group order (I <= J)
+    double *part;                // nG * nG * 128 tile partials
+    double *bp;                  // dot partials, 2 sets of kBp per block
+    const double *b;             // right-hand side, reference layout
+    double *x;                   // solution, reference layout (in: start, out: result)
+    double *xi, *r0, *r, *s, *t, *z, *Kr, *Kv, *Kt, *v, *yb[2];  // internal vectors (ni)
+    const float *dinv;           // inverse diagonal blocks, [G][c][o]
+    double tol, skip;
+    SolverScalars *ss;
+    CoopSync *sync;
+    unsigned long long *ptime;
+};
+
+// Reference row of internal row q (-1 for a padding slot).
+__device__ __forceinline__ int g_ref_row(const GroupArgs &A, int q)
+{
+    const int base = 128 * A.nG;
+    if (q >= base) return 4 * A.M + (q - base);
+    const int m = A.g_atoms[q >> 2];
+    if (m < 0) return -1;
+    const int c = q & 3;
+    return c < 3 ? 3 * m + c : 3 * A.M + m;
+}
+
+__device__ __forceinline__ void g_phase_mark(const GroupArgs &A, int iter, int k)
+{
+    if (A.ptime && blockIdx.x == 0 && threadIdx.x == 0 && iter < kPhaseIters) {
+        unsigned long long t;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+        A.ptime[iter * kPhases + k] = t;
+    }
+}
+
+// MODE_P, one internal row (see bj_p_row): y = K r + beta (y_old - omega K v)
+// with K r = z - omega K t; on `store` the deferred updates of the row.
+__device__ __forceinline__ double g_p_row(const GroupArgs &A, const PassScalars &S, int row, bool store)
+{
+    const double y_old = __ldcg(A.yb[S.cur] + row);
+    const double kr = S.first ? __ldcg(A.Kr + row) : fma(-S.omega, __ldcg(A.Kt + row), __ldcg(A.z + row));
+    const double yn = fma(S.beta, fma(-S.omega, __ldcg(A.Kv + row), y_old), kr);
+    if (store) {
+        if (!S.first) {
+            A.r[row] = fma(-S.omega, __ldcg(A.t + row), __ldcg(A.s + row));
+            A.Kr[row] = kr;
+            A.xi[row] += S.alpha * y_old + S.omega * __ldcg(A.z + row);
+        }
+        A.yb[S.cur ^ 1][row] = yn;
+    }
+    return yn;
+}
+
+// Tile pass on the group-ordered tiles (tiles_pass with contiguous inputs).
+template <int MODE>
+__device__ bool tiles_pass_g(const GroupArgs &A, const PassScalars &S, Ring<float> &ring, PassSmem<float> &sm)
+{
+    constexpr int Stages = Ring<float>::Stages;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int nT = A.nG;
+    if (MODE != MODE_X && threadIdx.x == 0) {
+        for (int k = blockIdx.x; k < A.n_nps; k += gridDim.x) {
+            const int row = 128 * nT + k;
+            if (MODE == MODE_P) {
+                g_p_row(A, S, row, true);
+            } else {
+                A.s[row] = fma(-S.alpha, __ldcg(A.v + row), __ldcg(A.r + row));
+                A.z[row] = fma(-S.alpha, __ldcg(A.Kv + row), __ldcg(A.Kr + row));
+            }
+        }
+    }
+    constexpr int kChunk = chunk_tiles<float>();
+    for (int c0 = 0; c0 < ring.n_my; c0 += kChunk) {
+        const int nc = min(kChunk, ring.n_my - c0);
+        if (threadIdx.x < nc) {
+            const int t = blockIdx.x + (c0 + threadIdx.x) * gridDim.x;
+            int I = 0;
+            while (tile_index(I + 1, I + 1, nT) <= (size_t)t && I + 1 < nT) ++I;
+            sm.tile_i[threadIdx.x] = I;
+            sm.tile_j[threadIdx.x] = I + (int)((size_t)t - tile_index(I, I, nT));
+        }
+        __syncthreads();
+#pragma unroll 4
+        for (int e = threadIdx.x; e < nc * 256; e += kBlock) {
+            const int kk = e >> 8, side = (e >> 7) & 1, q4 = e & 127;
+            const int I = sm.tile_i[kk], J = sm.tile_j[kk];
+            const int row = 128 * (side ? J : I) + q4;
+            double val;
+            if (MODE == MODE_X) {
+                val = __ldcg(A.xi + row);
+            } else if (MODE == MODE_P) {
+                val = g_p_row(A, S, row, I == J && side == 0);  // the diagonal-tile owner stores group I
+            } else {
+                val = fma(-S.alpha, __ldcg(A.Kv + row), __ldcg(A.Kr + row));
+                if (I == J && side == 0) {
+                    A.s[row] = fma(-S.alpha, __ldcg(A.v + row), __ldcg(A.r + row));
+                    A.z[row] = val;
+                }
+            }
+            sm.in[kk][side][q4 >> 2][q4 & 3] = (float)val;
+        }
+        __syncthreads();
+
+        for (int kk = 0; kk < nc; ++kk) {
+            const int I = sm.tile_i[kk], J = sm.tile_j[kk];
+            const int set = kk & 1;
+            const long q = ring.consumed;
+            const int st = (int)(q % Stages);
+            const unsigned parity = (unsigned)((q / Stages) & 1);
+            const bool landed = mbar_wait(ring.bar + st, parity);
+            const float *tile = ring.stage(st);
+            const float(*xr)[4] = sm.in[kk][0];
+            const float(*xc)[4] = sm.in[kk][1];
+            const int a = lane;
+            float ra[4] = {0, 0, 0, 0};
+            float cb[kCols * 4];
+            const float xa0 = xr[a][0], xa1 = xr[a][1], xa2 = xr[a][2], xa3 = xr[a][3];
+            if (landed) {
+                float vv[kPlanes][kCols];
+#pragma unroll
+                for (int pl = 0; pl < kPlanes; ++pl) ldsc(tile + elem_offset(pl, a, kCols * w), vv[pl]);
+#pragma unroll
+                for (int k = 0; k < kCols; ++k) {
+                    const int bb = kCols * w + k;
+                    const float Axx = vv[0][k], Axy = vv[1][k], Axz = vv[2][k], Ayy = vv[3][k], Ayz = vv[4][k],
+                                Azz = vv[5][k], m0 = vv[6][k], m1 = vv[7][k], m2 = vv[8][k], C = vv[9][k];
+                    const float xb0 = xc[bb][0], xb1 = xc[bb][1], xb2 = xc[bb][2], xb3 = xc[bb][3];
+                    ra[0] += Axx * xb0 + Axy * xb1 + Axz * xb2 + m0 * xb3;
+                    ra[1] += Axy * xb0 + Ayy * xb1 + Ayz * xb2 + m1 * xb3;
+                    ra[2] += Axz * xb0 + Ayz * xb1 + Azz * xb2 + m2 * xb3;
+                    ra[3] += -(m0 * xb0 + m1 * xb1 + m2 * xb2) + C * xb3;
+                    cb[4 * k + 0] = Axx * xa0 + Axy * xa1 + Axz * xa2 - m0 * xa3;
+                    cb[4 * k + 1] = Axy * xa0 + Ayy * xa1 + Ayz * xa2 - m1 * xa3;
+                    cb[4 * k + 2] = Axz * xa0 + Ayz * xa1 + Azz * xa2 - m2 * xa3;
+                    cb[4 * k + 3] = m0 * xa0 + m1 * xa1 + m2 * xa2 + C * xa3;
+                }
+            } else {
+#pragma unroll
+                for (int k = 0; k < kCols * 4; ++k) cb[k] = 0;
+            }
+            const float colsum = warp_sum_halving<kCols * 4>(cb, lane);
+#pragma unroll
+            for (int c = 0; c < 4; ++c) sm.rowacc[set][w][a][c] = ra[c];
+            constexpr int kShift = 5 - (kCols == 1 ? 2 : kCols == 2 ? 3 : kCols == 4 ? 4 : 5);
+            if ((lane & ((1 << kShift) - 1)) == 0) {
+                const int vv2 = lane >> kShift;
+                sm.colacc[set][kCols * w + (vv2 >> 2)][vv2 & 3] = (double)colsum;
+            }
+            if (__syncthreads_or(!landed)) return false;
+            ++ring.consumed;
+            if (threadIdx.x == 0) ring.issue(A.mat);
+            double *pr = A.part + ((size_t)I * nT + J) * (kT * 4);
+            double *pc = A.part + ((size_t)J * nT + I) * (kT * 4);
+            if (threadIdx.x < kT * 4) {
+                const int aa = threadIdx.x >> 2, c = threadIdx.x & 3;
+                double sacc = 0.0;
+#pragma unroll
+                for (int ww = 0; ww < kWarps; ++ww) sacc += (double)sm.rowacc[set][ww][aa][c];
+                pr[threadIdx.x] = I == J ? sacc + sm.colacc[set][aa][c] : sacc;
+            } else if (threadIdx.x < 2 * kT * 4 && I != J) {
+                const int c = threadIdx.x - kT * 4;
+                pc[c] = sm.colacc[set][c >> 2][c & 3];
+            }
+        }
+        __syncthreads();
+    }
+    return true;
+}
+
+// One group's reduction fused with its preconditioner block.  out = A in for
+// the group's 128 rows from the nG tile partials of its block row (two
+// halves of the threads sum alternate tiles, added in a fixed order), the
+// diagonal and the neutrality couplings; then K out with the group's inverse
+// block.  RED_START: r0 = r = b - A x (or b when x is zero), K r.
+// RED_V: v = A y, K v, dot (r0, v).  RED_T: t = A z, K t, the dots (K t, z),
+// (K t, K t), (r0, s), (r0, t), (s, s), (s, t), (t, t).  The Lagrange rows
+// (K = 1 there) follow from the sums of the nanoparticles' charges.
+template <int RED>
+__device__ void reduce_group(const GroupArgs &A, const PassScalars &S, double *bp, bool products)
+{
+    __shared__ double vrow[128];
+    __shared__ double hsum[128];
+    const int nG = A.nG, tid = threadIdx.x;
+    const double *in = RED == RED_START ? A.xi : (RED == RED_V ? A.yb[S.cur ^ 1] : A.z);
+    double d[7] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    for (int G = blockIdx.x; G < nG; G += gridDim.x) {
+        const int o = tid & 127, h = tid >> 7;
+        double sum = 0.0;
+        if (products) {
+            const double *src = A.part + (size_t)G * nG * (kT * 4) + o;
+            for (int K0 = h; K0 < nG; K0 += 2 * kBatch) {
+                double vals[kBatch];
+#pragma unroll
+                for (int u = 0; u < kBatch; ++u) {
+                    const int Kk = K0 + 2 * u;
+                    vals[u] = Kk < nG ? __ldcg(src + (size_t)Kk * (kT * 4)) : 0.0;
+                }
+#pragma unroll
+                for (int u = 0; u < kBatch; ++u) sum += vals[u];
+            }
+        }
+        if (h == 1) hsum[o] = sum;
+        __syncthreads();
+        if (h == 0) {
+            const int row = 128 * G + o;
+            sum += hsum[o];
+            const double xin = products ? __ldcg(in + row) : 0.0;
+            if ((o & 3) < 3) {
+                sum += A.inv_polar * xin;
+            } else {
+                sum += -A.inv_capac * xin;
+                const int k = A.slot_np[row >> 2];
+                if (products && k >= 0) sum += __ldcg(in + 128 * nG + k);
+            }
+            double out;
+            if (RED == RED_START) {
+                const int rr = g_ref_row(A, row);
+                const double bk = rr >= 0 ? A.b[rr] : 0.0;
+                out = bk - sum;
+                A.r0[row] = out;
+                A.r[row] = out;
+                d[0] += out * out;
+            } else if (RED == RED_V) {
+                out = sum;
+                A.v[row] = out;
+                d[0] += __ldcg(A.r0 + row) * out;
+            } else {
+                out = sum;
+                A.t[row] = out;
+                const double sr = __ldcg(A.s + row), r0 = __ldcg(A.r0 + row);
+                d[2] += r0 * sr;
+                d[3] += r0 * out;
+                d[4] += sr * sr;
+                d[5] += sr * out;
+                d[6] += out * out;
+            }
+            vrow[o] = out;
+        }
+        __syncthreads();
+        // K out: thread (row o2, half) sums 64 of the 128 columns
+        {
+            const int o2 = tid >> 1, half = tid & 1;
+            const float *col = A.dinv + (size_t)G * 128 * 128 + (size_t)(64 * half) * 128 + o2;
+            double acc = 0.0;
+#pragma unroll 16
+            for (int c = 0; c < 64; ++c) acc = fma((double)__ldg(col + (size_t)c * 128), vrow[64 * half + c], acc);
+            acc += __shfl_xor_sync(0xffffffffu, acc, 1);
+            if (half == 0) {
+                const int row = 128 * G + o2;
+                if (RED == RED_START) {
+                    A.Kr[row] = acc;
+                } else if (RED == RED_V) {
+                    A.Kv[row] = acc;
+                } else {
+                    A.Kt[row] = acc;
+                    d[0] += acc * __ldcg(A.z + row);
+                    d[1] += acc * acc;
+                }
+            }
+        }
+        __syncthreads();  // vrow and hsum free again
+    }
+    // Lagrange rows: the sum of the nanoparticle's charges of `in`
+    for (int k = (int)gridDim.x - 1 - (int)blockIdx.x; k < A.n_nps; k += gridDim.x) {
+        __shared__ double shl[32];
+        double acc[1] = {0.0};
+        if (products)
+            for (int q = A.np_off[k] + tid; q < A.np_off[k + 1]; q += blockDim.x) acc[0] += __ldcg(in + A.np_rows[q]);
+        block_sum<1>(acc, shl);
+        if (tid == 0) {
+            const int row = 128 * nG + k;
+            const double val = acc[0];
+            if (RED == RED_START) {
+                const double out = A.b[4 * A.M + k] - val;
+                A.r0[row] = out;
+                A.r[row] = out;
+                A.Kr[row] = out;
+                d[0] += out * out;
+            } else if (RED == RED_V) {
+                A.v[row] = val;
+                A.Kv[row] = val;
+                d[0] += __ldcg(A.r0 + row) * val;
+            } else {
+                A.t[row] = val;
+                A.Kt[row] = val;
+                const double zr = __ldcg(A.z + row), sr = __ldcg(A.s + row), r0 = __ldcg(A.r0 + row);
+                d[0] += val * zr;
+                d[1] += val * val;
+                d[2] += r0 * sr;
+                d[3] += r0 * val;
+                d[4] += sr * sr;
+                d[5] += sr * val;
+                d[6] += val * val;
+            }
+        }
+        __syncthreads();
+    }
+    if (RED == RED_T) {
+        put_bp<7>(bp, d);
+    } else {
+        double d1[1] = {d[0]};
+        put_bp<1>(bp, d1);
+    }
+}
+
+__global__ void __launch_bounds__(kBlock, 2) k_bicgstab_group(GroupArgs A)
+{
+    extern __shared__ __align__(128) unsigned char ring_smem[];
+    constexpr int Stages = Ring<float>::Stages;
+    __shared__ __align__(8) uint64_t ring_bar[Stages];
+    PassSmem<float> &psm = *reinterpret_cast<PassSmem<float> *>(ring_smem + ring_bytes<float>());
+    SolverScalars *ss = A.ss;
+    const int ni = A.ni;
+    const long gthreads = (long)gridDim.x * blockDim.x;
+    const long tid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int nb = gridDim.x;
+    double *bpA = A.bp, *bpB = A.bp + (size_t)kBp * nb;
+
+    Ring<float> ring;
+    ring.buf = reinterpret_cast<float *>(ring_smem);
+    ring.bar = ring_bar;
+    ring.issued = ring.consumed = 0;
+    ring.n_my = (int)blockIdx.x < A.ntiles ? (A.ntiles - 1 - (int)blockIdx.x) / nb + 1 : 0;
+    if (threadIdx.x == 0) {
+        for (int st = 0; st < Stages; ++st) mbar_init(ring_bar + st, 1);
+        fence_mbar_init();
+        if (ring.n_my > 0)
+            for (int st = 0; st < Stages; ++st) ring.issue(A.mat);
+    }
+    __syncthreads();
+
+    PassScalars S{0.0, 0.0, 0.0, 0, 1};
+    int iter = 0, status = 0;
+    double bTb = 0.0, crit = 0.0, rTr = 0.0, rr0 = 0.0;
+    bool ok = true;
+
+    // start: bTb, x gathered into the internal order (counting its non-zero
+    // entries), the first y buffer and K v zero
+    {
+        double pb[2] = {0.0, 0.0};
+        for (long k = tid; k < ni; k += gthreads) {
+            const int rr = g_ref_row(A, (int)k);
+            const double bk = rr >= 0 ? A.b[rr] : 0.0;
+            const double xk = rr >= 0 ? A.x[rr] : 0.0;
+            pb[0] += bk * bk;
+            pb[1] += xk != 0.0 ? 1.0 : 0.0;
+            A.xi[k] = xk;
+            A.yb[0][k] = 0.0;
+            A.Kv[k] = 0.0;
+        }
+        put_bp<2>(bpA, pb);
+    }
+    ok = grid_barrier(A.sync, A.spin_limit);
+    bool x_zero = false;
+    if (ok) {
+        double t2[2];
+        sum_bp<2>(bpA, nb, t2);
+        bTb = t2[0];
+        x_zero = t2[1] == 0.0;
+        crit = bTb * A.tol;
+    }
+    bool done = !ok || bTb < A.skip;  // zero right-hand side: x stays (bicg_stab.c:303-307)
+    if (!done) {
+        // r0 = r = b - A x, K r (x zero: no product pass; the ring is
+        // untouched, so the next pass starts on the same tiles)
+        if (!x_zero) ok = tiles_pass_g<MODE_X>(A, S, ring, psm) && grid_barrier(A.sync, A.spin_limit);
+        if (ok) reduce_group<RED_START>(A, S, bpB, !x_zero);
+        ok = ok && grid_barrier(A.sync, A.spin_limit);
+        done = !ok;
+    }
+    double rho = 0.0, rho_old = 1.0, alpha = 1.0, omega = 1.0;
+    if (!done) {
+        double t1[1];
+        sum_bp<1>(bpB, nb, t1);
+        rho = rTr = rr0 = t1[0];
+        if (rho < A.skip) done = true;  // warm start already converged (bicg_stab.c:368)
+    }
+    bool pending = false;
+    while (!done) {
+        g_phase_mark(A, iter, 0);
+        S.beta = (rho / rho_old) * (alpha / omega);
+        S.omega = omega;
+        S.alpha = alpha;
+        ok = tiles_pass_g<MODE_P>(A, S, ring, psm);
+        g_phase_mark(A, iter, 1);
+        ok = ok && grid_barrier(A.sync, A.spin_limit);
+        if (!ok) break;
+        pending = false;  // the P pass applied the previous iteration's x update
+        g_phase_mark(A, iter, 2);
+        S.first = 0;
+        reduce_group<RED_V>(A, S, bpA, true);
+        if (!grid_barrier(A.sync, A.spin_limit)) {
+            ok = false;
+            break;
+        }
+        g_phase_mark(A, iter, 3);
+        g_phase_mark(A, iter, 4);
+        double r0v[1];
+        sum_bp<1>(bpA, nb, r0v);
+        const double al = rho / r0v[0];
+        if (!isfinite(al)) {  // breakdown: x is the start of this iteration
+            status = rTr < crit * 100.0 ? 1 : -2;
+            break;
+        }
+        alpha = al;
+        S.cur ^= 1;
+        S.alpha = alpha;
+        ok = tiles_pass_g<MODE_S>(A, S, ring, psm) && grid_barrier(A.sync, A.spin_limit);
+        if (!ok) break;
+        g_phase_mark(A, iter, 5);
+        reduce_group<RED_T>(A, S, bpB, true);
+        if (!grid_barrier(A.sync, A.spin_limit)) {
+            ok = false;
+            break;
+        }
+        g_phase_mark(A, iter, 6);
+        g_phase_mark(A, iter, 7);
+        double d[7];
+        sum_bp<7>(bpB, nb, d);
+        const double om = d[0] / d[1];
+        if (!isfinite(om) || om == 0.0) {
+            status = rTr < crit * 100.0 ? 1 : -2;
+            break;
+        }
+        omega = om;
+        rho_old = rho;
+        rho = fma(-omega, d[3], d[2]);
+        rTr = fma(omega * omega, d[6], fma(-2.0 * omega, d[5], d[4]));
+        ++iter;
+        pending = true;
+        if (rTr < crit) {
+            done = true;
+        } else if (iter > A.max_iter) {
+            status = rTr < crit * 100.0 ? 1 : -1;
+            done = true;
+        }
+    }
+    if (ok) {
+        // the last update of x, (r, r) of the final residual, x back to the
+        // reference layout
+        double q[1] = {0.0};
+        for (long k = tid; k < ni; k += gthreads) {
+            double xk = A.xi[k];
+            if (pending) {
+                xk += alpha * __ldcg(A.yb[S.cur] + k) + omega * __ldcg(A.z + k);
+                const double rk = __ldcg(A.s + k) - omega * __ldcg(A.t + k);
+                A.r[k] = rk;
+                q[0] += rk * rk;
+            }
+            const int rr = g_ref_row(A, (int)k);
+            if (rr >= 0) A.x[rr] = xk;
+        }
+        if (pending) {
+            put_bp<1>(bpA, q);
+            ok = grid_barrier(A.sync, A.spin_limit);
+            if (ok) {
+                sum_bp<1>(bpA, nb, q);
+                rTr = q[0];
+            }
+        }
+    }
+    if (threadIdx.x == 0) {
+        if (!ok) atomicCAS(&A.sync->error, 0, 2);
+        ring.drain();
+    }
+    if (ok && tid == 0) {
+        ss->bTb = bTb;
+        ss->crit = crit;
+        ss->rTr = rTr;
+        ss->rr0 = rr0;
+        ss->iter = iter;
+        ss->done = 1;
+        ss->status = status;
+    }
+}
+
 }  // namespace
 
 size_t coop_barrier_bytes() { return sizeof(CoopSync); }
 size_t coop_partial_doubles(int grid) { return (size_t)2 * kBp * grid; }
 
+int finish_coop(capac_ctx *c, const unsigned long long *ptime, double skip);
+int bicgstab_group(capac_ctx *c, const double *b, double *x, double tol, double skip);
+
 // Launch the persistent solver; returns the status as bicgstab_core does.
 int bicgstab_coop(capac_ctx *c, const double *b, double *x, double tol, double skip)
 {
+    if (c->grouped) return bicgstab_group(c, b, x, tol, skip);
     const int n = c->n_mat;
     double *bw = c->bw;
     auto W = [&](int k) { return bw + (size_t)k * n; };
@@ -950,16 +1457,22 @@ int bicgstab_coop(capac_ctx *c, const double *b, double *x, double tol, double s
                                                    dim3(kBlock), args, dyn_smem_bytes<double>(), c->stream));
     }
     ++c->launches;
+    return finish_coop(c, A.ptime, skip);
+}
+
+// After a persistent launch: the error word, the phase timer, the status.
+int finish_coop(capac_ctx *c, const unsigned long long *ptime, double skip)
+{
     CAPAC_CUDA(cudaMemcpyAsync(c->h_ss, c->ss, sizeof(SolverScalars), cudaMemcpyDeviceToHost, c->stream));
     CoopSync hs;
     CAPAC_CUDA(cudaMemcpyAsync(&hs, c->coop_bar, sizeof hs, cudaMemcpyDeviceToHost, c->stream));
     CAPAC_CUDA(cudaStreamSynchronize(c->stream));
     if (hs.error) throw Error(CAPAC_ERR_CUDA, "persistent solver: a bounded wait timed out");
-    if (A.ptime && c->h_ss->iter > 1) {
+    if (ptime && c->h_ss->iter > 1) {
         // phase k of an iteration ends at mark k + 1 (the last at the next iteration's mark 0)
         const int it = std::min(c->h_ss->iter, kPhaseIters);
         std::vector<unsigned long long> t((size_t)kPhases * it);
-        CAPAC_CUDA(cudaMemcpy(t.data(), A.ptime, sizeof(unsigned long long) * t.size(), cudaMemcpyDeviceToHost));
+        CAPAC_CUDA(cudaMemcpy(t.data(), ptime, sizeof(unsigned long long) * t.size(), cudaMemcpyDeviceToHost));
         for (int i = 0; i + 1 < it; ++i) {
             for (int k = 0; k < kPhases; ++k) {
                 const unsigned long long a = t[(size_t)i * kPhases + k];
@@ -972,6 +1485,79 @@ int bicgstab_coop(capac_ctx *c, const double *b, double *x, double tol, double s
     if (c->prof.on && c->h_ss->bTb >= skip) c->prof.spmv_effective += 1 + 2L * c->h_ss->iter;
     if (c->h_ss->status < 0) return CAPAC_ERR_NOT_CONVERGED;
     return c->h_ss->status == 1 ? 1 : CAPAC_OK;
+}
+
+// The group-ordered persistent solver (mixed path, block-Jacobi).
+int bicgstab_group(capac_ctx *c, const double *b, double *x, double tol, double skip)
+{
+    GroupArgs A;
+    const int nG = precond_groups(c->M);
+    A.M = c->M;
+    A.nG = nG;
+    A.ntiles = nG * (nG + 1) / 2;
+    A.n_nps = c->n_nps;
+    A.ni = (int)group_rows(c->M, c->n_nps);
+    A.max_iter = solver_max_iter(c);
+    A.spin_limit = c->opt.wait_polls > 0 ? c->opt.wait_polls : kSpinLimit;
+    A.inv_polar = c->P.inv_polar;
+    A.inv_capac = c->P.inv_capac;
+    A.g_atoms = c->g_atoms;
+    A.slot_np = c->slot_np;
+    A.np_off = c->np_off;
+    A.np_rows = c->np_rows;
+    A.mat = static_cast<const float *>(c->msym);
+    A.part = c->sympart;
+    A.bp = c->coop_bp;
+    A.b = b;
+    A.x = x;
+    auto V = [&](int k) { return c->gvec + (size_t)k * A.ni; };
+    A.xi = V(0); A.r0 = V(1); A.r = V(2); A.s = V(3); A.t = V(4); A.z = V(5);
+    A.Kr = V(6); A.Kv = V(7); A.Kt = V(8); A.v = V(9); A.yb[0] = V(10); A.yb[1] = V(11);
+    A.dinv = c->dinv;
+    A.tol = tol;
+    A.skip = skip;
+    A.ss = c->ss;
+    A.sync = reinterpret_cast<CoopSync *>(c->coop_bar);
+    A.ptime = nullptr;
+    if (c->phase_timer) {
+        if (!c->phase_buf) CAPAC_CUDA(cudaMalloc(&c->phase_buf, sizeof(unsigned long long) * kPhases * kPhaseIters));
+        A.ptime = static_cast<unsigned long long *>(c->phase_buf);
+    }
+    CAPAC_CUDA(cudaMemsetAsync(c->coop_bar, 0, sizeof(CoopSync), c->stream));
+    void *args[] = {&A};
+    {
+        ProfScope ps(c, K_SOLVE);
+        CAPAC_CUDA(cudaLaunchCooperativeKernel((const void *)k_bicgstab_group, dim3(c->coop_grid), dim3(kBlock), args,
+                                               dyn_smem_bytes<float>(), c->stream));
+    }
+    ++c->launches;
+    return finish_coop(c, A.ptime, skip);
+}
+
+size_t group_rows(int M, int n_nps) { return (size_t)128 * precond_groups(M) + n_nps; }
+
+// Blocks of the group-ordered solver: two per SM when they fit, 0 if the
+// device cannot run it.
+int group_grid_size(int device)
+{
+    int coop = 0;
+    if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device) != cudaSuccess || !coop) return 0;
+    int sms = 0;
+    CAPAC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    const size_t dyn = dyn_smem_bytes<float>();
+    if (cudaFuncSetAttribute((const void *)k_bicgstab_group, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn) !=
+        cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)k_bicgstab_group, kBlock, dyn) !=
+            cudaSuccess ||
+        per_sm < 1) {
+        cudaGetLastError();
+        return 0;
+    }
+    return sms * std::min(per_sm, 2);
 }
 
 // Blocks of the persistent solver (two per SM for the FP32 matrix, one for

@@ -305,6 +305,8 @@ int capac_checkpoint_load(capac_ctx *ctx, const char *path);
  * adjoint_dedx (dE/dx), adjoint_dpsidx (dPsi/dx of the force matching),
  * adjoint_mu, adjoint_nu (the adjoint solutions).  Read-only diagnostics:
  * pair_list(2: 1 when the pair kernel walks the cluster list, cluster count),
+ * solver_layout(1: 1 when the mixed path's persistent solver works in the
+ * order of its block-Jacobi groups, its tiles assembled in that order),
  * solver_phases(9: mean ns per iteration of the persistent solver's phases
  * when CAPAC_SOLVER_PHASES is set, then the iterations timed).  Set only:
  * wait_polls(1), the option of that name on the live context.  capac_get
