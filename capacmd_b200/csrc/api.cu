@@ -663,6 +663,86 @@ int capac_cpim_matvec(capac_ctx *c, const double *x, double *y)
     });
 }
 
+int capac_cpim_blocks(capac_ctx *c, int row0, int rows, double *out)
+{
+    return guard([&] {
+        check_ctx(c);
+        if (!out) throw Error(CAPAC_ERR_INVALID, "null argument");
+        if (row0 < 0 || rows < 0 || row0 + (long)rows > c->M) throw Error(CAPAC_ERR_INVALID, "rows outside the metal atoms");
+        if (rows == 0) return;
+        launch_pack_positions(c);
+        // chunks of rows through a temporary device buffer of at most 64 MB
+        const size_t row_doubles = (size_t)c->M * 16;
+        const int chunk = (int)std::max<size_t>(1, std::min<size_t>(rows, (64u << 20) / (8 * row_doubles)));
+        double *tmp = nullptr;
+        CAPAC_CUDA(cudaMalloc(&tmp, sizeof(double) * row_doubles * chunk));
+        try {
+            for (int i = 0; i < rows; i += chunk) {
+                const int n = std::min(chunk, rows - i);
+                launch_cpim_block_rows(c, row0 + i, n, tmp);
+                CAPAC_CUDA(cudaMemcpyAsync(out + row_doubles * i, tmp, sizeof(double) * row_doubles * n,
+                                           cudaMemcpyDeviceToHost, c->stream));
+                CAPAC_CUDA(cudaStreamSynchronize(c->stream));
+            }
+        } catch (...) {
+            cudaFree(tmp);
+            throw;
+        }
+        CAPAC_CUDA(cudaFree(tmp));
+    });
+}
+
+int capac_cpim_set_coo(capac_ctx *c, long nnz, const double *val, const long *row, const long *col)
+{
+    return guard([&] {
+        check_ctx(c);
+        if (nnz < 0 || (nnz > 0 && (!val || !row || !col))) throw Error(CAPAC_ERR_INVALID, "null argument");
+        if (!c->msym || c->opt.precision != CAPAC_PREC_FP64)
+            throw Error(CAPAC_ERR_UNSUPPORTED, "a COO matrix loads into the FP64 symmetric layout only");
+        CAPAC_CUDA(cudaStreamSynchronize(c->stream));
+        sym_tiles_from_coo(c, nnz, val, row, col);
+        c->grad_ready = false;
+    });
+}
+
+int capac_rattle(capac_ctx *c, int stage, double dt, double *rx, double *ry, double *rz, const double *ox,
+                 const double *oy, const double *oz, double *vx, double *vy, double *vz, double *virial)
+{
+    return guard([&] {
+        check_ctx(c);
+        if (stage != 1 && stage != 2) throw Error(CAPAC_ERR_INVALID, "stage must be 1 or 2");
+        if (!rx || !ry || !rz || !vx || !vy || !vz || (stage == 1 && (!ox || !oy || !oz)) || (stage == 2 && !virial))
+            throw Error(CAPAC_ERR_INVALID, "null argument");
+        cudaStream_t s = c->stream;
+        const size_t nb = sizeof(double) * c->N;
+        double *pos[3] = {rx, ry, rz}, *vel[3] = {vx, vy, vz};
+        const double *old[3] = {ox, oy, oz};
+        double *dpos[3] = {c->rx, c->ry, c->rz}, *dvel[3] = {c->vx, c->vy, c->vz}, *dold[3] = {c->ox, c->oy, c->oz};
+        for (int a = 0; a < 3; ++a) {
+            CAPAC_CUDA(cudaMemcpyAsync(dpos[a], pos[a], nb, cudaMemcpyHostToDevice, s));
+            CAPAC_CUDA(cudaMemcpyAsync(dvel[a], vel[a], nb, cudaMemcpyHostToDevice, s));
+            if (stage == 1) CAPAC_CUDA(cudaMemcpyAsync(dold[a], old[a], nb, cudaMemcpyHostToDevice, s));
+        }
+        c->list_valid = false;  // the positions came from outside
+        c->grad_ready = false;
+        const double dt_run = c->dt;
+        c->dt = dt;
+        if (stage == 2) CAPAC_CUDA(cudaMemsetAsync(c->vir, 0, sizeof(double) * 9, s));
+        launch_rattle(c, stage == 2);
+        c->dt = dt_run;
+        for (int a = 0; a < 3; ++a) {
+            if (stage == 1) CAPAC_CUDA(cudaMemcpyAsync(pos[a], dpos[a], nb, cudaMemcpyDeviceToHost, s));
+            CAPAC_CUDA(cudaMemcpyAsync(vel[a], dvel[a], nb, cudaMemcpyDeviceToHost, s));
+        }
+        double w[9] = {0.0};
+        if (stage == 2 && c->has_cstr) CAPAC_CUDA(cudaMemcpyAsync(w, c->vir, sizeof w, cudaMemcpyDeviceToHost, s));
+        CAPAC_CUDA(cudaStreamSynchronize(s));
+        check_flags(c);
+        if (stage == 2)
+            for (int k = 0; k < 9; ++k) virial[k] += w[k];
+    });
+}
+
 int capac_qsc(capac_ctx *c)
 {
     return guard([&] {
@@ -1043,8 +1123,7 @@ int capac_set(capac_ctx *c, const char *name, const double *in)
         }
         int cnt = 0;
         double *p = state_array(c, n, &cnt);
-        if (!p || n == "potential" || n == "virial" || n == "inv_sqrt_dens" || n == "diag_relay" ||
-            n.rfind("adjoint_", 0) == 0)
+        if (!p || n == "inv_sqrt_dens" || n == "diag_relay" || n.rfind("adjoint_", 0) == 0)
             throw Error(CAPAC_ERR_INVALID, "array " + n + " cannot be set");
         if (cnt > 0) CAPAC_CUDA(cudaMemcpy(p, in, sizeof(double) * cnt, cudaMemcpyHostToDevice));
         if (n == "rx" || n == "ry" || n == "rz" || n == "vec_pq") c->grad_ready = false;

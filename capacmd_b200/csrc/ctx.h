@@ -260,6 +260,9 @@ void launch_cpim_matrix(capac_ctx *c);
 int run_bicgstab(capac_ctx *c);  // returns status
 int run_refined_solve(capac_ctx *c);  // mixed path: FP64 refinement around FP32-matrix BiCGSTAB
 void launch_cpim_spmv(capac_ctx *c, const double *x, double *y);  // plain y = A x
+void launch_cpim_block_rows(capac_ctx *c, int i0, int rows, double *out);  // dense FP64 blocks of some rows
+// the symmetric FP64 tiles from a matrix in the reference's COO form (k_cpim_sym.cu)
+void sym_tiles_from_coo(capac_ctx *c, long nnz, const double *val, const long *row, const long *col);
 // symmetric packed storage (k_cpim_sym.cu)
 int sym_tiles(int M);
 size_t sym_matrix_elems(int M);

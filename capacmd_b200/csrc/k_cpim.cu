@@ -228,6 +228,30 @@ __global__ void __launch_bounds__(128) k_cpim_matrix(DevParams P, const double4 
 
 constexpr long kPrecondEvery = 10;
 
+// Dense FP64 4x4 blocks of metal rows i0 .. i0 + rows - 1 against every metal
+// column j: out[((i - i0) M + j) 16 + 4 r + c], the entries of cpim_block
+// (the reference's |e| <= 1e-15 drop applied), diagonal blocks diag(1/polar
+// x3, -1/capac).
+__global__ void __launch_bounds__(128) k_cpim_block_rows(DevParams P, const double4 *__restrict__ pos4, int i0,
+                                                         int rows, double *__restrict__ out)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= P.M || (int)blockIdx.y >= rows) return;
+    const int i = i0 + (int)blockIdx.y;
+    double e[16];
+    cpim_block(P, pos4[P.metal_min + i], pos4[P.metal_min + j], i == j, e);
+    double *o = out + ((size_t)blockIdx.y * P.M + j) * 16;
+#pragma unroll
+    for (int k = 0; k < 16; ++k) o[k] = e[k];
+}
+
+void launch_cpim_block_rows(capac_ctx *c, int i0, int rows, double *out)
+{
+    dim3 grid(grid_for(c->M, 128), rows);
+    k_cpim_block_rows<<<grid, 128, 0, c->stream>>>(c->P, c->pos4, i0, rows, out);
+    ++c->launches;
+}
+
 void launch_cpim_matrix(capac_ctx *c)
 {
     if (c->msym) {

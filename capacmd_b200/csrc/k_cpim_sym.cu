@@ -21,6 +21,8 @@
 // part[I][J] and part[J][I] (summed together on diagonal tiles).  A second
 // kernel adds the nT partials of each block row in a fixed order, applies the
 // diagonal and neutrality terms, and writes y with the solver's dot products.
+#include <vector>
+
 #include "terms.cuh"
 
 namespace capac {
@@ -388,6 +390,33 @@ void launch_sym_assemble(capac_ctx *c)
         k_sym_assemble<double><<<tiles, 256, 0, c->stream>>>(c->P, c->pos4, nT, nullptr,
                                                               static_cast<double *>(c->msym));
     ++c->launches;
+}
+
+// The FP64 tiles from the reference's COO matrix (mpi_cpff_mat_relay_COO,
+// cpff.c:205-519; row and column indices in the reference vector layout).
+// The matrix is symmetric and its diagonal blocks and neutrality couplings
+// are the fixed constants the tile SpMV applies itself, so only the
+// off-diagonal metal-metal entries of the upper block triangle are stored:
+// for atoms i < j the six dipole-dipole entries with row comp <= column comp,
+// the three dipole (row) - charge (column) entries and the charge-charge one.
+// Entries absent from the COO (dropped by the reference) are zero.
+void sym_tiles_from_coo(capac_ctx *c, long nnz, const double *val, const long *row, const long *col)
+{
+    const int M = c->M, nT = sym_tiles(M);
+    std::vector<double> host(sym_matrix_elems(M), 0.0);
+    static const int plane[4][4] = {{0, 1, 2, 6}, {-1, 3, 4, 7}, {-1, -1, 5, 8}, {-1, -1, -1, 9}};
+    for (long k = 0; k < nnz; ++k) {
+        const long r = row[k], q = col[k];
+        if (r < 0 || q < 0 || r >= 4L * M || q >= 4L * M) continue;  // neutrality rows and columns
+        const int i = r < 3L * M ? (int)(r / 3) : (int)(r - 3L * M), a = r < 3L * M ? (int)(r % 3) : 3;
+        const int j = q < 3L * M ? (int)(q / 3) : (int)(q - 3L * M), b = q < 3L * M ? (int)(q % 3) : 3;
+        if (i >= j) continue;  // the diagonal blocks and the lower triangle
+        const int p = plane[a][b];
+        if (p < 0) continue;   // the symmetric half of a block
+        const int I = i / kT, J = j / kT;
+        host[tile_index(I, J, nT) * kTileElems + elem_offset(p, i % kT, j % kT)] = val[k];
+    }
+    CAPAC_CUDA(cudaMemcpy(c->msym, host.data(), sizeof(double) * host.size(), cudaMemcpyHostToDevice));
 }
 
 // Number of blocks whose dot partials the reduction writes (for the solver).

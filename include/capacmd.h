@@ -233,6 +233,37 @@ int capac_cpim_matvec(capac_ctx *ctx, const double *x, double *y);
  * induced vector currently held (set with capac_set "vec_pq"). */
 int capac_force_given_pq(capac_ctx *ctx);
 
+/* Dense FP64 4x4 CPIM blocks of the metal rows row0 .. row0 + rows - 1
+ * against every metal column, from the current positions:
+ * out[((i - row0) * n_metal + j) * 16 + 4 * r + c], r and c over
+ * (p_x, p_y, p_z, q).  The entries are those mpi_cpff_mat_relay_COO forms
+ * (cpff.c:245-436, |e| <= 1e-15 dropped); diagonal blocks are
+ * diag(1/polar x3, -1/capac).  For a caller that keeps the matrix on the host,
+ * e.g. in the reference's COO form (the drop-in mpi_cpff_mat_relay_COO). */
+int capac_cpim_blocks(capac_ctx *ctx, int row0, int rows, double *out);
+
+/* Load the CPIM matrix from the reference's COO form: nnz entries val, row,
+ * col in the reference vector layout, as mpi_cpff_mat_relay_COO leaves
+ * Metal.vec_val / vec_row_ind / vec_col_ind (cpff.c:205-519).  It replaces the
+ * assembled matrix until the next force call or assembly, and capac_bicgstab
+ * then solves with it (the drop-in mpi_precon_bicg_stab_COO,
+ * bicg_stab.h:58-59).  The matrix is symmetric, so the upper block triangle is
+ * read; the diagonal blocks and neutrality couplings are the context's own
+ * constants (equal to the reference's).  FP64 contexts with the symmetric
+ * matrix layout only (CAPAC_ERR_UNSUPPORTED otherwise). */
+int capac_cpim_set_coo(capac_ctx *ctx, long nnz, const double *val, const long *row, const long *col);
+
+/* rattle_1st / rattle_2nd (force.h:85-95, force.c:1907-2090) on host arrays
+ * of n_atoms doubles, for a caller that keeps its own integrator.  stage 1:
+ * positions rx..rz and velocities vx..vz corrected in place towards the
+ * constraint lengths along the old positions ox..oz (before the drift);
+ * stage 2: velocities corrected in place, the constraint virial added to
+ * virial[9] (ox..oz unused, may be NULL).  dt is the time step; constraints,
+ * masses and box are the context's.  CAPAC_ERR_RATTLE with the reference's
+ * message when a molecule does not converge. */
+int capac_rattle(capac_ctx *ctx, int stage, double dt, double *rx, double *ry, double *rz, const double *ox,
+                 const double *oy, const double *oz, double *vx, double *vy, double *vz, double *virial);
+
 /* CPIM solve that allocates no device memory.  No counterpart in the
  * reference: it serves callers that cannot call cudaMalloc -- a host code that
  * hands all device memory to its own pool at start-up and forbids later
@@ -305,6 +336,7 @@ int capac_checkpoint_load(capac_ctx *ctx, const char *path);
  * adjoint_dedx (dE/dx), adjoint_dpsidx (dPsi/dx of the force matching),
  * adjoint_mu, adjoint_nu (the adjoint solutions).  Read-only diagnostics:
  * pair_list(2: 1 when the pair kernel walks the cluster list, cluster count),
+ * potential and virial are settable too (to zero them before a stage call).
  * solver_layout(1: 1 when the mixed path's persistent solver works in the
  * order of its block-Jacobi groups, its tiles assembled in that order),
  * solver_phases(9: mean ns per iteration of the persistent solver's phases

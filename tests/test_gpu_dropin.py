@@ -1,10 +1,15 @@
-"""Drop-in mode: the reference's own driver calling the GPU mpi_force.
+"""Drop-in mode: the reference's own driver calling the GPU library.
 
 oracle/_ref/mpi-main is the unmodified reference program (CPU);
 oracle/_ref/mpi-main-gpu is the same objects with every mpi_force call
-redirected to the GPU library (capacmd_b200/dropin/force_gpu.cpp).  Both run
-the same input for 10 steps; the trajectories (traj.dat, full precision),
-the printed energies and the induced dipoles/charges (vec_pq.txt) must agree.
+redirected to the GPU library (capacmd_b200/dropin/force_gpu.cpp), and
+oracle/_ref/mpi-main-cpim the same objects with the reference's own mpi_force
+kept and its CPIM stages (mpi_cpff_vec_ext, mpi_cpff_mat_relay_COO,
+mpi_precon_bicg_stab_COO, mpi_cpff_force) and RATTLE (rattle_1st,
+rattle_2nd) redirected (capacmd_b200/dropin/cpim_gpu.cpp).  Each runs the same
+input for 10 steps as the reference; the trajectories (traj.dat, full
+precision), the printed energies and the induced dipoles/charges
+(vec_pq.txt) must agree.
 
 Without a CPIM solve the two differ by summation order only.  With one, each
 program stops BiCGSTAB at the reference's relative residual 1e-4, where the
@@ -26,14 +31,15 @@ pytestmark = pytest.mark.gpu
 
 CPU = os.path.join(ROOT, "oracle", "_ref", "mpi-main")
 GPU = os.path.join(ROOT, "oracle", "_ref", "mpi-main-gpu")
+CPIM = os.path.join(ROOT, "oracle", "_ref", "mpi-main-cpim")
 
 
 @pytest.fixture(autouse=True)
 def _need(gpu_available):
     if not gpu_available:
         pytest.fail("no sm_100 GPU: GPU tests must run on a B200")
-    if not (os.path.exists(CPU) and os.path.exists(GPU)):
-        pytest.fail("oracle/_ref/mpi-main and mpi-main-gpu are not built (python -m capacmd_b200.build)")
+    if not all(os.path.exists(p) for p in (CPU, GPU, CPIM)):
+        pytest.fail("oracle/_ref/mpi-main, mpi-main-gpu and mpi-main-cpim are not built (python -m capacmd_b200.build)")
 
 
 def _run(exe, case, work, steps=10, save=5):
@@ -49,6 +55,8 @@ def _run(exe, case, work, steps=10, save=5):
                          capture_output=True, text=True, timeout=300)
     assert out.returncode == 0, out.stdout[-2000:] + out.stderr[-2000:]
     assert "Calculation ended normally" in out.stdout
+    if exe == CPIM:
+        _run.announced = out.stderr
     return out.stdout
 
 
@@ -79,10 +87,18 @@ def _vec_pq(path):
     return np.array(vals)
 
 
+@pytest.mark.parametrize("exe", ["mpi_force", "cpim_rattle"])
 @pytest.mark.parametrize("case", ["t_water", "t_au13", "t_au55w", "t_2np", "t_bonded"])
-def test_reference_driver_with_gpu_force(case, tmp_path):
+def test_reference_driver_with_gpu_force(case, exe, tmp_path):
     out_c = _run(CPU, case, str(tmp_path / "cpu"))
-    out_g = _run(GPU, case, str(tmp_path / "gpu"))
+    out_g = _run(GPU if exe == "mpi_force" else CPIM, case, str(tmp_path / "gpu"))
+    if exe == "cpim_rattle":
+        # the shims that ran: RATTLE always, the CPIM stages where the input has metal
+        said = _run.announced
+        assert "rattle_1st on the GPU" in said and "rattle_2nd on the GPU" in said
+        if case != "t_water":
+            for f in ("mpi_cpff_vec_ext", "mpi_cpff_mat_relay_COO", "mpi_precon_bicg_stab_COO", "mpi_cpff_force"):
+                assert f + " on the GPU" in said, said
     fc, fg = _frames(str(tmp_path / "cpu" / "traj.dat")), _frames(str(tmp_path / "gpu" / "traj.dat"))
     assert [s for s, _ in fc] == [s for s, _ in fg] == [0, 5, 10]
     cpim = os.path.exists(str(tmp_path / "cpu" / "vec_pq.txt")) and np.any(_vec_pq(str(tmp_path / "cpu" / "vec_pq.txt")))
