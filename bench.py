@@ -210,8 +210,10 @@ def main() -> int:
     ap.add_argument("--workload", default="c5", choices=sorted(WORKLOAD_DESC))
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
     ap.add_argument("--no-compare", action="store_true", help="skip the comparison arms and the accuracy block")
-    ap.add_argument("--drift-steps", type=int, default=2000,
-                    help="NVE steps of the 9.3k-atom system for the energy-drift figures (0: skip)")
+    ap.add_argument("--drift-steps", type=int, default=1000,
+                    help="NVE steps per run of the 9.3k-atom system for the energy-drift figures (0: skip)")
+    ap.add_argument("--drift-only", action="store_true",
+                    help="run the energy-drift study alone (12 runs of --drift-steps) and print its JSON")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--e2e-calls", type=int, default=20)
@@ -235,6 +237,9 @@ def main() -> int:
     from capacmd_b200 import configs
 
     torch.cuda.set_device(local)
+    if args.drift_only:
+        print(json.dumps(nve_drift(cm, configs, args.drift_steps, local)))
+        return 0
     if world > 1:
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
@@ -413,34 +418,51 @@ def compare_arms(args, cm, desc, sim, prec, device) -> tuple[dict, dict]:
 
 
 def nve_drift(cm, configs, steps: int, device: int, every: int = 10) -> dict:
-    """Total-energy drift of an NVE run of the 9.3k-atom system (Au309 in
-    3,000 waters, dt 1 fs) for the mixed path, the FP64 path at the
-    reference's solver rule and the FP64 path solved to rTr < 1e-22 bTb:
-    slope of a least-squares line through E_pot + E_kin sampled every
-    `every` steps, per atom and per ns.  The reference's CPIM forces are the
-    gradient of its energy at fixed induced vector, and that energy is not
-    stationary in the induced vector, so even exact solves do not conserve
-    it: the tight FP64 arm is the floor the other two are compared with."""
-    paths = configs.cached("c2_nve")
-    d = cm.Desc.from_paths(paths)
-    out = {"workload": "Au309 + 3,000 waters (9,309 atoms), nve, dt 1 fs", "steps": steps,
+    """Total-energy drift of NVE runs of the 9.3k-atom system (Au309 in 3,000
+    waters, dt 1 fs), three seeds (initial configuration and velocities) per
+    arm: the mixed path, the FP64 path at the reference's solver rule, the
+    FP64 path solved to rTr < 1e-22 bTb, and the mixed path without CPIM (the
+    floor of the integrator and RATTLE).  Per run: the slope of a
+    least-squares line through E_pot + E_kin sampled every `every` steps, per
+    atom and per ns.  Per arm: the mean over the seeds and its standard
+    error; per seed the mixed-minus-tight difference (same initial state),
+    with its mean, standard error and 95% interval (Student t, 2 degrees of
+    freedom).  The reference's CPIM forces are the gradient of its energy at
+    fixed induced vector, and that energy is not stationary in the induced
+    vector, so even exact solves do not conserve it: the tight FP64 arm is
+    the floor the CPIM arms are compared with."""
+    seeds = (("c2_nve", "c2_nve_nocpim_s1"), ("c2_nve_s2", "c2_nve_nocpim_s2"), ("c2_nve_s3", "c2_nve_nocpim_s3"))
+    out = {"workload": "Au309 + 3,000 waters (9,309 atoms), nve, dt 1 fs, seeds 1-3", "steps": steps,
            "unit": "kJ/mol per atom per ns"}
-    arms = (("mixed", cm.PREC_MIXED, {}), ("fp64_plain", cm.PREC_FP64, {}),
-            ("fp64_tight", cm.PREC_FP64, {"solver_tol": 1e-22}))
-    for name, p, kw in arms:
-        s = cm.Simulation(d, precision=p, device=device, **kw)
-        s.md_init()
-        t, e = [], []
-        for k in range(steps // every + 1):
-            if k:
-                s.md_steps(every)
-            t.append(k * every * 1e-3)  # ps
-            e.append(s.get("potential")[0] + 0.5 * s.get("thermo")[0])
-        slope = float(np.polyfit(np.array(t), np.array(e), 1)[0])  # kJ/mol/ps
-        out[name] = {"drift": slope * 1e3 / d.n_atoms,
-                     "rms_fluctuation": float(np.std(np.array(e) - np.polyval(np.polyfit(t, e, 1), t))),
-                     "e_start": float(e[0])}
-        s.close()
+    arms = (("mixed", cm.PREC_MIXED, {}, 0), ("fp64_plain", cm.PREC_FP64, {}, 0),
+            ("fp64_tight", cm.PREC_FP64, {"solver_tol": 1e-22}, 0), ("mixed_no_cpim", cm.PREC_MIXED, {}, 1))
+    runs = {name: [] for name, *_ in arms}
+    for name, p, kw, variant in arms:
+        for pair in seeds:
+            d = cm.Desc.from_paths(configs.cached(pair[variant]))
+            s = cm.Simulation(d, precision=p, device=device, **kw)
+            s.md_init()
+            t, e = [], []
+            for k in range(steps // every + 1):
+                if k:
+                    s.md_steps(every)
+                t.append(k * every * 1e-3)  # ps
+                e.append(s.get("potential")[0] + 0.5 * s.get("thermo")[0])
+            t, e = np.array(t), np.array(e)
+            fit = np.polyfit(t, e, 1)
+            runs[name].append({"drift": float(fit[0]) * 1e3 / d.n_atoms,
+                               "rms_fluctuation": float(np.std(e - np.polyval(fit, t))), "e_start": float(e[0])})
+            s.close()
+    t95 = 4.303  # Student t, 2 degrees of freedom
+    for name, rs in runs.items():
+        v = np.array([r["drift"] for r in rs])
+        out[name] = {"drift_mean": float(v.mean()), "drift_se": float(v.std(ddof=1) / np.sqrt(len(v))),
+                     "runs": rs}
+    diff = np.array([a["drift"] - b["drift"] for a, b in zip(runs["mixed"], runs["fp64_tight"])])
+    se = float(diff.std(ddof=1) / np.sqrt(len(diff)))
+    out["mixed_minus_fp64_tight"] = {"mean": float(diff.mean()), "se": se,
+                                     "ci95": [float(diff.mean() - t95 * se), float(diff.mean() + t95 * se)],
+                                     "per_seed": diff.tolist()}
     return out
 
 

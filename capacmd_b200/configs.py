@@ -61,8 +61,14 @@ WORKLOADS = {
     "c1_field": Workload("c1_field", [3], 0, 6.0, seed=0, ensemble="nve", steps=1000,
                          efield_vnm=(0.0, 0.0, 0.5)),
     "c2": Workload("c2", [4], 3000, 4.5, seed=1, steps=5000),
-    # the same system without thermostat, for energy-drift measurements
+    # the same system without thermostat, for energy-drift measurements, with
+    # two more seeds and, per seed, a variant without CPIM (the floor of the
+    # integrator and RATTLE alone)
     "c2_nve": Workload("c2_nve", [4], 3000, 4.5, seed=1, ensemble="nve", steps=5000),
+    **{f"c2_nve_s{k}": Workload(f"c2_nve_s{k}", [4], 3000, 4.5, seed=k, ensemble="nve", steps=5000)
+       for k in (2, 3)},
+    **{f"c2_nve_nocpim_s{k}": Workload(f"c2_nve_nocpim_s{k}", [4], 3000, 4.5, seed=k, ensemble="nve", steps=5000,
+                                        use_cpff=0) for k in (1, 2, 3)},
     "c3": Workload("c3", [5, 5], 30000, 9.65, seed=2, steps=2000, efield_vnm=(0.0, 0.0, 0.5),
                    gap_z=1.5),
     "c4": Workload("c4", [3], 1000, 3.1, seed=3, steps=6400),
