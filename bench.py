@@ -219,6 +219,8 @@ def main() -> int:
     ap.add_argument("--e2e-calls", type=int, default=20)
     ap.add_argument("--solver-kernel", type=int, default=0, choices=[0, 1],
                     help="0: persistent cooperative BiCGSTAB launch per solve, 1: a launch per vector step")
+    ap.add_argument("--pair-list", type=int, default=0, choices=[0, 1, 2],
+                    help="mixed path nonbonded list: 0 clusters, 1 one list per atom, 2 clusters, every pair once")
     ap.add_argument("--predictor", type=int, default=3, choices=[0, 1, 2, 3],
                     help="mixed path warm start: order of the polynomial extrapolation of past solutions")
     args = ap.parse_args()
@@ -252,7 +254,7 @@ def main() -> int:
     prec = cm.PREC_MIXED if args.precision == "mixed" else cm.PREC_FP64
     desc = cm.Desc.from_paths(paths)
     sim = cm.Simulation(desc, precision=prec, device=local, solver_kernel=args.solver_kernel,
-                        predictor=args.predictor)
+                        predictor=args.predictor, pair_list=args.pair_list)
     N, M = desc.n_atoms, desc.n_metal
     sim.md_init()
     sim.md_steps(args.warmup)

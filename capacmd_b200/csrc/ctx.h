@@ -179,7 +179,10 @@ struct capac_ctx {
     int *cl_counts = nullptr;          // [cells + 1] scratch: clusters per cell
     uint32_t *cl_nbr = nullptr;        // [cl_max * cl_cap]
     int *cl_nnb = nullptr;             // [cl_max]
-    unsigned char *cl_metal = nullptr; // [cl_max] the cluster has a metal neighbour
+    unsigned char *cl_metal = nullptr; // [cl_max] the cluster has a metal neighbour (or, on the
+                                       // half list, a metal member)
+    bool cl_half = false;              // half list: every pair once, Newton's third law (pair_list 2)
+    int *cl_of = nullptr;              // [N] the cluster of each atom (half list)
     void *scan_tmp = nullptr;
     size_t scan_tmp_bytes = 0;
 

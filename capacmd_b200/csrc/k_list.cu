@@ -250,10 +250,11 @@ __device__ __forceinline__ int cluster_offsets(const int m[4], const double *__r
 // The clusters of one cell (a thread per cell), and in flags[5] the largest
 // component of a member's offset from its cluster's centroid (float bits,
 // rounded up).
+// cl_of (half list, else null): the cluster of each atom.
 __global__ void k_make_clusters(int n_cells, const int *__restrict__ cell_start, const int *__restrict__ cl_start,
                                 const int *__restrict__ cell_atoms, const double *__restrict__ rx,
                                 const double *__restrict__ ry, const double *__restrict__ rz, InvBox B,
-                                int4 *cl_atoms, int *flags)
+                                int4 *cl_atoms, int *cl_of, int *flags)
 {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= n_cells) return;
@@ -265,6 +266,9 @@ __global__ void k_make_clusters(int n_cells, const int *__restrict__ cell_start,
 #pragma unroll
         for (int t = 0; t < 4; ++t) m[t] = p + t < e ? cell_atoms[p + t] : -1;
         cl_atoms[cl] = make_int4(m[0], m[1], m[2], m[3]);
+        if (cl_of)
+            for (int t = 0; t < 4; ++t)
+                if (m[t] >= 0) cl_of[m[t]] = cl;
         double o[4][3], cc[3];
         const int nk = cluster_offsets(m, rx, ry, rz, B, o, cc);
         for (int k = 0; k < nk; ++k)
@@ -284,8 +288,11 @@ __global__ void __launch_bounds__(256) k_build_cluster_list(DevParams P, Grid g,
                                                             const int *__restrict__ n_cl, int cap,
                                                             uint32_t *__restrict__ nbr, int *__restrict__ nnb,
                                                             unsigned char *__restrict__ cl_metal, double *rx0,
-                                                            double *ry0, double *rz0, int *flags)
+                                                            double *ry0, double *rz0, int *flags,
+                                                            const int *__restrict__ cl_of)
 {
+    // cl_of (half list): a pair is listed once, by the lower-numbered cluster
+    // of its two atoms, and inside one cluster by the earlier member
     const int cl = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (cl >= *n_cl) return;
@@ -336,16 +343,19 @@ __global__ void __launch_bounds__(256) k_build_cluster_list(DevParams P, Grid g,
                     const int p = base + lane;
                     unsigned mask = 0;
                     int j = 0;
-                    if (p < e) {
-                        const double4 q = spos[p];
+                    const double4 q = p < e ? spos[p] : make_double4(0.0, 0.0, 0.0, 0.0);
+                    const int cj = p < e && cl_of ? cl_of[(int)q.w] : cl + 1;
+                    if (p < e && cj >= cl) {
                         j = (int)q.w;
+                        // on the half list, members before j's own position when j is one
+                        const int jpos = cj != cl ? 4 : (j == m[0] ? 0 : j == m[1] ? 1 : j == m[2] ? 2 : 3);
                         const double ex = min_image(q.x - cc[0], B.L[0], B.inv[0]);
                         const double ey = min_image(q.y - cc[1], B.L[1], B.inv[1]);
                         const double ez = min_image(q.z - cc[2], B.L[2], B.inv[2]);
                         if (ex * ex + ey * ey + ez * ez < pre2) {
 #pragma unroll
                             for (int k = 0; k < 4; ++k) {
-                                if (k >= nk || j == m[k]) continue;
+                                if (k >= nk || j == m[k] || k >= jpos) continue;
                                 const float ox = k == 0 ? ofx0 : k == 1 ? ofx1 : k == 2 ? ofx2 : ofx3;
                                 const float oy = k == 0 ? ofy0 : k == 1 ? ofy1 : k == 2 ? ofy2 : ofy3;
                                 const float oz = k == 0 ? ofz0 : k == 1 ? ofz1 : k == 2 ? ofz2 : ofz3;
@@ -367,6 +377,8 @@ __global__ void __launch_bounds__(256) k_build_cluster_list(DevParams P, Grid g,
             }
         }
     }
+    if (cl_of)  // the half list: a metal member takes water neighbours' CPIM terms too
+        for (int k = 0; k < nk; ++k) metal |= P.is_metal[m[k]] != 0;
     metal = __any_sync(0xffffffffu, metal);
     if (lane == 0) {
         nnb[cl] = count < cap ? count : cap;
@@ -382,10 +394,12 @@ __global__ void __launch_bounds__(256) k_build_cluster_list(DevParams P, Grid g,
 
 // Pair-set fingerprint over the cluster list: per member i the j < i
 // entries of its mask inside the cut-off.
+// On the half list each listed pair counts once, oriented as the reference
+// orients it (the larger index is i, r = r_j - r_i).
 __global__ void k_fingerprint_clusters(DevParams P, const double *__restrict__ rx, const double *__restrict__ ry,
                                        const double *__restrict__ rz, const int4 *__restrict__ cl_atoms,
                                        const int *__restrict__ n_cl, const uint32_t *__restrict__ nbr,
-                                       const int *__restrict__ nnb, int cap, unsigned long long *out)
+                                       const int *__restrict__ nnb, int cap, int half, unsigned long long *out)
 {
     const int cl = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
@@ -400,13 +414,17 @@ __global__ void k_fingerprint_clusters(DevParams P, const double *__restrict__ r
 #pragma unroll
         for (int t = 0; t < 4; ++t) {
             if (!((mask >> t) & 1u)) continue;
-            const int i = m[t];
-            if (j >= i) continue;
-            double dx = rx[j] - rx[i], dy = ry[j] - ry[i], dz = rz[j] - rz[i];
+            int i = m[t], jj = j;
+            if (half && jj > i) {
+                i = j;
+                jj = m[t];
+            }
+            if (jj >= i) continue;
+            double dx = rx[jj] - rx[i], dy = ry[jj] - ry[i], dz = rz[jj] - rz[i];
             image(dx, dy, dz, P.box);
             if (norm2_exact(dx, dy, dz) < P.rc2) {
                 ++cnt;
-                h += mix64(((uint64_t)(uint32_t)i << 32) | (uint32_t)j);
+                h += mix64(((uint64_t)(uint32_t)i << 32) | (uint32_t)jj);
             }
         }
     }
@@ -539,7 +557,8 @@ InvBox inv_box(const capac_ctx *c)
 
 bool cluster_list_allowed(const capac_ctx *c)
 {
-    return c->opt.precision == CAPAC_PREC_MIXED && c->opt.pair_list == 0 && c->N < (1 << kClIdxBits) &&
+    return c->opt.precision == CAPAC_PREC_MIXED && (c->opt.pair_list == 0 || c->opt.pair_list == 2) &&
+           c->N < (1 << kClIdxBits) &&
            c->P.n_types <= kClMaxTypes;
 }
 
@@ -580,6 +599,8 @@ void ensure_cluster_buffers(capac_ctx *c, int n_cells)
         CAPAC_CUDA(cudaMalloc(&c->cl_metal, need));
         c->cl_max = need;
     }
+    c->cl_half = c->opt.pair_list == 2;
+    if (c->cl_half && !c->cl_of) CAPAC_CUDA(cudaMalloc(&c->cl_of, sizeof(int) * N));
 }
 
 // Clusters of the sorted cells; returns false when the largest member offset
@@ -600,7 +621,8 @@ bool make_clusters(capac_ctx *c, int n_cells)
     CAPAC_CUDA(cub::DeviceScan::ExclusiveSum(c->scan_tmp, need, c->cl_counts, c->cl_cell_start, n_cells + 1, s));
     CAPAC_CUDA(cudaMemsetAsync(c->flags + 5, 0, sizeof(int), s));
     k_make_clusters<<<grid_for(n_cells, 128), 128, 0, s>>>(n_cells, c->cell_start, c->cl_cell_start, c->cell_atoms,
-                                                           c->rx, c->ry, c->rz, inv_box(c), c->cl_atoms, c->flags);
+                                                           c->rx, c->ry, c->rz, inv_box(c), c->cl_atoms,
+                                                           c->cl_half ? c->cl_of : nullptr, c->flags);
     c->launches += 3;
     CAPAC_CUDA(cudaMemcpyAsync(c->h_flags + 6, c->cl_cell_start + n_cells, sizeof(int), cudaMemcpyDeviceToHost, s));
     CAPAC_CUDA(cudaMemcpyAsync(c->h_flags + 5, c->flags + 5, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -622,7 +644,8 @@ void build_cluster_list(capac_ctx *c, const Grid &g, int n_cells)
             ProfScope ps(c, K_LIST);
             k_build_cluster_list<<<grid_for((long)c->n_clusters * 32, 256), 256, 0, s>>>(
                 c->P, g, inv_box(c), c->rx, c->ry, c->rz, c->spos, c->cell_start, c->cl_atoms, n_cl, c->cl_cap,
-                c->cl_nbr, c->cl_nnb, c->cl_metal, c->rx0, c->ry0, c->rz0, c->flags);
+                c->cl_nbr, c->cl_nnb, c->cl_metal, c->rx0, c->ry0, c->rz0, c->flags,
+                c->cl_half ? c->cl_of : nullptr);
         }
         ++c->launches;
         CAPAC_CUDA(cudaMemcpyAsync(c->h_flags + 4, c->flags + 4, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -758,7 +781,7 @@ void launch_pair_fingerprint(capac_ctx *c, int from_list, long *count, unsigned 
         if (c->clusters)
             k_fingerprint_clusters<<<grid_for((long)c->n_clusters * 32, 256), 256, 0, c->stream>>>(
                 c->P, c->rx, c->ry, c->rz, c->cl_atoms, c->cl_cell_start + c->n_cells, c->cl_nbr, c->cl_nnb,
-                c->cl_cap, d);
+                c->cl_cap, c->cl_half ? 1 : 0, d);
         else
             k_fingerprint_list<<<grid_for((long)c->N * 32, 256), 256, 0, c->stream>>>(
                 c->P, c->rx, c->ry, c->rz, c->nbr, c->nnb, c->cap, d);

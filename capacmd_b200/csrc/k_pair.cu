@@ -483,11 +483,18 @@ __global__ void __launch_bounds__(kPairWarps * 32, sizeof(Real) == 4 ? 3 : 2) k_
 // 128 pairs to the warp's queue (dynamic shared memory, kClQueue entries);
 // full flushes of 32 follow at one site, which keeps the pair terms in the
 // code once.
+//
+// HALF (pair_list 2): the list holds every pair once (k_list.cu), so each
+// survivor's force goes to both ends: the member's slot as above, the
+// neighbour's by FP64 atomic adds, and energies and virial count in full.
+// The CPIM force on a charged water atom from a metal atom is taken from
+// whichever end holds the metal.  The atomic adds make the order of the
+// neighbour-side sums vary from run to run (FP64 rounding of FP32 terms).
 constexpr int kClQueue = 160;  // < 32 left over + 4 x 32 appended
 constexpr int kClWarps = 8;      // warps per block of the cluster kernel
 constexpr int kClMinBlocks = 2;  // resident blocks per SM the register budget allows
 constexpr size_t kClQueueBytes = (size_t)kClWarps * kClQueue * sizeof(Cand<float>);
-template <bool NONBONDED, bool CPIM>
+template <bool NONBONDED, bool CPIM, bool HALF>
 __global__ void __launch_bounds__(kClWarps * 32, kClMinBlocks) k_pair_cl(DevParams P, PairConstsF K, const double4 *__restrict__ pos4,
                                                               const int4 *__restrict__ cl_atoms,
                                                               const int *__restrict__ n_cl,
@@ -503,6 +510,7 @@ __global__ void __launch_bounds__(kClWarps * 32, kClMinBlocks) k_pair_cl(DevPara
     __shared__ float4 s_mem[kClWarps][4];  // member offset from the centroid, charge
     __shared__ int s_trow[kClWarps][4];    // member type * n_types
     __shared__ unsigned char s_cpim[kClWarps][4];  // the member takes the CPIM force of metal neighbours
+    __shared__ int s_mmetal[kClWarps][4];          // half list: the member's metal index, -1 not metal
     __shared__ double s_acc[kClWarps][12][32];  // force on (member, axis) per lane slot
     __shared__ double sh[32 * 11];
     __shared__ double wacc[kClWarps][8];
@@ -554,6 +562,7 @@ __global__ void __launch_bounds__(kClWarps * 32, kClMinBlocks) k_pair_cl(DevPara
             s_mem[wib][lane] = make_float4((float)(ox - mx), (float)(oy - my), (float)(oz - mz), (float)pm.w);
             s_trow[wib][lane] = P.type[mine] * P.n_types;
             s_cpim[wib][lane] = CPIM && P.is_metal[mine] == 0 && pm.w != 0.0;
+            s_mmetal[wib][lane] = HALF && P.is_metal[mine] != 0 ? mine - P.metal_min : -1;
         }
 #pragma unroll
         for (int q = 0; q < 12; ++q) s_acc[wib][q][lane] = 0.0;
@@ -571,6 +580,7 @@ __global__ void __launch_bounds__(kClWarps * 32, kClMinBlocks) k_pair_cl(DevPara
         auto flush = [&](int head, int cnt) {
             if (lane < cnt) {
                 float g0 = 0.f, g1 = 0.f, g2 = 0.f;
+                float n0 = 0.f, n1 = 0.f, n2 = 0.f;  // the pair force on the member (reversed on the half list)
                 const Cand<float> c = Q[head + lane];
                 const int k = (int)((c.e >> kClMaskShift) & 3u);
                 const int tj = (int)(c.e >> kClTypeShift);
@@ -583,9 +593,9 @@ __global__ void __launch_bounds__(kClWarps * 32, kClMinBlocks) k_pair_cl(DevPara
                     e_qq += (double)eq;
                     e_vdw += (double)ev;
                     const float gx = f * c.dx, gy = f * c.dy, gz = f * c.dz;
-                    g0 = -gx;
-                    g1 = -gy;
-                    g2 = -gz;
+                    g0 = n0 = -gx;
+                    g1 = n1 = -gy;
+                    g2 = n2 = -gz;
                     v[0] -= c.dx * gx; v[1] -= c.dx * gy; v[2] -= c.dx * gz;
                     v[3] -= c.dy * gy; v[4] -= c.dy * gz; v[5] -= c.dz * gz;
                 }
@@ -607,6 +617,32 @@ __global__ void __launch_bounds__(kClWarps * 32, kClMinBlocks) k_pair_cl(DevPara
                 s_acc[wib][3 * k][lane] += (double)g0;
                 s_acc[wib][3 * k + 1][lane] += (double)g1;
                 s_acc[wib][3 * k + 2][lane] += (double)g2;
+                if (HALF) {
+                    // the neighbour's side: the pair force reversed, and the
+                    // CPIM force on it when the member is the metal atom
+                    float h0 = -n0, h1 = -n1, h2 = -n2;
+                    const int mm = s_mmetal[wib][k];
+                    if (CPIM && cpim_cl && mm >= 0 && c.qj != 0.f) {
+                        const int j = (int)(c.e & kClIdxMask);
+                        const bool mj = metal_by_type ? s_metal[tj] != 0 : P.is_metal[j] != 0;
+                        if (!mj) {
+                            const float r[3] = {-c.dx, -c.dy, -c.dz};  // metal - atom
+                            const float p[3] = {(float)vec_pq[3 * mm], (float)vec_pq[3 * mm + 1],
+                                                (float)vec_pq[3 * mm + 2]};
+                            float g[3];
+                            cpim_charge_pair_f(K, r, c.r2, c.qj, (float)vec_pq[3 * P.M + mm], p, g);
+                            h0 -= g[0];
+                            h1 -= g[1];
+                            h2 -= g[2];
+                        }
+                    }
+                    if (h0 != 0.f || h1 != 0.f || h2 != 0.f) {
+                        const int j = (int)(c.e & kClIdxMask);
+                        atomicAdd(fx + j, (double)h0);
+                        atomicAdd(fy + j, (double)h1);
+                        atomicAdd(fz + j, (double)h2);
+                    }
+                }
             }
         };
 
@@ -706,7 +742,10 @@ __global__ void __launch_bounds__(kClWarps * 32, kClMinBlocks) k_pair_cl(DevPara
             for (int q = 0; q < 32; ++q) s += s_acc[wib][lane][(q + lane) & 31];
             const int atom = k == 0 ? A.x : k == 1 ? A.y : k == 2 ? A.z : A.w;
             double *f = a == 0 ? fx : (a == 1 ? fy : fz);
-            f[atom] += s;
+            if (HALF)
+                atomicAdd(f + atom, s);  // other clusters add to this atom as a neighbour
+            else
+                f[atom] += s;
         }
         if (NONBONDED) {
             const double t[8] = {warp_sum(e_qq), warp_sum(e_vdw), warp_sum((double)v[0]),
@@ -714,7 +753,7 @@ __global__ void __launch_bounds__(kClWarps * 32, kClMinBlocks) k_pair_cl(DevPara
                                  warp_sum((double)v[4]), warp_sum((double)v[5])};
             if (lane == 0) {
 #pragma unroll
-                for (int q = 0; q < 8; ++q) wacc[wib][q] += 0.5 * t[q];
+                for (int q = 0; q < 8; ++q) wacc[wib][q] += (HALF ? 1.0 : 0.5) * t[q];
             }
         }
         __syncwarp();
@@ -770,13 +809,13 @@ void launch_pair_t(capac_ctx *c, int mode, unsigned grid)
     ++c->launches;
 }
 
-template <bool NONBONDED, bool CPIM>
+template <bool NONBONDED, bool CPIM, bool HALF>
 void launch_pair_cl_t(capac_ctx *c, unsigned grid)
 {
     // the queues and the static arrays together exceed the default 48 KB
-    CAPAC_CUDA(cudaFuncSetAttribute(k_pair_cl<NONBONDED, CPIM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    CAPAC_CUDA(cudaFuncSetAttribute(k_pair_cl<NONBONDED, CPIM, HALF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)kClQueueBytes));
-    k_pair_cl<NONBONDED, CPIM><<<grid, kClWarps * 32, kClQueueBytes, c->stream>>>(
+    k_pair_cl<NONBONDED, CPIM, HALF><<<grid, kClWarps * 32, kClQueueBytes, c->stream>>>(
         c->P, pair_consts_f(c), c->pos4, c->cl_atoms, c->cl_cell_start + c->n_cells, c->cl_nbr, c->cl_nnb,
         c->cl_metal, c->cl_cap, c->vec_pq, c->fx, c->fy, c->fz, c->partials);
 }
@@ -785,12 +824,19 @@ void launch_pair_clusters(capac_ctx *c, int mode, unsigned grid)
 {
     const bool cpim = c->M > 0 && c->use_cpff;
     ProfScope ps(c, K_PAIR);
-    if (mode == 0 && cpim)
-        launch_pair_cl_t<true, true>(c, grid);
+    if (c->cl_half) {
+        if (mode == 0 && cpim)
+            launch_pair_cl_t<true, true, true>(c, grid);
+        else if (mode == 0)
+            launch_pair_cl_t<true, false, true>(c, grid);
+        else
+            launch_pair_cl_t<false, true, true>(c, grid);
+    } else if (mode == 0 && cpim)
+        launch_pair_cl_t<true, true, false>(c, grid);
     else if (mode == 0)
-        launch_pair_cl_t<true, false>(c, grid);
+        launch_pair_cl_t<true, false, false>(c, grid);
     else
-        launch_pair_cl_t<false, true>(c, grid);
+        launch_pair_cl_t<false, true, false>(c, grid);
     ++c->launches;
 }
 

@@ -138,3 +138,49 @@ def test_gradients_on_the_cluster_path():
     cl.md_init()
     cl.md_steps(5)
     assert _uses_clusters(cl)
+
+
+@pytest.mark.parametrize("case", CLUSTER_CASES + ["c2"])
+def test_half_cluster_list(case):
+    """pair_list 2: every pair listed once, by the lower-numbered cluster of
+    its atoms, and applied to both ends.  The pair set is still the
+    reference's; forces, energies and virial agree with the full cluster list
+    within FP32 rounding of the pair terms."""
+    paths = configs.cached(case) if case == "c2" else golden_paths(case)
+    d, full = _mixed(paths, refine_tol=1e-11)
+    _, half = _mixed(paths, refine_tol=1e-11, pair_list=2)
+    ref = full.pair_fingerprint(from_list=False)
+    if case != "c2":
+        g = golden_ref(case)
+        assert ref == (int(g["pair_count"]), int(g["pair_hash"]))
+    assert half.pair_fingerprint(from_list=True) == ref
+    assert _uses_clusters(half)
+    assert half.stats().list_entries < full.stats().list_entries
+    for s in (full, half):
+        s.force()
+    assert rel_err(half.forces(), full.forces()) < 2e-6
+    pf, ph = full.get("potential"), half.get("potential")
+    scale = np.abs(pf[1:]).sum()
+    assert np.abs(ph - pf).max() <= 1e-6 * scale
+    assert rel_err(half.get("virial"), full.get("virial")) < 1e-5
+    if d.n_mat:
+        assert rel_err(half.get("vec_pq"), full.get("vec_pq")) < 1e-8
+
+
+def test_half_cluster_list_md_through_rebuilds():
+    p = configs.cached("c2")
+    d, full = _mixed(p)
+    _, half = _mixed(p, pair_list=2)
+    for s in (full, half):
+        s.md_init()
+    ef, eh = [], []
+    for _ in range(60):
+        full.md_steps(1)
+        half.md_steps(1)
+        ef.append(full.get("potential")[0])
+        eh.append(half.get("potential")[0])
+    assert half.stats().list_builds >= 2
+    assert _uses_clusters(half)
+    ef, eh = np.array(ef), np.array(eh)
+    assert np.abs(ef - eh).max() <= 1e-5 * np.abs(ef).max()
+    assert rel_err(half.get("rx"), full.get("rx")) < 1e-5
