@@ -400,13 +400,17 @@ def compare_arms(args, cm, desc, sim, prec, device) -> tuple[dict, dict]:
            "headline": state_errors(sim)}
     arms = {}
     other = cm.PREC_FP64 if prec == cm.PREC_MIXED else cm.PREC_MIXED
-    specs = [("fp64_plain" if other == cm.PREC_FP64 else "mixed", other, 0.0)]
+    specs = [("fp64_plain" if other == cm.PREC_FP64 else "mixed", other, 0.0, 0)]
     if desc.n_mat > 0:
         # rTr < 1e-20 bTb: relative residual 1e-10, the mixed path's target
-        specs.append(("fp64_equal_residual", cm.PREC_FP64, 1e-20))
-    for name, p, tol in specs:
+        specs.append(("fp64_equal_residual", cm.PREC_FP64, 1e-20, 0))
+    if prec == cm.PREC_MIXED:
+        # the other cluster list: every pair once (2) against four atoms sharing each neighbour (0)
+        other_list = 2 if args.pair_list != 2 else 0
+        specs.append((f"mixed_pair_list_{other_list}", cm.PREC_MIXED, 0.0, other_list))
+    for name, p, tol, plist in specs:
         s2 = cm.Simulation(desc, precision=p, device=device, solver_tol=tol, solver_kernel=args.solver_kernel,
-                           predictor=args.predictor)
+                           predictor=args.predictor, pair_list=plist)
         s2.md_init()
         s2.md_steps(args.warmup)
         ms2 = ctypes_time(s2, args.steps)
