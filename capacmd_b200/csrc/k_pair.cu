@@ -578,6 +578,8 @@ __global__ void __launch_bounds__(kClWarps * 32, kClMinBlocks) k_pair_cl(DevPara
         // pair terms of the queue entries head .. head + cnt - 1 into the
         // lanes' slots
         auto flush = [&](int head, int cnt) {
+            float hj0 = 0.f, hj1 = 0.f, hj2 = 0.f;  // half list: the neighbour's force of this lane's pair
+            int jj = -1;
             if (lane < cnt) {
                 float g0 = 0.f, g1 = 0.f, g2 = 0.f;
                 float n0 = 0.f, n1 = 0.f, n2 = 0.f;  // the pair force on the member (reversed on the half list)
@@ -636,12 +638,33 @@ __global__ void __launch_bounds__(kClWarps * 32, kClMinBlocks) k_pair_cl(DevPara
                             h2 -= g[2];
                         }
                     }
-                    if (h0 != 0.f || h1 != 0.f || h2 != 0.f) {
-                        const int j = (int)(c.e & kClIdxMask);
-                        atomicAdd(fx + j, (double)h0);
-                        atomicAdd(fy + j, (double)h1);
-                        atomicAdd(fz + j, (double)h2);
+                    hj0 = h0;
+                    hj1 = h1;
+                    hj2 = h2;
+                    jj = (int)(c.e & kClIdxMask);
+                }
+            }
+            if (HALF) {
+                // a neighbour's pairs are adjacent (at most four): sum them
+                // into the first lane of the run, which adds them to the atom
+                const int jl = lane < cnt ? jj : -1 - lane;
+#pragma unroll
+                for (int o = 1; o < 4; o <<= 1) {
+                    const float t0 = __shfl_down_sync(0xffffffffu, hj0, o);
+                    const float t1 = __shfl_down_sync(0xffffffffu, hj1, o);
+                    const float t2 = __shfl_down_sync(0xffffffffu, hj2, o);
+                    const int tj = __shfl_down_sync(0xffffffffu, jl, o);
+                    if (lane + o < 32 && tj == jl) {
+                        hj0 += t0;
+                        hj1 += t1;
+                        hj2 += t2;
                     }
+                }
+                const int prev = __shfl_up_sync(0xffffffffu, jl, 1);
+                if (lane < cnt && (lane == 0 || prev != jl) && (hj0 != 0.f || hj1 != 0.f || hj2 != 0.f)) {
+                    atomicAdd(fx + jl, (double)hj0);
+                    atomicAdd(fy + jl, (double)hj1);
+                    atomicAdd(fz + jl, (double)hj2);
                 }
             }
         };
@@ -694,24 +717,60 @@ __global__ void __launch_bounds__(kClWarps * 32, kClMinBlocks) k_pair_cl(DevPara
                 const float bq = hi ? qj[1] : qj[0];
                 const unsigned bm = hi ? mask[1] : mask[0];
                 const uint32_t bk = hi ? keep[1] : keep[0];
+                if (HALF) {
+                    // each entry's survivors appended next to each other (the
+                    // flush sums a neighbour's pairs before its atomic adds)
+                    unsigned smask = 0;
 #pragma unroll
-                for (int kk = 0; kk < 4; ++kk) {
-                    const float4 mk = s_mem[wib][kk];
-                    const float dx = bx - mk.x, dy = by - mk.y, dz = bz - mk.z;
-                    const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-                    const bool ok = ((bm >> kk) & 1u) && r2 < K.rc2;
-                    const unsigned ballot = __ballot_sync(0xffffffffu, ok);
-                    if (ok) {
-                        Cand<float> c;
-                        c.dx = dx;
-                        c.dy = dy;
-                        c.dz = dz;
-                        c.r2 = r2;
-                        c.qj = bq;
-                        c.e = bk | ((uint32_t)kk << kClMaskShift);
-                        Q[qn + __popc(ballot & lt_mask)] = c;
+                    for (int kk = 0; kk < 4; ++kk) {
+                        const float4 mk = s_mem[wib][kk];
+                        const float dx = bx - mk.x, dy = by - mk.y, dz = bz - mk.z;
+                        const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+                        if (((bm >> kk) & 1u) && r2 < K.rc2) smask |= 1u << kk;
                     }
-                    qn += __popc(ballot);
+                    const int cnt = __popc(smask);
+                    int incl = cnt;
+#pragma unroll
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const int t = __shfl_up_sync(0xffffffffu, incl, o);
+                        if (lane >= o) incl += t;
+                    }
+                    int pos = qn + incl - cnt;
+#pragma unroll
+                    for (int kk = 0; kk < 4; ++kk) {
+                        if ((smask >> kk) & 1u) {
+                            const float4 mk = s_mem[wib][kk];
+                            Cand<float> c;
+                            c.dx = bx - mk.x;
+                            c.dy = by - mk.y;
+                            c.dz = bz - mk.z;
+                            c.r2 = fmaf(c.dz, c.dz, fmaf(c.dy, c.dy, c.dx * c.dx));
+                            c.qj = bq;
+                            c.e = bk | ((uint32_t)kk << kClMaskShift);
+                            Q[pos++] = c;
+                        }
+                    }
+                    qn += __shfl_sync(0xffffffffu, incl, 31);
+                } else {
+#pragma unroll
+                    for (int kk = 0; kk < 4; ++kk) {
+                        const float4 mk = s_mem[wib][kk];
+                        const float dx = bx - mk.x, dy = by - mk.y, dz = bz - mk.z;
+                        const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+                        const bool ok = ((bm >> kk) & 1u) && r2 < K.rc2;
+                        const unsigned ballot = __ballot_sync(0xffffffffu, ok);
+                        if (ok) {
+                            Cand<float> c;
+                            c.dx = dx;
+                            c.dy = dy;
+                            c.dz = dz;
+                            c.r2 = r2;
+                            c.qj = bq;
+                            c.e = bk | ((uint32_t)kk << kClMaskShift);
+                            Q[qn + __popc(ballot & lt_mask)] = c;
+                        }
+                        qn += __popc(ballot);
+                    }
                 }
                 __syncwarp();
                 int head = 0;
