@@ -37,6 +37,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <new>
 #include <vector>
 
 #include "shim_desc.h"
@@ -108,6 +109,18 @@ extern "C" void __wrap__Z22mpi_cpff_mat_relay_COOP4TaskP5MetalP6SystemdiiPl(Task
 {
     announce(g_said[1], "mpi_cpff_mat_relay_COO");
     capac_ctx *c = need_context("mpi_cpff_mat_relay_COO");
+    // The driver allocates Metal with malloc (mpi-main.c:101) and never
+    // constructs its std::vector members; the reference's own push_back works
+    // only while that memory happens to be zero, which a process that has
+    // loaded a large runtime before main does not guarantee.  The first call
+    // constructs them (empty); later calls reuse them as cpff.c does.
+    static bool constructed = false;
+    if (!constructed) {
+        new (&m->vec_val) std::vector<double>();
+        new (&m->vec_row_ind) std::vector<long int>();
+        new (&m->vec_col_ind) std::vector<long int>();
+        constructed = true;
+    }
     set_positions(c, s, "mpi_cpff_mat_relay_COO");
     const int M = m->num, nps = m->n_NPs;
     const long nM3 = 3L * M;

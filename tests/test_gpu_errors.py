@@ -51,7 +51,8 @@ def test_resident_driver_exits_like_the_reference(tmp_path):
     if not os.path.exists(DRIVER):
         pytest.fail("capacmd_b200/capacmd-gpu is not built (python -m capacmd_b200.build)")
     variant("t_water", tmp_path, par=impossible_constraints)
-    out = subprocess.run([DRIVER], cwd=tmp_path, capture_output=True, text=True, timeout=300)
+    out = subprocess.run([DRIVER, "-gro", "init.gro", "-par", "param.txt", "-mds", "mdset.txt"], cwd=tmp_path,
+                         capture_output=True, text=True, timeout=300)
     assert out.returncode == 1
     assert "RATTLE_1 not converged!" in out.stdout
 

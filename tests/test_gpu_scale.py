@@ -81,8 +81,8 @@ def test_c2_against_the_reference(c2_reference):
 def test_c2_cluster_list_holds_the_reference_pair_set(c2_reference):
     paths, ref = c2_reference
     s = cm.Simulation(cm.Desc.from_paths(paths), precision=cm.PREC_MIXED)
-    assert s.get("pair_list")[0] == 1.0
     assert s.pair_fingerprint(from_list=True) == ref.pair_fingerprint()
+    assert s.get("pair_list")[0] == 1.0  # the list just built is the cluster list
 
 
 def test_c2_md_follows_the_reference(c2_reference):
@@ -157,8 +157,8 @@ def test_c3_mixed_path():
     paths, g = large_case("c3")
     d = cm.Desc.from_paths(paths)
     mix = cm.Simulation(d, precision=cm.PREC_MIXED)
-    assert mix.get("pair_list")[0] == 1.0
     assert mix.pair_fingerprint(from_list=True) == (int(g["pair_count"]), int(g["pair_hash"]))
+    assert mix.get("pair_list")[0] == 1.0
     f64 = cm.Simulation(d, solver_tol=1e-24)
     mix.force()
     f64.force()
@@ -179,8 +179,8 @@ def test_c5_pair_set_cpim_and_sampled_forces():
     o = Oracle(d)
     fp = o.pair_fingerprint(cells=True)
     mix = cm.Simulation(d, precision=cm.PREC_MIXED)
-    assert mix.get("pair_list")[0] == 1.0
     assert mix.pair_fingerprint(from_list=True) == fp
+    assert mix.get("pair_list")[0] == 1.0
     del mix
     s = cm.Simulation(d)
     assert s.pair_fingerprint(from_list=True) == fp
