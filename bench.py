@@ -223,8 +223,12 @@ def main() -> int:
                     help="mixed path nonbonded list: 0 clusters, 1 one list per atom, 2 clusters, every pair once")
     ap.add_argument("--predictor", type=int, default=3, choices=[0, 1, 2, 3],
                     help="mixed path warm start: order of the polynomial extrapolation of past solutions")
+    ap.add_argument("--solver-phases", action="store_true",
+                    help="time the persistent solver's phases in-kernel (globaltimer, block 0) and report them")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.solver_phases:
+        os.environ["CAPAC_SOLVER_PHASES"] = "1"  # read when the context is created
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -353,8 +357,10 @@ def main() -> int:
                        "initial_rel_residual_last": st.solver_initial_rel_residual,
                        "rel_residual_last": st.solver_rel_residual,
                        "ms_per_solve": (prof["spmv"][1] + prof["solver_vec"][1] + prof["resid"][1]
-                                        + prof["solve"][1]) / args.steps},
+                                        + prof["solve"][1]) / args.steps,
+                       "layout": "group order" if sim.get("solver_layout")[0] else "reference order"},
             "kernel_ms": {k: v[1] for k, v in prof.items()},
+            **({"solver_phase_us": solver_phases(sim)} if args.solver_phases else {}),
             "phase_ms_last_force": {"list": ps[10], "qsc": ps[1], "cpim_vec": ps[6], "cpim_matrix": ps[5],
                                     "cpim_solve": ps[7], "nonbonded": ps[4], "cpim_force": ps[8]},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "gpu_launches": launches,
@@ -365,6 +371,18 @@ def main() -> int:
     if world > 1:
         dist.destroy_process_group()
     return 0
+
+
+def solver_phases(sim) -> dict:
+    """Mean microseconds per iteration of the persistent solver's phases
+    (block 0's view, %globaltimer marks), over the iterations timed."""
+    ph = sim.get("solver_phases")
+    names = ["P tile pass", "P grid barrier", "V reduction (+ K v)", "K v pass", "alpha + S tile pass + barrier",
+             "T reduction (+ K t)", "K t pass", "dot sums + scalars"]
+    out = {n: ph[k] / 1e3 for k, n in enumerate(names)}
+    out["iterations_timed"] = ph[8]
+    out["total"] = float(sum(ph[:8]) / 1e3)
+    return out
 
 
 def compare_arms(args, cm, desc, sim, prec, device) -> tuple[dict, dict]:
