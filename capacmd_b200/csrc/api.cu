@@ -512,6 +512,7 @@ int capac_create(const capac_desc *d, const capac_options *opt, capac_ctx **out)
                                     c->gvec = dalloc<double>(nv);
                                     CAPAC_CUDA(cudaMemsetAsync(c->gvec, 0, sizeof(double) * nv, s));
                                     c->grouped = true;
+                                    c->tmem_tiles = getenv("CAPAC_SOLVER_TMEM") != nullptr;
                                 }
                             }
                         }
@@ -1083,9 +1084,11 @@ int capac_get(capac_ctx *c, const char *name, double *out)
             count = 2;
             return;
         }
-        if (n == "solver_layout") {  // 1 when the persistent solver runs in the block-Jacobi groups' order
+        if (n == "solver_layout") {  // 1 when the persistent solver runs in the block-Jacobi groups' order;
+                                     // its tiles per block held in tensor memory
             out[0] = c->grouped ? 1.0 : 0.0;
-            count = 1;
+            out[1] = c->grouped && c->tmem_tiles ? (double)group_tmem_tiles() : 0.0;
+            count = 2;
             return;
         }
         if (n == "solver_phases") {  // mean ns per iteration of each phase, then the iteration count

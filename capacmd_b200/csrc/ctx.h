@@ -200,6 +200,7 @@ struct capac_ctx {
     // group-ordered persistent solver (mixed path, block-Jacobi): the stored
     // tiles follow the groups' atom order and the solver works in that order
     bool grouped = false;
+    bool tmem_tiles = false;     // the grouped solver holds part of its tiles in tensor memory
     int *slot_np = nullptr;      // [32 nG] nanoparticle of each group slot's atom, -1 none
     int *np_off = nullptr;       // [n_nps + 1] offsets into np_rows
     int *np_rows = nullptr;      // [M] internal charge rows of each nanoparticle's atoms
@@ -292,6 +293,7 @@ size_t coop_barrier_bytes();
 size_t coop_partial_doubles(int grid);
 int bicgstab_coop(capac_ctx *c, const double *b, double *x, double tol, double skip);
 // group-ordered solver (k_solve_coop.cu): internal vector length, blocks
+int group_tmem_tiles();
 size_t group_rows(int M, int n_nps);
 int group_grid_size(int device);
 void launch_cpim_metal_forces(capac_ctx *c);

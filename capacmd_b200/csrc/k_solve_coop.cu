@@ -169,6 +169,59 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity)
     return false;
 }
 
+// Tensor memory (TMEM) as storage for matrix tiles that stay on chip for a
+// whole solve.  Allocation and release by one whole warp; a warp reads and
+// writes only the 32 lanes of its quadrant (warp rank mod 4).
+__device__ __forceinline__ void tmem_alloc(uint32_t *dst, uint32_t ncols)
+{
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(dst)),
+                 "r"(ncols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols)
+{
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+__device__ __forceinline__ void tmem_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tmem_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+// 40 consecutive columns of the thread's lane: one 32-column and one
+// 8-column access.
+__device__ __forceinline__ void tmem_st40(uint32_t taddr, const float (&v)[40])
+{
+    const uint32_t *u = reinterpret_cast<const uint32_t *>(v);
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, %32};" ::"r"(taddr),
+        "r"(u[0]), "r"(u[1]), "r"(u[2]), "r"(u[3]), "r"(u[4]), "r"(u[5]), "r"(u[6]), "r"(u[7]), "r"(u[8]), "r"(u[9]),
+        "r"(u[10]), "r"(u[11]), "r"(u[12]), "r"(u[13]), "r"(u[14]), "r"(u[15]), "r"(u[16]), "r"(u[17]), "r"(u[18]),
+        "r"(u[19]), "r"(u[20]), "r"(u[21]), "r"(u[22]), "r"(u[23]), "r"(u[24]), "r"(u[25]), "r"(u[26]), "r"(u[27]),
+        "r"(u[28]), "r"(u[29]), "r"(u[30]), "r"(u[31])
+        : "memory");
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"r"(taddr + 32),
+                 "r"(u[32]), "r"(u[33]), "r"(u[34]), "r"(u[35]), "r"(u[36]), "r"(u[37]), "r"(u[38]), "r"(u[39])
+                 : "memory");
+}
+__device__ __forceinline__ void tmem_ld40(uint32_t taddr, float (&v)[40])
+{
+    uint32_t *u = reinterpret_cast<uint32_t *>(v);
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+        : "=r"(u[0]), "=r"(u[1]), "=r"(u[2]), "=r"(u[3]), "=r"(u[4]), "=r"(u[5]), "=r"(u[6]), "=r"(u[7]), "=r"(u[8]),
+          "=r"(u[9]), "=r"(u[10]), "=r"(u[11]), "=r"(u[12]), "=r"(u[13]), "=r"(u[14]), "=r"(u[15]), "=r"(u[16]),
+          "=r"(u[17]), "=r"(u[18]), "=r"(u[19]), "=r"(u[20]), "=r"(u[21]), "=r"(u[22]), "=r"(u[23]), "=r"(u[24]),
+          "=r"(u[25]), "=r"(u[26]), "=r"(u[27]), "=r"(u[28]), "=r"(u[29]), "=r"(u[30]), "=r"(u[31])
+        : "r"(taddr)
+        : "memory");
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=r"(u[32]), "=r"(u[33]), "=r"(u[34]), "=r"(u[35]), "=r"(u[36]), "=r"(u[37]), "=r"(u[38]),
+                   "=r"(u[39])
+                 : "r"(taddr + 32)
+                 : "memory");
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
 }  // namespace
 
 struct CoopSync {
@@ -320,8 +373,9 @@ struct Ring {
     T *buf;
     uint64_t *bar;  // Stages mbarriers
     long issued, consumed;
-    int n_my;
-    __device__ int tile_of(long q) const { return blockIdx.x + (int)(q % n_my) * gridDim.x; }
+    int n_my;       // tiles streamed through the ring
+    int first = 0;  // tiles of the block before the streamed ones (held elsewhere)
+    __device__ int tile_of(long q) const { return blockIdx.x + (first + (int)(q % n_my)) * gridDim.x; }
     __device__ T *stage(int st) const { return buf + (size_t)st * kTileElems; }
     __device__ void issue(const T *mat)  // thread 0
     {
@@ -916,6 +970,7 @@ struct GroupArgs {
     SolverScalars *ss;
     CoopSync *sync;
     unsigned long long *ptime;
+    int tmem;                    // hold the first tiles of each block in tensor memory
 };
 
 // Reference row of internal row q (-1 for a padding slot).
@@ -957,8 +1012,16 @@ __device__ __forceinline__ double g_p_row(const GroupArgs &A, const PassScalars 
 }
 
 // Tile pass on the group-ordered tiles (tiles_pass with contiguous inputs).
+// The block's first n_res tiles are held in tensor memory (tw: this warp's
+// address of the first one, kResCols columns apart); the others stream
+// through the ring.
+constexpr int kResTiles = 3;           // tiles per block held in tensor memory
+constexpr int kResCols = 2 * kPlanes * kCols;  // columns per tile (two warps share a lane quadrant)
+constexpr uint32_t kTmemCols = 256;    // columns allocated per block (two blocks per SM: all 512)
+static_assert(kResTiles * kResCols <= (int)kTmemCols, "resident tiles exceed the allocation");
 template <int MODE>
-__device__ bool tiles_pass_g(const GroupArgs &A, const PassScalars &S, Ring<float> &ring, PassSmem<float> &sm)
+__device__ bool tiles_pass_g(const GroupArgs &A, const PassScalars &S, Ring<float> &ring, PassSmem<float> &sm,
+                             int n_res, uint32_t tw)
 {
     constexpr int Stages = Ring<float>::Stages;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -975,8 +1038,9 @@ __device__ bool tiles_pass_g(const GroupArgs &A, const PassScalars &S, Ring<floa
         }
     }
     constexpr int kChunk = chunk_tiles<float>();
-    for (int c0 = 0; c0 < ring.n_my; c0 += kChunk) {
-        const int nc = min(kChunk, ring.n_my - c0);
+    const int n_all = n_res + ring.n_my;
+    for (int c0 = 0; c0 < n_all; c0 += kChunk) {
+        const int nc = min(kChunk, n_all - c0);
         if (threadIdx.x < nc) {
             const int t = blockIdx.x + (c0 + threadIdx.x) * gridDim.x;
             int I = 0;
@@ -1009,11 +1073,17 @@ __device__ bool tiles_pass_g(const GroupArgs &A, const PassScalars &S, Ring<floa
         for (int kk = 0; kk < nc; ++kk) {
             const int I = sm.tile_i[kk], J = sm.tile_j[kk];
             const int set = kk & 1;
-            const long q = ring.consumed;
-            const int st = (int)(q % Stages);
-            const unsigned parity = (unsigned)((q / Stages) & 1);
-            const bool landed = mbar_wait(ring.bar + st, parity);
-            const float *tile = ring.stage(st);
+            const int qi = c0 + kk;
+            const bool res = qi < n_res;  // block-uniform
+            bool landed = true;
+            const float *tile = nullptr;
+            if (!res) {
+                const long q = ring.consumed;
+                const int st = (int)(q % Stages);
+                const unsigned parity = (unsigned)((q / Stages) & 1);
+                landed = mbar_wait(ring.bar + st, parity);
+                tile = ring.stage(st);
+            }
             const float(*xr)[4] = sm.in[kk][0];
             const float(*xc)[4] = sm.in[kk][1];
             const int a = lane;
@@ -1022,8 +1092,12 @@ __device__ bool tiles_pass_g(const GroupArgs &A, const PassScalars &S, Ring<floa
             const float xa0 = xr[a][0], xa1 = xr[a][1], xa2 = xr[a][2], xa3 = xr[a][3];
             if (landed) {
                 float vv[kPlanes][kCols];
+                if (res) {
+                    tmem_ld40(tw + (uint32_t)(qi * kResCols), reinterpret_cast<float(&)[40]>(vv));
+                } else {
 #pragma unroll
-                for (int pl = 0; pl < kPlanes; ++pl) ldsc(tile + elem_offset(pl, a, kCols * w), vv[pl]);
+                    for (int pl = 0; pl < kPlanes; ++pl) ldsc(tile + elem_offset(pl, a, kCols * w), vv[pl]);
+                }
 #pragma unroll
                 for (int k = 0; k < kCols; ++k) {
                     const int bb = kCols * w + k;
@@ -1052,8 +1126,10 @@ __device__ bool tiles_pass_g(const GroupArgs &A, const PassScalars &S, Ring<floa
                 sm.colacc[set][kCols * w + (vv2 >> 2)][vv2 & 3] = (double)colsum;
             }
             if (__syncthreads_or(!landed)) return false;
-            ++ring.consumed;
-            if (threadIdx.x == 0) ring.issue(A.mat);
+            if (!res) {
+                ++ring.consumed;
+                if (threadIdx.x == 0) ring.issue(A.mat);
+            }
             double *pr = A.part + ((size_t)I * nT + J) * (kT * 4);
             double *pc = A.part + ((size_t)J * nT + I) * (kT * 4);
             if (threadIdx.x < kT * 4) {
@@ -1221,18 +1297,49 @@ __global__ void __launch_bounds__(kBlock, 2) k_bicgstab_group(GroupArgs A)
     const int nb = gridDim.x;
     double *bpA = A.bp, *bpB = A.bp + (size_t)kBp * nb;
 
+    // the block's tiles: the first n_res held in tensor memory for the whole
+    // solve (A.tmem), the others streamed through the ring
+    const int n_all = (int)blockIdx.x < A.ntiles ? (A.ntiles - 1 - (int)blockIdx.x) / nb + 1 : 0;
+    const int n_res = A.tmem ? min(n_all, kResTiles) : 0;
     Ring<float> ring;
     ring.buf = reinterpret_cast<float *>(ring_smem);
     ring.bar = ring_bar;
     ring.issued = ring.consumed = 0;
-    ring.n_my = (int)blockIdx.x < A.ntiles ? (A.ntiles - 1 - (int)blockIdx.x) / nb + 1 : 0;
+    ring.first = n_res;
+    ring.n_my = n_all - n_res;
     if (threadIdx.x == 0) {
         for (int st = 0; st < Stages; ++st) mbar_init(ring_bar + st, 1);
         fence_mbar_init();
         if (ring.n_my > 0)
             for (int st = 0; st < Stages; ++st) ring.issue(A.mat);
     }
+    __shared__ uint32_t s_tmem;
+    uint32_t tw = 0;  // this warp's tensor-memory address of resident tile 0
+    if (n_res > 0) {
+        if (threadIdx.x < 32) tmem_alloc(&s_tmem, kTmemCols);
+        tmem_fence_before();
+        __syncthreads();
+        tmem_fence_after();
+        const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        tw = s_tmem + ((uint32_t)(32 * (w % 4)) << 16) + (uint32_t)((w / 4) * kPlanes * kCols);
+        for (int s = 0; s < n_res; ++s) {
+            const float *tile = A.mat + (size_t)(blockIdx.x + s * nb) * kTileElems;
+            float v[40];
+#pragma unroll
+            for (int pl = 0; pl < kPlanes; ++pl) {
+                const float4 q = __ldg(reinterpret_cast<const float4 *>(tile + elem_offset(pl, lane, kCols * w)));
+                v[4 * pl] = q.x;
+                v[4 * pl + 1] = q.y;
+                v[4 * pl + 2] = q.z;
+                v[4 * pl + 3] = q.w;
+            }
+            tmem_st40(tw + (uint32_t)(s * kResCols), v);
+        }
+        asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+        tmem_fence_before();
+    }
     __syncthreads();
+    if (n_res > 0) tmem_fence_after();
 
     PassScalars S{0.0, 0.0, 0.0, 0, 1};
     int iter = 0, status = 0;
@@ -1268,7 +1375,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_bicgstab_group(GroupArgs A)
     if (!done) {
         // r0 = r = b - A x, K r (x zero: no product pass; the ring is
         // untouched, so the next pass starts on the same tiles)
-        if (!x_zero) ok = tiles_pass_g<MODE_X>(A, S, ring, psm) && grid_barrier(A.sync, A.spin_limit);
+        if (!x_zero) ok = tiles_pass_g<MODE_X>(A, S, ring, psm, n_res, tw) && grid_barrier(A.sync, A.spin_limit);
         if (ok) reduce_group<RED_START>(A, S, bpB, !x_zero);
         ok = ok && grid_barrier(A.sync, A.spin_limit);
         done = !ok;
@@ -1286,7 +1393,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_bicgstab_group(GroupArgs A)
         S.beta = (rho / rho_old) * (alpha / omega);
         S.omega = omega;
         S.alpha = alpha;
-        ok = tiles_pass_g<MODE_P>(A, S, ring, psm);
+        ok = tiles_pass_g<MODE_P>(A, S, ring, psm, n_res, tw);
         g_phase_mark(A, iter, 1);
         ok = ok && grid_barrier(A.sync, A.spin_limit);
         if (!ok) break;
@@ -1310,7 +1417,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_bicgstab_group(GroupArgs A)
         alpha = al;
         S.cur ^= 1;
         S.alpha = alpha;
-        ok = tiles_pass_g<MODE_S>(A, S, ring, psm) && grid_barrier(A.sync, A.spin_limit);
+        ok = tiles_pass_g<MODE_S>(A, S, ring, psm, n_res, tw) && grid_barrier(A.sync, A.spin_limit);
         if (!ok) break;
         g_phase_mark(A, iter, 5);
         reduce_group<RED_T>(A, S, bpB, true);
@@ -1367,6 +1474,12 @@ __global__ void __launch_bounds__(kBlock, 2) k_bicgstab_group(GroupArgs A)
     if (threadIdx.x == 0) {
         if (!ok) atomicCAS(&A.sync->error, 0, 2);
         ring.drain();
+    }
+    if (n_res > 0) {  // every path comes here: the block's tensor memory is released
+        tmem_fence_before();
+        __syncthreads();
+        tmem_fence_after();
+        if (threadIdx.x < 32) tmem_dealloc(s_tmem, kTmemCols);
     }
     if (ok && tid == 0) {
         ss->bTb = bTb;
@@ -1518,6 +1631,7 @@ int bicgstab_group(capac_ctx *c, const double *b, double *x, double tol, double 
     A.skip = skip;
     A.ss = c->ss;
     A.sync = reinterpret_cast<CoopSync *>(c->coop_bar);
+    A.tmem = c->tmem_tiles ? 1 : 0;
     A.ptime = nullptr;
     if (c->phase_timer) {
         if (!c->phase_buf) CAPAC_CUDA(cudaMalloc(&c->phase_buf, sizeof(unsigned long long) * kPhases * kPhaseIters));
@@ -1534,6 +1648,7 @@ int bicgstab_group(capac_ctx *c, const double *b, double *x, double tol, double 
     return finish_coop(c, A.ptime, skip);
 }
 
+int group_tmem_tiles() { return kResTiles; }
 size_t group_rows(int M, int n_nps) { return (size_t)128 * precond_groups(M) + n_nps; }
 
 // Blocks of the group-ordered solver: two per SM when they fit, 0 if the

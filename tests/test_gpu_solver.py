@@ -116,3 +116,28 @@ def test_grouped_solver_matches_ungrouped(case, monkeypatch):
         plain.md_steps(1)
     assert rel_err(grouped.get("vec_pq"), plain.get("vec_pq")) < 1e-7
     assert rel_err(grouped.get("rx"), plain.get("rx")) < 1e-9
+
+
+@pytest.mark.parametrize("case", ["t_au55w", "t_2np", "c1_field"])
+def test_tmem_tiles_match_streamed(case, monkeypatch):
+    """The grouped solver with the first tiles of each block held in tensor
+    memory for the whole solve gives the same iterates as the one that streams
+    every tile each pass: the same FP32 products in the same order, so the
+    solutions agree to the last bits and the iteration counts are equal."""
+    d = cm.Desc.from_paths(golden_paths(case))
+    streamed = cm.Simulation(d, precision=cm.PREC_MIXED, refine_tol=1e-11)
+    monkeypatch.setenv("CAPAC_SOLVER_TMEM", "1")
+    held = cm.Simulation(d, precision=cm.PREC_MIXED, refine_tol=1e-11)
+    monkeypatch.delenv("CAPAC_SOLVER_TMEM")
+    assert streamed.get("solver_layout")[1] == 0.0
+    assert held.get("solver_layout")[1] > 0.0
+    for s in (streamed, held):
+        s.force()
+    assert held.stats().solver_iterations == streamed.stats().solver_iterations
+    assert rel_err(held.get("vec_pq"), streamed.get("vec_pq")) < 1e-12
+    held.md_init()
+    streamed.md_init()
+    for _ in range(6):
+        held.md_steps(1)
+        streamed.md_steps(1)
+    assert rel_err(held.get("rx"), streamed.get("rx")) < 1e-11
