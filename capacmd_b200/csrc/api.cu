@@ -493,7 +493,7 @@ int capac_create(const capac_desc *d, const capac_options *opt, capac_ctx **out)
                                 c->g_atoms = dupload(g.data(), g.size(), s);
                                 c->dinv = dalloc<float>(precond_inverse_floats(M));
                                 // the group-ordered solver (unless CAPAC_SOLVER_UNGROUPED is set)
-                                if (!getenv("CAPAC_SOLVER_UNGROUPED") && group_grid_size(c->device) == c->coop_grid) {
+                                if (!getenv("CAPAC_SOLVER_UNGROUPED") && group_grid_size(c->device, false) == c->coop_grid) {
                                     std::vector<int> slot_np(g.size(), -1), off(d->n_nps + 1, 0), rows;
                                     for (int k = 0; k < d->n_nps; ++k) {
                                         for (size_t q = 0; q < g.size(); ++q) {
@@ -512,7 +512,14 @@ int capac_create(const capac_desc *d, const capac_options *opt, capac_ctx **out)
                                     c->gvec = dalloc<double>(nv);
                                     CAPAC_CUDA(cudaMemsetAsync(c->gvec, 0, sizeof(double) * nv, s));
                                     c->grouped = true;
-                                    c->tmem_tiles = getenv("CAPAC_SOLVER_TMEM") != nullptr;
+                                    // the variant that holds tiles in tensor memory runs one
+                                    // block per SM
+                                    c->group_grid = c->coop_grid;
+                                    if (getenv("CAPAC_SOLVER_TMEM")) {
+                                        const int g = group_grid_size(c->device, true);
+                                        c->tmem_tiles = g > 0 && g <= c->coop_grid;
+                                        if (c->tmem_tiles) c->group_grid = g;
+                                    }
                                 }
                             }
                         }
@@ -1088,7 +1095,9 @@ int capac_get(capac_ctx *c, const char *name, double *out)
                                      // its tiles per block held in tensor memory
             out[0] = c->grouped ? 1.0 : 0.0;
             out[1] = c->grouped && c->tmem_tiles ? (double)group_tmem_tiles() : 0.0;
-            count = 2;
+            out[2] = (double)group_blocks_per_sm(c->device, false);
+            out[3] = (double)group_blocks_per_sm(c->device, true);
+            count = 4;
             return;
         }
         if (n == "solver_phases") {  // mean ns per iteration of each phase, then the iteration count

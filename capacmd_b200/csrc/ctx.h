@@ -201,6 +201,7 @@ struct capac_ctx {
     // tiles follow the groups' atom order and the solver works in that order
     bool grouped = false;
     bool tmem_tiles = false;     // the grouped solver holds part of its tiles in tensor memory
+    int group_grid = 0;          // blocks of the grouped solver's launch (<= coop_grid)
     int *slot_np = nullptr;      // [32 nG] nanoparticle of each group slot's atom, -1 none
     int *np_off = nullptr;       // [n_nps + 1] offsets into np_rows
     int *np_rows = nullptr;      // [M] internal charge rows of each nanoparticle's atoms
@@ -295,7 +296,8 @@ int bicgstab_coop(capac_ctx *c, const double *b, double *x, double tol, double s
 // group-ordered solver (k_solve_coop.cu): internal vector length, blocks
 int group_tmem_tiles();
 size_t group_rows(int M, int n_nps);
-int group_grid_size(int device);
+int group_grid_size(int device, bool hold);
+int group_blocks_per_sm(int device, bool hold);
 void launch_cpim_metal_forces(capac_ctx *c);
 void launch_external_field(capac_ctx *c);
 void launch_finalize(capac_ctx *c, int nblocks, int K, const int *slots_pot, const int *slots_vir);

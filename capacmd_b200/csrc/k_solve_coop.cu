@@ -970,7 +970,6 @@ struct GroupArgs {
     SolverScalars *ss;
     CoopSync *sync;
     unsigned long long *ptime;
-    int tmem;                    // hold the first tiles of each block in tensor memory
 };
 
 // Reference row of internal row q (-1 for a padding slot).
@@ -1015,9 +1014,11 @@ __device__ __forceinline__ double g_p_row(const GroupArgs &A, const PassScalars 
 // The block's first n_res tiles are held in tensor memory (tw: this warp's
 // address of the first one, kResCols columns apart); the others stream
 // through the ring.
-constexpr int kResTiles = 3;           // tiles per block held in tensor memory
+// A kernel that allocates tensor memory runs one block per SM, which takes
+// all 512 columns.
+constexpr int kResTiles = 6;           // tiles per block held in tensor memory
 constexpr int kResCols = 2 * kPlanes * kCols;  // columns per tile (two warps share a lane quadrant)
-constexpr uint32_t kTmemCols = 256;    // columns allocated per block (two blocks per SM: all 512)
+constexpr uint32_t kTmemCols = 512;    // columns allocated per block
 static_assert(kResTiles * kResCols <= (int)kTmemCols, "resident tiles exceed the allocation");
 template <int MODE>
 __device__ bool tiles_pass_g(const GroupArgs &A, const PassScalars &S, Ring<float> &ring, PassSmem<float> &sm,
@@ -1284,7 +1285,10 @@ __device__ void reduce_group(const GroupArgs &A, const PassScalars &S, double *b
     }
 }
 
-__global__ void __launch_bounds__(kBlock, 2) k_bicgstab_group(GroupArgs A)
+// At most 120 registers a thread (two blocks of kBlock threads per SM with
+// room to spare; both variants fit without spilling).
+template <bool HOLD>
+__global__ void __maxnreg__(120) k_bicgstab_group(GroupArgs A)
 {
     extern __shared__ __align__(128) unsigned char ring_smem[];
     constexpr int Stages = Ring<float>::Stages;
@@ -1298,9 +1302,9 @@ __global__ void __launch_bounds__(kBlock, 2) k_bicgstab_group(GroupArgs A)
     double *bpA = A.bp, *bpB = A.bp + (size_t)kBp * nb;
 
     // the block's tiles: the first n_res held in tensor memory for the whole
-    // solve (A.tmem), the others streamed through the ring
+    // solve (HOLD), the others streamed through the ring
     const int n_all = (int)blockIdx.x < A.ntiles ? (A.ntiles - 1 - (int)blockIdx.x) / nb + 1 : 0;
-    const int n_res = A.tmem ? min(n_all, kResTiles) : 0;
+    const int n_res = HOLD ? min(n_all, kResTiles) : 0;
     Ring<float> ring;
     ring.buf = reinterpret_cast<float *>(ring_smem);
     ring.bar = ring_bar;
@@ -1631,7 +1635,6 @@ int bicgstab_group(capac_ctx *c, const double *b, double *x, double tol, double 
     A.skip = skip;
     A.ss = c->ss;
     A.sync = reinterpret_cast<CoopSync *>(c->coop_bar);
-    A.tmem = c->tmem_tiles ? 1 : 0;
     A.ptime = nullptr;
     if (c->phase_timer) {
         if (!c->phase_buf) CAPAC_CUDA(cudaMalloc(&c->phase_buf, sizeof(unsigned long long) * kPhases * kPhaseIters));
@@ -1641,7 +1644,8 @@ int bicgstab_group(capac_ctx *c, const double *b, double *x, double tol, double 
     void *args[] = {&A};
     {
         ProfScope ps(c, K_SOLVE);
-        CAPAC_CUDA(cudaLaunchCooperativeKernel((const void *)k_bicgstab_group, dim3(c->coop_grid), dim3(kBlock), args,
+        const void *kern = c->tmem_tiles ? (const void *)k_bicgstab_group<true> : (const void *)k_bicgstab_group<false>;
+        CAPAC_CUDA(cudaLaunchCooperativeKernel(kern, dim3(c->group_grid), dim3(kBlock), args,
                                                dyn_smem_bytes<float>(), c->stream));
     }
     ++c->launches;
@@ -1653,26 +1657,33 @@ size_t group_rows(int M, int n_nps) { return (size_t)128 * precond_groups(M) + n
 
 // Blocks of the group-ordered solver: two per SM when they fit, 0 if the
 // device cannot run it.
-int group_grid_size(int device)
+int group_blocks_per_sm(int device, bool hold)
+{
+    const void *kern = hold ? (const void *)k_bicgstab_group<true> : (const void *)k_bicgstab_group<false>;
+    const size_t dyn = dyn_smem_bytes<float>();
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBlock, dyn) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return per_sm;
+}
+
+int group_grid_size(int device, bool hold)
 {
     int coop = 0;
     if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device) != cudaSuccess || !coop) return 0;
     int sms = 0;
     CAPAC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
-    const size_t dyn = dyn_smem_bytes<float>();
-    if (cudaFuncSetAttribute((const void *)k_bicgstab_group, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn) !=
-        cudaSuccess) {
-        cudaGetLastError();
-        return 0;
-    }
-    int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)k_bicgstab_group, kBlock, dyn) !=
-            cudaSuccess ||
-        per_sm < 1) {
-        cudaGetLastError();
-        return 0;
-    }
-    return sms * std::min(per_sm, 2);
+    const int per_sm = group_blocks_per_sm(device, hold);
+    // the variant that holds tiles allocates all of an SM's tensor memory:
+    // it runs only where no second block can share the SM
+    if (hold) return per_sm == 1 ? sms : 0;
+    return per_sm < 1 ? 0 : sms * std::min(per_sm, 2);
 }
 
 // Blocks of the persistent solver (two per SM for the FP32 matrix, one for

@@ -339,10 +339,11 @@ int capac_checkpoint_load(capac_ctx *ctx, const char *path);
  * adjoint_mu, adjoint_nu (the adjoint solutions).  Read-only diagnostics:
  * pair_list(2: 1 when the pair kernel walks the cluster list, cluster count),
  * potential and virial are settable too (to zero them before a stage call).
- * solver_layout(2: 1 when the mixed path's persistent solver works in the
+ * solver_layout(4: 1 when the mixed path's persistent solver works in the
  * order of its block-Jacobi groups, its tiles assembled in that order; the
  * tiles each of its blocks holds in tensor memory for the whole solve, 0 when
- * all are streamed from HBM each pass),
+ * all are streamed from HBM each pass; the resident blocks per SM of the
+ * group-ordered solver without and with tiles in tensor memory),
  * solver_phases(9: mean ns per iteration of the persistent solver's phases
  * when CAPAC_SOLVER_PHASES is set, then the iterations timed).  Set only:
  * wait_polls(1), the option of that name on the live context.  capac_get

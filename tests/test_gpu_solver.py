@@ -99,7 +99,7 @@ def test_grouped_solver_matches_ungrouped(case, monkeypatch):
     plain = cm.Simulation(d, precision=cm.PREC_MIXED, refine_tol=1e-11)
     monkeypatch.delenv("CAPAC_SOLVER_UNGROUPED")
     f64 = cm.Simulation(d, solver_tol=1e-26)
-    assert grouped.get("solver_layout")[0] == 1.0
+    assert grouped.get("solver_layout")[0] == 1.0, grouped.get("solver_layout")
     assert plain.get("solver_layout")[0] == 0.0
     for s in (grouped, plain, f64):
         s.force()
@@ -121,19 +121,21 @@ def test_grouped_solver_matches_ungrouped(case, monkeypatch):
 @pytest.mark.parametrize("case", ["t_au55w", "t_2np", "c1_field"])
 def test_tmem_tiles_match_streamed(case, monkeypatch):
     """The grouped solver with the first tiles of each block held in tensor
-    memory for the whole solve gives the same iterates as the one that streams
-    every tile each pass: the same FP32 products in the same order, so the
-    solutions agree to the last bits and the iteration counts are equal."""
+    memory for the whole solve (one block per SM) gives the same solution as
+    the one that streams every tile each pass (two blocks per SM): the same
+    FP32 tile products, summed over a different split of the tiles among
+    blocks, so the solutions agree to rounding and the iteration counts
+    match."""
     d = cm.Desc.from_paths(golden_paths(case))
     streamed = cm.Simulation(d, precision=cm.PREC_MIXED, refine_tol=1e-11)
     monkeypatch.setenv("CAPAC_SOLVER_TMEM", "1")
     held = cm.Simulation(d, precision=cm.PREC_MIXED, refine_tol=1e-11)
     monkeypatch.delenv("CAPAC_SOLVER_TMEM")
     assert streamed.get("solver_layout")[1] == 0.0
-    assert held.get("solver_layout")[1] > 0.0
+    assert held.get("solver_layout")[1] > 0.0, held.get("solver_layout")
     for s in (streamed, held):
         s.force()
-    assert held.stats().solver_iterations == streamed.stats().solver_iterations
+    assert abs(held.stats().solver_iterations - streamed.stats().solver_iterations) <= 1
     assert rel_err(held.get("vec_pq"), streamed.get("vec_pq")) < 1e-12
     held.md_init()
     streamed.md_init()
