@@ -513,13 +513,17 @@ int capac_create(const capac_desc *d, const capac_options *opt, capac_ctx **out)
                                     CAPAC_CUDA(cudaMemsetAsync(c->gvec, 0, sizeof(double) * nv, s));
                                     c->grouped = true;
                                     // the variant that holds tiles in tensor memory runs one
-                                    // block per SM
+                                    // block per SM: the default when every tile fits there
+                                    // (CAPAC_SOLVER_STREAM streams them all the same,
+                                    // CAPAC_SOLVER_TMEM holds part of a larger matrix)
                                     c->group_grid = c->coop_grid;
-                                    if (getenv("CAPAC_SOLVER_TMEM")) {
-                                        const int g = group_grid_size(c->device, true);
-                                        c->tmem_tiles = g > 0 && g <= c->coop_grid;
-                                        if (c->tmem_tiles) c->group_grid = g;
-                                    }
+                                    const int g = group_grid_size(c->device, true);
+                                    const long nG = precond_groups(M), ntiles = nG * (nG + 1) / 2;
+                                    const bool fits = (long)g * group_tmem_tiles() >= ntiles;
+                                    c->tmem_tiles = g > 0 && g <= c->coop_grid &&
+                                                    ((fits && !getenv("CAPAC_SOLVER_STREAM")) ||
+                                                     getenv("CAPAC_SOLVER_TMEM") != nullptr);
+                                    if (c->tmem_tiles) c->group_grid = g;
                                 }
                             }
                         }

@@ -205,3 +205,22 @@ def test_c5_pair_set_cpim_and_sampled_forces():
     p, po = s.get("potential"), o.get("potential")
     for k in (1, 9, 10, 11, 12, 13, 14):  # every term outside the pair loop
         assert abs(p[k] - po[k]) <= 1e-10 * abs(po[k]), k
+
+
+def test_c5_solver_with_part_of_the_tiles_in_tensor_memory(monkeypatch):
+    """At 452k atoms the 2,145 tiles do not all fit in tensor memory: by
+    default every tile streams from HBM; asked to, the solver holds six tiles
+    per block there and streams the rest.  Both reach the refinement target
+    and agree on the induced vector."""
+    d = cm.Desc.from_paths(configs.cached("c5"))
+    streamed = cm.Simulation(d, precision=cm.PREC_MIXED)
+    monkeypatch.setenv("CAPAC_SOLVER_TMEM", "1")
+    held = cm.Simulation(d, precision=cm.PREC_MIXED)
+    monkeypatch.delenv("CAPAC_SOLVER_TMEM")
+    assert streamed.get("solver_layout")[:2].tolist() == [1.0, 0.0]
+    assert held.get("solver_layout")[1] > 0.0, held.get("solver_layout")
+    for s in (streamed, held):
+        s.force()
+        assert s.stats().solver_rel_residual <= 1e-10
+    assert rel_err(held.get("vec_pq"), streamed.get("vec_pq")) < 1e-8
+    assert rel_err(held.forces(), streamed.forces()) < 1e-8

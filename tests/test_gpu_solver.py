@@ -127,10 +127,10 @@ def test_tmem_tiles_match_streamed(case, monkeypatch):
     blocks, so the solutions agree to rounding and the iteration counts
     match."""
     d = cm.Desc.from_paths(golden_paths(case))
+    held = cm.Simulation(d, precision=cm.PREC_MIXED, refine_tol=1e-11)  # every tile fits: held by default
+    monkeypatch.setenv("CAPAC_SOLVER_STREAM", "1")
     streamed = cm.Simulation(d, precision=cm.PREC_MIXED, refine_tol=1e-11)
-    monkeypatch.setenv("CAPAC_SOLVER_TMEM", "1")
-    held = cm.Simulation(d, precision=cm.PREC_MIXED, refine_tol=1e-11)
-    monkeypatch.delenv("CAPAC_SOLVER_TMEM")
+    monkeypatch.delenv("CAPAC_SOLVER_STREAM")
     assert streamed.get("solver_layout")[1] == 0.0
     assert held.get("solver_layout")[1] > 0.0, held.get("solver_layout")
     for s in (streamed, held):
