@@ -219,8 +219,9 @@ def main() -> int:
     ap.add_argument("--e2e-calls", type=int, default=20)
     ap.add_argument("--solver-kernel", type=int, default=0, choices=[0, 1],
                     help="0: persistent cooperative BiCGSTAB launch per solve, 1: a launch per vector step")
-    ap.add_argument("--pair-list", type=int, default=0, choices=[0, 1, 2],
-                    help="mixed path nonbonded list: 0 clusters, 1 one list per atom, 2 clusters, every pair once")
+    ap.add_argument("--pair-list", type=int, default=0, choices=[0, 1, 2, 3],
+                    help="mixed path nonbonded list: 0 (= 2) clusters with every pair once, 1 one list per "
+                         "atom, 3 clusters with every pair from both ends")
     ap.add_argument("--predictor", type=int, default=3, choices=[0, 1, 2, 3],
                     help="mixed path warm start: order of the polynomial extrapolation of past solutions")
     ap.add_argument("--solver-phases", action="store_true",
@@ -424,7 +425,7 @@ def compare_arms(args, cm, desc, sim, prec, device) -> tuple[dict, dict]:
         specs.append(("fp64_equal_residual", cm.PREC_FP64, 1e-20, 0))
     if prec == cm.PREC_MIXED:
         # the other cluster list: every pair once (2) against four atoms sharing each neighbour (0)
-        other_list = 2 if args.pair_list != 2 else 0
+        other_list = 3 if args.pair_list in (0, 2) else 0  # the full cluster list against the half one
         specs.append((f"mixed_pair_list_{other_list}", cm.PREC_MIXED, 0.0, other_list))
     for name, p, tol, plist in specs:
         s2 = cm.Simulation(desc, precision=p, device=device, solver_tol=tol, solver_kernel=args.solver_kernel,

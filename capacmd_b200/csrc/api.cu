@@ -583,7 +583,7 @@ int capac_destroy(capac_ctx *c)
                    c->cstr_cnt, c->cstr_i, c->cstr_j, c->cstr_r, c->np_start, c->np_end, c->np_charge,
                    c->nbr, c->nnb, c->cell_key, c->cell_key_sorted, c->atom_ids, c->cell_atoms,
                    c->cell_start, c->spos, c->sort_tmp, c->flags, c->cl_atoms, c->cl_cell_start, c->cl_counts,
-                   c->cl_nbr, c->cl_nnb, c->cl_metal, c->cl_of, c->scan_tmp, c->isd, c->vec_ext, c->vec_pq,
+                   c->cl_nbr, c->cl_nnb, c->cl_metal, c->cl_of, c->cl_next, c->scan_tmp, c->isd, c->vec_ext, c->vec_pq,
                    c->diag, c->mat, c->matf, c->msym, c->sympart, c->coop_bp, c->coop_bar, c->g_atoms, c->dinv, c->slot_np, c->np_off, c->np_rows, c->gvec, c->gw, c->em_buf, c->phase_buf, c->rres, c->dcorr, c->xprev, c->bw, c->bwf, c->ss, c->partials, c->pot, c->vir, c->th};
     for (void *p : dev)
         if (p) cudaFree(p);

@@ -183,6 +183,8 @@ struct capac_ctx {
                                        // half list, a metal member)
     bool cl_half = false;              // half list: every pair once, Newton's third law (pair_list 2)
     int *cl_of = nullptr;              // [N] the cluster of each atom (half list)
+    int *cl_next = nullptr;            // the cluster pair kernel's work counter (next cluster to take)
+    int cl_pair_blocks = 0;            // resident blocks of the cluster pair kernel (its grid)
     void *scan_tmp = nullptr;
     size_t scan_tmp_bytes = 0;
 

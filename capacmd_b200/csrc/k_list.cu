@@ -557,7 +557,7 @@ InvBox inv_box(const capac_ctx *c)
 
 bool cluster_list_allowed(const capac_ctx *c)
 {
-    return c->opt.precision == CAPAC_PREC_MIXED && (c->opt.pair_list == 0 || c->opt.pair_list == 2) &&
+    return c->opt.precision == CAPAC_PREC_MIXED && c->opt.pair_list != 1 &&
            c->N < (1 << kClIdxBits) &&
            c->P.n_types <= kClMaxTypes;
 }
@@ -599,8 +599,9 @@ void ensure_cluster_buffers(capac_ctx *c, int n_cells)
         CAPAC_CUDA(cudaMalloc(&c->cl_metal, need));
         c->cl_max = need;
     }
-    c->cl_half = c->opt.pair_list == 2;
+    c->cl_half = c->opt.pair_list != 3;  // 0 (default) and 2: every pair once; 3: the full cluster list
     if (c->cl_half && !c->cl_of) CAPAC_CUDA(cudaMalloc(&c->cl_of, sizeof(int) * N));
+    if (!c->cl_next) CAPAC_CUDA(cudaMalloc(&c->cl_next, sizeof(int)));
 }
 
 // Clusters of the sorted cells; returns false when the largest member offset

@@ -484,7 +484,7 @@ __global__ void __launch_bounds__(kPairWarps * 32, sizeof(Real) == 4 ? 3 : 2) k_
 // full flushes of 32 follow at one site, which keeps the pair terms in the
 // code once.
 //
-// HALF (pair_list 2): the list holds every pair once (k_list.cu), so each
+// HALF (pair_list 0, the default, or 2): the list holds every pair once (k_list.cu), so each
 // survivor's force goes to both ends: the member's slot as above, the
 // neighbour's by FP64 atomic adds, and energies and virial count in full.
 // The CPIM force on a charged water atom from a metal atom is taken from
@@ -503,7 +503,8 @@ __global__ void __launch_bounds__(kClWarps * 32, kClMinBlocks) k_pair_cl(DevPara
                                                               const unsigned char *__restrict__ cl_metal, int cap,
                                                               const double *__restrict__ vec_pq,
                                                               double *__restrict__ fx, double *__restrict__ fy,
-                                                              double *__restrict__ fz, double *__restrict__ partials)
+                                                              double *__restrict__ fz, double *__restrict__ partials,
+                                                              int *__restrict__ next)
 {
     constexpr int NB = 2;
     extern __shared__ __align__(16) unsigned char s_dyn[];  // the warps' queues
@@ -531,8 +532,18 @@ __global__ void __launch_bounds__(kClWarps * 32, kClMinBlocks) k_pair_cl(DevPara
     const double L[3] = {P.box.L[0], P.box.L[1], P.box.L[2]};
     const double iL[3] = {1.0 / L[0], 1.0 / L[1], 1.0 / L[2]};
     const int ncl = *n_cl;
-    const int stride = gridDim.x * kClWarps;
-    for (int cl = blockIdx.x * kClWarps + wib; cl < ncl; cl += stride) {
+    // next (the half list): a resident grid whose warps take the next cluster
+    // from the counter (zeroed before the launch) until none is left, so
+    // list lengths that differ from cluster to cluster leave no warp idle at
+    // the end; else the fixed grid-stride order, which keeps the energy and
+    // virial sums in the same order from run to run
+    for (int k = 0;; ++k) {
+        int cl = blockIdx.x * kClWarps + wib + k * gridDim.x * kClWarps;
+        if (next) {
+            if (lane == 0) cl = atomicAdd(next, 1);
+            cl = __shfl_sync(0xffffffffu, cl, 0);
+        }
+        if (cl >= ncl) break;
         const int4 A = cl_atoms[cl];
         const int nk = 1 + (A.y >= 0) + (A.z >= 0) + (A.w >= 0);
         const int mine = lane == 0 ? A.x : lane == 1 ? A.y : lane == 2 ? A.z : A.w;
@@ -874,9 +885,10 @@ void launch_pair_cl_t(capac_ctx *c, unsigned grid)
     // the queues and the static arrays together exceed the default 48 KB
     CAPAC_CUDA(cudaFuncSetAttribute(k_pair_cl<NONBONDED, CPIM, HALF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)kClQueueBytes));
+    if (HALF) CAPAC_CUDA(cudaMemsetAsync(c->cl_next, 0, sizeof(int), c->stream));
     k_pair_cl<NONBONDED, CPIM, HALF><<<grid, kClWarps * 32, kClQueueBytes, c->stream>>>(
         c->P, pair_consts_f(c), c->pos4, c->cl_atoms, c->cl_cell_start + c->n_cells, c->cl_nbr, c->cl_nnb,
-        c->cl_metal, c->cl_cap, c->vec_pq, c->fx, c->fy, c->fz, c->partials);
+        c->cl_metal, c->cl_cap, c->vec_pq, c->fx, c->fy, c->fz, c->partials, HALF ? c->cl_next : nullptr);
 }
 
 void launch_pair_clusters(capac_ctx *c, int mode, unsigned grid)
@@ -902,13 +914,14 @@ void launch_pair_clusters(capac_ctx *c, int mode, unsigned grid)
 }  // namespace
 
 // Blocks of the pair launch: one warp per atom (or per cluster), at most 16
-// blocks per SM (grid-stride beyond).
+// blocks per SM (grid-stride beyond); on the half cluster list the resident
+// blocks only (its warps take clusters from a counter).
 unsigned pair_grid(const capac_ctx *c)
 {
     const long units = c->clusters ? c->n_clusters : c->N;
     const int warps = c->clusters ? kClWarps : kPairWarps;
     const long need = (units + warps - 1) / warps;
-    const long cap = (long)c->num_sms * 16;
+    const long cap = (long)c->num_sms * (c->clusters && c->cl_half ? kClMinBlocks : 16);
     return (unsigned)std::max(1L, std::min(need, cap));
 }
 

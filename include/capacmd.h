@@ -184,11 +184,13 @@ typedef struct capac_options {
                                solve when the device supports it (default), 1 a launch per vector step */
     int inner_precond;      /* mixed path, persistent solver: preconditioner of the inner solves,
                                0 the reference's Jacobi, 1 block-Jacobi on 32-atom groups (default) */
-    int pair_list;          /* mixed path nonbonded list: 0 clusters of four atoms sharing each
-                               neighbour's load where the box is large enough (default), 1 one list
-                               per atom, 2 clusters with every pair listed once (Newton's third law:
-                               the neighbour's force by FP64 atomic adds, so its summation order
-                               varies from run to run); the FP64 path always uses one list per atom */
+    int pair_list;          /* mixed path nonbonded list: 0 (default) or 2 clusters of four atoms
+                               sharing each neighbour's load, where the box is large enough, with
+                               every pair listed once (Newton's third law: the neighbour's force by
+                               FP64 atomic adds, so its summation order varies from run to run);
+                               3 the same clusters with every pair listed from both ends (fixed
+                               summation order, run-to-run identical); 1 one list per atom; the
+                               FP64 path always uses one list per atom */
     int max_iter;           /* BiCGSTAB iteration limit before the 100x fallback and
                                CAPAC_ERR_NOT_CONVERGED; 0 = the reference's MAX_ITER, 1000
                                (typedef.h:85, bicg_stab.c:546-570) */

@@ -142,13 +142,14 @@ def test_gradients_on_the_cluster_path():
 
 @pytest.mark.parametrize("case", CLUSTER_CASES + ["c2"])
 def test_half_cluster_list(case):
-    """pair_list 2: every pair listed once, by the lower-numbered cluster of
-    its atoms, and applied to both ends.  The pair set is still the
-    reference's; forces, energies and virial agree with the full cluster list
-    within FP32 rounding of the pair terms."""
+    """The default cluster list (pair_list 0, as 2): every pair listed once,
+    by the lower-numbered cluster of its atoms, and applied to both ends.  The
+    pair set is still the reference's; forces, energies and virial agree with
+    the full cluster list (pair_list 3) within FP32 rounding of the pair
+    terms."""
     paths = configs.cached(case) if case == "c2" else golden_paths(case)
-    d, full = _mixed(paths, refine_tol=1e-11)
-    _, half = _mixed(paths, refine_tol=1e-11, pair_list=2)
+    d, full = _mixed(paths, refine_tol=1e-11, pair_list=3)
+    _, half = _mixed(paths, refine_tol=1e-11)
     ref = full.pair_fingerprint(from_list=False)
     if case != "c2":
         g = golden_ref(case)
@@ -169,7 +170,7 @@ def test_half_cluster_list(case):
 
 def test_half_cluster_list_md_through_rebuilds():
     p = configs.cached("c2")
-    d, full = _mixed(p)
+    d, full = _mixed(p, pair_list=3)
     _, half = _mixed(p, pair_list=2)
     for s in (full, half):
         s.md_init()
@@ -184,3 +185,21 @@ def test_half_cluster_list_md_through_rebuilds():
     ef, eh = np.array(ef), np.array(eh)
     assert np.abs(ef - eh).max() <= 1e-5 * np.abs(ef).max()
     assert rel_err(half.get("rx"), full.get("rx")) < 1e-5
+
+
+def test_full_cluster_list_repeats_exactly():
+    """pair_list 3 (every pair from both ends, fixed grid-stride order) gives
+    run-to-run identical forces, energies and virial; the default half list
+    agrees with it within FP32 rounding and does not use more entries."""
+    p = configs.cached("c2")
+    d, a = _mixed(p, pair_list=3)
+    _, b = _mixed(p, pair_list=3)
+    _, h = _mixed(p)
+    for s in (a, b, h):
+        s.set("vec_pq", np.zeros(d.n_mat))
+        s.force()
+    assert np.array_equal(a.forces(), b.forces())
+    assert np.array_equal(a.get("potential"), b.get("potential"))
+    assert np.array_equal(a.get("virial"), b.get("virial"))
+    assert rel_err(h.forces(), a.forces()) < 2e-6
+    assert h.stats().list_entries < a.stats().list_entries
