@@ -359,7 +359,9 @@ def main() -> int:
                        "rel_residual_last": st.solver_rel_residual,
                        "ms_per_solve": (prof["spmv"][1] + prof["solver_vec"][1] + prof["resid"][1]
                                         + prof["solve"][1]) / args.steps,
-                       "layout": "group order" if sim.get("solver_layout")[0] else "reference order"},
+                       "layout": "group order" if sim.get("solver_layout")[0] else "reference order",
+                       "tiles_in_tensor_memory_per_block": int(sim.get("solver_layout")[1]),
+                       "inner_stalls": int(sim.get("inner_stalls")[0])},
             "kernel_ms": {k: v[1] for k, v in prof.items()},
             **({"solver_phase_us": solver_phases(sim)} if args.solver_phases else {}),
             "phase_ms_last_force": {"list": ps[10], "qsc": ps[1], "cpim_vec": ps[6], "cpim_matrix": ps[5],

@@ -583,7 +583,8 @@ int capac_destroy(capac_ctx *c)
                    c->cstr_cnt, c->cstr_i, c->cstr_j, c->cstr_r, c->np_start, c->np_end, c->np_charge,
                    c->nbr, c->nnb, c->cell_key, c->cell_key_sorted, c->atom_ids, c->cell_atoms,
                    c->cell_start, c->spos, c->sort_tmp, c->flags, c->cl_atoms, c->cl_cell_start, c->cl_counts,
-                   c->cl_nbr, c->cl_nnb, c->cl_metal, c->cl_of, c->cl_next, c->scan_tmp, c->isd, c->vec_ext, c->vec_pq,
+                   c->cl_nbr, c->cl_nnb, c->cl_metal, c->cl_of, c->cl_next, c->cp_list,
+                   c->cp_n, c->cp_cent, c->cp_off, c->cp_ti, c->scan_tmp, c->isd, c->vec_ext, c->vec_pq,
                    c->diag, c->mat, c->matf, c->msym, c->sympart, c->coop_bp, c->coop_bar, c->g_atoms, c->dinv, c->slot_np, c->np_off, c->np_rows, c->gvec, c->gw, c->em_buf, c->phase_buf, c->rres, c->dcorr, c->xprev, c->bw, c->bwf, c->ss, c->partials, c->pot, c->vir, c->th};
     for (void *p : dev)
         if (p) cudaFree(p);
@@ -1089,8 +1090,8 @@ int capac_get(capac_ctx *c, const char *name, double *out)
             }
             return;
         }
-        if (n == "pair_list") {  // 1 when the pair kernel walks the cluster list, then the cluster count
-            out[0] = c->clusters ? 1.0 : 0.0;
+        if (n == "pair_list") {  // 1 on the cluster list, 2 on the cluster-pair list, then the cluster count
+            out[0] = c->cpairs ? 2.0 : (c->clusters ? 1.0 : 0.0);
             out[1] = (double)c->n_clusters;
             count = 2;
             return;
@@ -1102,6 +1103,11 @@ int capac_get(capac_ctx *c, const char *name, double *out)
             out[2] = (double)group_blocks_per_sm(c->device, false);
             out[3] = (double)group_blocks_per_sm(c->device, true);
             count = 4;
+            return;
+        }
+        if (n == "inner_stalls") {  // inner solves of the refinement stopped for lack of progress
+            out[0] = (double)c->inner_stalls;
+            count = 1;
             return;
         }
         if (n == "solver_phases") {  // mean ns per iteration of each phase, then the iteration count
@@ -1162,15 +1168,16 @@ int capac_get_stats(capac_ctx *c, capac_stats *out)
         out->solver_rel_residual = c->last_rel_res;
         out->solver_initial_rel_residual = c->last_init_res;
         out->list_builds = c->list_builds;
-        out->list_capacity = c->clusters ? c->cl_cap : c->cap;
+        out->list_capacity = c->cpairs ? c->cp_cap : (c->clusters ? c->cl_cap : c->cap);
         out->md_step = c->md_step;
         if (c->list_valid) {
-            // entries of the list the pair kernel walks: per cluster or per atom
-            const int rows = c->clusters ? c->n_clusters : c->N;
+            // entries of the list the pair kernel walks: per cluster (atoms, or
+            // clusters on the cluster-pair list) or per atom
+            const int rows = c->clusters || c->cpairs ? c->n_clusters : c->N;
             std::vector<int> nn(rows);
             CAPAC_CUDA(cudaStreamSynchronize(c->stream));
-            CAPAC_CUDA(cudaMemcpy(nn.data(), c->clusters ? c->cl_nnb : c->nnb, sizeof(int) * rows,
-                                  cudaMemcpyDeviceToHost));
+            CAPAC_CUDA(cudaMemcpy(nn.data(), c->cpairs ? c->cp_n : (c->clusters ? c->cl_nnb : c->nnb),
+                                  sizeof(int) * rows, cudaMemcpyDeviceToHost));
             long tot = 0, mx = 0;
             for (int v : nn) {
                 tot += v;

@@ -159,7 +159,8 @@ struct capac_ctx {
     void *sort_tmp = nullptr;
     size_t sort_tmp_bytes = 0;
     int *flags = nullptr;      // [0] rebuild needed, [1] list overflow max count, [2] rattle error,
-                               // [4] cluster-list overflow max count, [5] cluster extent (float bits)
+                               // [4] cluster-list overflow max count, [5] cluster extent (float bits),
+                               // [7] cluster-pair list overflow max count
     int *h_flags = nullptr;    // pinned mirror
     bool list_valid = false;
     int cell_sub_bits = 0;     // sub-cell Morton bits below the cell index in cell_key
@@ -184,7 +185,18 @@ struct capac_ctx {
     bool cl_half = false;              // half list: every pair once, Newton's third law (pair_list 2)
     int *cl_of = nullptr;              // [N] the cluster of each atom (half list)
     int *cl_next = nullptr;            // the cluster pair kernel's work counter (next cluster to take)
-    int cl_pair_blocks = 0;            // resident blocks of the cluster pair kernel (its grid)
+
+    // i-cluster x j-cluster list (pair_list 4): per cluster the clusters of
+    // the same or a higher index with a 4 x 4 mask of the member pairs within
+    // the list radius, every pair once (see k_list.cu, k_pair.cu)
+    bool cpairs = false;               // the pair kernel runs on the cluster-pair list (decided at each build)
+    int cp_cap = 0;                    // entries per cluster
+    int cp_max = 0;                    // cluster slots the cluster-pair arrays were sized for
+    uint2 *cp_list = nullptr;          // [cl_max * cp_cap] j-cluster, mask | (either has metal) << 16
+    int *cp_n = nullptr;               // [cl_max] entries of each cluster
+    double4 *cp_cent = nullptr;        // [cl_max] centroid of each cluster (recomputed every step)
+    float4 *cp_off = nullptr;          // [4 cl_max] member offsets from the centroid and charge (every step)
+    int *cp_ti = nullptr;              // [4 cl_max] member atom | type << 24, -1 for an empty slot
     void *scan_tmp = nullptr;
     size_t scan_tmp_bytes = 0;
 
@@ -204,6 +216,8 @@ struct capac_ctx {
     bool grouped = false;
     bool tmem_tiles = false;     // the grouped solver holds part of its tiles in tensor memory
     int group_grid = 0;          // blocks of the grouped solver's launch (<= coop_grid)
+    int inner_stall = 0;         // set during the refinement's inner solves: see GroupArgs::stall
+    long inner_stalls = 0;       // inner solves ended that way
     int *slot_np = nullptr;      // [32 nG] nanoparticle of each group slot's atom, -1 none
     int *np_off = nullptr;       // [n_nps + 1] offsets into np_rows
     int *np_rows = nullptr;      // [M] internal charge rows of each nanoparticle's atoms
@@ -256,6 +270,8 @@ void cuda_check(cudaError_t e, const char *what);
 
 // Kernel launchers (one stream; every launch is counted).
 void launch_pack_positions(capac_ctx *c);
+// cluster centroids and member offsets (pair_list 4); statics: atoms, types, metal flags too
+void launch_cluster_frames(capac_ctx *c, bool statics);
 void launch_list_maintenance(capac_ctx *c, bool force_rebuild);
 // Rebuild the lists with an atom-list row for every atom, now and at every
 // later build (the gradient kernels walk all rows).

@@ -119,6 +119,11 @@ __host__ __device__ __forceinline__ int nb_type(uint32_t e) { return (int)(e >> 
 constexpr int kClIdxBits = 22, kClMaskShift = 22, kClTypeShift = 26;
 constexpr uint32_t kClIdxMask = (1u << kClIdxBits) - 1u;
 constexpr int kClMaxTypes = 64;
+// cluster-pair list: a member slot holds atom | type << kCpTypeShift; an
+// entry's second word the 16-bit member-pair mask and kCpMetalBit
+constexpr int kCpTypeShift = 24;
+constexpr int kCpIdxMask = (1 << kCpTypeShift) - 1;
+constexpr uint32_t kCpMetalBit = 1u << 16;
 __host__ __device__ __forceinline__ uint32_t pack_cl(int j, unsigned mask, int t)
 {
     return (uint32_t)j | (mask << kClMaskShift) | ((uint32_t)t << kClTypeShift);

@@ -790,6 +790,9 @@ int run_bicgstab(capac_ctx *c)
 // updates x += d, until |r| <= refine_tol |b|.  The reference's zero-field
 // early exit (bTb < 1e-10) is kept.
 constexpr double kInnerReduction = 1.0e-5;
+// an inner solve whose (r, r) has not halved for this many iterations stops
+// and returns its iterate to the refinement
+constexpr int kInnerStall = 60;
 int run_refined_solve(capac_ctx *c)
 {
     const int n = c->n_mat;
@@ -832,8 +835,15 @@ int run_refined_solve(capac_ctx *c)
         // left to the target with a margin of 3
         const double need = 0.3 * rtol * sqrt(bTb / rr);
         const double tau = std::min(std::max(need, kInnerReduction), 0.1);
+        struct StallGuard {  // the guard applies to this inner solve only
+            capac_ctx *c;
+            ~StallGuard() { c->inner_stall = 0; }
+        } guard{c};
+        c->inner_stall = kInnerStall;
         const int st = bicgstab_core(c, c->rres, c->dcorr, tau * tau, 1.0e-300);
+        c->inner_stall = 0;
         total += c->h_ss->iter;
+        if (st == 1 && c->h_ss->rTr >= c->h_ss->crit) ++c->inner_stalls;
         if (st < 0 && c->h_ss->iter == 0) break;  // no progress possible
         k_axpy1<<<nbv, 256, 0, s>>>(n, c->dcorr, c->vec_pq);
         ++c->launches;

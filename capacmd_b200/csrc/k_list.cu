@@ -439,6 +439,200 @@ __global__ void k_fingerprint_clusters(DevParams P, const double *__restrict__ r
     }
 }
 
+// ------------------------------------------------------------ cluster pairs
+//
+// pair_list 4: the clusters above, paired.  Before each pair launch
+// k_cluster_frames writes every cluster's centroid (FP64: the first member
+// plus the mean of the members' minimum images from it) and its members'
+// offsets from the centroid (FP32) with their charges; at a build also each
+// member's atom and type.  The list of cluster I holds every cluster J >= I
+// of the 5 x 5 x 5 cell window with at least one member pair (a in I, b in
+// J; for J = I only b after a) that is not excluded and lies within the list
+// radius (widened by 1e-5 relative) in FP32, measured as the FP64 minimum
+// image of the centroid difference, rounded once, plus the two offsets: a
+// 16-bit mask, bit 4 k + m for member k of I with member m of J.  The pair
+// kernel applies the cut-off to the masked pairs every step.  That composite
+// difference is the pair's minimum image while rc + 2 (largest offset
+// component) < half the shortest box edge; offsets grow by at most the skin
+// between builds, so each build checks rc + skin + 2 (largest offset at the
+// build + skin) < half the edge and otherwise falls back to the cluster list.
+
+// Centroids and member offsets of every cluster; with `statics` also the
+// member atoms and types and whether the cluster has a metal member.
+__global__ void k_cluster_frames(int ncl, const int4 *__restrict__ cl_atoms, const double *__restrict__ rx,
+                                 const double *__restrict__ ry, const double *__restrict__ rz,
+                                 const double *__restrict__ charge, InvBox B, double4 *__restrict__ cent,
+                                 float4 *__restrict__ off, int statics, const int *__restrict__ type,
+                                 const unsigned char *__restrict__ is_metal, int *__restrict__ ti,
+                                 unsigned char *__restrict__ cl_metal)
+{
+    const int cl = blockIdx.x * blockDim.x + threadIdx.x;
+    if (cl >= ncl) return;
+    const int4 A = cl_atoms[cl];
+    const int m[4] = {A.x, A.y, A.z, A.w};
+    double o[4][3], cc[3];
+    const int nk = cluster_offsets(m, rx, ry, rz, B, o, cc);
+    cent[cl] = make_double4(cc[0], cc[1], cc[2], 0.0);
+    bool metal = false;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const bool in = k < nk;
+        off[4 * cl + k] = in ? make_float4((float)o[k][0], (float)o[k][1], (float)o[k][2], (float)charge[m[k]])
+                             : make_float4(0.f, 0.f, 0.f, 0.f);
+        if (statics) {
+            ti[4 * cl + k] = in ? (m[k] | (type[m[k]] << kCpTypeShift)) : -1;
+            metal |= in && is_metal[m[k]] != 0;
+        }
+    }
+    if (statics) cl_metal[cl] = metal ? 1 : 0;
+}
+
+// One warp per cluster I: its cluster-pair list (see above).  Lanes take the
+// window's clusters J >= I in turn; each computes the 16 member distances.
+__global__ void __launch_bounds__(256) k_build_cpair_list(DevParams P, Grid g, InvBox B, int ncl,
+                                                          const double4 *__restrict__ cent,
+                                                          const float4 *__restrict__ off,
+                                                          const int *__restrict__ ti,
+                                                          const unsigned char *__restrict__ cl_metal,
+                                                          const int *__restrict__ cl_cell_start, int cap,
+                                                          uint2 *__restrict__ list, int *__restrict__ cnt,
+                                                          int *flags, const double *__restrict__ rx,
+                                                          const double *__restrict__ ry,
+                                                          const double *__restrict__ rz, double *rx0, double *ry0,
+                                                          double *rz0)
+{
+    const int ic = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (ic >= ncl) return;
+    const double4 ci = cent[ic];
+    float oix[4], oiy[4], oiz[4];
+    int ai[4];
+    float Ri = 0.f;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const float4 o = off[4 * ic + k];
+        const int t = ti[4 * ic + k];
+        ai[k] = t < 0 ? -1 : (t & kCpIdxMask);
+        oix[k] = o.x;
+        oiy[k] = o.y;
+        oiz[k] = o.z;
+        if (t >= 0) Ri = fmaxf(Ri, sqrtf(o.x * o.x + o.y * o.y + o.z * o.z));
+    }
+    const bool metal_i = cl_metal[ic] != 0;
+    const double rl = sqrt(P.list_r2);
+    const float lr2f = (float)(P.list_r2 * (1.0 + 1e-5));
+    const int a0 = ai[0];
+    const int c0[3] = {cell_coord(rx[a0], P.box.L[0], g.inv_len[0], g.n[0]),
+                       cell_coord(ry[a0], P.box.L[1], g.inv_len[1], g.n[1]),
+                       cell_coord(rz[a0], P.box.L[2], g.inv_len[2], g.n[2])};
+    const int nxs = axis_count(g.n[0]), nys = axis_count(g.n[1]);
+    const int nz = g.n[2];
+    const ZRuns zr = z_runs(c0[2], nz);
+    const unsigned lt_mask = (1u << lane) - 1u;
+    uint2 *row = list + (size_t)ic * cap;
+    int count = 0;
+    for (int ix = 0; ix < nxs; ++ix) {
+        for (int iy = 0; iy < nys; ++iy) {
+            const int col = (axis_cell(c0[0], g.n[0], ix) * g.n[1] + axis_cell(c0[1], g.n[1], iy)) * nz;
+            for (int r = 0; r < zr.n; ++r) {
+                const int s = max(cl_cell_start[col + zr.a[r]], ic), e = cl_cell_start[col + zr.b[r] + 1];
+                for (int base = s; base < e; base += 32) {
+                    const int jc = base + lane;
+                    unsigned mask = 0;
+                    if (jc < e) {
+                        const double4 cj = cent[jc];
+                        const double dx = min_image(cj.x - ci.x, B.L[0], B.inv[0]);
+                        const double dy = min_image(cj.y - ci.y, B.L[1], B.inv[1]);
+                        const double dz = min_image(cj.z - ci.z, B.L[2], B.inv[2]);
+                        float ojx[4], ojy[4], ojz[4];
+                        int aj[4];
+                        float Rj = 0.f;
+#pragma unroll
+                        for (int m = 0; m < 4; ++m) {
+                            const float4 o = off[4 * jc + m];
+                            const int t = ti[4 * jc + m];
+                            aj[m] = t < 0 ? -1 : (t & kCpIdxMask);
+                            ojx[m] = o.x;
+                            ojy[m] = o.y;
+                            ojz[m] = o.z;
+                            if (t >= 0) Rj = fmaxf(Rj, sqrtf(o.x * o.x + o.y * o.y + o.z * o.z));
+                        }
+                        // centroid prefilter, widened against rounding
+                        const double pre = (rl + (double)Ri + (double)Rj) * (1.0 + 1e-6);
+                        if (dx * dx + dy * dy + dz * dz < pre * pre) {
+                            const float fx = (float)dx, fy = (float)dy, fz = (float)dz;
+#pragma unroll
+                            for (int k = 0; k < 4; ++k) {
+#pragma unroll
+                                for (int m = 0; m < 4; ++m) {
+                                    if (ai[k] < 0 || aj[m] < 0 || (jc == ic && m <= k)) continue;
+                                    const float sx = fx + (ojx[m] - oix[k]), sy = fy + (ojy[m] - oiy[k]),
+                                                sz = fz + (ojz[m] - oiz[k]);
+                                    if (fmaf(sz, sz, fmaf(sy, sy, sx * sx)) < lr2f && !excluded(P, ai[k], aj[m]))
+                                        mask |= 1u << (4 * k + m);
+                                }
+                            }
+                        }
+                    }
+                    const bool ok = mask != 0;
+                    const unsigned ballot = __ballot_sync(0xffffffffu, ok);
+                    const int pos = count + __popc(ballot & lt_mask);
+                    if (ok && pos < cap)
+                        row[pos] = make_uint2((uint32_t)jc, mask | ((metal_i || cl_metal[jc] != 0) ? kCpMetalBit : 0u));
+                    count += __popc(ballot);
+                }
+            }
+        }
+    }
+    if (lane == 0) {
+        cnt[ic] = count < cap ? count : cap;
+        if (count > cap) atomicMax(&flags[7], count);
+    }
+    if (lane < 4 && ai[lane] >= 0) {  // displacement reference of the members
+        const int a = ai[lane];
+        rx0[a] = rx[a];
+        ry0[a] = ry[a];
+        rz0[a] = rz[a];
+    }
+}
+
+// Pair-set fingerprint over the cluster-pair list: every masked member pair
+// inside the cut-off, oriented as the reference orients it.
+__global__ void k_fingerprint_cpairs(DevParams P, const double *__restrict__ rx, const double *__restrict__ ry,
+                                     const double *__restrict__ rz, int ncl, const int *__restrict__ ti,
+                                     const uint2 *__restrict__ list, const int *__restrict__ cnt, int cap,
+                                     unsigned long long *out)
+{
+    const int ic = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (ic >= ncl) return;
+    unsigned long long n = 0, h = 0;
+    for (int q = lane; q < cnt[ic]; q += 32) {
+        const uint2 e = list[(size_t)ic * cap + q];
+        const int jc = (int)e.x;
+        for (int b = 0; b < 16; ++b) {
+            if (!((e.y >> b) & 1u)) continue;
+            const int a = ti[4 * ic + (b >> 2)] & kCpIdxMask, c = ti[4 * jc + (b & 3)] & kCpIdxMask;
+            const int i = max(a, c), j = min(a, c);
+            double dx = rx[j] - rx[i], dy = ry[j] - ry[i], dz = rz[j] - rz[i];
+            image(dx, dy, dz, P.box);
+            if (norm2_exact(dx, dy, dz) < P.rc2) {
+                ++n;
+                h += mix64(((uint64_t)(uint32_t)i << 32) | (uint32_t)j);
+            }
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        n += __shfl_xor_sync(0xffffffffu, n, o);
+        h += __shfl_xor_sync(0xffffffffu, h, o);
+    }
+    if (lane == 0 && n) {
+        atomicAdd(&out[0], n);
+        atomicAdd(&out[1], h);
+    }
+}
+
 __global__ void k_displacement(int N, Box box, double half_skin2, const double *__restrict__ rx,
                                const double *__restrict__ ry, const double *__restrict__ rz,
                                const double *__restrict__ rx0, const double *__restrict__ ry0,
@@ -663,6 +857,77 @@ void build_cluster_list(capac_ctx *c, const Grid &g, int n_cells)
     }
 }
 
+// Cluster-pair arrays for the current cluster slots; the first per-cluster
+// capacity from the densest plausible environment (radius rc + skin + 0.6 nm,
+// clusters of four, each pair once).
+void ensure_cpair_buffers(capac_ctx *c)
+{
+    if (c->cp_max != c->cl_max || !c->cp_cent) {
+        cudaFree(c->cp_cent);
+        cudaFree(c->cp_off);
+        cudaFree(c->cp_ti);
+        cudaFree(c->cp_n);
+        cudaFree(c->cp_list);
+        c->cp_cent = nullptr;
+        c->cp_off = nullptr;
+        c->cp_ti = nullptr;
+        c->cp_n = nullptr;
+        c->cp_list = nullptr;
+        if (c->cp_cap == 0) {
+            const double V = c->P.box.L[0] * c->P.box.L[1] * c->P.box.L[2];
+            const double rl = c->P.rc + c->opt.skin + 0.6;
+            const double dens = std::max((double)c->N / V, 60.0);
+            long est = (long)(1.3 * dens * 4.0 / 3.0 * M_PI * rl * rl * rl / 8.0) + 64;
+            est = std::min<long>(est, (long)c->cl_max);
+            c->cp_cap = (int)((est + 31) & ~31L);
+        }
+        CAPAC_CUDA(cudaMalloc(&c->cp_cent, sizeof(double4) * c->cl_max));
+        CAPAC_CUDA(cudaMalloc(&c->cp_off, sizeof(float4) * 4 * (size_t)c->cl_max));
+        CAPAC_CUDA(cudaMalloc(&c->cp_ti, sizeof(int) * 4 * (size_t)c->cl_max));
+        CAPAC_CUDA(cudaMalloc(&c->cp_n, sizeof(int) * c->cl_max));
+        CAPAC_CUDA(cudaMalloc(&c->cp_list, sizeof(uint2) * (size_t)c->cl_max * c->cp_cap));
+        c->cp_max = c->cl_max;
+    }
+}
+
+// The cluster-pair list is usable while the composite minimum image holds
+// (see the comment above k_cluster_frames); ext is the largest member offset
+// component of the clusters just made.
+bool cpair_list_allowed(const capac_ctx *c, double ext)
+{
+    const double half = 0.5 * std::min(c->P.box.L[0], std::min(c->P.box.L[1], c->P.box.L[2]));
+    return c->opt.pair_list == 4 && c->P.rc + c->opt.skin + 2.0 * (ext + c->opt.skin) < half;
+}
+
+void build_cpair_list(capac_ctx *c, const Grid &g)
+{
+    cudaStream_t s = c->stream;
+    ensure_cpair_buffers(c);
+    launch_cluster_frames(c, true);
+    const int *cs = c->cl_cell_start;
+    for (int attempt = 0; attempt < 4; ++attempt) {
+        CAPAC_CUDA(cudaMemsetAsync(c->flags + 7, 0, sizeof(int), s));
+        {
+            ProfScope ps(c, K_LIST);
+            k_build_cpair_list<<<grid_for((long)c->n_clusters * 32, 256), 256, 0, s>>>(
+                c->P, g, inv_box(c), c->n_clusters, c->cp_cent, c->cp_off, c->cp_ti, c->cl_metal, cs, c->cp_cap,
+                c->cp_list, c->cp_n, c->flags, c->rx, c->ry, c->rz, c->rx0, c->ry0, c->rz0);
+        }
+        ++c->launches;
+        CAPAC_CUDA(cudaMemcpyAsync(c->h_flags + 7, c->flags + 7, sizeof(int), cudaMemcpyDeviceToHost, s));
+        CAPAC_CUDA(cudaStreamSynchronize(s));
+        const int need_cap = c->h_flags[7];
+        if (need_cap <= c->cp_cap) return;
+        if (attempt == 3) throw Error(CAPAC_ERR_CAPACITY, "cluster-pair list capacity could not be met");
+        int new_cap = (int)std::min<long>((long)(need_cap * 1.25) + 32, 1L << 20);
+        new_cap = (new_cap + 31) & ~31;
+        cudaFree(c->cp_list);
+        c->cp_list = nullptr;
+        CAPAC_CUDA(cudaMalloc(&c->cp_list, sizeof(uint2) * (size_t)c->cl_max * new_cap));
+        c->cp_cap = new_cap;
+    }
+}
+
 // Atom-list rows i0 .. i0 + rows - 1, growing the per-atom capacity as needed.
 void build_atom_rows(capac_ctx *c, const Grid &g, int i0, int rows)
 {
@@ -729,20 +994,35 @@ void build_list(capac_ctx *c)
     c->launches += 2;
 
     bool use_cl = cluster_list_allowed(c) && make_clusters(c, n_cells);
-    if (use_cl) build_cluster_list(c, g, n_cells);
+    float ext = 0.f;
+    memcpy(&ext, &c->h_flags[5], sizeof ext);  // written by make_clusters
+    const bool use_cp = use_cl && cpair_list_allowed(c, (double)ext);
+    if (use_cp)
+        build_cpair_list(c, g);
+    else if (use_cl)
+        build_cluster_list(c, g, n_cells);
     // atom-list rows: every atom on the atom path or when asked for, else
     // the metal atoms (the CPIM kernels walk their rows)
     if (!use_cl || c->need_full_list)
         build_atom_rows(c, g, 0, N);
     else if (c->M > 0)
         build_atom_rows(c, g, c->metal_min, c->M);
-    c->clusters = use_cl;
+    c->clusters = use_cl && !use_cp;
+    c->cpairs = use_cp;
     c->atom_list_full = !use_cl || c->need_full_list;
     c->list_valid = true;
     ++c->list_builds;
 }
 
 }  // namespace
+
+void launch_cluster_frames(capac_ctx *c, bool statics)
+{
+    k_cluster_frames<<<grid_for(c->n_clusters, 128), 128, 0, c->stream>>>(
+        c->n_clusters, c->cl_atoms, c->rx, c->ry, c->rz, c->charge, inv_box(c), c->cp_cent, c->cp_off,
+        statics ? 1 : 0, c->type, c->is_metal, c->cp_ti, c->cl_metal);
+    ++c->launches;
+}
 
 void launch_pack_positions(capac_ctx *c)
 {
@@ -779,7 +1059,10 @@ void launch_pair_fingerprint(capac_ctx *c, int from_list, long *count, unsigned 
     CAPAC_CUDA(cudaMemsetAsync(d, 0, 2 * sizeof(unsigned long long), c->stream));
     if (from_list) {
         launch_list_maintenance(c, false);
-        if (c->clusters)
+        if (c->cpairs)
+            k_fingerprint_cpairs<<<grid_for((long)c->n_clusters * 32, 256), 256, 0, c->stream>>>(
+                c->P, c->rx, c->ry, c->rz, c->n_clusters, c->cp_ti, c->cp_list, c->cp_n, c->cp_cap, d);
+        else if (c->clusters)
             k_fingerprint_clusters<<<grid_for((long)c->n_clusters * 32, 256), 256, 0, c->stream>>>(
                 c->P, c->rx, c->ry, c->rz, c->cl_atoms, c->cl_cell_start + c->n_cells, c->cl_nbr, c->cl_nnb,
                 c->cl_cap, c->cl_half ? 1 : 0, d);

@@ -843,6 +843,183 @@ __global__ void __launch_bounds__(kClWarps * 32, kClMinBlocks) k_pair_cl(DevPara
     }
 }
 
+// Mixed path on the cluster-pair list (pair_list 4, k_list.cu): one warp per
+// cluster I at a time (taken from a counter, as on the half cluster list),
+// two entries (clusters J) per step.  Lane l works on member k = l & 3 of I
+// with member m = (l >> 2) & 3 of entry h = l >> 4: the 32 lanes cover the
+// 2 x 16 member pairs with no compaction, and a pair that is masked at the
+// build or outside the cut-off now contributes nothing.  I's member stays in
+// the lane's registers for the whole list; each step a lane loads J's
+// centroid, its member's offset and charge, and its atom and type (the four
+// lanes of one J member read the same addresses).  The pair difference is
+// the FP64 minimum image of the centroid difference, rounded once, plus the
+// FP32 offsets; the FP32 cut-off decides the pair as in k_pair.  Each pair
+// counts once: the force on I's member accumulates in FP64 in the lane (the
+// eight lanes of a member summed at the end, then added with FP64 atomic
+// adds, since other clusters add to the same atom), the force on J's member
+// is summed over its four lanes by shuffles and added with FP64 atomic adds;
+// pair energies are summed per lane in FP64, the virial per lane in FP32 per
+// cluster.  CPIM: on entries where either cluster has a metal member, the
+// CPIM force on a charged non-metal atom from a metal atom of the pair,
+// whichever end holds the metal.
+constexpr int kCpWarps = 8;
+constexpr int kCpMinBlocks = 2;
+template <bool NONBONDED, bool CPIM>
+__global__ void __launch_bounds__(kCpWarps * 32, kCpMinBlocks)
+    k_pair_cp(DevParams P, PairConstsF K, const double4 *__restrict__ cent, const float4 *__restrict__ off,
+              const int *__restrict__ ti, const uint2 *__restrict__ list, const int *__restrict__ cnt, int cap,
+              int ncl, const double *__restrict__ vec_pq, double *__restrict__ fx, double *__restrict__ fy,
+              double *__restrict__ fz, double *__restrict__ partials, int *__restrict__ next)
+{
+    __shared__ double sh[32 * 11];
+    __shared__ double wacc[kCpWarps][8];
+    __shared__ __align__(16) TypePairF s_tpf[kSmemTypes * kSmemTypes];
+    __shared__ unsigned char s_metal[kSmemTypes];
+    const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int ki = lane & 3, mj = (lane >> 2) & 3, h = lane >> 4;
+    if (lane < 8) wacc[wib][lane] = 0.0;
+    const bool smem_types = P.n_types <= kSmemTypes;
+    if (smem_types) {
+        const int nt2 = P.n_types * P.n_types;
+        for (int k = threadIdx.x; k < nt2; k += blockDim.x) s_tpf[k] = make_type_pair_f(P, K, k);
+        for (int k = threadIdx.x; k < P.n_types; k += blockDim.x) s_metal[k] = P.type_metal[k];
+    }
+    __syncthreads();
+    const bool metal_by_type = smem_types && P.metal_by_type;
+    const double L[3] = {P.box.L[0], P.box.L[1], P.box.L[2]};
+    const double iL[3] = {1.0 / L[0], 1.0 / L[1], 1.0 / L[2]};
+    for (;;) {
+        int ic = 0;
+        if (lane == 0) ic = atomicAdd(next, 1);
+        ic = __shfl_sync(0xffffffffu, ic, 0);
+        if (ic >= ncl) break;
+        const double4 ci = cent[ic];
+        const float4 oi = off[4 * ic + ki];
+        const int tii = ti[4 * ic + ki];
+        const bool vi = tii >= 0;
+        const int ai = tii & kCpIdxMask;
+        const int tyi = vi ? (tii >> kCpTypeShift) : 0;
+        const int trow = tyi * P.n_types;
+        const bool metal_i = vi && (metal_by_type ? s_metal[tyi] != 0 : P.is_metal[ai] != 0);
+        const int mi = metal_i ? ai - P.metal_min : 0;
+        const bool water_i = CPIM && vi && !metal_i && oi.w != 0.f;  // takes the CPIM force of metal atoms
+        double fix = 0.0, fiy = 0.0, fiz = 0.0, e_qq = 0.0, e_vdw = 0.0;
+        float v[6];
+#pragma unroll
+        for (int q = 0; q < 6; ++q) v[q] = 0.f;
+        const int n = cnt[ic];
+        const uint2 *row = list + (size_t)ic * cap;
+        for (int q0 = 0; q0 < n; q0 += 2) {
+            const int q = q0 + h;
+            const bool ve = q < n;
+            const uint2 e = ve ? row[q] : make_uint2((uint32_t)ic, 0u);
+            const int jc = (int)e.x;
+            const double4 cj = cent[jc];
+            const float4 oj = off[4 * jc + mj];
+            const int tij = ti[4 * jc + mj];
+            const float dcx = (float)min_image(cj.x - ci.x, L[0], iL[0]);
+            const float dcy = (float)min_image(cj.y - ci.y, L[1], iL[1]);
+            const float dcz = (float)min_image(cj.z - ci.z, L[2], iL[2]);
+            const float dx = dcx + (oj.x - oi.x), dy = dcy + (oj.y - oi.y), dz = dcz + (oj.z - oi.z);
+            const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+            const bool act = ((e.y >> (4 * ki + mj)) & 1u) && r2 < K.rc2;
+            float gx = 0.f, gy = 0.f, gz = 0.f;  // force on I's member
+            float hx = 0.f, hy = 0.f, hz = 0.f;  // force on J's member
+            if (act) {
+                const int aj = tij & kCpIdxMask, tyj = tij >> kCpTypeShift;
+                if (NONBONDED) {
+                    const int tp = trow + tyj;
+                    float eq = 0.f, ev = 0.f;
+                    const float f = pair_term_f(K, smem_types ? s_tpf[tp] : make_type_pair_f(P, K, tp), oi.w, oj.w,
+                                                r2, eq, ev);
+                    e_qq += (double)eq;
+                    e_vdw += (double)ev;
+                    hx = f * dx;
+                    hy = f * dy;
+                    hz = f * dz;
+                    gx = -hx;
+                    gy = -hy;
+                    gz = -hz;
+                    v[0] -= dx * hx; v[1] -= dx * hy; v[2] -= dx * hz;
+                    v[3] -= dy * hy; v[4] -= dy * hz; v[5] -= dz * hz;
+                }
+                if (CPIM && (e.y & kCpMetalBit)) {
+                    const bool metal_j = metal_by_type ? s_metal[tyj] != 0 : P.is_metal[aj] != 0;
+                    if (water_i && metal_j) {
+                        const int jm = aj - P.metal_min;
+                        const float r[3] = {dx, dy, dz};  // metal - atom
+                        const float p[3] = {(float)vec_pq[3 * jm], (float)vec_pq[3 * jm + 1], (float)vec_pq[3 * jm + 2]};
+                        float g[3];
+                        cpim_charge_pair_f(K, r, r2, oi.w, (float)vec_pq[3 * P.M + jm], p, g);
+                        gx -= g[0];
+                        gy -= g[1];
+                        gz -= g[2];
+                    } else if (metal_i && !metal_j && oj.w != 0.f) {
+                        const float r[3] = {-dx, -dy, -dz};  // metal - atom
+                        const float p[3] = {(float)vec_pq[3 * mi], (float)vec_pq[3 * mi + 1], (float)vec_pq[3 * mi + 2]};
+                        float g[3];
+                        cpim_charge_pair_f(K, r, r2, oj.w, (float)vec_pq[3 * P.M + mi], p, g);
+                        hx -= g[0];
+                        hy -= g[1];
+                        hz -= g[2];
+                    }
+                }
+            }
+            fix += (double)gx;
+            fiy += (double)gy;
+            fiz += (double)gz;
+            // J's member: the four lanes of (h, m) summed, added by the first
+#pragma unroll
+            for (int o = 1; o <= 2; o <<= 1) {
+                hx += __shfl_xor_sync(0xffffffffu, hx, o);
+                hy += __shfl_xor_sync(0xffffffffu, hy, o);
+                hz += __shfl_xor_sync(0xffffffffu, hz, o);
+            }
+            if (ki == 0 && (hx != 0.f || hy != 0.f || hz != 0.f)) {
+                const int aj = tij & kCpIdxMask;
+                atomicAdd(fx + aj, (double)hx);
+                atomicAdd(fy + aj, (double)hy);
+                atomicAdd(fz + aj, (double)hz);
+            }
+        }
+        // I's member: its eight lanes summed in a fixed order
+#pragma unroll
+        for (int o = 4; o < 32; o <<= 1) {
+            fix += __shfl_xor_sync(0xffffffffu, fix, o);
+            fiy += __shfl_xor_sync(0xffffffffu, fiy, o);
+            fiz += __shfl_xor_sync(0xffffffffu, fiz, o);
+        }
+        if (lane < 4 && vi && (fix != 0.0 || fiy != 0.0 || fiz != 0.0)) {
+            atomicAdd(fx + ai, fix);
+            atomicAdd(fy + ai, fiy);
+            atomicAdd(fz + ai, fiz);
+        }
+        if (NONBONDED) {
+            const double t[8] = {warp_sum(e_qq), warp_sum(e_vdw), warp_sum((double)v[0]),
+                                 warp_sum((double)v[1]), warp_sum((double)v[2]), warp_sum((double)v[3]),
+                                 warp_sum((double)v[4]), warp_sum((double)v[5])};
+            if (lane == 0) {
+#pragma unroll
+                for (int q = 0; q < 8; ++q) wacc[wib][q] += t[q];
+            }
+        }
+        __syncwarp();
+    }
+    if (NONBONDED) {
+        __syncthreads();
+        double acc[11] = {0.0};
+        if (threadIdx.x < kCpWarps) {
+            const double *w = wacc[threadIdx.x];
+            acc[0] = w[0];
+            acc[1] = w[1];
+            acc[2] = w[2]; acc[3] = w[3]; acc[4] = w[4];
+            acc[5] = w[3]; acc[6] = w[5]; acc[7] = w[6];
+            acc[8] = w[4]; acc[9] = w[6]; acc[10] = w[7];
+        }
+        block_partials<11>(acc, sh, partials);
+    }
+}
+
 PairConstsF pair_consts_f(const capac_ctx *c)
 {
     PairConstsF K;
@@ -891,6 +1068,30 @@ void launch_pair_cl_t(capac_ctx *c, unsigned grid)
         c->cl_metal, c->cl_cap, c->vec_pq, c->fx, c->fy, c->fz, c->partials, HALF ? c->cl_next : nullptr);
 }
 
+template <bool NONBONDED, bool CPIM>
+void launch_pair_cp_t(capac_ctx *c, unsigned grid)
+{
+    CAPAC_CUDA(cudaMemsetAsync(c->cl_next, 0, sizeof(int), c->stream));
+    k_pair_cp<NONBONDED, CPIM><<<grid, kCpWarps * 32, 0, c->stream>>>(
+        c->P, pair_consts_f(c), c->cp_cent, c->cp_off, c->cp_ti, c->cp_list, c->cp_n, c->cp_cap, c->n_clusters,
+        c->vec_pq, c->fx, c->fy, c->fz, c->partials, c->cl_next);
+}
+
+// The cluster frames of the current positions, then the cluster-pair kernel.
+void launch_pair_cpairs(capac_ctx *c, int mode, unsigned grid)
+{
+    const bool cpim = c->M > 0 && c->use_cpff;
+    ProfScope ps(c, K_PAIR);
+    launch_cluster_frames(c, false);
+    if (mode == 0 && cpim)
+        launch_pair_cp_t<true, true>(c, grid);
+    else if (mode == 0)
+        launch_pair_cp_t<true, false>(c, grid);
+    else
+        launch_pair_cp_t<false, true>(c, grid);
+    ++c->launches;
+}
+
 void launch_pair_clusters(capac_ctx *c, int mode, unsigned grid)
 {
     const bool cpim = c->M > 0 && c->use_cpff;
@@ -918,6 +1119,7 @@ void launch_pair_clusters(capac_ctx *c, int mode, unsigned grid)
 // blocks only (its warps take clusters from a counter).
 unsigned pair_grid(const capac_ctx *c)
 {
+    if (c->cpairs) return (unsigned)c->num_sms * kCpMinBlocks;
     const long units = c->clusters ? c->n_clusters : c->N;
     const int warps = c->clusters ? kClWarps : kPairWarps;
     const long need = (units + warps - 1) / warps;
@@ -928,7 +1130,9 @@ unsigned pair_grid(const capac_ctx *c)
 void launch_pair_forces(capac_ctx *c, int mode)
 {
     const unsigned grid = pair_grid(c);
-    if (c->clusters)
+    if (c->cpairs)
+        launch_pair_cpairs(c, mode, grid);
+    else if (c->clusters)
         launch_pair_clusters(c, mode, grid);
     else if (c->opt.precision == CAPAC_PREC_MIXED)
         launch_pair_t<float>(c, mode, grid);

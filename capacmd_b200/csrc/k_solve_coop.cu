@@ -954,6 +954,7 @@ size_t dyn_smem_bytes()
 // at the start and written back at the end.
 struct GroupArgs {
     int M, nG, ntiles, n_nps, ni, max_iter;
+    int stall;                   // > 0: stop (status 1) after this many iterations without halving (r, r)
     long spin_limit;
     double inv_polar, inv_capac;
     const int *g_atoms;          // [32 nG] metal-local atom of each slot, -1 padding
@@ -1348,6 +1349,8 @@ __global__ void __maxnreg__(120) k_bicgstab_group(GroupArgs A)
     PassScalars S{0.0, 0.0, 0.0, 0, 1};
     int iter = 0, status = 0;
     double bTb = 0.0, crit = 0.0, rTr = 0.0, rr0 = 0.0;
+    double ref_rTr = 0.0;  // (r, r) when it last halved
+    int last_gain = 0;
     bool ok = true;
 
     // start: bTb, x gathered into the internal order (counting its non-zero
@@ -1389,6 +1392,7 @@ __global__ void __maxnreg__(120) k_bicgstab_group(GroupArgs A)
         double t1[1];
         sum_bp<1>(bpB, nb, t1);
         rho = rTr = rr0 = t1[0];
+        ref_rTr = rTr;
         if (rho < A.skip) done = true;  // warm start already converged (bicg_stab.c:368)
     }
     bool pending = false;
@@ -1449,6 +1453,17 @@ __global__ void __maxnreg__(120) k_bicgstab_group(GroupArgs A)
         } else if (iter > A.max_iter) {
             status = rTr < crit * 100.0 ? 1 : -1;
             done = true;
+        } else if (A.stall > 0) {
+            // an inner solve of the refinement that has stopped making
+            // progress (FP32 products limit what it can reach) hands its
+            // iterate back; the FP64 residual decides what follows
+            if (rTr < 0.5 * ref_rTr) {
+                ref_rTr = rTr;
+                last_gain = iter;
+            } else if (iter - last_gain >= A.stall) {
+                status = 1;
+                done = true;
+            }
         }
     }
     if (ok) {
@@ -1615,6 +1630,7 @@ int bicgstab_group(capac_ctx *c, const double *b, double *x, double tol, double 
     A.n_nps = c->n_nps;
     A.ni = (int)group_rows(c->M, c->n_nps);
     A.max_iter = solver_max_iter(c);
+    A.stall = c->inner_stall;
     A.spin_limit = c->opt.wait_polls > 0 ? c->opt.wait_polls : kSpinLimit;
     A.inv_polar = c->P.inv_polar;
     A.inv_capac = c->P.inv_capac;

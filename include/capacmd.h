@@ -346,6 +346,9 @@ int capac_checkpoint_load(capac_ctx *ctx, const char *path);
  * tiles each of its blocks holds in tensor memory for the whole solve, 0 when
  * all are streamed from HBM each pass; the resident blocks per SM of the
  * group-ordered solver without and with tiles in tensor memory),
+ * inner_stalls(1: inner solves of the mixed path's refinement that stopped
+ * because their (r, r) had not halved in 60 iterations and handed their
+ * iterate back to the FP64 refinement),
  * solver_phases(9: mean ns per iteration of the persistent solver's phases
  * when CAPAC_SOLVER_PHASES is set, then the iterations timed).  Set only:
  * wait_polls(1), the option of that name on the live context.  capac_get

@@ -15,7 +15,7 @@ import pytest
 
 import capacmd_b200 as cm
 from capacmd_b200 import configs
-from conftest import golden_paths, golden_ref, rel_err
+from conftest import golden_paths, golden_ref, large_case, rel_err
 
 pytestmark = pytest.mark.gpu
 
@@ -203,3 +203,62 @@ def test_full_cluster_list_repeats_exactly():
     assert np.array_equal(a.get("virial"), b.get("virial"))
     assert rel_err(h.forces(), a.forces()) < 2e-6
     assert h.stats().list_entries < a.stats().list_entries
+
+
+def test_cluster_pair_list_at_91k_atoms():
+    """pair_list 4: i-cluster x j-cluster pairs, each member pair once.  At
+    91k atoms (box large enough for the composite minimum image) the list
+    holds the reference's pair set, and forces, energies, virial and induced
+    vector agree with the full cluster list within FP32 rounding of the pair
+    terms and with a tight FP64 solve within the mixed path's bars."""
+    paths, g = large_case("c3")
+    d, cp = _mixed(paths, refine_tol=1e-11, pair_list=4)
+    _, full = _mixed(paths, refine_tol=1e-11, pair_list=3)
+    assert cp.get("pair_list")[0] == 2.0
+    assert cp.pair_fingerprint(from_list=True) == (int(g["pair_count"]), int(g["pair_hash"]))
+    f64 = cm.Simulation(d, precision=cm.PREC_FP64, solver_tol=1e-24)
+    for s in (cp, full, f64):
+        s.force()
+    assert rel_err(cp.forces(), full.forces()) < 2e-6
+    assert rel_err(cp.forces(), f64.forces()) < 1e-5
+    pc, pf, p64 = cp.get("potential"), full.get("potential"), f64.get("potential")
+    scale = np.abs(p64[1:]).sum()
+    assert np.abs(pc - pf).max() <= 1e-6 * scale
+    assert abs(pc[1:].sum() - p64[1:].sum()) <= 1e-5 * scale
+    assert rel_err(cp.get("virial"), full.get("virial")) < 1e-5
+    M = d.n_metal
+    x, x64 = cp.get("vec_pq"), f64.get("vec_pq")
+    assert rel_err(x[3 * M:4 * M], x64[3 * M:4 * M]) < 1e-8
+    assert rel_err(x[:3 * M], x64[:3 * M]) < 1e-8
+
+
+def test_cluster_pair_list_md_through_rebuilds():
+    """40 MD steps at 91k atoms on the cluster-pair list against the full
+    cluster list: energies within FP32 rounding, the pair set still the
+    reference's rule after the rebuilds (checked against all pairs)."""
+    paths, _ = large_case("c3")
+    d, cp = _mixed(paths, pair_list=4)
+    _, full = _mixed(paths, pair_list=3)
+    for s in (cp, full):
+        s.md_init()
+    ec, ef = [], []
+    for _ in range(40):
+        cp.md_steps(1)
+        full.md_steps(1)
+        ec.append(cp.get("potential")[0])
+        ef.append(full.get("potential")[0])
+    assert cp.stats().list_builds >= 2
+    assert cp.get("pair_list")[0] == 2.0
+    ec, ef = np.array(ec), np.array(ef)
+    assert np.abs(ec - ef).max() <= 1e-5 * np.abs(ef).max()
+    assert rel_err(cp.get("rx"), full.get("rx")) < 1e-5
+    assert cp.pair_fingerprint(from_list=True) == cp.pair_fingerprint(from_list=False)
+
+
+def test_cluster_pair_list_falls_back_in_a_small_box():
+    """Where the box is too small for the composite minimum image the build
+    takes the half cluster list instead, with the same pair set."""
+    p = configs.cached("c2")
+    d, cp = _mixed(p, pair_list=4)
+    assert cp.get("pair_list")[0] in (1.0, 2.0)
+    assert cp.pair_fingerprint(from_list=True) == cp.pair_fingerprint(from_list=False)
