@@ -219,9 +219,9 @@ def main() -> int:
     ap.add_argument("--e2e-calls", type=int, default=20)
     ap.add_argument("--solver-kernel", type=int, default=0, choices=[0, 1],
                     help="0: persistent cooperative BiCGSTAB launch per solve, 1: a launch per vector step")
-    ap.add_argument("--pair-list", type=int, default=0, choices=[0, 1, 2, 3],
+    ap.add_argument("--pair-list", type=int, default=0, choices=[0, 1, 2, 3, 4],
                     help="mixed path nonbonded list: 0 (= 2) clusters with every pair once, 1 one list per "
-                         "atom, 3 clusters with every pair from both ends")
+                         "atom, 3 clusters with every pair from both ends, 4 cluster pairs")
     ap.add_argument("--predictor", type=int, default=3, choices=[0, 1, 2, 3],
                     help="mixed path warm start: order of the polynomial extrapolation of past solutions")
     ap.add_argument("--solver-phases", action="store_true",

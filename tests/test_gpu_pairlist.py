@@ -214,8 +214,8 @@ def test_cluster_pair_list_at_91k_atoms():
     paths, g = large_case("c3")
     d, cp = _mixed(paths, refine_tol=1e-11, pair_list=4)
     _, full = _mixed(paths, refine_tol=1e-11, pair_list=3)
-    assert cp.get("pair_list")[0] == 2.0
     assert cp.pair_fingerprint(from_list=True) == (int(g["pair_count"]), int(g["pair_hash"]))
+    assert cp.get("pair_list")[0] == 2.0
     f64 = cm.Simulation(d, precision=cm.PREC_FP64, solver_tol=1e-24)
     for s in (cp, full, f64):
         s.force()
@@ -260,5 +260,5 @@ def test_cluster_pair_list_falls_back_in_a_small_box():
     takes the half cluster list instead, with the same pair set."""
     p = configs.cached("c2")
     d, cp = _mixed(p, pair_list=4)
-    assert cp.get("pair_list")[0] in (1.0, 2.0)
     assert cp.pair_fingerprint(from_list=True) == cp.pair_fingerprint(from_list=False)
+    assert cp.get("pair_list")[0] == 1.0
