@@ -289,10 +289,12 @@ __global__ void __launch_bounds__(256) k_build_cluster_list(DevParams P, Grid g,
                                                             uint32_t *__restrict__ nbr, int *__restrict__ nnb,
                                                             unsigned char *__restrict__ cl_metal, double *rx0,
                                                             double *ry0, double *rz0, int *flags,
-                                                            const int *__restrict__ cl_of)
+                                                            const int *__restrict__ cl_of,
+                                                            const int *__restrict__ cl_cell_start)
 {
     // cl_of (half list): a pair is listed once, by the lower-numbered cluster
-    // of its two atoms, and inside one cluster by the earlier member
+    // of its two atoms, and inside one cluster by the earlier member; cells
+    // whose clusters all precede this one are skipped
     const int cl = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (cl >= *n_cl) return;
@@ -338,7 +340,10 @@ __global__ void __launch_bounds__(256) k_build_cluster_list(DevParams P, Grid g,
         for (int iy = 0; iy < nys; ++iy) {
             const int col = (axis_cell(c0[0], g.n[0], ix) * g.n[1] + axis_cell(c0[1], g.n[1], iy)) * nz;
             for (int r = 0; r < zr.n; ++r) {
-                const int s = cell_start[col + zr.a[r]], e = cell_start[col + zr.b[r] + 1];
+                int za = zr.a[r];
+                if (cl_of)
+                    while (za <= zr.b[r] && cl_cell_start[col + za + 1] <= cl) ++za;
+                const int s = cell_start[col + za], e = cell_start[col + zr.b[r] + 1];
                 for (int base = s; base < e; base += 32) {
                     const int p = base + lane;
                     unsigned mask = 0;
@@ -840,7 +845,7 @@ void build_cluster_list(capac_ctx *c, const Grid &g, int n_cells)
             k_build_cluster_list<<<grid_for((long)c->n_clusters * 32, 256), 256, 0, s>>>(
                 c->P, g, inv_box(c), c->rx, c->ry, c->rz, c->spos, c->cell_start, c->cl_atoms, n_cl, c->cl_cap,
                 c->cl_nbr, c->cl_nnb, c->cl_metal, c->rx0, c->ry0, c->rz0, c->flags,
-                c->cl_half ? c->cl_of : nullptr);
+                c->cl_half ? c->cl_of : nullptr, c->cl_cell_start);
         }
         ++c->launches;
         CAPAC_CUDA(cudaMemcpyAsync(c->h_flags + 4, c->flags + 4, sizeof(int), cudaMemcpyDeviceToHost, s));
