@@ -164,7 +164,7 @@ struct Mol3 {
 };
 
 // rattle_1st, force.c:1907-1997: one thread per molecule.
-__global__ void k_rattle1(MdParams m, CstrView cv, double *rx, double *ry, double *rz, const double *ox,
+__global__ void __launch_bounds__(256, 2) k_rattle1(MdParams m, CstrView cv, double *rx, double *ry, double *rz, const double *ox,
                           const double *oy, const double *oz, double *vx, double *vy, double *vz, int *flags)
 {
     const int im = blockIdx.x * blockDim.x + threadIdx.x;
