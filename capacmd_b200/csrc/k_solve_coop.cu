@@ -367,9 +367,9 @@ __device__ __forceinline__ double p_row(const CoopArgs &A, const PassScalars &S,
 // k & 1; tile of q = blockIdx.x + (q mod n_my) * gridDim.x.  Every thread
 // counts `consumed`; thread 0 alone issues the copies and counts `issued`
 // (always consumed + Stages).
-template <typename T, int NS = ring_tiles_bytes<T>() / (int)(kTileElems * sizeof(T))>
+template <typename T>
 struct Ring {
-    static constexpr int Stages = NS;
+    static constexpr int Stages = ring_tiles_bytes<T>() / (int)(kTileElems * sizeof(T));
     T *buf;
     uint64_t *bar;  // Stages mbarriers
     long issued, consumed;
@@ -1016,39 +1016,16 @@ __device__ __forceinline__ double g_p_row(const GroupArgs &A, const PassScalars 
 // address of the first one, kResCols columns apart); the others stream
 // through the ring.
 // A kernel that allocates tensor memory runs one block per SM, which takes
-// all 512 columns; with the shared memory of a whole SM it streams through a
-// four-tile ring and keeps the warps' partial sums of a whole chunk of tiles,
-// so its blocks meet once per chunk instead of once per tile.
+// all 512 columns.
 constexpr int kResTiles = 6;           // tiles per block held in tensor memory
 constexpr int kResCols = 2 * kPlanes * kCols;  // columns per tile (two warps share a lane quadrant)
 constexpr uint32_t kTmemCols = 512;    // columns allocated per block
 static_assert(kResTiles * kResCols <= (int)kTmemCols, "resident tiles exceed the allocation");
-constexpr int kHoldStages = 4;          // ring tiles of the variant that holds tiles in tensor memory
-// Pass scratch of the group kernel: inputs of a chunk of tiles and the warps'
-// partial sums of NB tiles (2: alternate tiles, a block barrier per tile;
-// chunk_tiles: a whole chunk, a block barrier per chunk).
-template <int NB>
-struct PassSmemG {
-    float in[chunk_tiles<float>()][2][kT][4];
-    float rowacc[NB][kWarps][kT][4];
-    double colacc[NB][kT][4];
-    int tile_i[chunk_tiles<float>()], tile_j[chunk_tiles<float>()];
-};
-template <bool HOLD>
-using GroupRing = Ring<float, HOLD ? kHoldStages : Ring<float>::Stages>;
-template <bool HOLD>
-using GroupSmem = PassSmemG<HOLD ? chunk_tiles<float>() : 2>;
-template <bool HOLD>
-__host__ __device__ constexpr size_t group_ring_bytes()
-{
-    return (size_t)GroupRing<HOLD>::Stages * kTileElems * sizeof(float);
-}
-template <int MODE, bool HOLD>
-__device__ bool tiles_pass_g(const GroupArgs &A, const PassScalars &S, GroupRing<HOLD> &ring, GroupSmem<HOLD> &sm,
+template <int MODE>
+__device__ bool tiles_pass_g(const GroupArgs &A, const PassScalars &S, Ring<float> &ring, PassSmem<float> &sm,
                              int n_res, uint32_t tw)
 {
-    constexpr int Stages = GroupRing<HOLD>::Stages;
-    constexpr bool BATCH = HOLD;  // partial sums kept for the whole chunk
+    constexpr int Stages = Ring<float>::Stages;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int nT = A.nG;
     if (MODE != MODE_X && threadIdx.x == 0) {
@@ -1064,10 +1041,8 @@ __device__ bool tiles_pass_g(const GroupArgs &A, const PassScalars &S, GroupRing
     }
     constexpr int kChunk = chunk_tiles<float>();
     const int n_all = n_res + ring.n_my;
-    for (int c0 = 0, nc = 0; c0 < n_all; c0 += BATCH ? nc : kChunk) {
-        // BATCH: held tiles in chunks of up to kChunk, streamed ones of up to
-        // the ring's stages (their slots are released at the chunk's end)
-        nc = BATCH ? (c0 < n_res ? min(kChunk, n_res - c0) : min(Stages, n_all - c0)) : min(kChunk, n_all - c0);
+    for (int c0 = 0; c0 < n_all; c0 += kChunk) {
+        const int nc = min(kChunk, n_all - c0);
         if (threadIdx.x < nc) {
             const int t = blockIdx.x + (c0 + threadIdx.x) * gridDim.x;
             int I = 0;
@@ -1097,16 +1072,15 @@ __device__ bool tiles_pass_g(const GroupArgs &A, const PassScalars &S, GroupRing
         }
         __syncthreads();
 
-        bool bad = false;
         for (int kk = 0; kk < nc; ++kk) {
             const int I = sm.tile_i[kk], J = sm.tile_j[kk];
-            const int set = BATCH ? kk : (kk & 1);
+            const int set = kk & 1;
             const int qi = c0 + kk;
             const bool res = qi < n_res;  // block-uniform
             bool landed = true;
             const float *tile = nullptr;
             if (!res) {
-                const long q = ring.consumed + (BATCH ? kk : 0);
+                const long q = ring.consumed;
                 const int st = (int)(q % Stages);
                 const unsigned parity = (unsigned)((q / Stages) & 1);
                 landed = mbar_wait(ring.bar + st, parity);
@@ -1153,50 +1127,22 @@ __device__ bool tiles_pass_g(const GroupArgs &A, const PassScalars &S, GroupRing
                 const int vv2 = lane >> kShift;
                 sm.colacc[set][kCols * w + (vv2 >> 2)][vv2 & 3] = (double)colsum;
             }
-            if constexpr (BATCH) {
-                bad = bad || !landed;
-            } else {
-                if (__syncthreads_or(!landed)) return false;
-                if (!res) {
-                    ++ring.consumed;
-                    if (threadIdx.x == 0) ring.issue(A.mat);
-                }
-                double *pr = A.part + ((size_t)I * nT + J) * (kT * 4);
-                double *pc = A.part + ((size_t)J * nT + I) * (kT * 4);
-                if (threadIdx.x < kT * 4) {
-                    const int aa = threadIdx.x >> 2, c = threadIdx.x & 3;
-                    double sacc = 0.0;
-#pragma unroll
-                    for (int ww = 0; ww < kWarps; ++ww) sacc += (double)sm.rowacc[set][ww][aa][c];
-                    pr[threadIdx.x] = I == J ? sacc + sm.colacc[set][aa][c] : sacc;
-                } else if (threadIdx.x < 2 * kT * 4 && I != J) {
-                    const int c = threadIdx.x - kT * 4;
-                    pc[c] = sm.colacc[set][c >> 2][c & 3];
-                }
+            if (__syncthreads_or(!landed)) return false;
+            if (!res) {
+                ++ring.consumed;
+                if (threadIdx.x == 0) ring.issue(A.mat);
             }
-        }
-        if constexpr (BATCH) {
-            // one block barrier for the chunk, then its streamed slots are
-            // refilled and every tile's partials written out
-            if (__syncthreads_or(bad)) return false;
-            if (c0 >= n_res) {
-                ring.consumed += nc;
-                if (threadIdx.x == 0)
-                    for (int k = 0; k < nc; ++k) ring.issue(A.mat);
-            }
-            for (int it = threadIdx.x; it < nc * 2 * kT * 4; it += kBlock) {
-                const int kk = it / (2 * kT * 4), x = it - kk * (2 * kT * 4);
-                const int I = sm.tile_i[kk], J = sm.tile_j[kk];
-                if (x < kT * 4) {
-                    const int aa = x >> 2, c = x & 3;
-                    double sacc = 0.0;
+            double *pr = A.part + ((size_t)I * nT + J) * (kT * 4);
+            double *pc = A.part + ((size_t)J * nT + I) * (kT * 4);
+            if (threadIdx.x < kT * 4) {
+                const int aa = threadIdx.x >> 2, c = threadIdx.x & 3;
+                double sacc = 0.0;
 #pragma unroll
-                    for (int ww = 0; ww < kWarps; ++ww) sacc += (double)sm.rowacc[kk][ww][aa][c];
-                    A.part[((size_t)I * nT + J) * (kT * 4) + x] = I == J ? sacc + sm.colacc[kk][aa][c] : sacc;
-                } else if (I != J) {
-                    const int c = x - kT * 4;
-                    A.part[((size_t)J * nT + I) * (kT * 4) + c] = sm.colacc[kk][c >> 2][c & 3];
-                }
+                for (int ww = 0; ww < kWarps; ++ww) sacc += (double)sm.rowacc[set][ww][aa][c];
+                pr[threadIdx.x] = I == J ? sacc + sm.colacc[set][aa][c] : sacc;
+            } else if (threadIdx.x < 2 * kT * 4 && I != J) {
+                const int c = threadIdx.x - kT * 4;
+                pc[c] = sm.colacc[set][c >> 2][c & 3];
             }
         }
         __syncthreads();
@@ -1346,9 +1292,9 @@ template <bool HOLD>
 __global__ void __launch_bounds__(kBlock, 2) k_bicgstab_group(GroupArgs A)
 {
     extern __shared__ __align__(128) unsigned char ring_smem[];
-    constexpr int Stages = GroupRing<HOLD>::Stages;
+    constexpr int Stages = Ring<float>::Stages;
     __shared__ __align__(8) uint64_t ring_bar[Stages];
-    GroupSmem<HOLD> &psm = *reinterpret_cast<GroupSmem<HOLD> *>(ring_smem + group_ring_bytes<HOLD>());
+    PassSmem<float> &psm = *reinterpret_cast<PassSmem<float> *>(ring_smem + ring_bytes<float>());
     SolverScalars *ss = A.ss;
     const int ni = A.ni;
     const long gthreads = (long)gridDim.x * blockDim.x;
@@ -1360,7 +1306,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_bicgstab_group(GroupArgs A)
     // solve (HOLD), the others streamed through the ring
     const int n_all = (int)blockIdx.x < A.ntiles ? (A.ntiles - 1 - (int)blockIdx.x) / nb + 1 : 0;
     const int n_res = HOLD ? min(n_all, kResTiles) : 0;
-    GroupRing<HOLD> ring;
+    Ring<float> ring;
     ring.buf = reinterpret_cast<float *>(ring_smem);
     ring.bar = ring_bar;
     ring.issued = ring.consumed = 0;
@@ -1436,7 +1382,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_bicgstab_group(GroupArgs A)
     if (!done) {
         // r0 = r = b - A x, K r (x zero: no product pass; the ring is
         // untouched, so the next pass starts on the same tiles)
-        if (!x_zero) ok = tiles_pass_g<MODE_X, HOLD>(A, S, ring, psm, n_res, tw) && grid_barrier(A.sync, A.spin_limit);
+        if (!x_zero) ok = tiles_pass_g<MODE_X>(A, S, ring, psm, n_res, tw) && grid_barrier(A.sync, A.spin_limit);
         if (ok) reduce_group<RED_START>(A, S, bpB, !x_zero);
         ok = ok && grid_barrier(A.sync, A.spin_limit);
         done = !ok;
@@ -1455,7 +1401,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_bicgstab_group(GroupArgs A)
         S.beta = (rho / rho_old) * (alpha / omega);
         S.omega = omega;
         S.alpha = alpha;
-        ok = tiles_pass_g<MODE_P, HOLD>(A, S, ring, psm, n_res, tw);
+        ok = tiles_pass_g<MODE_P>(A, S, ring, psm, n_res, tw);
         g_phase_mark(A, iter, 1);
         ok = ok && grid_barrier(A.sync, A.spin_limit);
         if (!ok) break;
@@ -1479,7 +1425,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_bicgstab_group(GroupArgs A)
         alpha = al;
         S.cur ^= 1;
         S.alpha = alpha;
-        ok = tiles_pass_g<MODE_S, HOLD>(A, S, ring, psm, n_res, tw) && grid_barrier(A.sync, A.spin_limit);
+        ok = tiles_pass_g<MODE_S>(A, S, ring, psm, n_res, tw) && grid_barrier(A.sync, A.spin_limit);
         if (!ok) break;
         g_phase_mark(A, iter, 5);
         reduce_group<RED_T>(A, S, bpB, true);
@@ -1673,8 +1619,6 @@ int finish_coop(capac_ctx *c, const unsigned long long *ptime, double skip)
     return c->h_ss->status == 1 ? 1 : CAPAC_OK;
 }
 
-size_t group_dyn_bytes(bool hold);
-
 // The group-ordered persistent solver (mixed path, block-Jacobi).
 int bicgstab_group(capac_ctx *c, const double *b, double *x, double tol, double skip)
 {
@@ -1718,7 +1662,7 @@ int bicgstab_group(capac_ctx *c, const double *b, double *x, double tol, double 
         ProfScope ps(c, K_SOLVE);
         const void *kern = c->tmem_tiles ? (const void *)k_bicgstab_group<true> : (const void *)k_bicgstab_group<false>;
         CAPAC_CUDA(cudaLaunchCooperativeKernel(kern, dim3(c->group_grid), dim3(kBlock), args,
-                                               group_dyn_bytes(c->tmem_tiles), c->stream));
+                                               dyn_smem_bytes<float>(), c->stream));
     }
     ++c->launches;
     return finish_coop(c, A.ptime, skip);
@@ -1729,15 +1673,10 @@ size_t group_rows(int M, int n_nps) { return (size_t)128 * precond_groups(M) + n
 
 // Blocks of the group-ordered solver: two per SM when they fit, 0 if the
 // device cannot run it.
-size_t group_dyn_bytes(bool hold)
-{
-    return hold ? group_ring_bytes<true>() + sizeof(GroupSmem<true>) : group_ring_bytes<false>() + sizeof(GroupSmem<false>);
-}
-
 int group_blocks_per_sm(int device, bool hold)
 {
     const void *kern = hold ? (const void *)k_bicgstab_group<true> : (const void *)k_bicgstab_group<false>;
-    const size_t dyn = group_dyn_bytes(hold);
+    const size_t dyn = dyn_smem_bytes<float>();
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn) != cudaSuccess) {
         cudaGetLastError();
         return 0;
