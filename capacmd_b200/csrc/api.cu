@@ -68,15 +68,26 @@ void force(capac_ctx *c, bool solve = true)
     const bool cpim = c->M > 0 && c->use_cpff;
     launch_bonded(c);
     if (c->M > 0) launch_qsc(c);
+    // the nonbonded pairs (their own stream) meanwhile with the CPIM stages
+    const bool ovl = c->overlap && cpim && solve && c->clusters && c->cl_half;
+    if (ovl) launch_pair_nonbonded_async(c);
     record(c, 2);
-    if (cpim) launch_cpim_rhs(c);
-    record(c, 3);
-    if (cpim) launch_cpim_matrix(c);
-    record(c, 4);
     int st = CAPAC_OK;
-    if (cpim && solve) st = c->opt.precision == CAPAC_PREC_MIXED ? run_refined_solve(c) : run_bicgstab(c);
+    try {
+        if (cpim) launch_cpim_rhs(c);
+        record(c, 3);
+        if (cpim) launch_cpim_matrix(c);
+        record(c, 4);
+        if (cpim && solve) st = c->opt.precision == CAPAC_PREC_MIXED ? run_refined_solve(c) : run_bicgstab(c);
+    } catch (...) {
+        if (ovl) cudaStreamWaitEvent(c->stream, c->ev_join, 0);  // nothing left running on stream2
+        throw;
+    }
     record(c, 5);
-    launch_pair_forces(c, 0);
+    if (ovl)
+        launch_pair_join(c);
+    else
+        launch_pair_forces(c, 0);
     record(c, 6);
     if (cpim) launch_cpim_metal_forces(c);
     launch_external_field(c);
@@ -178,7 +189,7 @@ void prof_begin(capac_ctx *c, int cls)
     }
     if (p.used == kProfSlots) prof_flush(c);
     p.cls[p.used] = cls;
-    CAPAC_CUDA(cudaEventRecord(p.ev[2 * p.used], c->stream));
+    CAPAC_CUDA(cudaEventRecord(p.ev[2 * p.used], c->work_stream ? c->work_stream : c->stream));
 }
 
 void prof_end(capac_ctx *c)
@@ -189,7 +200,7 @@ void prof_end(capac_ctx *c)
         CAPAC_CUDA(cudaEventRecordWithFlags(g->ev.back(), c->stream, cudaEventRecordExternal));
         return;
     }
-    CAPAC_CUDA(cudaEventRecord(p.ev[2 * p.used + 1], c->stream));
+    CAPAC_CUDA(cudaEventRecord(p.ev[2 * p.used + 1], c->work_stream ? c->work_stream : c->stream));
     ++p.used;
 }
 
@@ -549,6 +560,25 @@ int capac_create(const capac_desc *d, const capac_options *opt, capac_ctx **out)
 
             c->partials_cap = partials_needed(c);
             c->partials = dalloc<double>(c->partials_cap);
+            if (o.precision == CAPAC_PREC_MIXED && d->n_metal > 0 && d->use_cpff && !getenv("CAPAC_NO_OVERLAP")) {
+                c->overlap = true;
+                CAPAC_CUDA(cudaStreamCreateWithFlags(&c->stream2, cudaStreamNonBlocking));
+                CAPAC_CUDA(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
+                CAPAC_CUDA(cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming));
+                c->partials2 = dalloc<double>(c->partials_cap);
+                // the solver then runs one block per SM beside the pair kernel's:
+                // the variant that holds tiles in tensor memory where it runs
+                if (c->grouped) {
+                    const int g = group_grid_size(c->device, true);
+                    if (g > 0 && g <= c->coop_grid && !getenv("CAPAC_SOLVER_STREAM")) {
+                        c->tmem_tiles = true;
+                        c->group_grid = g;
+                    } else {
+                        c->tmem_tiles = false;
+                        c->group_grid = std::min(c->coop_grid, c->num_sms);
+                    }
+                }
+            }
             c->pot = dalloc<double>(15);
             c->vir = dalloc<double>(9);
             CAPAC_CUDA(cudaMemsetAsync(c->pot, 0, sizeof(double) * 15, s));
@@ -583,7 +613,8 @@ int capac_destroy(capac_ctx *c)
                    c->cstr_cnt, c->cstr_i, c->cstr_j, c->cstr_r, c->np_start, c->np_end, c->np_charge,
                    c->nbr, c->nnb, c->cell_key, c->cell_key_sorted, c->atom_ids, c->cell_atoms,
                    c->cell_start, c->spos, c->sort_tmp, c->flags, c->cl_atoms, c->cl_cell_start, c->cl_counts,
-                   c->cl_nbr, c->cl_nnb, c->cl_metal, c->cl_of, c->cl_next, c->cp_list,
+                   c->cl_nbr, c->cl_nnb, c->cl_metal, c->cl_of, c->cl_next, c->cl_sel, c->n_cl_sel, c->partials2,
+                   c->cp_list,
                    c->cp_n, c->cp_cent, c->cp_off, c->cp_ti, c->scan_tmp, c->isd, c->vec_ext, c->vec_pq,
                    c->diag, c->mat, c->matf, c->msym, c->sympart, c->coop_bp, c->coop_bar, c->g_atoms, c->dinv, c->slot_np, c->np_off, c->np_rows, c->gvec, c->gw, c->em_buf, c->phase_buf, c->rres, c->dcorr, c->xprev, c->bw, c->bwf, c->ss, c->partials, c->pot, c->vir, c->th};
     for (void *p : dev)
@@ -602,6 +633,9 @@ int capac_destroy(capac_ctx *c)
         for (auto &e : g.ev)
             if (e) cudaEventDestroy(e);
     }
+    if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+    if (c->ev_join) cudaEventDestroy(c->ev_join);
+    if (c->stream2) cudaStreamDestroy(c->stream2);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return CAPAC_OK;

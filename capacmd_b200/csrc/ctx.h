@@ -185,6 +185,17 @@ struct capac_ctx {
     bool cl_half = false;              // half list: every pair once, Newton's third law (pair_list 2)
     int *cl_of = nullptr;              // [N] the cluster of each atom (half list)
     int *cl_next = nullptr;            // the cluster pair kernel's work counter (next cluster to take)
+    int *cl_sel = nullptr;             // [cl_max] clusters with a metal member or neighbour (any order)
+    int *n_cl_sel = nullptr;           // their count (device)
+
+    // the nonbonded pairs run on a second stream, one block per SM, while the
+    // CPIM right-hand side, matrix and solve run on `stream` (mixed path on
+    // the half cluster list); the CPIM forces on water atoms follow the solve
+    bool overlap = false;
+    cudaStream_t stream2 = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    double *partials2 = nullptr;       // block partials of the overlapped pair launch
+    cudaStream_t work_stream = nullptr; // stream of the launches being issued (null: `stream`)
 
     // i-cluster x j-cluster list (pair_list 4): per cluster the clusters of
     // the same or a higher index with a 4 x 4 mask of the member pairs within
@@ -272,6 +283,9 @@ void cuda_check(cudaError_t e, const char *what);
 void launch_pack_positions(capac_ctx *c);
 // cluster centroids and member offsets (pair_list 4); statics: atoms, types, metal flags too
 void launch_cluster_frames(capac_ctx *c, bool statics);
+// overlap of the nonbonded pairs with the CPIM solve (half cluster list)
+void launch_pair_nonbonded_async(capac_ctx *c);
+void launch_pair_join(capac_ctx *c);
 void launch_list_maintenance(capac_ctx *c, bool force_rebuild);
 // Rebuild the lists with an atom-list row for every atom, now and at every
 // later build (the gradient kernels walk all rows).
@@ -318,7 +332,9 @@ int group_grid_size(int device, bool hold);
 int group_blocks_per_sm(int device, bool hold);
 void launch_cpim_metal_forces(capac_ctx *c);
 void launch_external_field(capac_ctx *c);
-void launch_finalize(capac_ctx *c, int nblocks, int K, const int *slots_pot, const int *slots_vir);
+// per-block partials (src, default c->partials) summed into energy and virial slots
+void launch_finalize(capac_ctx *c, int nblocks, int K, const int *slots_pot, const int *slots_vir,
+                     const double *src = nullptr);
 void launch_pair_fingerprint(capac_ctx *c, int from_list, long *count, unsigned long long *hash);
 
 // integrator

@@ -41,7 +41,7 @@ __global__ void __launch_bounds__(256) k_finalize(const double *__restrict__ par
     }
 }
 
-void launch_finalize(capac_ctx *c, int nblocks, int K, const int *slots_pot, const int *slots_vir)
+void launch_finalize(capac_ctx *c, int nblocks, int K, const int *slots_pot, const int *slots_vir, const double *src)
 {
     Slots s;
     for (int k = 0; k < 24; ++k) {
@@ -53,7 +53,7 @@ void launch_finalize(capac_ctx *c, int nblocks, int K, const int *slots_pot, con
         for (int b = a + 1; b < K; ++b)
             if ((s.pot[a] >= 0 && s.pot[a] == s.pot[b]) || (s.vir[a] >= 0 && s.vir[a] == s.vir[b]))
                 throw Error(CAPAC_ERR_INVALID, "finalize: two values share an energy or virial slot");
-    k_finalize<<<K, 256, 0, c->stream>>>(c->partials, nblocks, K, s, c->pot, c->vir);
+    k_finalize<<<K, 256, 0, c->stream>>>(src ? src : c->partials, nblocks, K, s, c->pot, c->vir);
     ++c->launches;
 }
 

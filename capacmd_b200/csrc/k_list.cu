@@ -444,6 +444,16 @@ __global__ void k_fingerprint_clusters(DevParams P, const double *__restrict__ r
     }
 }
 
+// The clusters with a metal member or a metal list neighbour (cl_metal), in
+// any order: the CPIM pass over the water side visits only these.
+__global__ void k_select_metal_clusters(const int *__restrict__ n_cl, const unsigned char *__restrict__ cl_metal,
+                                        int *__restrict__ sel, int *__restrict__ n_sel)
+{
+    const int ncl = *n_cl;
+    for (int cl = blockIdx.x * blockDim.x + threadIdx.x; cl < ncl; cl += gridDim.x * blockDim.x)
+        if (cl_metal[cl]) sel[atomicAdd(n_sel, 1)] = cl;
+}
+
 // ------------------------------------------------------------ cluster pairs
 //
 // pair_list 4: the clusters above, paired.  Before each pair launch
@@ -788,19 +798,23 @@ void ensure_cluster_buffers(capac_ctx *c, int n_cells)
         cudaFree(c->cl_nbr);
         cudaFree(c->cl_nnb);
         cudaFree(c->cl_metal);
+        cudaFree(c->cl_sel);
         c->cl_atoms = nullptr;
         c->cl_nbr = nullptr;
         c->cl_nnb = nullptr;
         c->cl_metal = nullptr;
+        c->cl_sel = nullptr;
         CAPAC_CUDA(cudaMalloc(&c->cl_atoms, sizeof(int4) * need));
         CAPAC_CUDA(cudaMalloc(&c->cl_nbr, sizeof(uint32_t) * (size_t)need * c->cl_cap));
         CAPAC_CUDA(cudaMalloc(&c->cl_nnb, sizeof(int) * need));
         CAPAC_CUDA(cudaMalloc(&c->cl_metal, need));
+        CAPAC_CUDA(cudaMalloc(&c->cl_sel, sizeof(int) * need));
         c->cl_max = need;
     }
     c->cl_half = c->opt.pair_list != 3;  // 0 (default) and 2: every pair once; 3: the full cluster list
     if (c->cl_half && !c->cl_of) CAPAC_CUDA(cudaMalloc(&c->cl_of, sizeof(int) * N));
     if (!c->cl_next) CAPAC_CUDA(cudaMalloc(&c->cl_next, sizeof(int)));
+    if (!c->n_cl_sel) CAPAC_CUDA(cudaMalloc(&c->n_cl_sel, sizeof(int)));
 }
 
 // Clusters of the sorted cells; returns false when the largest member offset
@@ -851,7 +865,13 @@ void build_cluster_list(capac_ctx *c, const Grid &g, int n_cells)
         CAPAC_CUDA(cudaMemcpyAsync(c->h_flags + 4, c->flags + 4, sizeof(int), cudaMemcpyDeviceToHost, s));
         CAPAC_CUDA(cudaStreamSynchronize(s));
         const int need_cap = c->h_flags[4];
-        if (need_cap <= c->cl_cap) return;
+        if (need_cap <= c->cl_cap) {
+            CAPAC_CUDA(cudaMemsetAsync(c->n_cl_sel, 0, sizeof(int), s));
+            k_select_metal_clusters<<<grid_for(c->n_clusters, 256), 256, 0, s>>>(n_cl, c->cl_metal, c->cl_sel,
+                                                                                  c->n_cl_sel);
+            ++c->launches;
+            return;
+        }
         if (attempt == 3) throw Error(CAPAC_ERR_CAPACITY, "cluster list capacity could not be met");
         int new_cap = (int)std::min<long>((long)(need_cap * 1.25) + 32, 1L << 20);
         new_cap = (new_cap + 31) & ~31;

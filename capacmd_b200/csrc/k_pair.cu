@@ -504,7 +504,7 @@ __global__ void __launch_bounds__(kClWarps * 32, kClMinBlocks) k_pair_cl(DevPara
                                                               const double *__restrict__ vec_pq,
                                                               double *__restrict__ fx, double *__restrict__ fy,
                                                               double *__restrict__ fz, double *__restrict__ partials,
-                                                              int *__restrict__ next)
+                                                              int *__restrict__ next, const int *__restrict__ sel)
 {
     constexpr int NB = 2;
     extern __shared__ __align__(16) unsigned char s_dyn[];  // the warps' queues
@@ -537,13 +537,15 @@ __global__ void __launch_bounds__(kClWarps * 32, kClMinBlocks) k_pair_cl(DevPara
     // list lengths that differ from cluster to cluster leave no warp idle at
     // the end; else the fixed grid-stride order, which keeps the energy and
     // virial sums in the same order from run to run
+    // sel: only the listed clusters (n_cl then counts them)
     for (int k = 0;; ++k) {
-        int cl = blockIdx.x * kClWarps + wib + k * gridDim.x * kClWarps;
+        int ci = blockIdx.x * kClWarps + wib + k * gridDim.x * kClWarps;
         if (next) {
-            if (lane == 0) cl = atomicAdd(next, 1);
-            cl = __shfl_sync(0xffffffffu, cl, 0);
+            if (lane == 0) ci = atomicAdd(next, 1);
+            ci = __shfl_sync(0xffffffffu, ci, 0);
         }
-        if (cl >= ncl) break;
+        if (ci >= ncl) break;
+        const int cl = sel ? __ldg(sel + ci) : ci;
         const int4 A = cl_atoms[cl];
         const int nk = 1 + (A.y >= 0) + (A.z >= 0) + (A.w >= 0);
         const int mine = lane == 0 ? A.x : lane == 1 ? A.y : lane == 2 ? A.z : A.w;
@@ -1056,16 +1058,19 @@ void launch_pair_t(capac_ctx *c, int mode, unsigned grid)
     ++c->launches;
 }
 
+// The cluster pair kernel on stream st, its block partials to `partials`;
+// sel: only the clusters with a metal member or neighbour.
 template <bool NONBONDED, bool CPIM, bool HALF>
-void launch_pair_cl_t(capac_ctx *c, unsigned grid)
+void launch_pair_cl_t(capac_ctx *c, unsigned grid, cudaStream_t st, double *partials, bool sel)
 {
     // the queues and the static arrays together exceed the default 48 KB
     CAPAC_CUDA(cudaFuncSetAttribute(k_pair_cl<NONBONDED, CPIM, HALF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)kClQueueBytes));
-    if (HALF) CAPAC_CUDA(cudaMemsetAsync(c->cl_next, 0, sizeof(int), c->stream));
-    k_pair_cl<NONBONDED, CPIM, HALF><<<grid, kClWarps * 32, kClQueueBytes, c->stream>>>(
-        c->P, pair_consts_f(c), c->pos4, c->cl_atoms, c->cl_cell_start + c->n_cells, c->cl_nbr, c->cl_nnb,
-        c->cl_metal, c->cl_cap, c->vec_pq, c->fx, c->fy, c->fz, c->partials, HALF ? c->cl_next : nullptr);
+    if (HALF) CAPAC_CUDA(cudaMemsetAsync(c->cl_next, 0, sizeof(int), st));
+    k_pair_cl<NONBONDED, CPIM, HALF><<<grid, kClWarps * 32, kClQueueBytes, st>>>(
+        c->P, pair_consts_f(c), c->pos4, c->cl_atoms, sel ? c->n_cl_sel : c->cl_cell_start + c->n_cells, c->cl_nbr,
+        c->cl_nnb, c->cl_metal, c->cl_cap, c->vec_pq, c->fx, c->fy, c->fz, partials, HALF ? c->cl_next : nullptr,
+        sel ? c->cl_sel : nullptr);
 }
 
 template <bool NONBONDED, bool CPIM>
@@ -1098,17 +1103,17 @@ void launch_pair_clusters(capac_ctx *c, int mode, unsigned grid)
     ProfScope ps(c, K_PAIR);
     if (c->cl_half) {
         if (mode == 0 && cpim)
-            launch_pair_cl_t<true, true, true>(c, grid);
+            launch_pair_cl_t<true, true, true>(c, grid, c->stream, c->partials, false);
         else if (mode == 0)
-            launch_pair_cl_t<true, false, true>(c, grid);
+            launch_pair_cl_t<true, false, true>(c, grid, c->stream, c->partials, false);
         else
-            launch_pair_cl_t<false, true, true>(c, grid);
+            launch_pair_cl_t<false, true, true>(c, grid, c->stream, c->partials, false);
     } else if (mode == 0 && cpim)
-        launch_pair_cl_t<true, true, false>(c, grid);
+        launch_pair_cl_t<true, true, false>(c, grid, c->stream, c->partials, false);
     else if (mode == 0)
-        launch_pair_cl_t<true, false, false>(c, grid);
+        launch_pair_cl_t<true, false, false>(c, grid, c->stream, c->partials, false);
     else
-        launch_pair_cl_t<false, true, false>(c, grid);
+        launch_pair_cl_t<false, true, false>(c, grid, c->stream, c->partials, false);
     ++c->launches;
 }
 
@@ -1125,6 +1130,42 @@ unsigned pair_grid(const capac_ctx *c)
     const long need = (units + warps - 1) / warps;
     const long cap = (long)c->num_sms * (c->clusters && c->cl_half ? kClMinBlocks : 16);
     return (unsigned)std::max(1L, std::min(need, cap));
+}
+
+// Overlap, first half (on stream2, once `stream` has reached this point):
+// the nonbonded terms of the half cluster list, one block per SM so that the
+// CPIM solve's blocks find room beside it; energies and virial into
+// partials2.  The forces go to fx, fy, fz by atomic adds only, so the
+// kernels that run meanwhile on `stream` must leave them alone (the CPIM
+// right-hand side, matrix and solve do).
+void launch_pair_nonbonded_async(capac_ctx *c)
+{
+    CAPAC_CUDA(cudaEventRecord(c->ev_fork, c->stream));
+    CAPAC_CUDA(cudaStreamWaitEvent(c->stream2, c->ev_fork, 0));
+    c->work_stream = c->stream2;
+    {
+        ProfScope ps(c, K_PAIR);
+        launch_pair_cl_t<true, false, true>(c, (unsigned)c->num_sms, c->stream2, c->partials2, false);
+    }
+    c->work_stream = nullptr;
+    ++c->launches;
+    CAPAC_CUDA(cudaEventRecord(c->ev_join, c->stream2));
+}
+
+// Overlap, second half (on `stream`, after the solve): wait for the first,
+// sum its energies and virial, then the CPIM forces on water atoms from the
+// solved induced vector over the clusters with a metal member or neighbour.
+void launch_pair_join(capac_ctx *c)
+{
+    CAPAC_CUDA(cudaStreamWaitEvent(c->stream, c->ev_join, 0));
+    static const int pot_slots[11] = {7, 8, -1, -1, -1, -1, -1, -1, -1, -1, -1};
+    static const int vir_slots[11] = {-1, -1, 0, 1, 2, 3, 4, 5, 6, 7, 8};
+    launch_finalize(c, c->num_sms, 11, pot_slots, vir_slots, c->partials2);
+    {
+        ProfScope ps(c, K_PAIR);
+        launch_pair_cl_t<false, true, true>(c, pair_grid(c), c->stream, c->partials, true);
+    }
+    ++c->launches;
 }
 
 void launch_pair_forces(capac_ctx *c, int mode)

@@ -262,3 +262,34 @@ def test_cluster_pair_list_falls_back_in_a_small_box():
     d, cp = _mixed(p, pair_list=4)
     assert cp.pair_fingerprint(from_list=True) == cp.pair_fingerprint(from_list=False)
     assert cp.get("pair_list")[0] == 1.0
+
+
+@pytest.mark.parametrize("case", ["t_2np", "c2"])
+def test_pairs_overlapped_with_the_solve(case, monkeypatch):
+    """The mixed path runs the nonbonded pairs on a second stream while the
+    CPIM stages and solve run, then the CPIM forces on water atoms over the
+    clusters next to metal; against the same path run in one stream
+    (CAPAC_NO_OVERLAP): forces, energies, virial and induced vector agree
+    within the rounding of the neighbour-side atomic adds, through MD steps
+    and list rebuilds."""
+    paths = configs.cached(case) if case == "c2" else golden_paths(case)
+    d, ovl = _mixed(paths, refine_tol=1e-11)
+    monkeypatch.setenv("CAPAC_NO_OVERLAP", "1")
+    _, one = _mixed(paths, refine_tol=1e-11)
+    monkeypatch.delenv("CAPAC_NO_OVERLAP")
+    for s in (ovl, one):
+        s.set("vec_pq", np.zeros(d.n_mat))
+        s.force()
+    assert _uses_clusters(ovl)
+    assert rel_err(ovl.forces(), one.forces()) < 1e-12
+    po, p1 = ovl.get("potential"), one.get("potential")
+    assert np.abs(po - p1).max() <= 1e-12 * np.abs(p1[1:]).sum()
+    assert rel_err(ovl.get("virial"), one.get("virial")) < 1e-12
+    assert rel_err(ovl.get("vec_pq"), one.get("vec_pq")) < 1e-12
+    for s in (ovl, one):
+        s.md_init()
+    for _ in range(30):
+        ovl.md_steps(1)
+        one.md_steps(1)
+    assert rel_err(ovl.get("rx"), one.get("rx")) < 1e-9
+    assert abs(ovl.get("potential")[0] - one.get("potential")[0]) <= 1e-7 * abs(one.get("potential")[0])
