@@ -222,6 +222,8 @@ def main() -> int:
     ap.add_argument("--pair-list", type=int, default=0, choices=[0, 1, 2, 3, 4],
                     help="mixed path nonbonded list: 0 (= 2) clusters with every pair once, 1 one list per "
                          "atom, 3 clusters with every pair from both ends, 4 cluster pairs")
+    ap.add_argument("--inner-precond", type=int, default=1, choices=[0, 1, 2],
+                    help="mixed path inner solves: 0 Jacobi, 1 block-Jacobi, 2 block-Jacobi with a coarse correction")
     ap.add_argument("--predictor", type=int, default=3, choices=[0, 1, 2, 3],
                     help="mixed path warm start: order of the polynomial extrapolation of past solutions")
     ap.add_argument("--solver-phases", action="store_true",
@@ -259,7 +261,7 @@ def main() -> int:
     prec = cm.PREC_MIXED if args.precision == "mixed" else cm.PREC_FP64
     desc = cm.Desc.from_paths(paths)
     sim = cm.Simulation(desc, precision=prec, device=local, solver_kernel=args.solver_kernel,
-                        predictor=args.predictor, pair_list=args.pair_list)
+                        predictor=args.predictor, pair_list=args.pair_list, inner_precond=args.inner_precond)
     N, M = desc.n_atoms, desc.n_metal
     sim.md_init()
     sim.md_steps(args.warmup)
@@ -431,7 +433,7 @@ def compare_arms(args, cm, desc, sim, prec, device) -> tuple[dict, dict]:
         specs.append((f"mixed_pair_list_{other_list}", cm.PREC_MIXED, 0.0, other_list))
     for name, p, tol, plist in specs:
         s2 = cm.Simulation(desc, precision=p, device=device, solver_tol=tol, solver_kernel=args.solver_kernel,
-                           predictor=args.predictor, pair_list=plist)
+                           predictor=args.predictor, pair_list=plist, inner_precond=args.inner_precond)
         s2.md_init()
         s2.md_steps(args.warmup)
         ms2 = ctypes_time(s2, args.steps)

@@ -25,7 +25,7 @@ LIB = os.path.join(PKG, "libcapacmd_gpu.so")
 DRIVER = os.path.join(PKG, "capacmd-gpu")
 
 SOURCES = ["io.cpp", "api.cu", "k_list.cu", "k_pair.cu", "k_cpim.cu", "k_md.cu", "k_cpim_sym.cu", "k_solve_static.cu", "k_solve_coop.cu",
-           "k_precond.cu", "k_grad.cu", "k_grad_forces.cu", "k_bonded.cu"]
+           "k_precond.cu", "k_coarse.cu", "k_grad.cu", "k_grad_forces.cu", "k_bonded.cu"]
 
 
 def nvcc() -> str:

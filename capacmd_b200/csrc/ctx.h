@@ -228,6 +228,13 @@ struct capac_ctx {
     bool tmem_tiles = false;     // the grouped solver holds part of its tiles in tensor memory
     int group_grid = 0;          // blocks of the grouped solver's launch (<= coop_grid)
     int inner_stall = 0;         // set during the refinement's inner solves: see GroupArgs::stall
+    // two-level inner preconditioner (inner_precond 2, k_coarse.cu)
+    bool twolevel = false;
+    int cz_nc = 0;               // coarse columns: 4 per group and one per nanoparticle
+    float *cz_az = nullptr;      // A Z
+    float *cz_einv = nullptr;    // E^-1
+    double *cz_aug = nullptr;    // [E | I] workspace of the inversion
+    double *cz_zbuf = nullptr;   // Z^T v inside the solver
     long inner_stalls = 0;       // inner solves ended that way
     int *slot_np = nullptr;      // [32 nG] nanoparticle of each group slot's atom, -1 none
     int *np_off = nullptr;       // [n_nps + 1] offsets into np_rows
@@ -327,6 +334,9 @@ size_t coop_partial_doubles(int grid);
 int bicgstab_coop(capac_ctx *c, const double *b, double *x, double tol, double skip);
 // group-ordered solver (k_solve_coop.cu): internal vector length, blocks
 int group_tmem_tiles();
+int coarse_columns(int M, int n_nps);
+size_t coarse_az_floats(int M, int n_nps);
+void launch_coarse_refresh(capac_ctx *c);
 size_t group_rows(int M, int n_nps);
 int group_grid_size(int device, bool hold);
 int group_blocks_per_sm(int device, bool hold);

@@ -259,7 +259,10 @@ void launch_cpim_matrix(capac_ctx *c)
         // the preconditioner only steers the inner solves (the FP64 residual
         // defines the answer), so its inverse blocks are refreshed every
         // kPrecondEvery matrix builds, not every step
-        if (c->dinv && c->precond_age++ % kPrecondEvery == 0) launch_block_inverse(c);
+        if (c->dinv && c->precond_age++ % kPrecondEvery == 0) {
+            launch_block_inverse(c);
+            if (c->twolevel) launch_coarse_refresh(c);
+        }
         return;
     }
     dim3 grid(grid_for(c->Mp, 128), c->M);

@@ -955,6 +955,9 @@ size_t dyn_smem_bytes()
 struct GroupArgs {
     int M, nG, ntiles, n_nps, ni, max_iter;
     int stall;                   // > 0: stop (status 1) after this many iterations without halving (r, r)
+    int nc;                      // > 0: the two-level operator with nc coarse columns (k_coarse.cu)
+    const float *az, *einv;      // A Z, E^-1 of the coarse space
+    double *zbuf;                // Z^T of the vector being preconditioned (nc)
     long spin_limit;
     double inv_polar, inv_capac;
     const int *g_atoms;          // [32 nG] metal-local atom of each slot, -1 padding
@@ -1286,6 +1289,183 @@ __device__ void reduce_group(const GroupArgs &A, const PassScalars &S, double *b
     }
 }
 
+constexpr int kCoarseMax = 512;  // coarse columns the solver's shared buffer holds
+
+// The reductions of reduce_group with the two-level operator of k_coarse.cu
+// in place of the block-Jacobi K alone: first every group's rows of `out`
+// (v, t or r), the dots that do not involve K out, and the group's four mode
+// sums (and the constraint rows) into zbuf; a grid barrier; then in every
+// block c = E^-1 zbuf, and for its groups K out = Z c + K (out - (A Z) c)
+// with the dots of K out.  Returns false when the grid barrier gave up.
+// scratch: 256 + kCoarseMax doubles of shared memory (the pass inputs' buffer,
+// idle between passes).
+template <int RED>
+__device__ bool reduce_group2(const GroupArgs &A, const PassScalars &S, double *bp, bool products, double *scratch)
+{
+    double *vrow = scratch, *hsum = scratch + 128, *cc = scratch + 256;
+    const int nG = A.nG, nc = A.nc, tid = threadIdx.x;
+    const double *in = RED == RED_START ? A.xi : (RED == RED_V ? A.yb[S.cur ^ 1] : A.z);
+    double *outv = RED == RED_START ? A.r : (RED == RED_V ? A.v : A.t);
+    double *kout = RED == RED_START ? A.Kr : (RED == RED_V ? A.Kv : A.Kt);
+    double d[7] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    for (int G = blockIdx.x; G < nG; G += gridDim.x) {
+        const int o = tid & 127, h = tid >> 7;
+        double sum = 0.0;
+        if (products) {
+            const double *src = A.part + (size_t)G * nG * (kT * 4) + o;
+            for (int K0 = h; K0 < nG; K0 += 2 * kBatch) {
+                double vals[kBatch];
+#pragma unroll
+                for (int u = 0; u < kBatch; ++u) {
+                    const int Kk = K0 + 2 * u;
+                    vals[u] = Kk < nG ? __ldcg(src + (size_t)Kk * (kT * 4)) : 0.0;
+                }
+#pragma unroll
+                for (int u = 0; u < kBatch; ++u) sum += vals[u];
+            }
+        }
+        if (h == 1) hsum[o] = sum;
+        __syncthreads();
+        if (h == 0) {
+            const int row = 128 * G + o;
+            sum += hsum[o];
+            const double xin = products ? __ldcg(in + row) : 0.0;
+            if ((o & 3) < 3) {
+                sum += A.inv_polar * xin;
+            } else {
+                sum += -A.inv_capac * xin;
+                const int k = A.slot_np[row >> 2];
+                if (products && k >= 0) sum += __ldcg(in + 128 * nG + k);
+            }
+            double out;
+            if (RED == RED_START) {
+                const int rr = g_ref_row(A, row);
+                const double bk = rr >= 0 ? A.b[rr] : 0.0;
+                out = bk - sum;
+                A.r0[row] = out;
+                d[0] += out * out;
+            } else if (RED == RED_V) {
+                out = sum;
+                d[0] += __ldcg(A.r0 + row) * out;
+            } else {
+                out = sum;
+                const double sr = __ldcg(A.s + row), r0 = __ldcg(A.r0 + row);
+                d[2] += r0 * sr;
+                d[3] += r0 * out;
+                d[4] += sr * sr;
+                d[5] += sr * out;
+                d[6] += out * out;
+            }
+            outv[row] = out;
+            vrow[o] = A.g_atoms[row >> 2] >= 0 ? out : 0.0;
+        }
+        __syncthreads();
+        if (tid < 4) {  // the group's mode sums (padding rows hold zero)
+            double zs = 0.0;
+            for (int a = 0; a < kT; ++a) zs += vrow[4 * a + tid];
+            A.zbuf[4 * G + tid] = zs;
+        }
+        __syncthreads();
+    }
+    for (int k = (int)gridDim.x - 1 - (int)blockIdx.x; k < A.n_nps; k += gridDim.x) {
+        __shared__ double shl[32];
+        double acc[1] = {0.0};
+        if (products)
+            for (int q = A.np_off[k] + tid; q < A.np_off[k + 1]; q += blockDim.x) acc[0] += __ldcg(in + A.np_rows[q]);
+        block_sum<1>(acc, shl);
+        if (tid == 0) {
+            const int row = 128 * nG + k;
+            const double val = acc[0];
+            double out = val;
+            if (RED == RED_START) {
+                out = A.b[4 * A.M + k] - val;
+                A.r0[row] = out;
+                d[0] += out * out;
+            } else if (RED == RED_V) {
+                d[0] += __ldcg(A.r0 + row) * val;
+            } else {
+                const double sr = __ldcg(A.s + row), r0 = __ldcg(A.r0 + row);
+                d[2] += r0 * sr;
+                d[3] += r0 * val;
+                d[4] += sr * sr;
+                d[5] += sr * val;
+                d[6] += val * val;
+            }
+            outv[row] = out;
+            A.zbuf[4 * nG + k] = out;
+        }
+        __syncthreads();
+    }
+    if (!grid_barrier(A.sync, A.spin_limit)) return false;
+
+    const bool mine = (int)blockIdx.x < nG || (int)gridDim.x - 1 - (int)blockIdx.x < A.n_nps;
+    if (mine) {
+        // c = E^-1 zbuf (E^-1 symmetric, stored so that thread i reads a column)
+        for (int i = tid; i < nc; i += blockDim.x) {
+            double s = 0.0;
+            for (int j = 0; j < nc; ++j) s = fma((double)__ldg(A.einv + (size_t)j * nc + i), __ldcg(A.zbuf + j), s);
+            cc[i] = s;
+        }
+        __syncthreads();
+    }
+    for (int G = blockIdx.x; G < nG; G += gridDim.x) {
+        const int o = tid & 127, h = tid >> 7;
+        // (A Z c) of the group's rows: two halves of the columns
+        const float *az = A.az + (size_t)G * nc * 128 + o;
+        double s = 0.0;
+        for (int j = h; j < nc; j += 2) s = fma((double)__ldg(az + (size_t)j * 128), cc[j], s);
+        if (h == 1) hsum[o] = s;
+        __syncthreads();
+        if (h == 0) {
+            const int row = 128 * G + o;
+            const bool valid = A.g_atoms[row >> 2] >= 0;
+            vrow[o] = valid ? __ldcg(outv + row) - (s + hsum[o]) : 0.0;
+        }
+        __syncthreads();
+        // K w with the group's inverse block, plus Z c
+        {
+            const int o2 = tid >> 1, half = tid & 1;
+            const float *col = A.dinv + (size_t)G * 128 * 128 + (size_t)(64 * half) * 128 + o2;
+            double acc = 0.0;
+#pragma unroll 16
+            for (int c = 0; c < 64; ++c) acc = fma((double)__ldg(col + (size_t)c * 128), vrow[64 * half + c], acc);
+            acc += __shfl_xor_sync(0xffffffffu, acc, 1);
+            if (half == 0) {
+                const int row = 128 * G + o2;
+                if (A.g_atoms[row >> 2] >= 0) acc += cc[4 * G + (o2 & 3)];
+                kout[row] = acc;
+                if (RED == RED_T) {
+                    d[0] += acc * __ldcg(A.z + row);
+                    d[1] += acc * acc;
+                }
+            }
+        }
+        __syncthreads();
+    }
+    for (int k = (int)gridDim.x - 1 - (int)blockIdx.x; k < A.n_nps; k += gridDim.x) {
+        if (tid == 0) {
+            const int row = 128 * nG + k;
+            const float *azl = A.az + (size_t)nG * nc * 128 + (size_t)k * nc;
+            double s = 0.0;
+            for (int j = 0; j < nc; ++j) s = fma((double)__ldg(azl + j), cc[j], s);
+            const double kv = __ldcg(outv + row) - s + cc[4 * nG + k];  // K = 1 on the constraint rows
+            kout[row] = kv;
+            if (RED == RED_T) {
+                d[0] += kv * __ldcg(A.z + row);
+                d[1] += kv * kv;
+            }
+        }
+        __syncthreads();
+    }
+    if (RED == RED_T) {
+        put_bp<7>(bp, d);
+    } else {
+        double d1[1] = {d[0]};
+        put_bp<1>(bp, d1);
+    }
+    return true;
+}
+
 // Two blocks of kBlock threads per SM (the variant that holds tiles in
 // tensor memory runs one).
 template <bool HOLD>
@@ -1295,6 +1475,9 @@ __global__ void __launch_bounds__(kBlock, 2) k_bicgstab_group(GroupArgs A)
     constexpr int Stages = Ring<float>::Stages;
     __shared__ __align__(8) uint64_t ring_bar[Stages];
     PassSmem<float> &psm = *reinterpret_cast<PassSmem<float> *>(ring_smem + ring_bytes<float>());
+    // the pass inputs' buffer, idle between passes, holds the two-level reductions' scratch
+    static_assert(sizeof(psm.in) >= (256 + kCoarseMax) * sizeof(double), "reduction scratch does not fit");
+    double *pscratch = reinterpret_cast<double *>(&psm.in[0][0][0][0]);
     SolverScalars *ss = A.ss;
     const int ni = A.ni;
     const long gthreads = (long)gridDim.x * blockDim.x;
@@ -1383,7 +1566,12 @@ __global__ void __launch_bounds__(kBlock, 2) k_bicgstab_group(GroupArgs A)
         // r0 = r = b - A x, K r (x zero: no product pass; the ring is
         // untouched, so the next pass starts on the same tiles)
         if (!x_zero) ok = tiles_pass_g<MODE_X>(A, S, ring, psm, n_res, tw) && grid_barrier(A.sync, A.spin_limit);
-        if (ok) reduce_group<RED_START>(A, S, bpB, !x_zero);
+        if (ok) {
+            if (A.nc > 0)
+                ok = reduce_group2<RED_START>(A, S, bpB, !x_zero, pscratch);
+            else
+                reduce_group<RED_START>(A, S, bpB, !x_zero);
+        }
         ok = ok && grid_barrier(A.sync, A.spin_limit);
         done = !ok;
     }
@@ -1408,7 +1596,14 @@ __global__ void __launch_bounds__(kBlock, 2) k_bicgstab_group(GroupArgs A)
         pending = false;  // the P pass applied the previous iteration's x update
         g_phase_mark(A, iter, 2);
         S.first = 0;
-        reduce_group<RED_V>(A, S, bpA, true);
+        if (A.nc > 0) {
+            if (!reduce_group2<RED_V>(A, S, bpA, true, pscratch)) {
+                ok = false;
+                break;
+            }
+        } else {
+            reduce_group<RED_V>(A, S, bpA, true);
+        }
         if (!grid_barrier(A.sync, A.spin_limit)) {
             ok = false;
             break;
@@ -1428,7 +1623,14 @@ __global__ void __launch_bounds__(kBlock, 2) k_bicgstab_group(GroupArgs A)
         ok = tiles_pass_g<MODE_S>(A, S, ring, psm, n_res, tw) && grid_barrier(A.sync, A.spin_limit);
         if (!ok) break;
         g_phase_mark(A, iter, 5);
-        reduce_group<RED_T>(A, S, bpB, true);
+        if (A.nc > 0) {
+            if (!reduce_group2<RED_T>(A, S, bpB, true, pscratch)) {
+                ok = false;
+                break;
+            }
+        } else {
+            reduce_group<RED_T>(A, S, bpB, true);
+        }
         if (!grid_barrier(A.sync, A.spin_limit)) {
             ok = false;
             break;
@@ -1631,6 +1833,10 @@ int bicgstab_group(capac_ctx *c, const double *b, double *x, double tol, double 
     A.ni = (int)group_rows(c->M, c->n_nps);
     A.max_iter = solver_max_iter(c);
     A.stall = c->inner_stall;
+    A.nc = c->twolevel ? c->cz_nc : 0;
+    A.az = c->cz_az;
+    A.einv = c->cz_einv;
+    A.zbuf = c->cz_zbuf;
     A.spin_limit = c->opt.wait_polls > 0 ? c->opt.wait_polls : kSpinLimit;
     A.inv_polar = c->P.inv_polar;
     A.inv_capac = c->P.inv_capac;

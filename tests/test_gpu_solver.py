@@ -11,6 +11,7 @@ import pytest
 
 import capacmd_b200 as cm
 from conftest import golden_paths, rel_err
+from capacmd_b200 import configs
 
 pytestmark = pytest.mark.gpu
 
@@ -143,3 +144,31 @@ def test_tmem_tiles_match_streamed(case, monkeypatch):
         held.md_steps(1)
         streamed.md_steps(1)
     assert rel_err(held.get("rx"), streamed.get("rx")) < 1e-11
+
+
+@pytest.mark.parametrize("case", ["t_2np", "c1_field", "c2"])
+def test_two_level_inner_solves(case):
+    """inner_precond 2: the block-Jacobi inverse with a coarse correction on
+    each group's charge and dipole sums and the nanoparticle constraints
+    (multiplicative: Z c + K (v - A Z c), c = E^-1 Z^T v).  The refined
+    solution meets the same bars against a tight FP64 solve as the
+    block-Jacobi inner solves, through MD steps and preconditioner refreshes."""
+    paths = configs.cached(case) if case == "c2" else golden_paths(case)
+    d = cm.Desc.from_paths(paths)
+    two = cm.Simulation(d, precision=cm.PREC_MIXED, refine_tol=1e-11, inner_precond=2)
+    bj = cm.Simulation(d, precision=cm.PREC_MIXED, refine_tol=1e-11, inner_precond=1)
+    f64 = cm.Simulation(d, solver_tol=1e-26)
+    for s in (two, bj, f64):
+        s.force()
+    x64 = f64.get("vec_pq")
+    assert rel_err(two.get("vec_pq"), x64) < 1e-8
+    assert rel_err(two.forces(), bj.forces()) < 1e-8
+    assert two.stats().solver_rel_residual <= 1e-11
+    two.md_init()
+    bj.md_init()
+    for _ in range(12):
+        two.md_steps(1)
+        bj.md_steps(1)
+    assert rel_err(two.get("vec_pq"), bj.get("vec_pq")) < 1e-7
+    assert rel_err(two.get("rx"), bj.get("rx")) < 1e-9
+    assert two.stats().solver_rel_residual <= 1e-11
