@@ -194,7 +194,8 @@ struct capac_ctx {
     bool overlap = false;
     cudaStream_t stream2 = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
-    double *partials2 = nullptr;       // block partials of the overlapped pair launch
+    double *partials2 = nullptr;       // block partials of the overlapped pair launch (partials_cap)
+    unsigned async_grid = 0;           // blocks of the overlapped pair launch
     cudaStream_t work_stream = nullptr; // stream of the launches being issued (null: `stream`)
 
     // i-cluster x j-cluster list (pair_list 4): per cluster the clusters of

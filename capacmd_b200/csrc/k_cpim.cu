@@ -1071,6 +1071,7 @@ size_t partials_needed(const capac_ctx *c)
 {
     const size_t pair_blocks = grid_for((long)c->N * 32, 256);
     size_t need = pair_blocks * 11;
+    need = std::max(need, (size_t)c->num_sms * 2 * 11);  // resident pair grids (two blocks per SM)
     need = std::max(need, (size_t)grid_for((long)c->N, 256) * 16);
     need = std::max(need, (size_t)(c->M + c->n_nps + 8) * 16);
     need = std::max(need, (size_t)grid_for((long)c->n_mols, 256) * 16);

@@ -1145,7 +1145,9 @@ void launch_pair_nonbonded_async(capac_ctx *c)
     c->work_stream = c->stream2;
     {
         ProfScope ps(c, K_PAIR);
-        launch_pair_cl_t<true, false, true>(c, (unsigned)c->num_sms, c->stream2, c->partials2, false);
+        // one block per SM, and no more blocks than warps have clusters to take
+        c->async_grid = std::min((unsigned)c->num_sms, pair_grid(c));
+        launch_pair_cl_t<true, false, true>(c, c->async_grid, c->stream2, c->partials2, false);
     }
     c->work_stream = nullptr;
     ++c->launches;
@@ -1160,7 +1162,7 @@ void launch_pair_join(capac_ctx *c)
     CAPAC_CUDA(cudaStreamWaitEvent(c->stream, c->ev_join, 0));
     static const int pot_slots[11] = {7, 8, -1, -1, -1, -1, -1, -1, -1, -1, -1};
     static const int vir_slots[11] = {-1, -1, 0, 1, 2, 3, 4, 5, 6, 7, 8};
-    launch_finalize(c, c->num_sms, 11, pot_slots, vir_slots, c->partials2);
+    launch_finalize(c, (int)c->async_grid, 11, pot_slots, vir_slots, c->partials2);
     {
         ProfScope ps(c, K_PAIR);
         launch_pair_cl_t<false, true, true>(c, pair_grid(c), c->stream, c->partials, true);
