@@ -524,7 +524,7 @@ int capac_create(const capac_desc *d, const capac_options *opt, capac_ctx **out)
                                     CAPAC_CUDA(cudaMemsetAsync(c->gvec, 0, sizeof(double) * nv, s));
                                     c->grouped = true;
                                     const int nc = coarse_columns(M, d->n_nps);
-                                    if (o.inner_precond == 2 && nc <= 512) {
+                                    if (o.inner_precond == 2 && nc <= coarse_columns_max()) {
                                         c->twolevel = true;
                                         c->cz_nc = nc;
                                         c->cz_az = dalloc<float>(coarse_az_floats(M, d->n_nps));

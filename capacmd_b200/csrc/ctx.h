@@ -336,6 +336,7 @@ int bicgstab_coop(capac_ctx *c, const double *b, double *x, double tol, double s
 // group-ordered solver (k_solve_coop.cu): internal vector length, blocks
 int group_tmem_tiles();
 int coarse_columns(int M, int n_nps);
+int coarse_columns_max();  // the most coarse columns the solver holds
 size_t coarse_az_floats(int M, int n_nps);
 void launch_coarse_refresh(capac_ctx *c);
 size_t group_rows(int M, int n_nps);

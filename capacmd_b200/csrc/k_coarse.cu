@@ -35,6 +35,7 @@ constexpr int kPlanes = 10;
 constexpr int kTileElems = kPlanes * kT * kT;
 constexpr int kRows = 4 * kT;  // internal rows of a group
 constexpr int kInvThreads = 1024;
+constexpr int kMaxCoarse = 384;  // coarse columns the inversion handles (2 kMaxCoarse <= kInvThreads)
 
 __host__ __device__ __forceinline__ size_t tile_index(int I, int J, int nT)
 {
@@ -161,6 +162,7 @@ __global__ void __launch_bounds__(kInvThreads) k_coarse_invert(int nc, double *_
     __shared__ int wi[kInvThreads / 32];
     __shared__ int piv, bad;
     __shared__ double amax;
+    __shared__ double fcol[kMaxCoarse];
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, w2 = 2 * nc;
     if (tid == 0) bad = 0;
     {
@@ -224,15 +226,18 @@ __global__ void __launch_bounds__(kInvThreads) k_coarse_invert(int nc, double *_
             }
         __syncthreads();
         const double inv = 1.0 / aug[(size_t)k * w2 + k];
+        for (int i = tid; i < nc; i += blockDim.x) fcol[i] = i == k ? 0.0 : aug[(size_t)i * w2 + k];
         __syncthreads();
         for (int j = tid; j < w2; j += blockDim.x) aug[(size_t)k * w2 + j] *= inv;
         __syncthreads();
-        // eliminate column k from every other row (row i's factor read
-        // before any thread of the row changes it: one row per thread group)
-        for (int q = tid; q < nc * w2; q += blockDim.x) {
-            const int i = q / w2, j = q % w2;
-            if (i == k || j == k) continue;
-            aug[(size_t)i * w2 + j] -= aug[(size_t)i * w2 + k] * aug[(size_t)k * w2 + j];
+        // eliminate column k from every other row: thread j owns column j
+        // (the factors of column k were saved in fcol before any change)
+        if (tid < w2 && tid != k) {
+            const double rk = aug[(size_t)k * w2 + tid];
+            double *colj = aug + tid;
+#pragma unroll 4
+            for (int i = 0; i < nc; ++i)
+                if (i != k) colj[(size_t)i * w2] = fma(-fcol[i], rk, colj[(size_t)i * w2]);
         }
         __syncthreads();
         for (int i = tid; i < nc; i += blockDim.x)
@@ -250,6 +255,7 @@ __global__ void __launch_bounds__(kInvThreads) k_coarse_invert(int nc, double *_
 }  // namespace
 
 int coarse_columns(int M, int n_nps) { return 4 * precond_groups(M) + n_nps; }
+static_assert(2 * kMaxCoarse <= kInvThreads, "one thread per column of [E | I]");
 
 size_t coarse_az_floats(int M, int n_nps)
 {

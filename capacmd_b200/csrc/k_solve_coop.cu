@@ -1289,7 +1289,7 @@ __device__ void reduce_group(const GroupArgs &A, const PassScalars &S, double *b
     }
 }
 
-constexpr int kCoarseMax = 512;  // coarse columns the solver's shared buffer holds
+constexpr int kCoarseMax = 384;  // coarse columns the solver's shared buffer holds
 
 // The reductions of reduce_group with the two-level operator of k_coarse.cu
 // in place of the block-Jacobi K alone: first every group's rows of `out`
@@ -1297,12 +1297,12 @@ constexpr int kCoarseMax = 512;  // coarse columns the solver's shared buffer ho
 // sums (and the constraint rows) into zbuf; a grid barrier; then in every
 // block c = E^-1 zbuf, and for its groups K out = Z c + K (out - (A Z) c)
 // with the dots of K out.  Returns false when the grid barrier gave up.
-// scratch: 256 + kCoarseMax doubles of shared memory (the pass inputs' buffer,
-// idle between passes).
+// scratch: 256 + 2 kCoarseMax doubles of shared memory (the pass inputs'
+// buffer, idle between passes).
 template <int RED>
 __device__ bool reduce_group2(const GroupArgs &A, const PassScalars &S, double *bp, bool products, double *scratch)
 {
-    double *vrow = scratch, *hsum = scratch + 128, *cc = scratch + 256;
+    double *vrow = scratch, *hsum = scratch + 128, *cc = scratch + 256, *zs = scratch + 256 + kCoarseMax;
     const int nG = A.nG, nc = A.nc, tid = threadIdx.x;
     const double *in = RED == RED_START ? A.xi : (RED == RED_V ? A.yb[S.cur ^ 1] : A.z);
     double *outv = RED == RED_START ? A.r : (RED == RED_V ? A.v : A.t);
@@ -1400,11 +1400,22 @@ __device__ bool reduce_group2(const GroupArgs &A, const PassScalars &S, double *
 
     const bool mine = (int)blockIdx.x < nG || (int)gridDim.x - 1 - (int)blockIdx.x < A.n_nps;
     if (mine) {
-        // c = E^-1 zbuf (E^-1 symmetric, stored so that thread i reads a column)
+        // c = E^-1 zbuf (E^-1 symmetric, stored so that thread i reads a
+        // column; four independent sums keep the loads in flight)
+        for (int j = tid; j < nc; j += blockDim.x) zs[j] = __ldcg(A.zbuf + j);
+        __syncthreads();
         for (int i = tid; i < nc; i += blockDim.x) {
-            double s = 0.0;
-            for (int j = 0; j < nc; ++j) s = fma((double)__ldg(A.einv + (size_t)j * nc + i), __ldcg(A.zbuf + j), s);
-            cc[i] = s;
+            const float *col = A.einv + i;
+            double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+            int j = 0;
+            for (; j + 4 <= nc; j += 4) {
+                s0 = fma((double)__ldg(col + (size_t)j * nc), zs[j], s0);
+                s1 = fma((double)__ldg(col + (size_t)(j + 1) * nc), zs[j + 1], s1);
+                s2 = fma((double)__ldg(col + (size_t)(j + 2) * nc), zs[j + 2], s2);
+                s3 = fma((double)__ldg(col + (size_t)(j + 3) * nc), zs[j + 3], s3);
+            }
+            for (; j < nc; ++j) s0 = fma((double)__ldg(col + (size_t)j * nc), zs[j], s0);
+            cc[i] = (s0 + s1) + (s2 + s3);
         }
         __syncthreads();
     }
@@ -1412,8 +1423,16 @@ __device__ bool reduce_group2(const GroupArgs &A, const PassScalars &S, double *
         const int o = tid & 127, h = tid >> 7;
         // (A Z c) of the group's rows: two halves of the columns
         const float *az = A.az + (size_t)G * nc * 128 + o;
-        double s = 0.0;
-        for (int j = h; j < nc; j += 2) s = fma((double)__ldg(az + (size_t)j * 128), cc[j], s);
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+        int j = h;
+        for (; j + 6 < nc; j += 8) {
+            s0 = fma((double)__ldg(az + (size_t)j * 128), cc[j], s0);
+            s1 = fma((double)__ldg(az + (size_t)(j + 2) * 128), cc[j + 2], s1);
+            s2 = fma((double)__ldg(az + (size_t)(j + 4) * 128), cc[j + 4], s2);
+            s3 = fma((double)__ldg(az + (size_t)(j + 6) * 128), cc[j + 6], s3);
+        }
+        for (; j < nc; j += 2) s0 = fma((double)__ldg(az + (size_t)j * 128), cc[j], s0);
+        const double s = (s0 + s1) + (s2 + s3);
         if (h == 1) hsum[o] = s;
         __syncthreads();
         if (h == 0) {
@@ -1476,7 +1495,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_bicgstab_group(GroupArgs A)
     __shared__ __align__(8) uint64_t ring_bar[Stages];
     PassSmem<float> &psm = *reinterpret_cast<PassSmem<float> *>(ring_smem + ring_bytes<float>());
     // the pass inputs' buffer, idle between passes, holds the two-level reductions' scratch
-    static_assert(sizeof(psm.in) >= (256 + kCoarseMax) * sizeof(double), "reduction scratch does not fit");
+    static_assert(sizeof(psm.in) >= (256 + 2 * kCoarseMax) * sizeof(double), "reduction scratch does not fit");
     double *pscratch = reinterpret_cast<double *>(&psm.in[0][0][0][0]);
     SolverScalars *ss = A.ss;
     const int ni = A.ni;
@@ -1875,6 +1894,7 @@ int bicgstab_group(capac_ctx *c, const double *b, double *x, double tol, double 
 }
 
 int group_tmem_tiles() { return kResTiles; }
+int coarse_columns_max() { return kCoarseMax; }
 size_t group_rows(int M, int n_nps) { return (size_t)128 * precond_groups(M) + n_nps; }
 
 // Blocks of the group-ordered solver: two per SM when they fit, 0 if the
