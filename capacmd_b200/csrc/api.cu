@@ -498,7 +498,7 @@ int capac_create(const capac_desc *d, const capac_options *opt, capac_ctx **out)
                         if (c->coop_grid > 0) {
                             c->coop_bp = dalloc<double>(coop_partial_doubles(c->coop_grid));
                             c->coop_bar = dalloc<unsigned char>(coop_barrier_bytes());
-                            if (mixed && (o.inner_precond == 1 || o.inner_precond == 2)) {
+                            if (mixed && o.inner_precond >= 1 && o.inner_precond <= 3) {
                                 const std::vector<int> g =
                                     precond_group_atoms(M, d->metal_min, d->rx, d->ry, d->rz);
                                 c->g_atoms = dupload(g.data(), g.size(), s);
@@ -523,11 +523,13 @@ int capac_create(const capac_desc *d, const capac_options *opt, capac_ctx **out)
                                     c->gvec = dalloc<double>(nv);
                                     CAPAC_CUDA(cudaMemsetAsync(c->gvec, 0, sizeof(double) * nv, s));
                                     c->grouped = true;
-                                    const int nc = coarse_columns(M, d->n_nps);
-                                    if (o.inner_precond == 2 && nc <= coarse_columns_max()) {
+                                    const int nm = o.inner_precond == 3 ? 4 : 1;
+                                    const int nc = coarse_columns(M, d->n_nps, nm);
+                                    if (o.inner_precond >= 2 && nc <= coarse_columns_max()) {
                                         c->twolevel = true;
+                                        c->cz_modes = nm;
                                         c->cz_nc = nc;
-                                        c->cz_az = dalloc<float>(coarse_az_floats(M, d->n_nps));
+                                        c->cz_az = dalloc<float>(coarse_az_floats(M, d->n_nps, nm));
                                         c->cz_einv = dalloc<float>((size_t)nc * nc);
                                         c->cz_aug = dalloc<double>((size_t)nc * 2 * nc);
                                         c->cz_zbuf = dalloc<double>(nc);
@@ -569,7 +571,7 @@ int capac_create(const capac_desc *d, const capac_options *opt, capac_ctx **out)
 
             c->partials_cap = partials_needed(c);
             c->partials = dalloc<double>(c->partials_cap);
-            if (o.precision == CAPAC_PREC_MIXED && d->n_metal > 0 && d->use_cpff && !getenv("CAPAC_NO_OVERLAP")) {
+            if (o.precision == CAPAC_PREC_MIXED && d->n_metal > 0 && d->use_cpff && getenv("CAPAC_OVERLAP")) {
                 c->overlap = true;
                 CAPAC_CUDA(cudaStreamCreateWithFlags(&c->stream2, cudaStreamNonBlocking));
                 CAPAC_CUDA(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));

@@ -231,7 +231,8 @@ struct capac_ctx {
     int inner_stall = 0;         // set during the refinement's inner solves: see GroupArgs::stall
     // two-level inner preconditioner (inner_precond 2, k_coarse.cu)
     bool twolevel = false;
-    int cz_nc = 0;               // coarse columns: 4 per group and one per nanoparticle
+    int cz_nc = 0;               // coarse columns: cz_modes per group and one per nanoparticle
+    int cz_modes = 1;            // 1: the group's charge sum; 4: its dipole sums and charge sum
     float *cz_az = nullptr;      // A Z
     float *cz_einv = nullptr;    // E^-1
     double *cz_aug = nullptr;    // [E | I] workspace of the inversion
@@ -335,9 +336,9 @@ size_t coop_partial_doubles(int grid);
 int bicgstab_coop(capac_ctx *c, const double *b, double *x, double tol, double skip);
 // group-ordered solver (k_solve_coop.cu): internal vector length, blocks
 int group_tmem_tiles();
-int coarse_columns(int M, int n_nps);
+int coarse_columns(int M, int n_nps, int modes);
 int coarse_columns_max();  // the most coarse columns the solver holds
-size_t coarse_az_floats(int M, int n_nps);
+size_t coarse_az_floats(int M, int n_nps, int modes);
 void launch_coarse_refresh(capac_ctx *c);
 size_t group_rows(int M, int n_nps);
 int group_grid_size(int device, bool hold);

@@ -1,11 +1,12 @@
-// Two-level preconditioner of the mixed path's inner solves (inner_precond 2).
+// Two-level preconditioner of the mixed path's inner solves (inner_precond 2, 3).
 //
 // The block-Jacobi inverse K of the 32-atom groups leaves the smooth error
 // modes of the CPIM system (a group's total charge and total dipole against
 // the others', the nanoparticles' constraint rows) to the Krylov iteration.
-// The coarse space Z holds, per group g, four columns (the indicator of its
-// atoms' x, y, z dipole rows and of their charge rows) and one column per
-// nanoparticle constraint row; E = Z^T A Z (nc = 4 nG + n_NP).  The inner
+// The coarse space Z holds, per group g, the indicator of its atoms' charge
+// rows (inner_precond 2) or four columns, the indicators of their x, y, z
+// dipole rows and of their charge rows (3), and one column per nanoparticle
+// constraint row; E = Z^T A Z (nc = nm nG + n_NP, nm = 1 or 4).  The inner
 // solves use the multiplicative two-level operator
 //     K2 v = Z c + K (v - A Z c),   c = E^-1 Z^T v,
 // a fixed linear operator as long as Z, A Z and E^-1 are (they are refreshed
@@ -18,7 +19,7 @@
 // couplings.  E sums A Z over each group's rows; E^-1 by Gauss-Jordan with
 // partial pivoting in FP64 in one block.
 //
-// Layout: az[(g * nc + j) * 128 + r] for internal row 128 g + r (column
+// Layout (group g's columns at nm g ..): az[(g * nc + j) * 128 + r] for internal row 128 g + r (column
 // j contiguous over the group's rows), then az[128 nG nc + k * nc + j] for
 // constraint row k; einv[j * nc + i] = (E^-1)[i][j] (E is symmetric).
 #include <algorithm>
@@ -65,7 +66,7 @@ __device__ __forceinline__ float block_entry(const float (&s)[kPlanes], int c, i
 // One block per tile (I, J), I <= J: the A Z entries of the rows of group I
 // in the columns of group J and, for I < J, of the rows of J in the columns
 // of I; for I = J the strict upper tile gives both halves, plus the diagonal.
-__global__ void __launch_bounds__(256) k_coarse_az(const float *__restrict__ mat, int nG, int nc,
+__global__ void __launch_bounds__(256) k_coarse_az(const float *__restrict__ mat, int nG, int nc, int nm,
                                                    const int *__restrict__ g_atoms, double inv_polar,
                                                    double inv_capac, float *__restrict__ az)
 {
@@ -82,8 +83,8 @@ __global__ void __launch_bounds__(256) k_coarse_az(const float *__restrict__ mat
         (col ? cs : rs)[p][i] = s;
     }
     __syncthreads();
-    for (int q = threadIdx.x; q < kRows * 4; q += blockDim.x) {
-        const int r = q >> 2, d = q & 3, a = r >> 2, c = r & 3;
+    for (int q = threadIdx.x; q < kRows * nm; q += blockDim.x) {
+        const int r = q / nm, m = q % nm, d = nm == 4 ? m : 3, a = r >> 2, c = r & 3;
         float sr[kPlanes], sc[kPlanes];
 #pragma unroll
         for (int p = 0; p < kPlanes; ++p) {
@@ -96,11 +97,11 @@ __global__ void __launch_bounds__(256) k_coarse_az(const float *__restrict__ mat
             v += block_entry(sc, d, c);  // the pairs b < a, stored as (b, a)
             if (c == d && g_atoms[(size_t)I * kT + a] >= 0) v += (float)(c < 3 ? inv_polar : -inv_capac);
         }
-        az[((size_t)I * nc + 4 * J + d) * kRows + r] = v;
+        az[((size_t)I * nc + nm * J + m) * kRows + r] = v;
         if (I != J) {
             // rows of J (atom a of J here), column (I, d): sum over the atoms
             // of I of block (i, a)^T[c][d] = block (i, a)[d][c]
-            az[((size_t)J * nc + 4 * I + d) * kRows + r] = block_entry(sc, d, c);
+            az[((size_t)J * nc + nm * I + m) * kRows + r] = block_entry(sc, d, c);
         }
     }
 }
@@ -108,7 +109,8 @@ __global__ void __launch_bounds__(256) k_coarse_az(const float *__restrict__ mat
 // The constraint columns and rows of A Z: charge row of an atom of NP k in
 // column 4 nG + k; constraint row k in the charge column of each group with
 // the count of that group's atoms in NP k.
-__global__ void k_coarse_az_np(int nG, int nc, int n_nps, const int *__restrict__ slot_np, float *__restrict__ az)
+__global__ void k_coarse_az_np(int nG, int nc, int nm, int n_nps, const int *__restrict__ slot_np,
+                               float *__restrict__ az)
 {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     const size_t base = (size_t)nG * nc * kRows;
@@ -116,13 +118,13 @@ __global__ void k_coarse_az_np(int nG, int nc, int n_nps, const int *__restrict_
         const int g = q / kRows, r = q % kRows, a = r >> 2, c = r & 3;
         const int k = slot_np[(size_t)g * kT + a];
         for (int j = 0; j < n_nps; ++j)
-            az[((size_t)g * nc + 4 * nG + j) * kRows + r] = (c == 3 && k == j) ? 1.f : 0.f;
+            az[((size_t)g * nc + nm * nG + j) * kRows + r] = (c == 3 && k == j) ? 1.f : 0.f;
     }
     if (q < n_nps * nc) {
         const int k = q / nc, j = q % nc;
         float v = 0.f;
-        if (j < 4 * nG && (j & 3) == 3) {
-            const int g = j >> 2;
+        if (j < nm * nG && (nm == 1 || (j & 3) == 3)) {  // a group's charge column
+            const int g = j / nm;
             for (int a = 0; a < kT; ++a) v += slot_np[(size_t)g * kT + a] == k ? 1.f : 0.f;
         }
         az[base + (size_t)k * nc + j] = v;
@@ -130,20 +132,20 @@ __global__ void k_coarse_az_np(int nG, int nc, int n_nps, const int *__restrict_
 }
 
 // E = Z^T (A Z) into the left half of the augmented [E | I] (FP64, nc x 2 nc).
-__global__ void k_coarse_e(int nG, int nc, const int *__restrict__ g_atoms, const float *__restrict__ az,
+__global__ void k_coarse_e(int nG, int nc, int nm, const int *__restrict__ g_atoms, const float *__restrict__ az,
                            double *__restrict__ aug)
 {
     const int i = blockIdx.x;
     for (int j = threadIdx.x; j < 2 * nc; j += blockDim.x) {
         double v = 0.0;
         if (j < nc) {
-            if (i < 4 * nG) {
-                const int g = i >> 2, c = i & 3;
+            if (i < nm * nG) {
+                const int g = i / nm, c = nm == 4 ? (i & 3) : 3;
                 const float *col = az + ((size_t)g * nc + j) * kRows;
                 for (int a = 0; a < kT; ++a)
                     if (g_atoms[(size_t)g * kT + a] >= 0) v += (double)col[4 * a + c];
             } else {
-                v = (double)az[(size_t)nG * nc * kRows + (size_t)(i - 4 * nG) * nc + j];
+                v = (double)az[(size_t)nG * nc * kRows + (size_t)(i - nm * nG) * nc + j];
             }
         } else {
             v = (j - nc == i) ? 1.0 : 0.0;
@@ -254,26 +256,26 @@ __global__ void __launch_bounds__(kInvThreads) k_coarse_invert(int nc, double *_
 
 }  // namespace
 
-int coarse_columns(int M, int n_nps) { return 4 * precond_groups(M) + n_nps; }
+int coarse_columns(int M, int n_nps, int nm) { return nm * precond_groups(M) + n_nps; }
 static_assert(2 * kMaxCoarse <= kInvThreads, "one thread per column of [E | I]");
 
-size_t coarse_az_floats(int M, int n_nps)
+size_t coarse_az_floats(int M, int n_nps, int nm)
 {
-    const int nG = precond_groups(M), nc = coarse_columns(M, n_nps);
+    const int nG = precond_groups(M), nc = coarse_columns(M, n_nps, nm);
     return (size_t)nG * nc * kRows + (size_t)n_nps * nc;
 }
 
 void launch_coarse_refresh(capac_ctx *c)
 {
-    const int nG = precond_groups(c->M), nc = coarse_columns(c->M, c->n_nps);
+    const int nG = precond_groups(c->M), nm = c->cz_modes, nc = coarse_columns(c->M, c->n_nps, nm);
     const int ntiles = nG * (nG + 1) / 2;
     cudaStream_t s = c->stream;
     ProfScope ps(c, K_MATRIX);
-    k_coarse_az<<<ntiles, 256, 0, s>>>(static_cast<const float *>(c->msym), nG, nc, c->g_atoms, c->P.inv_polar,
-                                       c->P.inv_capac, c->cz_az);
+    k_coarse_az<<<ntiles, 256, 0, s>>>(static_cast<const float *>(c->msym), nG, nc, nm, c->g_atoms,
+                                       c->P.inv_polar, c->P.inv_capac, c->cz_az);
     const int nq = std::max(nG * kRows, c->n_nps * nc);
-    k_coarse_az_np<<<grid_for(nq, 256), 256, 0, s>>>(nG, nc, c->n_nps, c->slot_np, c->cz_az);
-    k_coarse_e<<<nc, 256, 0, s>>>(nG, nc, c->g_atoms, c->cz_az, c->cz_aug);
+    k_coarse_az_np<<<grid_for(nq, 256), 256, 0, s>>>(nG, nc, nm, c->n_nps, c->slot_np, c->cz_az);
+    k_coarse_e<<<nc, 256, 0, s>>>(nG, nc, nm, c->g_atoms, c->cz_az, c->cz_aug);
     k_coarse_invert<<<1, kInvThreads, 0, s>>>(nc, c->cz_aug, c->cz_einv, c->flags + 6);
     c->launches += 4;
 }

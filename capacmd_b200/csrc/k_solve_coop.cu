@@ -956,6 +956,7 @@ struct GroupArgs {
     int M, nG, ntiles, n_nps, ni, max_iter;
     int stall;                   // > 0: stop (status 1) after this many iterations without halving (r, r)
     int nc;                      // > 0: the two-level operator with nc coarse columns (k_coarse.cu)
+    int nm;                      // coarse columns per group: 1 (charge) or 4 (dipole x, y, z, charge)
     const float *az, *einv;      // A Z, E^-1 of the coarse space
     double *zbuf;                // Z^T of the vector being preconditioned (nc)
     long spin_limit;
@@ -1360,10 +1361,11 @@ __device__ bool reduce_group2(const GroupArgs &A, const PassScalars &S, double *
             vrow[o] = A.g_atoms[row >> 2] >= 0 ? out : 0.0;
         }
         __syncthreads();
-        if (tid < 4) {  // the group's mode sums (padding rows hold zero)
+        if (tid < A.nm) {  // the group's mode sums (padding rows hold zero)
+            const int c = A.nm == 4 ? tid : 3;
             double zs = 0.0;
-            for (int a = 0; a < kT; ++a) zs += vrow[4 * a + tid];
-            A.zbuf[4 * G + tid] = zs;
+            for (int a = 0; a < kT; ++a) zs += vrow[4 * a + c];
+            A.zbuf[A.nm * G + tid] = zs;
         }
         __syncthreads();
     }
@@ -1392,7 +1394,7 @@ __device__ bool reduce_group2(const GroupArgs &A, const PassScalars &S, double *
                 d[6] += val * val;
             }
             outv[row] = out;
-            A.zbuf[4 * nG + k] = out;
+            A.zbuf[A.nm * nG + k] = out;
         }
         __syncthreads();
     }
@@ -1451,7 +1453,8 @@ __device__ bool reduce_group2(const GroupArgs &A, const PassScalars &S, double *
             acc += __shfl_xor_sync(0xffffffffu, acc, 1);
             if (half == 0) {
                 const int row = 128 * G + o2;
-                if (A.g_atoms[row >> 2] >= 0) acc += cc[4 * G + (o2 & 3)];
+                if (A.g_atoms[row >> 2] >= 0 && (A.nm == 4 || (o2 & 3) == 3))
+                    acc += cc[A.nm * G + (A.nm == 4 ? (o2 & 3) : 0)];
                 kout[row] = acc;
                 if (RED == RED_T) {
                     d[0] += acc * __ldcg(A.z + row);
@@ -1467,7 +1470,7 @@ __device__ bool reduce_group2(const GroupArgs &A, const PassScalars &S, double *
             const float *azl = A.az + (size_t)nG * nc * 128 + (size_t)k * nc;
             double s = 0.0;
             for (int j = 0; j < nc; ++j) s = fma((double)__ldg(azl + j), cc[j], s);
-            const double kv = __ldcg(outv + row) - s + cc[4 * nG + k];  // K = 1 on the constraint rows
+            const double kv = __ldcg(outv + row) - s + cc[A.nm * nG + k];  // K = 1 on the constraint rows
             kout[row] = kv;
             if (RED == RED_T) {
                 d[0] += kv * __ldcg(A.z + row);
@@ -1853,6 +1856,7 @@ int bicgstab_group(capac_ctx *c, const double *b, double *x, double tol, double 
     A.max_iter = solver_max_iter(c);
     A.stall = c->inner_stall;
     A.nc = c->twolevel ? c->cz_nc : 0;
+    A.nm = c->cz_modes;
     A.az = c->cz_az;
     A.einv = c->cz_einv;
     A.zbuf = c->cz_zbuf;

@@ -266,22 +266,23 @@ def test_cluster_pair_list_falls_back_in_a_small_box():
 
 @pytest.mark.parametrize("case", ["t_2np", "c2"])
 def test_pairs_overlapped_with_the_solve(case, monkeypatch):
-    """The mixed path runs the nonbonded pairs on a second stream while the
-    CPIM stages and solve run, then the CPIM forces on water atoms over the
-    clusters next to metal; against the same path run in one stream
-    (CAPAC_NO_OVERLAP): forces, energies, virial and induced vector agree
-    within the rounding of the neighbour-side atomic adds, through MD steps
-    and list rebuilds."""
+    """CAPAC_OVERLAP: the mixed path runs the nonbonded pairs on a second
+    stream while the CPIM stages and solve run, then the CPIM forces on water
+    atoms over the clusters next to metal; against the same path in one
+    stream: forces, energies, virial and induced vector agree within FP32
+    rounding, through MD steps and list rebuilds."""
     paths = configs.cached(case) if case == "c2" else golden_paths(case)
+    monkeypatch.setenv("CAPAC_OVERLAP", "1")
     d, ovl = _mixed(paths, refine_tol=1e-11)
-    monkeypatch.setenv("CAPAC_NO_OVERLAP", "1")
+    monkeypatch.delenv("CAPAC_OVERLAP")
     _, one = _mixed(paths, refine_tol=1e-11)
-    monkeypatch.delenv("CAPAC_NO_OVERLAP")
     for s in (ovl, one):
         s.set("vec_pq", np.zeros(d.n_mat))
         s.force()
     assert _uses_clusters(ovl)
-    assert rel_err(ovl.forces(), one.forces()) < 1e-12
+    # the pair force and the CPIM force of a water atom are rounded to FP32
+    # separately here and as one sum on one stream
+    assert rel_err(ovl.forces(), one.forces()) < 1e-6
     po, p1 = ovl.get("potential"), one.get("potential")
     assert np.abs(po - p1).max() <= 1e-12 * np.abs(p1[1:]).sum()
     assert rel_err(ovl.get("virial"), one.get("virial")) < 1e-12

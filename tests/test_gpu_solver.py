@@ -146,16 +146,18 @@ def test_tmem_tiles_match_streamed(case, monkeypatch):
     assert rel_err(held.get("rx"), streamed.get("rx")) < 1e-11
 
 
+@pytest.mark.parametrize("precond", [2, 3])
 @pytest.mark.parametrize("case", ["t_2np", "c1_field", "c2"])
-def test_two_level_inner_solves(case):
-    """inner_precond 2: the block-Jacobi inverse with a coarse correction on
-    each group's charge and dipole sums and the nanoparticle constraints
-    (multiplicative: Z c + K (v - A Z c), c = E^-1 Z^T v).  The refined
+def test_two_level_inner_solves(case, precond):
+    """inner_precond 2 and 3: the block-Jacobi inverse with a coarse
+    correction on each group's charge sum (3: and its dipole sums) and the
+    nanoparticle constraints (multiplicative: Z c + K (v - A Z c),
+    c = E^-1 Z^T v).  The refined
     solution meets the same bars against a tight FP64 solve as the
     block-Jacobi inner solves, through MD steps and preconditioner refreshes."""
     paths = configs.cached(case) if case == "c2" else golden_paths(case)
     d = cm.Desc.from_paths(paths)
-    two = cm.Simulation(d, precision=cm.PREC_MIXED, refine_tol=1e-11, inner_precond=2)
+    two = cm.Simulation(d, precision=cm.PREC_MIXED, refine_tol=1e-11, inner_precond=precond)
     bj = cm.Simulation(d, precision=cm.PREC_MIXED, refine_tol=1e-11, inner_precond=1)
     f64 = cm.Simulation(d, solver_tol=1e-26)
     for s in (two, bj, f64):
