@@ -530,6 +530,7 @@ int capac_create(const capac_desc *d, const capac_options *opt, capac_ctx **out)
                                         c->cz_modes = nm;
                                         c->cz_nc = nc;
                                         c->cz_az = dalloc<float>(coarse_az_floats(M, d->n_nps, nm));
+                                        c->cz_w = dalloc<float>(coarse_az_floats(M, d->n_nps, nm));
                                         c->cz_einv = dalloc<float>((size_t)nc * nc);
                                         c->cz_aug = dalloc<double>((size_t)nc * 2 * nc);
                                         c->cz_zbuf = dalloc<double>(nc);
@@ -626,7 +627,7 @@ int capac_destroy(capac_ctx *c)
                    c->cell_start, c->spos, c->sort_tmp, c->flags, c->cl_atoms, c->cl_cell_start, c->cl_counts,
                    c->cl_nbr, c->cl_nnb, c->cl_metal, c->cl_of, c->cl_next, c->cl_sel, c->n_cl_sel, c->partials2,
                    c->cp_list,
-                   c->cp_n, c->cp_cent, c->cp_off, c->cp_ti, c->cz_az, c->cz_einv, c->cz_aug, c->cz_zbuf, c->scan_tmp, c->isd, c->vec_ext, c->vec_pq,
+                   c->cp_n, c->cp_cent, c->cp_off, c->cp_ti, c->cz_az, c->cz_w, c->cz_einv, c->cz_aug, c->cz_zbuf, c->scan_tmp, c->isd, c->vec_ext, c->vec_pq,
                    c->diag, c->mat, c->matf, c->msym, c->sympart, c->coop_bp, c->coop_bar, c->g_atoms, c->dinv, c->slot_np, c->np_off, c->np_rows, c->gvec, c->gw, c->em_buf, c->phase_buf, c->rres, c->dcorr, c->xprev, c->bw, c->bwf, c->ss, c->partials, c->pot, c->vir, c->th};
     for (void *p : dev)
         if (p) cudaFree(p);

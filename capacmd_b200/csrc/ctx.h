@@ -234,6 +234,7 @@ struct capac_ctx {
     int cz_nc = 0;               // coarse columns: cz_modes per group and one per nanoparticle
     int cz_modes = 1;            // 1: the group's charge sum; 4: its dipole sums and charge sum
     float *cz_az = nullptr;      // A Z
+    float *cz_w = nullptr;       // (A Z) E^-1
     float *cz_einv = nullptr;    // E^-1
     double *cz_aug = nullptr;    // [E | I] workspace of the inversion
     double *cz_zbuf = nullptr;   // Z^T v inside the solver

@@ -19,6 +19,7 @@
 // couplings.  E sums A Z over each group's rows; E^-1 by Gauss-Jordan with
 // partial pivoting in FP64 in one block.
 //
+// W = (A Z) E^-1, in the layout of A Z, is what the solver reads.
 // Layout (group g's columns at nm g ..): az[(g * nc + j) * 128 + r] for internal row 128 g + r (column
 // j contiguous over the group's rows), then az[128 nG nc + k * nc + j] for
 // constraint row k; einv[j * nc + i] = (E^-1)[i][j] (E is symmetric).
@@ -254,6 +255,45 @@ __global__ void __launch_bounds__(kInvThreads) k_coarse_invert(int nc, double *_
     if (tid == 0) *bad_out = bad;
 }
 
+// W = (A Z) E^-1 in the layout of A Z, so that the solver forms A Z c as
+// W (Z^T v) with no product by E^-1 of its own: block (g, 32 columns of W),
+// thread r one internal row of group g (the constraint rows: g = nG), the
+// 32 columns of E^-1 staged per chunk of k in shared memory.
+__global__ void __launch_bounds__(128) k_coarse_w(int nG, int nc, int n_nps, const float *__restrict__ az,
+                                                  const float *__restrict__ einv, float *__restrict__ w)
+{
+    __shared__ float es[32][33];
+    const int g = blockIdx.x, j0 = blockIdx.y * 32, r = threadIdx.x;
+    const size_t lam = (size_t)nG * nc * kRows;
+    const bool rows_ok = g < nG || r < n_nps;
+    float acc[32];
+#pragma unroll
+    for (int q = 0; q < 32; ++q) acc[q] = 0.f;
+    for (int k0 = 0; k0 < nc; k0 += 32) {
+        __syncthreads();
+        for (int q = threadIdx.x; q < 32 * 32; q += blockDim.x) {
+            const int kk = q >> 5, jj = q & 31;
+            es[kk][jj] = (k0 + kk < nc && j0 + jj < nc) ? einv[(size_t)(k0 + kk) * nc + j0 + jj] : 0.f;
+        }
+        __syncthreads();
+        if (rows_ok) {
+            const int kn = min(32, nc - k0);
+            for (int kk = 0; kk < kn; ++kk) {
+                const float a = g < nG ? az[((size_t)g * nc + k0 + kk) * kRows + r] : az[lam + (size_t)r * nc + k0 + kk];
+#pragma unroll
+                for (int q = 0; q < 32; ++q) acc[q] = fmaf(a, es[kk][q], acc[q]);
+            }
+        }
+    }
+    if (!rows_ok) return;
+    for (int q = 0; q < 32 && j0 + q < nc; ++q) {
+        if (g < nG)
+            w[((size_t)g * nc + j0 + q) * kRows + r] = acc[q];
+        else
+            w[lam + (size_t)r * nc + j0 + q] = acc[q];
+    }
+}
+
 }  // namespace
 
 int coarse_columns(int M, int n_nps, int nm) { return nm * precond_groups(M) + n_nps; }
@@ -277,7 +317,9 @@ void launch_coarse_refresh(capac_ctx *c)
     k_coarse_az_np<<<grid_for(nq, 256), 256, 0, s>>>(nG, nc, nm, c->n_nps, c->slot_np, c->cz_az);
     k_coarse_e<<<nc, 256, 0, s>>>(nG, nc, nm, c->g_atoms, c->cz_az, c->cz_aug);
     k_coarse_invert<<<1, kInvThreads, 0, s>>>(nc, c->cz_aug, c->cz_einv, c->flags + 6);
-    c->launches += 4;
+    k_coarse_w<<<dim3(nG + (c->n_nps > 0 ? 1 : 0), (nc + 31) / 32), kRows, 0, s>>>(nG, nc, c->n_nps, c->cz_az,
+                                                                                    c->cz_einv, c->cz_w);
+    c->launches += 5;
 }
 
 }  // namespace capac

@@ -957,7 +957,7 @@ struct GroupArgs {
     int stall;                   // > 0: stop (status 1) after this many iterations without halving (r, r)
     int nc;                      // > 0: the two-level operator with nc coarse columns (k_coarse.cu)
     int nm;                      // coarse columns per group: 1 (charge) or 4 (dipole x, y, z, charge)
-    const float *az, *einv;      // A Z, E^-1 of the coarse space
+    const float *w, *einv;       // (A Z) E^-1 and E^-1 of the coarse space
     double *zbuf;                // Z^T of the vector being preconditioned (nc)
     long spin_limit;
     double inv_polar, inv_capac;
@@ -1402,38 +1402,33 @@ __device__ bool reduce_group2(const GroupArgs &A, const PassScalars &S, double *
 
     const bool mine = (int)blockIdx.x < nG || (int)gridDim.x - 1 - (int)blockIdx.x < A.n_nps;
     if (mine) {
-        // c = E^-1 zbuf (E^-1 symmetric, stored so that thread i reads a
-        // column; four independent sums keep the loads in flight)
         for (int j = tid; j < nc; j += blockDim.x) zs[j] = __ldcg(A.zbuf + j);
         __syncthreads();
-        for (int i = tid; i < nc; i += blockDim.x) {
-            const float *col = A.einv + i;
-            double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
-            int j = 0;
-            for (; j + 4 <= nc; j += 4) {
-                s0 = fma((double)__ldg(col + (size_t)j * nc), zs[j], s0);
-                s1 = fma((double)__ldg(col + (size_t)(j + 1) * nc), zs[j + 1], s1);
-                s2 = fma((double)__ldg(col + (size_t)(j + 2) * nc), zs[j + 2], s2);
-                s3 = fma((double)__ldg(col + (size_t)(j + 3) * nc), zs[j + 3], s3);
-            }
-            for (; j < nc; ++j) s0 = fma((double)__ldg(col + (size_t)j * nc), zs[j], s0);
-            cc[i] = (s0 + s1) + (s2 + s3);
-        }
-        __syncthreads();
     }
+    const int lane = tid & 31, wid = tid >> 5;
     for (int G = blockIdx.x; G < nG; G += gridDim.x) {
         const int o = tid & 127, h = tid >> 7;
-        // (A Z c) of the group's rows: two halves of the columns
-        const float *az = A.az + (size_t)G * nc * 128 + o;
+        // c of the group's own columns: warp m, lanes over the columns of
+        // row nm G + m of E^-1
+        if (wid < A.nm) {
+            const float *er = A.einv + (size_t)(A.nm * G + wid) * nc;
+            double s = 0.0;
+            for (int j = lane; j < nc; j += 32) s = fma((double)__ldg(er + j), zs[j], s);
+#pragma unroll
+            for (int m = 16; m > 0; m >>= 1) s += __shfl_xor_sync(0xffffffffu, s, m);
+            if (lane == 0) cc[wid] = s;
+        }
+        // (A Z c) of the group's rows = W zbuf: two halves of the columns
+        const float *wg = A.w + (size_t)G * nc * 128 + o;
         double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
         int j = h;
         for (; j + 6 < nc; j += 8) {
-            s0 = fma((double)__ldg(az + (size_t)j * 128), cc[j], s0);
-            s1 = fma((double)__ldg(az + (size_t)(j + 2) * 128), cc[j + 2], s1);
-            s2 = fma((double)__ldg(az + (size_t)(j + 4) * 128), cc[j + 4], s2);
-            s3 = fma((double)__ldg(az + (size_t)(j + 6) * 128), cc[j + 6], s3);
+            s0 = fma((double)__ldg(wg + (size_t)j * 128), zs[j], s0);
+            s1 = fma((double)__ldg(wg + (size_t)(j + 2) * 128), zs[j + 2], s1);
+            s2 = fma((double)__ldg(wg + (size_t)(j + 4) * 128), zs[j + 4], s2);
+            s3 = fma((double)__ldg(wg + (size_t)(j + 6) * 128), zs[j + 6], s3);
         }
-        for (; j < nc; j += 2) s0 = fma((double)__ldg(az + (size_t)j * 128), cc[j], s0);
+        for (; j < nc; j += 2) s0 = fma((double)__ldg(wg + (size_t)j * 128), zs[j], s0);
         const double s = (s0 + s1) + (s2 + s3);
         if (h == 1) hsum[o] = s;
         __syncthreads();
@@ -1453,8 +1448,7 @@ __device__ bool reduce_group2(const GroupArgs &A, const PassScalars &S, double *
             acc += __shfl_xor_sync(0xffffffffu, acc, 1);
             if (half == 0) {
                 const int row = 128 * G + o2;
-                if (A.g_atoms[row >> 2] >= 0 && (A.nm == 4 || (o2 & 3) == 3))
-                    acc += cc[A.nm * G + (A.nm == 4 ? (o2 & 3) : 0)];
+                if (A.g_atoms[row >> 2] >= 0 && (A.nm == 4 || (o2 & 3) == 3)) acc += cc[A.nm == 4 ? (o2 & 3) : 0];
                 kout[row] = acc;
                 if (RED == RED_T) {
                     d[0] += acc * __ldcg(A.z + row);
@@ -1465,16 +1459,27 @@ __device__ bool reduce_group2(const GroupArgs &A, const PassScalars &S, double *
         __syncthreads();
     }
     for (int k = (int)gridDim.x - 1 - (int)blockIdx.x; k < A.n_nps; k += gridDim.x) {
-        if (tid == 0) {
+        if (wid == 0) {
             const int row = 128 * nG + k;
-            const float *azl = A.az + (size_t)nG * nc * 128 + (size_t)k * nc;
-            double s = 0.0;
-            for (int j = 0; j < nc; ++j) s = fma((double)__ldg(azl + j), cc[j], s);
-            const double kv = __ldcg(outv + row) - s + cc[A.nm * nG + k];  // K = 1 on the constraint rows
-            kout[row] = kv;
-            if (RED == RED_T) {
-                d[0] += kv * __ldcg(A.z + row);
-                d[1] += kv * kv;
+            const float *er = A.einv + (size_t)(A.nm * nG + k) * nc;
+            const float *wl = A.w + (size_t)nG * nc * 128 + (size_t)k * nc;
+            double cs = 0.0, ws = 0.0;
+            for (int j = lane; j < nc; j += 32) {
+                cs = fma((double)__ldg(er + j), zs[j], cs);
+                ws = fma((double)__ldg(wl + j), zs[j], ws);
+            }
+#pragma unroll
+            for (int m = 16; m > 0; m >>= 1) {
+                cs += __shfl_xor_sync(0xffffffffu, cs, m);
+                ws += __shfl_xor_sync(0xffffffffu, ws, m);
+            }
+            if (lane == 0) {
+                const double kv = __ldcg(outv + row) - ws + cs;  // K = 1 on the constraint rows
+                kout[row] = kv;
+                if (RED == RED_T) {
+                    d[0] += kv * __ldcg(A.z + row);
+                    d[1] += kv * kv;
+                }
             }
         }
         __syncthreads();
@@ -1857,7 +1862,7 @@ int bicgstab_group(capac_ctx *c, const double *b, double *x, double tol, double 
     A.stall = c->inner_stall;
     A.nc = c->twolevel ? c->cz_nc : 0;
     A.nm = c->cz_modes;
-    A.az = c->cz_az;
+    A.w = c->cz_w;
     A.einv = c->cz_einv;
     A.zbuf = c->cz_zbuf;
     A.spin_limit = c->opt.wait_polls > 0 ? c->opt.wait_polls : kSpinLimit;
