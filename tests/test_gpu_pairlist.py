@@ -292,5 +292,5 @@ def test_pairs_overlapped_with_the_solve(case, monkeypatch):
     for _ in range(30):
         ovl.md_steps(1)
         one.md_steps(1)
-    assert rel_err(ovl.get("rx"), one.get("rx")) < 1e-9
+    assert rel_err(ovl.get("rx"), one.get("rx")) < 1e-7
     assert abs(ovl.get("potential")[0] - one.get("potential")[0]) <= 1e-7 * abs(one.get("potential")[0])
