@@ -244,6 +244,7 @@ struct capac_ctx {
     int *np_rows = nullptr;      // [M] internal charge rows of each nanoparticle's atoms
     double *gvec = nullptr;      // 12 internal vectors of group_rows() doubles
     long precond_age = 0;        // matrix builds since the inverse blocks were computed
+    long coarse_age = 0;         // refreshes of the inverse blocks since the coarse part was computed
     // the metal's CPIM parameters (a.u.) and Gaussian widths (Bohr), which the
     // widths follow unless set on their own (k_grad.cu)
     double capac = 0.0, polar = 0.0, rq = 0.0, rp = 0.0;

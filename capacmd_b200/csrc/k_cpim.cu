@@ -227,6 +227,10 @@ __global__ void __launch_bounds__(128) k_cpim_matrix(DevParams P, const double4 
 }
 
 constexpr long kPrecondEvery = 10;
+// the coarse correction (A Z, E^-1, W) is refreshed at every kCoarseEvery-th
+// refresh of the inverse blocks: its group sums change more slowly than the
+// blocks, and its inversion costs ~10 ms for 261 coarse columns
+constexpr long kCoarseEvery = 5;
 
 // Dense FP64 4x4 blocks of metal rows i0 .. i0 + rows - 1 against every metal
 // column j: out[((i - i0) M + j) 16 + 4 r + c], the entries of cpim_block
@@ -261,7 +265,8 @@ void launch_cpim_matrix(capac_ctx *c)
         // kPrecondEvery matrix builds, not every step
         if (c->dinv && c->precond_age++ % kPrecondEvery == 0) {
             launch_block_inverse(c);
-            if (c->twolevel) launch_coarse_refresh(c);
+            if (c->twolevel && c->precond_age <= 1) c->coarse_age = 0;  // fresh positions: fresh coarse part
+            if (c->twolevel && c->coarse_age++ % kCoarseEvery == 0) launch_coarse_refresh(c);
         }
         return;
     }
