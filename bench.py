@@ -222,7 +222,7 @@ def main() -> int:
     ap.add_argument("--pair-list", type=int, default=0, choices=[0, 1, 2, 3, 4],
                     help="mixed path nonbonded list: 0 (= 2) clusters with every pair once, 1 one list per "
                          "atom, 3 clusters with every pair from both ends, 4 cluster pairs")
-    ap.add_argument("--inner-precond", type=int, default=1, choices=[0, 1, 2, 3],
+    ap.add_argument("--inner-precond", type=int, default=3, choices=[0, 1, 2, 3],
                     help="mixed path inner solves: 0 Jacobi, 1 block-Jacobi, 2 (3) block-Jacobi with a coarse "
                          "correction on group charges (and dipoles)")
     ap.add_argument("--predictor", type=int, default=3, choices=[0, 1, 2, 3],

@@ -168,7 +168,7 @@ class Simulation:
 
     def __init__(self, desc: Desc, precision: int = PREC_FP64, device: int = 0, skin: float = 0.2,
                  solver_tol: float = 0.0, refine_tol: float = 1e-10, max_neighbors: int = 0,
-                 matrix_layout: int = 0, predictor: int = 3, solver_kernel: int = 0, inner_precond: int = 1,
+                 matrix_layout: int = 0, predictor: int = 3, solver_kernel: int = 0, inner_precond: int = 3,
                  pair_list: int = 0, max_iter: int = 0, wait_polls: int = 0):
         self.desc = desc
         o = Options()

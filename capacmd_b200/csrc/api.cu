@@ -243,7 +243,7 @@ void capac_options_default(capac_options *o)
     o->matrix_layout = 0;
     o->predictor = 3;
     o->solver_kernel = 0;
-    o->inner_precond = 1;
+    o->inner_precond = 3;
     o->pair_list = 0;
 }
 

@@ -183,10 +183,11 @@ typedef struct capac_options {
     int solver_kernel;      /* BiCGSTAB on the symmetric layout: 0 one persistent cooperative launch per
                                solve when the device supports it (default), 1 a launch per vector step */
     int inner_precond;      /* mixed path, persistent solver: preconditioner of the inner solves,
-                               0 the reference's Jacobi, 1 block-Jacobi on 32-atom groups (default),
+                               0 the reference's Jacobi, 1 block-Jacobi on 32-atom groups,
                                2 block-Jacobi with a coarse correction on each group's total charge
-                               and the nanoparticle constraints, 3 the same with the groups' dipole
-                               sums as well (up to 384 coarse columns; beyond, as 1) */
+                               and the nanoparticle constraints, 3 (default) the same with the
+                               groups' dipole sums as well (up to 384 coarse columns, about 3,000
+                               metal atoms; beyond, as 1) */
     int pair_list;          /* mixed path nonbonded list: 0 (default) or 2 clusters of four atoms
                                sharing each neighbour's load, where the box is large enough, with
                                every pair listed once (Newton's third law: the neighbour's force by

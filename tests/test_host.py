@@ -38,7 +38,7 @@ def test_options_mirror_matches_library_defaults():
     cm.lib().capac_options_default(ctypes.byref(o))
     assert (o.precision, o.device, o.skin) == (cm.PREC_FP64, 0, 0.2)
     assert (o.list_every, o.max_neighbors, o.solver_tol, o.refine_tol) == (0, 0, 0.0, 1e-10)
-    assert (o.matrix_layout, o.predictor, o.solver_kernel, o.inner_precond, o.pair_list) == (0, 3, 0, 1, 0)
+    assert (o.matrix_layout, o.predictor, o.solver_kernel, o.inner_precond, o.pair_list) == (0, 3, 0, 3, 0)
     assert (o.max_iter, o.wait_polls) == (0, 0)
     src = open(os.path.join(ROOT, "include", "capacmd.h")).read()
     body = src[src.index("typedef struct capac_options {"):src.index("} capac_options;")]
