@@ -1148,7 +1148,8 @@ int capac_get(capac_ctx *c, const char *name, double *out)
             out[1] = c->grouped && c->tmem_tiles ? (double)group_tmem_tiles() : 0.0;
             out[2] = (double)group_blocks_per_sm(c->device, false);
             out[3] = (double)group_blocks_per_sm(c->device, true);
-            count = 4;
+            out[4] = (double)c->cz_cluster;
+            count = 5;
             return;
         }
         if (n == "inner_stalls") {  // inner solves of the refinement stopped for lack of progress

@@ -23,8 +23,11 @@
 // Layout (group g's columns at nm g ..): az[(g * nc + j) * 128 + r] for internal row 128 g + r (column
 // j contiguous over the group's rows), then az[128 nG nc + k * nc + j] for
 // constraint row k; einv[j * nc + i] = (E^-1)[i][j] (E is symmetric).
+#include <cooperative_groups.h>
+
 #include <algorithm>
 #include <cstdint>
+#include <cstdlib>
 
 #include "ctx.h"
 
@@ -255,6 +258,161 @@ __global__ void __launch_bounds__(kInvThreads) k_coarse_invert(int nc, double *_
     if (tid == 0) *bad_out = bad;
 }
 
+// The same inversion by a thread-block cluster: CTA q of the cluster holds
+// rows q rp .. q rp + rp - 1 of [E | I] (FP64) in its shared memory, and the
+// CTAs exchange the pivot candidates, the swapped rows and the pivot row
+// through distributed shared memory with a cluster barrier around each
+// exchange.  Every CTA takes the same branches (the pivot and the singular
+// case are decided from the same gathered candidates), so every cluster
+// barrier is reached by all of them.
+__global__ void __launch_bounds__(kInvThreads) k_coarse_invert_cluster(int nc, const double *__restrict__ aug,
+                                                                        float *__restrict__ einv, int *bad_out)
+{
+    namespace cg = cooperative_groups;
+    cg::cluster_group cl = cg::this_cluster();
+    const int rank = (int)cl.block_rank(), ncta = (int)cl.num_blocks();
+    extern __shared__ __align__(16) double csm[];
+    __shared__ double wv[kInvThreads / 32];
+    __shared__ int wi[kInvThreads / 32];
+    __shared__ double cand_v, amax_l;
+    __shared__ int cand_i, piv_s, bad_s;
+    __shared__ double fcol[kMaxCoarse];
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, w2 = 2 * nc;
+    const int rp = (nc + ncta - 1) / ncta, r0 = rank * rp, r1 = min(nc, r0 + rp), nr = max(0, r1 - r0);
+    double *rows = csm;          // nr x w2
+    double *prow = csm + (size_t)rp * w2;
+    double *trow = prow + w2;
+    for (int q = tid; q < nr * w2; q += blockDim.x) rows[q] = aug[(size_t)(r0 + q / w2) * w2 + q % w2];
+    // the largest |E| entry, over the cluster
+    {
+        double m = 0.0;
+        for (int q = tid; q < nr * nc; q += blockDim.x) m = fmax(m, fabs(rows[(size_t)(q / nc) * w2 + q % nc]));
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if (lane == 0) wv[wid] = m;
+        __syncthreads();
+        if (tid == 0) {
+            double mm = 0.0;
+            for (int w = 0; w < kInvThreads / 32; ++w) mm = fmax(mm, wv[w]);
+            amax_l = mm;
+            bad_s = 0;
+        }
+    }
+    cl.sync();
+    double tiny = 0.0;
+    for (int q = 0; q < ncta; ++q) tiny = fmax(tiny, *cl.map_shared_rank(&amax_l, q));
+    tiny *= 1e-13;
+    int bad = 0;
+    for (int k = 0; k < nc; ++k) {
+        // this CTA's candidate: largest |a[i][k]|, i >= k, lowest i on ties
+        double v = -1.0;
+        int vi = nc;
+        for (int i = max(k, r0) + tid; i < r1; i += blockDim.x) {
+            const double x = fabs(rows[(size_t)(i - r0) * w2 + k]);
+            if (x > v) {
+                v = x;
+                vi = i;
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double v2 = __shfl_xor_sync(0xffffffffu, v, o);
+            const int i2 = __shfl_xor_sync(0xffffffffu, vi, o);
+            if (v2 > v || (v2 == v && i2 < vi)) {
+                v = v2;
+                vi = i2;
+            }
+        }
+        if (lane == 0) {
+            wv[wid] = v;
+            wi[wid] = vi;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            double bv = -1.0;
+            int bi = nc;
+            for (int w = 0; w < kInvThreads / 32; ++w)
+                if (wv[w] > bv || (wv[w] == bv && wi[w] < bi)) {
+                    bv = wv[w];
+                    bi = wi[w];
+                }
+            cand_v = bv;
+            cand_i = bi;
+        }
+        cl.sync();
+        if (tid == 0) {
+            double bv = -1.0;
+            int bi = nc;
+            for (int q = 0; q < ncta; ++q) {
+                const double x = *cl.map_shared_rank(&cand_v, q);
+                const int xi = *cl.map_shared_rank(&cand_i, q);
+                if (x > bv || (x == bv && xi < bi)) {
+                    bv = x;
+                    bi = xi;
+                }
+            }
+            piv_s = bi;
+            bad_s = !(bv > tiny) || bi >= nc;
+        }
+        __syncthreads();
+        if (bad_s) {
+            bad = 1;
+            break;
+        }
+        const int p = piv_s, ok = k / rp, op = p / rp;
+        if (p != k) {
+            if (ok == op) {
+                if (rank == ok)
+                    for (int j = tid; j < w2; j += blockDim.x) {
+                        const double t = rows[(size_t)(k - r0) * w2 + j];
+                        rows[(size_t)(k - r0) * w2 + j] = rows[(size_t)(p - r0) * w2 + j];
+                        rows[(size_t)(p - r0) * w2 + j] = t;
+                    }
+                cl.sync();
+            } else {
+                if (rank == ok)
+                    for (int j = tid; j < w2; j += blockDim.x) trow[j] = rows[(size_t)(k - r0) * w2 + j];
+                if (rank == op)
+                    for (int j = tid; j < w2; j += blockDim.x) trow[j] = rows[(size_t)(p - r0) * w2 + j];
+                cl.sync();
+                if (rank == ok) {
+                    const double *src = cl.map_shared_rank(trow, op);
+                    for (int j = tid; j < w2; j += blockDim.x) rows[(size_t)(k - r0) * w2 + j] = src[j];
+                }
+                if (rank == op) {
+                    const double *src = cl.map_shared_rank(trow, ok);
+                    for (int j = tid; j < w2; j += blockDim.x) rows[(size_t)(p - r0) * w2 + j] = src[j];
+                }
+                cl.sync();
+            }
+        }
+        if (rank == ok) {
+            const double inv = 1.0 / rows[(size_t)(k - r0) * w2 + k];
+            __syncthreads();
+            for (int j = tid; j < w2; j += blockDim.x) rows[(size_t)(k - r0) * w2 + j] *= inv;
+        }
+        cl.sync();
+        {
+            const double *src = cl.map_shared_rank(csm, ok) + (size_t)(k - ok * rp) * w2;
+            for (int j = tid; j < w2; j += blockDim.x) prow[j] = src[j];
+        }
+        for (int i = r0 + tid; i < r1; i += blockDim.x) fcol[i - r0] = i == k ? 0.0 : rows[(size_t)(i - r0) * w2 + k];
+        __syncthreads();
+        for (int q = tid; q < nr * w2; q += blockDim.x) {
+            const int il = q / w2, j = q % w2;
+            if (r0 + il == k) continue;
+            rows[q] = j == k ? 0.0 : fma(-fcol[il], prow[j], rows[q]);
+        }
+        __syncthreads();
+    }
+    for (int q = tid; q < nr * nc; q += blockDim.x) {
+        const int il = q / nc, j = q % nc;
+        einv[(size_t)j * nc + r0 + il] = bad ? 0.f : (float)rows[(size_t)il * w2 + nc + j];
+    }
+    if (rank == 0 && tid == 0) *bad_out = bad;
+    cl.sync();  // no CTA leaves while another may still read its shared memory
+}
+
 // W = (A Z) E^-1 in the layout of A Z, so that the solver forms A Z c as
 // W (Z^T v) with no product by E^-1 of its own: block (g, 32 columns of W),
 // thread r one internal row of group g (the constraint rows: g = nG), the
@@ -305,6 +463,49 @@ size_t coarse_az_floats(int M, int n_nps, int nm)
     return (size_t)nG * nc * kRows + (size_t)n_nps * nc;
 }
 
+// E^-1 by a cluster of 8 (or 16) CTAs when its rows fit their shared memory
+// and such a cluster can be resident, else by one block.
+void launch_coarse_invert(capac_ctx *c, int nc)
+{
+    const int w2 = 2 * nc;
+    for (int ncta : {8, 16}) {
+        const int rp = (nc + ncta - 1) / ncta;
+        const size_t smem = (size_t)(rp + 2) * w2 * sizeof(double);
+        if (smem > 200 * 1024) continue;
+        if (cudaFuncSetAttribute(k_coarse_invert_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+                cudaSuccess ||
+            (ncta > 8 &&
+             cudaFuncSetAttribute(k_coarse_invert_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+                 cudaSuccess)) {
+            cudaGetLastError();
+            continue;
+        }
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(ncta);
+        cfg.blockDim = dim3(kInvThreads);
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = c->stream;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = ncta;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        int clusters = 0;
+        if (cudaOccupancyMaxActiveClusters(&clusters, k_coarse_invert_cluster, &cfg) != cudaSuccess || clusters < 1) {
+            cudaGetLastError();
+            continue;
+        }
+        CAPAC_CUDA(cudaLaunchKernelEx(&cfg, k_coarse_invert_cluster, nc, (const double *)c->cz_aug, c->cz_einv,
+                                      c->flags + 6));
+        c->cz_cluster = ncta;
+        return;
+    }
+    c->cz_cluster = 1;
+    k_coarse_invert<<<1, kInvThreads, 0, c->stream>>>(nc, c->cz_aug, c->cz_einv, c->flags + 6);
+}
+
 void launch_coarse_refresh(capac_ctx *c)
 {
     const int nG = precond_groups(c->M), nm = c->cz_modes, nc = coarse_columns(c->M, c->n_nps, nm);
@@ -316,7 +517,10 @@ void launch_coarse_refresh(capac_ctx *c)
     const int nq = std::max(nG * kRows, c->n_nps * nc);
     k_coarse_az_np<<<grid_for(nq, 256), 256, 0, s>>>(nG, nc, nm, c->n_nps, c->slot_np, c->cz_az);
     k_coarse_e<<<nc, 256, 0, s>>>(nG, nc, nm, c->g_atoms, c->cz_az, c->cz_aug);
-    k_coarse_invert<<<1, kInvThreads, 0, s>>>(nc, c->cz_aug, c->cz_einv, c->flags + 6);
+    if (getenv("CAPAC_COARSE_ONE_BLOCK"))
+        k_coarse_invert<<<1, kInvThreads, 0, s>>>(nc, c->cz_aug, c->cz_einv, c->flags + 6);
+    else
+        launch_coarse_invert(c, nc);
     k_coarse_w<<<dim3(nG + (c->n_nps > 0 ? 1 : 0), (nc + 31) / 32), kRows, 0, s>>>(nG, nc, c->n_nps, c->cz_az,
                                                                                     c->cz_einv, c->cz_w);
     c->launches += 5;

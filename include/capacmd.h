@@ -349,7 +349,8 @@ int capac_checkpoint_load(capac_ctx *ctx, const char *path);
  * order of its block-Jacobi groups, its tiles assembled in that order; the
  * tiles each of its blocks holds in tensor memory for the whole solve, 0 when
  * all are streamed from HBM each pass; the resident blocks per SM of the
- * group-ordered solver without and with tiles in tensor memory),
+ * group-ordered solver without and with tiles in tensor memory; the CTAs of
+ * the cluster that last inverted the coarse matrix, 1 for one block, 0 none),
  * inner_stalls(1: inner solves of the mixed path's refinement that stopped
  * because their (r, r) had not halved in 60 iterations and handed their
  * iterate back to the FP64 refinement),

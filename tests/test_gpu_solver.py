@@ -174,3 +174,23 @@ def test_two_level_inner_solves(case, precond):
     assert rel_err(two.get("vec_pq"), bj.get("vec_pq")) < 1e-7
     assert rel_err(two.get("rx"), bj.get("rx")) < 1e-9
     assert two.stats().solver_rel_residual <= 1e-11
+
+
+@pytest.mark.parametrize("case", ["c2", "t_2np"])
+def test_coarse_inversion_by_a_cluster(case, monkeypatch):
+    """The coarse matrix E inverted by a cluster of CTAs exchanging rows
+    through distributed shared memory gives the same solve as the inversion
+    by one block (the same pivots and operations)."""
+    paths = configs.cached(case) if case == "c2" else golden_paths(case)
+    d = cm.Desc.from_paths(paths)
+    cl = cm.Simulation(d, precision=cm.PREC_MIXED, refine_tol=1e-11)
+    monkeypatch.setenv("CAPAC_COARSE_ONE_BLOCK", "1")
+    one = cm.Simulation(d, precision=cm.PREC_MIXED, refine_tol=1e-11)
+    monkeypatch.delenv("CAPAC_COARSE_ONE_BLOCK")
+    for s in (cl, one):
+        s.set("vec_pq", np.zeros(d.n_mat))
+        s.force()
+    assert cl.get("solver_layout")[4] >= 8, cl.get("solver_layout")
+    assert one.get("solver_layout")[4] == 0.0 or one.get("solver_layout")[4] == 1.0
+    assert cl.stats().solver_iterations == one.stats().solver_iterations
+    assert rel_err(cl.get("vec_pq"), one.get("vec_pq")) < 1e-12
