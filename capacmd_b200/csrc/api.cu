@@ -528,6 +528,7 @@ int capac_create(const capac_desc *d, const capac_options *opt, capac_ctx **out)
                                     if (o.inner_precond >= 2 && nc <= coarse_columns_max()) {
                                         c->twolevel = true;
                                         c->cz_modes = nm;
+                                        c->cz_one_block = getenv("CAPAC_COARSE_ONE_BLOCK") != nullptr;
                                         c->cz_nc = nc;
                                         c->cz_az = dalloc<float>(coarse_az_floats(M, d->n_nps, nm));
                                         c->cz_w = dalloc<float>(coarse_az_floats(M, d->n_nps, nm));

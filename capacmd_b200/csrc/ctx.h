@@ -239,6 +239,7 @@ struct capac_ctx {
     double *cz_aug = nullptr;    // [E | I] workspace of the inversion
     double *cz_zbuf = nullptr;   // Z^T v inside the solver
     int cz_cluster = 0;          // CTAs of the last inversion's cluster (1: one block)
+    bool cz_one_block = false;   // invert in one block (CAPAC_COARSE_ONE_BLOCK at creation)
     long inner_stalls = 0;       // inner solves ended that way
     int *slot_np = nullptr;      // [32 nG] nanoparticle of each group slot's atom, -1 none
     int *np_off = nullptr;       // [n_nps + 1] offsets into np_rows

@@ -517,10 +517,12 @@ void launch_coarse_refresh(capac_ctx *c)
     const int nq = std::max(nG * kRows, c->n_nps * nc);
     k_coarse_az_np<<<grid_for(nq, 256), 256, 0, s>>>(nG, nc, nm, c->n_nps, c->slot_np, c->cz_az);
     k_coarse_e<<<nc, 256, 0, s>>>(nG, nc, nm, c->g_atoms, c->cz_az, c->cz_aug);
-    if (getenv("CAPAC_COARSE_ONE_BLOCK"))
+    if (c->cz_one_block) {
+        c->cz_cluster = 1;
         k_coarse_invert<<<1, kInvThreads, 0, s>>>(nc, c->cz_aug, c->cz_einv, c->flags + 6);
-    else
+    } else {
         launch_coarse_invert(c, nc);
+    }
     k_coarse_w<<<dim3(nG + (c->n_nps > 0 ? 1 : 0), (nc + 31) / 32), kRows, 0, s>>>(nG, nc, c->n_nps, c->cz_az,
                                                                                     c->cz_einv, c->cz_w);
     c->launches += 5;
