@@ -383,6 +383,9 @@ def solver_phases(sim) -> dict:
     """Mean microseconds per iteration of the persistent solver's phases
     (block 0's view, %globaltimer marks), over the iterations timed."""
     ph = sim.get("solver_phases")
+    # two-level inner solves: each reduction's first step (with its grid
+    # barrier) under "V reduction" / "T reduction", its coarse step (with the
+    # next barrier) under "K v pass" / "K t pass"
     names = ["P tile pass", "P grid barrier", "V reduction (+ K v)", "K v pass", "alpha + S tile pass + barrier",
              "T reduction (+ K t)", "K t pass", "dot sums + scalars"]
     out = {n: ph[k] / 1e3 for k, n in enumerate(names)}

@@ -495,6 +495,7 @@ int capac_create(const capac_desc *d, const capac_options *opt, capac_ctx **out)
                         c->msym = mixed ? (void *)dalloc<float>(ne) : (void *)dalloc<double>(ne);
                         c->sympart = dalloc<double>(sym_partial_doubles(M));
                         if (o.solver_kernel == 0) c->coop_grid = coop_grid_size(c->device, mixed);
+                        if (const char *l2 = getenv("CAPAC_TILE_L2")) c->tile_l2 = (float)atof(l2);
                         if (c->coop_grid > 0) {
                             c->coop_bp = dalloc<double>(coop_partial_doubles(c->coop_grid));
                             c->coop_bar = dalloc<unsigned char>(coop_barrier_bytes());

@@ -228,6 +228,7 @@ struct capac_ctx {
     bool grouped = false;
     bool tmem_tiles = false;     // the grouped solver holds part of its tiles in tensor memory
     int group_grid = 0;          // blocks of the grouped solver's launch (<= coop_grid)
+    float tile_l2 = -1.f;        // L2 policy of the persistent solvers' streamed tiles: -1 evict-first (default), 0 none, f > 0 keep f (CAPAC_TILE_L2)
     int inner_stall = 0;         // set during the refinement's inner solves: see GroupArgs::stall
     // two-level inner preconditioner (inner_precond 2, k_coarse.cu)
     bool twolevel = false;

@@ -150,6 +150,30 @@ __device__ __forceinline__ void bulk_load(void *dst, const void *src, unsigned b
                  "l"(src), "r"(bytes), "r"(smem_u32(bar))
                  : "memory");
 }
+// The same copy with an L2 eviction-priority policy for the copied lines.
+__device__ __forceinline__ void bulk_load_hint(void *dst, const void *src, unsigned bytes, uint64_t *bar,
+                                               uint64_t policy)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar)), "l"(policy)
+        : "memory");
+}
+// L2 policy for streamed matrix tiles: frac > 0 keeps that fraction of the
+// lines at evict_last priority and marks the rest evict_first; frac < 0
+// marks every line evict_first.
+__device__ __forceinline__ uint64_t tile_l2_policy(float frac)
+{
+    uint64_t pol;
+    if (frac > 0.f)
+        asm volatile("createpolicy.fractional.L2::evict_last.L2::evict_first.b64 %0, %1;" : "=l"(pol) : "f"(frac));
+    else
+        asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
 __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity)
 {
     unsigned ok;
@@ -225,8 +249,8 @@ __device__ __forceinline__ void tmem_ld40(uint32_t taddr, float (&v)[40])
 }  // namespace
 
 struct CoopSync {
-    unsigned count;
-    unsigned gen;
+    unsigned count;  // grid-barrier arrivals of the launch; bit 31: a block gave up
+    unsigned unused;
     int error;  // 1 grid barrier timed out, 2 ring-stage wait timed out
     int pad;
 };
@@ -256,6 +280,7 @@ struct CoopArgs {
     // phase timer (null: off): block 0 records %globaltimer at the end of
     // each phase of the first kPhaseIters iterations, kPhases per iteration
     unsigned long long *ptime;
+    float l2_frac;  // L2 policy of the streamed tiles (tile_l2_policy; 0: none)
 };
 
 constexpr int kPhases = 8;
@@ -273,34 +298,61 @@ __device__ __forceinline__ void phase_mark(const CoopArgs &A, int iter, int k)
 }
 
 // Bounded grid barrier (`limit` polls); false if any block gave up.
+//
+// count only grows during a launch (zeroed before it): the k-th barrier of
+// the launch is complete when it reaches k * gridDim.x, so each block learns
+// its target from the value its own arrival returns and then polls the same
+// word, with nothing to reset and no second word to read (a block cannot
+// arrive at barrier k + 1 before every block has arrived at k).  A block that
+// gives up sets the error word and bit 31 of count, which ends every other
+// block's wait at once.  Release: this block's writes are ordered before its
+// arrival by the fence (after the block barrier); acquire: the polling load,
+// then the block barrier orders the block's later reads after it.
+constexpr unsigned kBarAbort = 0x80000000u;
+
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned *p)
+{
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
 __device__ bool grid_barrier(CoopSync *bar, long limit)
 {
     __shared__ int ok;
     __syncthreads();
     if (threadIdx.x == 0) {
-        volatile unsigned *gen = &bar->gen;
-        const unsigned g = *gen;
         __threadfence();
         const unsigned arrived = atomicAdd(&bar->count, 1u);
-        if (arrived == gridDim.x - 1) {
-            bar->count = 0;
-            __threadfence();
-            atomicAdd(&bar->gen, 1u);
-        } else {
-            long spins = 0;
-            while (*gen == g) {
-                if (++spins > limit) {
-                    atomicCAS(&bar->error, 0, 1);
-                    break;
-                }
+        bool good = (arrived & kBarAbort) == 0;
+        const unsigned target = ((arrived & ~kBarAbort) / gridDim.x + 1) * gridDim.x;
+        long spins = 0;
+        while (good) {
+            const unsigned cnt = ld_acquire_gpu(&bar->count);
+            if (cnt & kBarAbort) {
+                good = false;
+            } else if (cnt >= target) {
+                break;
+            } else if (++spins > limit) {
+                atomicCAS(&bar->error, 0, 1);
+                atomicOr(&bar->count, kBarAbort);
+                good = false;
+            } else {
                 __nanosleep(32);
             }
         }
-        __threadfence();
-        ok = *(volatile int *)&bar->error == 0;
+        ok = good;
     }
     __syncthreads();
     return ok != 0;
+}
+
+// A block that stops early (a ring wait that gave up) ends the other blocks'
+// barrier waits.
+__device__ __forceinline__ void grid_abort(CoopSync *bar, int code)
+{
+    atomicCAS(&bar->error, 0, code);
+    atomicOr(&bar->count, kBarAbort);
 }
 
 // Dot partials: kBp doubles per block.  sum_bp sums them over the blocks
@@ -375,13 +427,24 @@ struct Ring {
     long issued, consumed;
     int n_my;       // tiles streamed through the ring
     int first = 0;  // tiles of the block before the streamed ones (held elsewhere)
+    bool hint = false;   // copy with the L2 policy `pol`
+    uint64_t pol = 0;
     __device__ int tile_of(long q) const { return blockIdx.x + (first + (int)(q % n_my)) * gridDim.x; }
     __device__ T *stage(int st) const { return buf + (size_t)st * kTileElems; }
+    __device__ void set_l2(float frac)
+    {
+        hint = frac != 0.f;
+        if (hint) pol = tile_l2_policy(frac);
+    }
     __device__ void issue(const T *mat)  // thread 0
     {
         const long q = issued++;
         const int st = (int)(q % Stages);
-        bulk_load(stage(st), mat + (size_t)tile_of(q) * kTileElems, kTileElems * sizeof(T), bar + st);
+        const T *src = mat + (size_t)tile_of(q) * kTileElems;
+        if (hint)
+            bulk_load_hint(stage(st), src, kTileElems * sizeof(T), bar + st, pol);
+        else
+            bulk_load(stage(st), src, kTileElems * sizeof(T), bar + st);
     }
     // thread 0: bounded wait for every copy still in flight
     __device__ void drain()
@@ -747,6 +810,7 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? 2 : 1) k_bicgstab_coo
     ring.bar = ring_bar;
     ring.issued = ring.consumed = 0;
     ring.n_my = (int)blockIdx.x < A.ntiles ? (A.ntiles - 1 - (int)blockIdx.x) / nb + 1 : 0;
+    if (threadIdx.x == 0) ring.set_l2(A.l2_frac);
     if (threadIdx.x == 0) {
         for (int st = 0; st < Stages; ++st) mbar_init(ring_bar + st, 1);
         fence_mbar_init();
@@ -915,7 +979,7 @@ __global__ void __launch_bounds__(kBlock, sizeof(T) == 4 ? 2 : 1) k_bicgstab_coo
         }
     }
     if (threadIdx.x == 0) {
-        if (!ok) atomicCAS(&A.sync->error, 0, 2);
+        if (!ok) grid_abort(A.sync, 2);
         ring.drain();
     }
     if (ok && tid == 0) {
@@ -975,6 +1039,7 @@ struct GroupArgs {
     SolverScalars *ss;
     CoopSync *sync;
     unsigned long long *ptime;
+    float l2_frac;  // L2 policy of the streamed tiles (tile_l2_policy; 0: none)
 };
 
 // Reference row of internal row q (-1 for a padding slot).
@@ -1154,6 +1219,30 @@ __device__ bool tiles_pass_g(const GroupArgs &A, const PassScalars &S, Ring<floa
     return true;
 }
 
+// This thread's share of the sum of `in` over the charge rows of
+// nanoparticle k (the constraint row's product): the rows' indices and then
+// their values loaded kBatch at a time, so a block covers 16 x 256 atoms per
+// round of loads.
+__device__ __forceinline__ double np_charge_sum(const GroupArgs &A, const double *in, int k)
+{
+    const int q0 = A.np_off[k], q1 = A.np_off[k + 1];
+    double acc = 0.0;
+    for (int qb = q0 + (int)threadIdx.x; qb < q1; qb += kBatch * (int)blockDim.x) {
+        int rows[kBatch];
+#pragma unroll
+        for (int u = 0; u < kBatch; ++u) {
+            const int q = qb + u * (int)blockDim.x;
+            rows[u] = q < q1 ? __ldg(A.np_rows + q) : -1;
+        }
+        double vals[kBatch];
+#pragma unroll
+        for (int u = 0; u < kBatch; ++u) vals[u] = rows[u] >= 0 ? __ldcg(in + rows[u]) : 0.0;
+#pragma unroll
+        for (int u = 0; u < kBatch; ++u) acc += vals[u];
+    }
+    return acc;
+}
+
 // One group's reduction fused with its preconditioner block.  out = A in for
 // the group's 128 rows from the nG tile partials of its block row (two
 // halves of the threads sum alternate tiles, added in a fixed order), the
@@ -1252,7 +1341,7 @@ __device__ void reduce_group(const GroupArgs &A, const PassScalars &S, double *b
         __shared__ double shl[32];
         double acc[1] = {0.0};
         if (products)
-            for (int q = A.np_off[k] + tid; q < A.np_off[k + 1]; q += blockDim.x) acc[0] += __ldcg(in + A.np_rows[q]);
+            acc[0] = np_charge_sum(A, in, k);
         block_sum<1>(acc, shl);
         if (tid == 0) {
             const int row = 128 * nG + k;
@@ -1301,7 +1390,8 @@ constexpr int kCoarseMax = 384;  // coarse columns the solver's shared buffer ho
 // scratch: 256 + 2 kCoarseMax doubles of shared memory (the pass inputs'
 // buffer, idle between passes).
 template <int RED>
-__device__ bool reduce_group2(const GroupArgs &A, const PassScalars &S, double *bp, bool products, double *scratch)
+__device__ bool reduce_group2(const GroupArgs &A, const PassScalars &S, double *bp, bool products, double *scratch,
+                              int iter = 0, int mark = -1)
 {
     double *vrow = scratch, *hsum = scratch + 128, *cc = scratch + 256, *zs = scratch + 256 + kCoarseMax;
     const int nG = A.nG, nc = A.nc, tid = threadIdx.x;
@@ -1373,7 +1463,7 @@ __device__ bool reduce_group2(const GroupArgs &A, const PassScalars &S, double *
         __shared__ double shl[32];
         double acc[1] = {0.0};
         if (products)
-            for (int q = A.np_off[k] + tid; q < A.np_off[k + 1]; q += blockDim.x) acc[0] += __ldcg(in + A.np_rows[q]);
+            acc[0] = np_charge_sum(A, in, k);
         block_sum<1>(acc, shl);
         if (tid == 0) {
             const int row = 128 * nG + k;
@@ -1399,13 +1489,14 @@ __device__ bool reduce_group2(const GroupArgs &A, const PassScalars &S, double *
         __syncthreads();
     }
     if (!grid_barrier(A.sync, A.spin_limit)) return false;
+    if (mark >= 0) g_phase_mark(A, iter, mark);  // the phase timer splits the two steps
 
+    const int lane = tid & 31, wid = tid >> 5;
     const bool mine = (int)blockIdx.x < nG || (int)gridDim.x - 1 - (int)blockIdx.x < A.n_nps;
     if (mine) {
         for (int j = tid; j < nc; j += blockDim.x) zs[j] = __ldcg(A.zbuf + j);
         __syncthreads();
     }
-    const int lane = tid & 31, wid = tid >> 5;
     for (int G = blockIdx.x; G < nG; G += gridDim.x) {
         const int o = tid & 127, h = tid >> 7;
         // c of the group's own columns: warp m, lanes over the columns of
@@ -1459,27 +1550,23 @@ __device__ bool reduce_group2(const GroupArgs &A, const PassScalars &S, double *
         __syncthreads();
     }
     for (int k = (int)gridDim.x - 1 - (int)blockIdx.x; k < A.n_nps; k += gridDim.x) {
-        if (wid == 0) {
-            const int row = 128 * nG + k;
-            const float *er = A.einv + (size_t)(A.nm * nG + k) * nc;
-            const float *wl = A.w + (size_t)nG * nc * 128 + (size_t)k * nc;
-            double cs = 0.0, ws = 0.0;
-            for (int j = lane; j < nc; j += 32) {
-                cs = fma((double)__ldg(er + j), zs[j], cs);
-                ws = fma((double)__ldg(wl + j), zs[j], ws);
-            }
-#pragma unroll
-            for (int m = 16; m > 0; m >>= 1) {
-                cs += __shfl_xor_sync(0xffffffffu, cs, m);
-                ws += __shfl_xor_sync(0xffffffffu, ws, m);
-            }
-            if (lane == 0) {
-                const double kv = __ldcg(outv + row) - ws + cs;  // K = 1 on the constraint rows
-                kout[row] = kv;
-                if (RED == RED_T) {
-                    d[0] += kv * __ldcg(A.z + row);
-                    d[1] += kv * kv;
-                }
+        // the whole block over the coarse columns, two per thread at most
+        __shared__ double shc[2 * kWarps];
+        const int row = 128 * nG + k;
+        const float *er = A.einv + (size_t)(A.nm * nG + k) * nc;
+        const float *wl = A.w + (size_t)nG * nc * 128 + (size_t)k * nc;
+        double cw[2] = {0.0, 0.0};
+        for (int j = tid; j < nc; j += blockDim.x) {
+            cw[0] = fma((double)__ldg(er + j), zs[j], cw[0]);
+            cw[1] = fma((double)__ldg(wl + j), zs[j], cw[1]);
+        }
+        block_sum<2>(cw, shc);
+        if (tid == 0) {
+            const double kv = __ldcg(outv + row) - cw[1] + cw[0];  // K = 1 on the constraint rows
+            kout[row] = kv;
+            if (RED == RED_T) {
+                d[0] += kv * __ldcg(A.z + row);
+                d[1] += kv * kv;
             }
         }
         __syncthreads();
@@ -1522,6 +1609,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_bicgstab_group(GroupArgs A)
     ring.issued = ring.consumed = 0;
     ring.first = n_res;
     ring.n_my = n_all - n_res;
+    if (threadIdx.x == 0) ring.set_l2(A.l2_frac);
     if (threadIdx.x == 0) {
         for (int st = 0; st < Stages; ++st) mbar_init(ring_bar + st, 1);
         fence_mbar_init();
@@ -1624,7 +1712,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_bicgstab_group(GroupArgs A)
         g_phase_mark(A, iter, 2);
         S.first = 0;
         if (A.nc > 0) {
-            if (!reduce_group2<RED_V>(A, S, bpA, true, pscratch)) {
+            if (!reduce_group2<RED_V>(A, S, bpA, true, pscratch, iter, 3)) {
                 ok = false;
                 break;
             }
@@ -1635,7 +1723,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_bicgstab_group(GroupArgs A)
             ok = false;
             break;
         }
-        g_phase_mark(A, iter, 3);
+        if (A.nc == 0) g_phase_mark(A, iter, 3);
         g_phase_mark(A, iter, 4);
         double r0v[1];
         sum_bp<1>(bpA, nb, r0v);
@@ -1651,7 +1739,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_bicgstab_group(GroupArgs A)
         if (!ok) break;
         g_phase_mark(A, iter, 5);
         if (A.nc > 0) {
-            if (!reduce_group2<RED_T>(A, S, bpB, true, pscratch)) {
+            if (!reduce_group2<RED_T>(A, S, bpB, true, pscratch, iter, 6)) {
                 ok = false;
                 break;
             }
@@ -1662,7 +1750,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_bicgstab_group(GroupArgs A)
             ok = false;
             break;
         }
-        g_phase_mark(A, iter, 6);
+        if (A.nc == 0) g_phase_mark(A, iter, 6);
         g_phase_mark(A, iter, 7);
         double d[7];
         sum_bp<7>(bpB, nb, d);
@@ -1720,7 +1808,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_bicgstab_group(GroupArgs A)
         }
     }
     if (threadIdx.x == 0) {
-        if (!ok) atomicCAS(&A.sync->error, 0, 2);
+        if (!ok) grid_abort(A.sync, 2);
         ring.drain();
     }
     if (n_res > 0) {  // every path comes here: the block's tensor memory is released
@@ -1800,6 +1888,7 @@ int bicgstab_coop(capac_ctx *c, const double *b, double *x, double tol, double s
     A.skip = skip;
     A.ss = c->ss;
     A.sync = reinterpret_cast<CoopSync *>(c->coop_bar);
+    A.l2_frac = c->tile_l2;
     A.ptime = nullptr;
     if (c->phase_timer) {
         if (!c->phase_buf) CAPAC_CUDA(cudaMalloc(&c->phase_buf, sizeof(unsigned long long) * kPhases * kPhaseIters));
@@ -1885,6 +1974,7 @@ int bicgstab_group(capac_ctx *c, const double *b, double *x, double tol, double 
     A.skip = skip;
     A.ss = c->ss;
     A.sync = reinterpret_cast<CoopSync *>(c->coop_bar);
+    A.l2_frac = c->tile_l2;
     A.ptime = nullptr;
     if (c->phase_timer) {
         if (!c->phase_buf) CAPAC_CUDA(cudaMalloc(&c->phase_buf, sizeof(unsigned long long) * kPhases * kPhaseIters));

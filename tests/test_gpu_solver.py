@@ -194,3 +194,30 @@ def test_coarse_inversion_by_a_cluster(case, monkeypatch):
     assert one.get("solver_layout")[4] == 1.0
     assert cl.stats().solver_iterations == one.stats().solver_iterations
     assert rel_err(cl.get("vec_pq"), one.get("vec_pq")) < 1e-12
+
+
+@pytest.mark.parametrize("prec", [cm.PREC_FP64, cm.PREC_MIXED])
+def test_tile_l2_policy_changes_no_result(prec, monkeypatch):
+    """The persistent solvers stream their matrix tiles with an L2
+    evict-first policy by default, so the vectors, partial sums and
+    preconditioner blocks of the reduction phases stay in L2.  The policy
+    only steers the cache: the solve is bit for bit the one without it
+    (CAPAC_TILE_L2=0) and with part of the tiles kept (CAPAC_TILE_L2=0.5)."""
+    d = cm.Desc.from_paths(configs.cached("c2"))
+    sims = []
+    for v in (None, "0", "0.5"):
+        if v is None:
+            monkeypatch.delenv("CAPAC_TILE_L2", raising=False)
+        else:
+            monkeypatch.setenv("CAPAC_TILE_L2", v)
+        sims.append(cm.Simulation(d, precision=prec, refine_tol=1e-11))
+    monkeypatch.delenv("CAPAC_TILE_L2", raising=False)
+    for s in sims:
+        s.force()
+        s.md_init()
+        s.md_steps(3)
+    x0 = sims[0].get("vec_pq")
+    for s in sims[1:]:
+        assert s.stats().solver_iterations == sims[0].stats().solver_iterations
+        assert np.array_equal(s.get("vec_pq"), x0)
+        assert np.array_equal(s.get("rx"), sims[0].get("rx"))
