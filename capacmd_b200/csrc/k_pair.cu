@@ -58,6 +58,15 @@ __device__ __forceinline__ TypePairF make_type_pair_f(const DevParams &P, const 
     return t;
 }
 
+// 1/x by the hardware approximation (rcp.approx.ftz.f32, within about one
+// ulp); 1 <= x <= 3.5 here.
+__device__ __forceinline__ float rcp_approx(float x)
+{
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
 // erfc(x) for 0 <= x in FP32 as exp(-x^2) R(x), with R(x) = erfc(x) exp(x^2)
 // (the scaled complementary error function) fitted on [0, 5] by a degree-9
 // polynomial in t = 1 / (1 + x / 2), least squares in relative error
@@ -67,7 +76,7 @@ __device__ __forceinline__ TypePairF make_type_pair_f(const DevParams &P, const 
 __device__ __forceinline__ float erfc_from_gauss_f(float x, float gauss)
 {
     if (x >= 5.0f) return erfcf(x);
-    const float t = __frcp_rn(fmaf(0.5f, x, 1.0f));
+    const float t = rcp_approx(fmaf(0.5f, x, 1.0f));
     float r = -3.71903017e-02f;
     r = fmaf(r, t, 1.64898831e-01f);
     r = fmaf(r, t, -2.03180485e-01f);
@@ -493,7 +502,17 @@ __global__ void __launch_bounds__(kPairWarps * 32, sizeof(Real) == 4 ? 3 : 2) k_
 constexpr int kClQueue = 160;  // < 32 left over + 4 x 32 appended
 constexpr int kClWarps = 8;      // warps per block of the cluster kernel
 constexpr int kClMinBlocks = 2;  // resident blocks per SM the register budget allows
-constexpr size_t kClQueueBytes = (size_t)kClWarps * kClQueue * sizeof(Cand<float>);
+constexpr size_t kClQueueBytes = (size_t)kClWarps * kClQueue * (sizeof(float4) + sizeof(uint32_t));
+// A warp's queue as two arrays: the neighbour's FP32 difference from the
+// cluster centroid with its charge, and the list entry with the member
+// index in its mask bits; the flush forms the member's difference from them
+// by the same operations as the member test, so the pair's r^2 is the one
+// the test accepted.  An append or a read is one 16-byte and one 4-byte
+// shared-memory access.
+struct ClQueue {
+    float4 *a;
+    uint32_t *b;
+};
 template <bool NONBONDED, bool CPIM, bool HALF>
 __global__ void __launch_bounds__(kClWarps * 32, kClMinBlocks) k_pair_cl(DevParams P, PairConstsF K, const double4 *__restrict__ pos4,
                                                               const int4 *__restrict__ cl_atoms,
@@ -519,7 +538,9 @@ __global__ void __launch_bounds__(kClWarps * 32, kClMinBlocks) k_pair_cl(DevPara
     __shared__ unsigned char s_metal[kSmemTypes];
     const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const unsigned lt_mask = (1u << lane) - 1u;
-    Cand<float> *Q = reinterpret_cast<Cand<float> *>(s_dyn) + wib * kClQueue;
+    ClQueue Q;
+    Q.a = reinterpret_cast<float4 *>(s_dyn) + wib * kClQueue;
+    Q.b = reinterpret_cast<uint32_t *>(s_dyn + (size_t)kClWarps * kClQueue * sizeof(float4)) + wib * kClQueue;
     if (lane < 8) wacc[wib][lane] = 0.0;
     const bool smem_types = P.n_types <= kSmemTypes;
     if (smem_types) {
@@ -596,10 +617,17 @@ __global__ void __launch_bounds__(kClWarps * 32, kClMinBlocks) k_pair_cl(DevPara
             if (lane < cnt) {
                 float g0 = 0.f, g1 = 0.f, g2 = 0.f;
                 float n0 = 0.f, n1 = 0.f, n2 = 0.f;  // the pair force on the member (reversed on the half list)
-                const Cand<float> c = Q[head + lane];
+                const float4 bq4 = Q.a[head + lane];
+                Cand<float> c;
+                c.e = Q.b[head + lane];
                 const int k = (int)((c.e >> kClMaskShift) & 3u);
                 const int tj = (int)(c.e >> kClTypeShift);
                 const float4 mk = s_mem[wib][k];
+                c.dx = bq4.x - mk.x;
+                c.dy = bq4.y - mk.y;
+                c.dz = bq4.z - mk.z;
+                c.r2 = fmaf(c.dz, c.dz, fmaf(c.dy, c.dy, c.dx * c.dx));
+                c.qj = bq4.w;
                 if (NONBONDED) {
                     const int tp = s_trow[wib][k] + tj;
                     float eq = 0.f, ev = 0.f;
@@ -750,17 +778,13 @@ __global__ void __launch_bounds__(kClWarps * 32, kClMinBlocks) k_pair_cl(DevPara
                     }
                     int pos = qn + incl - cnt;
 #pragma unroll
+                    const float4 b4 = make_float4(bx, by, bz, bq);
+#pragma unroll
                     for (int kk = 0; kk < 4; ++kk) {
                         if ((smask >> kk) & 1u) {
-                            const float4 mk = s_mem[wib][kk];
-                            Cand<float> c;
-                            c.dx = bx - mk.x;
-                            c.dy = by - mk.y;
-                            c.dz = bz - mk.z;
-                            c.r2 = fmaf(c.dz, c.dz, fmaf(c.dy, c.dy, c.dx * c.dx));
-                            c.qj = bq;
-                            c.e = bk | ((uint32_t)kk << kClMaskShift);
-                            Q[pos++] = c;
+                            Q.a[pos] = b4;
+                            Q.b[pos] = bk | ((uint32_t)kk << kClMaskShift);
+                            ++pos;
                         }
                     }
                     qn += __shfl_sync(0xffffffffu, incl, 31);
@@ -773,14 +797,9 @@ __global__ void __launch_bounds__(kClWarps * 32, kClMinBlocks) k_pair_cl(DevPara
                         const bool ok = ((bm >> kk) & 1u) && r2 < K.rc2;
                         const unsigned ballot = __ballot_sync(0xffffffffu, ok);
                         if (ok) {
-                            Cand<float> c;
-                            c.dx = dx;
-                            c.dy = dy;
-                            c.dz = dz;
-                            c.r2 = r2;
-                            c.qj = bq;
-                            c.e = bk | ((uint32_t)kk << kClMaskShift);
-                            Q[qn + __popc(ballot & lt_mask)] = c;
+                            const int at = qn + __popc(ballot & lt_mask);
+                            Q.a[at] = make_float4(bx, by, bz, bq);
+                            Q.b[at] = bk | ((uint32_t)kk << kClMaskShift);
                         }
                         qn += __popc(ballot);
                     }
@@ -793,10 +812,17 @@ __global__ void __launch_bounds__(kClWarps * 32, kClMinBlocks) k_pair_cl(DevPara
                 }
                 if (head > 0) {
                     const int rest = qn - head;
-                    Cand<float> tmp;
-                    if (lane < rest) tmp = Q[head + lane];
+                    float4 ta;
+                    uint32_t tb = 0;
+                    if (lane < rest) {
+                        ta = Q.a[head + lane];
+                        tb = Q.b[head + lane];
+                    }
                     __syncwarp();
-                    if (lane < rest) Q[lane] = tmp;
+                    if (lane < rest) {
+                        Q.a[lane] = ta;
+                        Q.b[lane] = tb;
+                    }
                     __syncwarp();
                     qn = rest;
                 }

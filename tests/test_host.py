@@ -229,11 +229,14 @@ def test_fp32_erfc_fit_error_bound():
     assert len(coef) == 10  # Horner order: highest degree first
     x = np.linspace(0.0, 5.0, 200001).astype(np.float32)
     t = (np.float32(1.0) / (np.float32(0.5) * x + np.float32(1.0))).astype(np.float32)
-    r = np.float32(coef[0]) * np.ones_like(x)
-    for c in coef[1:]:
-        r = (r * t + np.float32(c)).astype(np.float32)
     gauss = np.exp(-(x.astype(np.float64) ** 2)).astype(np.float32)
-    approx = (gauss * r).astype(np.float64)
     exact = np.array([math.erfc(float(v)) for v in x])
-    rel = np.abs(approx / exact - 1.0)
-    assert rel.max() < 6e-7  # a few FP32 ulp, as the library erfcf
+    # the kernel's reciprocal is the hardware approximation (within one ulp):
+    # t exact, and one ulp either side
+    for tt in (t, np.nextafter(t, np.float32(2.0)), np.nextafter(t, np.float32(0.0))):
+        r = np.float32(coef[0]) * np.ones_like(x)
+        for c in coef[1:]:
+            r = (r * tt + np.float32(c)).astype(np.float32)
+        approx = (gauss * r).astype(np.float64)
+        rel = np.abs(approx / exact - 1.0)
+        assert rel.max() < 6e-7  # a few FP32 ulp, as the library erfcf
