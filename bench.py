@@ -293,30 +293,41 @@ def main() -> int:
     value = N * args.steps * world / (ms / 1e3)
     st = sim.stats()
 
-    # dominant kernel and its roofline
+    # dominant kernel and its roofline, and the persistent solve's beside it
     peak, peak_kind = _peaks()
+
+    def kernel_roofline(cls):
+        n_launch, tot_ms = prof[cls]
+        if cls == "spmv":
+            n_launch = n_spmv or n_launch
+        avg_s = tot_ms / max(n_launch, 1) / 1e3
+        if cls == "solve":
+            # one launch = a whole solve: its SpMV products plus the BiCGSTAB
+            # vector updates (19 n doubles per iteration beyond the products)
+            iters = max(n_spmv - n_launch, 0) / 2
+            bytes_launch = (n_spmv * algorithmic_bytes(sim, "spmv", N, M, args.precision)
+                            + iters * 19 * desc.n_mat * 8.0) / max(n_launch, 1)
+        else:
+            bytes_launch = algorithmic_bytes(sim, cls, N, M, args.precision)
+        achieved = bytes_launch / avg_s / 1e9 if avg_s > 0 else None
+        r = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+             "frac": achieved / peak if achieved else None, "traffic": _traffic(args.workload, args.precision, cls),
+             "kernel": cls, "algorithmic_bytes_per_launch": bytes_launch, "avg_launch_ms": avg_s * 1e3,
+             "launches": n_launch, "peak_kind": peak_kind}
+        if r["traffic"] and r["traffic"] < 0.5 * bytes_launch:
+            r["note"] = (f"operands stay in the 126 MB L2 across the launch: measured DRAM traffic is "
+                         f"{r['traffic'] / bytes_launch:.0%} of the algorithmic bytes, so the launch is "
+                         f"bound by L2 and latency, not HBM")
+        if cls == "pair" and args.precision == "mixed":
+            ia = _issue_active("pair")
+            r["note"] = ("FP32 pair terms on the CUDA cores, one list pass per step: bound by instruction issue "
+                         "and latency, not by bytes" + (f" (ncu issue active {ia:.0%} of peak on the 91k-atom "
+                                                         f"workload, profiles/k_pair_cl_half_c3.md)" if ia else ""))
+        return r
+
     dom = max(("pair", "spmv", "matrix", "solve"), key=lambda k: prof[k][1])
-    n_launch, tot_ms = prof[dom]
-    if dom == "spmv":
-        n_launch = n_spmv or n_launch
-    avg_s = tot_ms / max(n_launch, 1) / 1e3
-    if dom == "solve":
-        # one launch = a whole solve: its SpMV products plus the BiCGSTAB
-        # vector updates (19 n doubles per iteration beyond the products)
-        iters = max(n_spmv - n_launch, 0) / 2
-        bytes_launch = (n_spmv * algorithmic_bytes(sim, "spmv", N, M, args.precision)
-                        + iters * 19 * desc.n_mat * 8.0) / max(n_launch, 1)
-    else:
-        bytes_launch = algorithmic_bytes(sim, dom, N, M, args.precision)
-    achieved = bytes_launch / avg_s / 1e9 if avg_s > 0 else None
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak if achieved else None, "traffic": _traffic(args.workload, args.precision, dom),
-                "kernel": dom, "algorithmic_bytes_per_launch": bytes_launch, "avg_launch_ms": avg_s * 1e3,
-                "launches": n_launch, "peak_kind": peak_kind}
-    if roofline["traffic"] and roofline["traffic"] < 0.5 * bytes_launch:
-        roofline["note"] = (f"operands stay in the 126 MB L2 across the launch: measured DRAM traffic is "
-                            f"{roofline['traffic'] / bytes_launch:.0%} of the algorithmic bytes, so the launch is "
-                            f"bound by L2 and latency, not HBM")
+    roofline = kernel_roofline(dom)
+    roofline_solve = kernel_roofline("solve") if dom != "solve" and prof["solve"][0] > 0 else None
 
     # the other precision on the same workload and step count, the FP64 path
     # also at the mixed path's residual target, and the accuracy of the arms
@@ -369,7 +380,8 @@ def main() -> int:
             **({"solver_phase_us": solver_phases(sim)} if args.solver_phases else {}),
             "phase_ms_last_force": {"list": ps[10], "qsc": ps[1], "cpim_vec": ps[6], "cpim_matrix": ps[5],
                                     "cpim_solve": ps[7], "nonbonded": ps[4], "cpim_force": ps[8]},
-            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "gpu_launches": launches,
+            "roofline": roofline, **({"roofline_solve": roofline_solve} if roofline_solve else {}),
+            "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "gpu_launches": launches,
             "compare": compare, "accuracy": accuracy,
         }
         print(json.dumps(line))
@@ -564,6 +576,16 @@ def spmv_effective(sim, launched: int) -> int:
     return immediately once it has converged)."""
     n, _ = profile_get(sim, "spmv_effective")
     return n if n > 0 else launched
+
+
+def _issue_active(kernel: str):
+    """ncu issue-active fraction of the mixed path's kernel on the 91k-atom
+    workload, if its capture summary is committed (profiles/ncu_traffic.json)."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "ncu_traffic.json")) as f:
+            return json.load(f)["issue_active"]["c3"]["mixed"].get(kernel)
+    except Exception:
+        return None
 
 
 def _traffic(workload: str, precision: str, kernel: str):
