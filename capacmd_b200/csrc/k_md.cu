@@ -172,7 +172,7 @@ __global__ void __launch_bounds__(256, 2) k_rattle1(MdParams m, CstrView cv, dou
     const int first = cv.mol_first[im], mt = cv.mol_type[first];
     const int nc = cv.cnt[mt], c0 = cv.off[mt];
     if (nc == 0) return;
-    const double tol2 = 2.0e-05;
+    const double tol2 = 2.0e-05, inv_dt = 1.0 / m.dt;  // the velocity update multiplies by 1/dt
     int iter = 0, done = 0;
     if (cv.mol_atoms[mt] == 3 && nc <= 3) {
         Mol3 X, Y, Z, VX, VY, VZ, OX, OY, OZ, IM;
@@ -209,7 +209,7 @@ __global__ void __launch_bounds__(256, 2) k_rattle1(MdParams m, CstrView cv, dou
                     double dx = qx * g, dy = qy * g, dz = qz * g;
                     X.add(a, ma * dx); Y.add(a, ma * dy); Z.add(a, ma * dz);
                     X.add(b, -(mb * dx)); Y.add(b, -(mb * dy)); Z.add(b, -(mb * dz));
-                    dx /= m.dt; dy /= m.dt; dz /= m.dt;
+                    dx *= inv_dt; dy *= inv_dt; dz *= inv_dt;
                     VX.add(a, ma * dx); VY.add(a, ma * dy); VZ.add(a, ma * dz);
                     VX.add(b, -(mb * dx)); VY.add(b, -(mb * dy)); VZ.add(b, -(mb * dz));
                     done = 0;
@@ -240,7 +240,7 @@ __global__ void __launch_bounds__(256, 2) k_rattle1(MdParams m, CstrView cv, dou
                 double dx = qx * g, dy = qy * g, dz = qz * g;
                 rx[a] += ma * dx; ry[a] += ma * dy; rz[a] += ma * dz;
                 rx[b] -= mb * dx; ry[b] -= mb * dy; rz[b] -= mb * dz;
-                dx /= m.dt; dy /= m.dt; dz /= m.dt;
+                dx *= inv_dt; dy *= inv_dt; dz *= inv_dt;
                 vx[a] += ma * dx; vy[a] += ma * dy; vz[a] += ma * dz;
                 vx[b] -= mb * dx; vy[b] -= mb * dy; vz[b] -= mb * dz;
                 done = 0;
@@ -263,7 +263,11 @@ __global__ void __launch_bounds__(256) k_rattle2(MdParams m, CstrView cv, const 
     if (im < m.n_mols) {
         const int first = cv.mol_first[im], mt = cv.mol_type[first];
         const int nc = cv.cnt[mt], c0 = cv.off[mt];
-        const double tol = 1.0e-05, hdt = 0.5 * m.dt;
+        // 1/(dt/2) and, per constraint of a three-atom molecule, the
+        // reciprocal of its fixed denominator (m_a + m_b) len^2 taken once:
+        // the iterations multiply where the reference divides (equal to
+        // within a rounding of each product)
+        const double tol = 1.0e-05, inv_hdt = 2.0 / m.dt;
         int iter = 0, done = nc == 0;
         const bool fast = !done && cv.mol_atoms[mt] == 3 && nc <= 3;
         if (fast) {
@@ -272,13 +276,14 @@ __global__ void __launch_bounds__(256) k_rattle2(MdParams m, CstrView cv, const 
             VX.load(vx, first); VY.load(vy, first); VZ.load(vz, first);
             IM.load(cv.inv_mass, first);
             int ca[3] = {0, 0, 0}, cb[3] = {0, 0, 0};
-            double l2[3] = {0.0, 0.0, 0.0};
+            double inv_den[3] = {0.0, 0.0, 0.0};
 #pragma unroll
             for (int k = 0; k < 3; ++k)
                 if (k < nc) {
                     ca[k] = cv.ci[c0 + k];
                     cb[k] = cv.cj[c0 + k];
-                    l2[k] = cv.len[c0 + k] * cv.len[c0 + k];
+                    const double len = cv.len[c0 + k];
+                    inv_den[k] = 1.0 / ((IM.get(ca[k]) + IM.get(cb[k])) * (len * len));
                 }
             while (!done) {
                 done = 1;
@@ -286,18 +291,17 @@ __global__ void __launch_bounds__(256) k_rattle2(MdParams m, CstrView cv, const 
                 for (int k = 0; k < 3; ++k) {
                     if (k >= nc) continue;
                     const int a = ca[k], b = cb[k];
-                    const double len2 = l2[k];
                     const double ux = VX.get(a) - VX.get(b), uy = VY.get(a) - VY.get(b), uz = VZ.get(a) - VZ.get(b);
                     const double px = wrap1(X.get(a) - X.get(b), m.box.L[0]);
                     const double py = wrap1(Y.get(a) - Y.get(b), m.box.L[1]);
                     const double pz = wrap1(Z.get(a) - Z.get(b), m.box.L[2]);
                     const double ma = IM.get(a), mb = IM.get(b);
-                    const double g = -(px * ux + py * uy + pz * uz) / ((ma + mb) * len2);
+                    const double g = -(px * ux + py * uy + pz * uz) * inv_den[k];
                     if (fabs(g) > tol) {
                         double dx = px * g, dy = py * g, dz = pz * g;
                         VX.add(a, ma * dx); VY.add(a, ma * dy); VZ.add(a, ma * dz);
                         VX.add(b, -(mb * dx)); VY.add(b, -(mb * dy)); VZ.add(b, -(mb * dz));
-                        dx /= hdt; dy /= hdt; dz /= hdt;
+                        dx *= inv_hdt; dy *= inv_hdt; dz *= inv_hdt;
                         vir[0] -= px * dx; vir[1] -= px * dy; vir[2] -= px * dz;
                         vir[3] -= py * dx; vir[4] -= py * dy; vir[5] -= py * dz;
                         vir[6] -= pz * dx; vir[7] -= pz * dy; vir[8] -= pz * dz;
@@ -323,7 +327,7 @@ __global__ void __launch_bounds__(256) k_rattle2(MdParams m, CstrView cv, const 
                     double dx = px * g, dy = py * g, dz = pz * g;
                     vx[a] += ma * dx; vy[a] += ma * dy; vz[a] += ma * dz;
                     vx[b] -= mb * dx; vy[b] -= mb * dy; vz[b] -= mb * dz;
-                    dx /= hdt; dy /= hdt; dz /= hdt;
+                    dx *= inv_hdt; dy *= inv_hdt; dz *= inv_hdt;
                     vir[0] -= px * dx; vir[1] -= px * dy; vir[2] -= px * dz;
                     vir[3] -= py * dx; vir[4] -= py * dy; vir[5] -= py * dz;
                     vir[6] -= pz * dx; vir[7] -= pz * dy; vir[8] -= pz * dz;
