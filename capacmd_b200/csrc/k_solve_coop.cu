@@ -366,9 +366,19 @@ __device__ void sum_bp(const double *bp, int nb, double (&out)[K])
     double v[K];
 #pragma unroll
     for (int q = 0; q < K; ++q) v[q] = 0.0;
-    for (int k = threadIdx.x; k < nb; k += blockDim.x)
+    // two blocks' partials per thread per round of loads (the grid is at
+    // most two blocks per SM, so one round covers it)
+    for (int k = threadIdx.x; k < nb; k += 2 * blockDim.x) {
+        const int k2 = k + (int)blockDim.x;
+        double a[K], b[K];
 #pragma unroll
-        for (int q = 0; q < K; ++q) v[q] += __ldcg(bp + (size_t)kBp * k + q);
+        for (int q = 0; q < K; ++q) {
+            a[q] = __ldcg(bp + (size_t)kBp * k + q);
+            b[q] = k2 < nb ? __ldcg(bp + (size_t)kBp * k2 + q) : 0.0;
+        }
+#pragma unroll
+        for (int q = 0; q < K; ++q) v[q] += a[q] + b[q];
+    }
     block_sum<K>(v, sh);
     if (threadIdx.x == 0)
 #pragma unroll
