@@ -33,13 +33,17 @@
 // preconditioner's group order (k_bicgstab_group below): four grid barriers
 // per iteration instead of six.
 //
-// Every wait is bounded.  The grid barrier (counter and generation word)
-// gives up after 2^24 polls (the context's wait_polls option when set), a
-// ring-stage wait after 2^20 polls of at most
-// 1 us each; either sets the error word, the block then waits (bounded) for
-// its own copies in flight and returns, the other blocks give up at their
-// next barrier, and the host reports the error.  The launch is cooperative,
-// so either all blocks are resident or the launch fails.
+// Every wait is bounded.  The grid barrier (one arrival word, see
+// grid_barrier) gives up after 2^24 polls (the context's wait_polls option
+// when set), a ring-stage wait after 2^20 polls of at most 1 us each; either
+// sets the error word and the barrier word's abort bit, the block then waits
+// (bounded) for its own copies in flight and returns, the other blocks leave
+// their current or next barrier at once, and the host reports the error.  The
+// launch is cooperative, so either all blocks are resident or the launch
+// fails.  The tiles are copied with an L2 evict-first policy (CAPAC_TILE_L2
+// at context creation: 0 none, a fraction f > 0 keeps f of the lines
+// evict-last), so the matrix streamed every pass leaves the vectors and
+// partial sums of the reduction phases in L2.
 #include <algorithm>
 #include <cstdint>
 #include <vector>
