@@ -574,6 +574,7 @@ int capac_create(const capac_desc *d, const capac_options *opt, capac_ctx **out)
 
             c->partials_cap = partials_needed(c);
             c->partials = dalloc<double>(c->partials_cap);
+            c->pair_split = o.precision == CAPAC_PREC_MIXED && getenv("CAPAC_PAIR_SPLIT") != nullptr;
             if (o.precision == CAPAC_PREC_MIXED && d->n_metal > 0 && d->use_cpff && getenv("CAPAC_OVERLAP")) {
                 c->overlap = true;
                 CAPAC_CUDA(cudaStreamCreateWithFlags(&c->stream2, cudaStreamNonBlocking));

@@ -192,6 +192,7 @@ struct capac_ctx {
     // CPIM right-hand side, matrix and solve run on `stream` (mixed path on
     // the half cluster list); the CPIM forces on water atoms follow the solve
     bool overlap = false;
+    bool pair_split = false;     // half cluster list: pair terms over all clusters, then the water-side CPIM term over the metal clusters (CAPAC_PAIR_SPLIT)
     cudaStream_t stream2 = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     double *partials2 = nullptr;       // block partials of the overlapped pair launch (partials_cap)

@@ -1128,7 +1128,13 @@ void launch_pair_clusters(capac_ctx *c, int mode, unsigned grid)
     const bool cpim = c->M > 0 && c->use_cpff;
     ProfScope ps(c, K_PAIR);
     if (c->cl_half) {
-        if (mode == 0 && cpim)
+        if (mode == 0 && cpim && c->pair_split) {
+            // the pair terms without the CPIM branches, then the water-side
+            // CPIM term over the clusters with a metal member or neighbour
+            launch_pair_cl_t<true, false, true>(c, grid, c->stream, c->partials, false);
+            launch_pair_cl_t<false, true, true>(c, grid, c->stream, c->partials, true);
+            ++c->launches;
+        } else if (mode == 0 && cpim)
             launch_pair_cl_t<true, true, true>(c, grid, c->stream, c->partials, false);
         else if (mode == 0)
             launch_pair_cl_t<true, false, true>(c, grid, c->stream, c->partials, false);
