@@ -376,6 +376,8 @@ def main() -> int:
                        "layout": "group order" if sim.get("solver_layout")[0] else "reference order",
                        "tiles_in_tensor_memory_per_block": int(sim.get("solver_layout")[1]),
                        "inner_stalls": int(sim.get("inner_stalls")[0])},
+            "pair_launch": (lambda ps: {"split": bool(ps[0]), "clusters_next_to_metal": int(ps[1]),
+                                        "clusters": int(ps[2])})(sim.get("pair_split")),
             "kernel_ms": {k: v[1] for k, v in prof.items()},
             **({"solver_phase_us": solver_phases(sim)} if args.solver_phases else {}),
             "phase_ms_last_force": {"list": ps[10], "qsc": ps[1], "cpim_vec": ps[6], "cpim_matrix": ps[5],

@@ -574,7 +574,7 @@ int capac_create(const capac_desc *d, const capac_options *opt, capac_ctx **out)
 
             c->partials_cap = partials_needed(c);
             c->partials = dalloc<double>(c->partials_cap);
-            c->pair_split = o.precision == CAPAC_PREC_MIXED && getenv("CAPAC_PAIR_SPLIT") != nullptr;
+            if (const char *ps = getenv("CAPAC_PAIR_SPLIT")) c->pair_split_force = ps[0] == '0' ? 0 : 1;
             if (o.precision == CAPAC_PREC_MIXED && d->n_metal > 0 && d->use_cpff && getenv("CAPAC_OVERLAP")) {
                 c->overlap = true;
                 CAPAC_CUDA(cudaStreamCreateWithFlags(&c->stream2, cudaStreamNonBlocking));
@@ -1143,6 +1143,13 @@ int capac_get(capac_ctx *c, const char *name, double *out)
             out[0] = c->cpairs ? 2.0 : (c->clusters ? 1.0 : 0.0);
             out[1] = (double)c->n_clusters;
             count = 2;
+            return;
+        }
+        if (n == "pair_split") {  // 1 when the pair launch is split; clusters next to metal; all clusters
+            out[0] = c->pair_split ? 1.0 : 0.0;
+            out[1] = (double)c->n_sel_host;
+            out[2] = (double)c->n_clusters;
+            count = 3;
             return;
         }
         if (n == "solver_layout") {  // 1 when the persistent solver runs in the block-Jacobi groups' order;

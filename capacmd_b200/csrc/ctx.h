@@ -192,7 +192,13 @@ struct capac_ctx {
     // CPIM right-hand side, matrix and solve run on `stream` (mixed path on
     // the half cluster list); the CPIM forces on water atoms follow the solve
     bool overlap = false;
-    bool pair_split = false;     // half cluster list: pair terms over all clusters, then the water-side CPIM term over the metal clusters (CAPAC_PAIR_SPLIT)
+    // half cluster list: the pair terms over all clusters, then the
+    // water-side CPIM term over the clusters next to metal, in two launches
+    // when those clusters are fewer than kPairSplitShare of all (decided at
+    // every list build; CAPAC_PAIR_SPLIT=1 or 0 at creation forces it)
+    bool pair_split = false;
+    int pair_split_force = -1;   // -1 decide, 0 never, 1 always
+    int n_sel_host = 0;          // clusters next to metal at the last build
     cudaStream_t stream2 = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     double *partials2 = nullptr;       // block partials of the overlapped pair launch (partials_cap)
@@ -335,6 +341,7 @@ int bicgstab_core(capac_ctx *c, const double *b, double *x, double tol, double s
 void launch_force_derivative(capac_ctx *c, const double *wdir, double *dfx, double *dfy, double *dfz, double *isd_v,
                              double *isd_d);  // k_grad_forces.cu
 constexpr int W_Y_SLOT = 7, W_V_SLOT = 4;  // BiCGSTAB work-vector slots used as scratch
+constexpr double kPairSplitShare = 0.08;  // share of clusters next to metal below which the pair launch is split
 // persistent cooperative solver (k_solve_coop.cu)
 int coop_grid_size(int device, bool mixed);
 size_t coop_barrier_bytes();

@@ -344,6 +344,9 @@ int capac_checkpoint_load(capac_ctx *ctx, const char *path);
  * adjoint_dedx (dE/dx), adjoint_dpsidx (dPsi/dx of the force matching),
  * adjoint_mu, adjoint_nu (the adjoint solutions).  Read-only diagnostics:
  * pair_list(2: 1 when the pair kernel walks the cluster list, cluster count),
+ * pair_split(3: 1 when the half-list pair launch is split in two -- the
+ * pair terms, then the CPIM term over the clusters next to metal -- as it
+ * is when those are under 8% of the clusters; their count; all clusters),
  * potential and virial are settable too (to zero them before a stage call).
  * solver_layout(4: 1 when the mixed path's persistent solver works in the
  * order of its block-Jacobi groups, its tiles assembled in that order; the

@@ -294,3 +294,38 @@ def test_pairs_overlapped_with_the_solve(case, monkeypatch):
         one.md_steps(1)
     assert rel_err(ovl.get("rx"), one.get("rx")) < 1e-7
     assert abs(ovl.get("potential")[0] - one.get("potential")[0]) <= 1e-7 * abs(one.get("potential")[0])
+
+
+@pytest.mark.parametrize("case", ["c2", "t_2np"])
+def test_split_pair_launch_matches_one_launch(case, monkeypatch):
+    """The half-list pair launch split in two (the pair terms over every
+    cluster, then the water-side CPIM term over the clusters next to metal)
+    gives the energies and virial of the single launch to rounding and its
+    forces to FP32 rounding (the single launch adds a pair's CPIM force to
+    its pair force in FP32 before the FP64 sum, the split adds both in FP64);
+    left to itself the context splits only when fewer than 8% of the clusters
+    are next to metal."""
+    paths = configs.cached(case) if case == "c2" else golden_paths(case)
+    d = cm.Desc.from_paths(paths)
+    sims = {}
+    for v in ("1", "0", None):
+        if v is None:
+            monkeypatch.delenv("CAPAC_PAIR_SPLIT", raising=False)
+        else:
+            monkeypatch.setenv("CAPAC_PAIR_SPLIT", v)
+        sims[v] = _mixed(paths)[1]
+    monkeypatch.delenv("CAPAC_PAIR_SPLIT", raising=False)
+    for s in sims.values():
+        s.set("vec_pq", np.zeros(d.n_mat))
+        s.force()
+    if not _uses_clusters(sims["1"]):
+        pytest.skip("the box is too small for the cluster list")
+    on, off, auto = sims["1"], sims["0"], sims[None]
+    assert on.get("pair_split")[0] == 1.0 and off.get("pair_split")[0] == 0.0
+    share = auto.get("pair_split")
+    assert share[0] == (1.0 if share[1] < 0.08 * share[2] else 0.0)
+    assert rel_err(on.forces(), off.forces()) < 1e-6
+    p_on, p_off = on.get("potential"), off.get("potential")
+    m = np.abs(p_off) > 0
+    assert np.all(np.abs(p_on[m] - p_off[m]) <= 1e-12 * np.abs(p_off[m]))
+    assert rel_err(on.get("virial"), off.get("virial")) < 1e-12
