@@ -340,7 +340,8 @@ int capac_checkpoint_load(capac_ctx *ctx, const char *path);
 /* State transfer.  Names for per-atom arrays (n_atoms doubles):
  * rx ry rz vx vy vz fx fy fz.  Others: potential(15) virial(9) vec_pq vec_ext
  * diag_relay (n_mat) inv_sqrt_dens(n_metal) vQ(10) thermo(4: eKsum inst_temp
- * ref_temp ndf) box(6); after a gradient call (read only, n_mat each):
+ * ref_temp ndf) box(6) fmax_rms(2: get_fmax_rms's largest and rms force at
+ * the last n_save step); after a gradient call (read only, n_mat each):
  * adjoint_dedx (dE/dx), adjoint_dpsidx (dPsi/dx of the force matching),
  * adjoint_mu, adjoint_nu (the adjoint solutions).  Read-only diagnostics:
  * pair_list(2: 1 when the pair kernel walks the cluster list, cluster count),

@@ -31,6 +31,20 @@ def test_library_exports_every_declared_symbol():
     assert not missing, missing
 
 
+def test_every_state_name_is_documented():
+    """Every name capac_get answers (the library's name table and its
+    diagnostics) appears in the header's description of capac_get."""
+    api = open(os.path.join(ROOT, "capacmd_b200", "csrc", "api.cu")).read()
+    body = api[api.index("int capac_get(capac_ctx *c, const char *name, double *out)"):]
+    body = body[:body.index("\nint capac_set(")]
+    names = set(re.findall(r'n == "([a-z_0-9A-Z]+)"', body)) | set(re.findall(r'\{"([a-z_0-9]+)", c->', api))
+    hdr = open(os.path.join(ROOT, "include", "capacmd.h")).read()
+    doc = hdr[hdr.index("/* State transfer."):hdr.index("int capac_get(")]
+    assert len(names) > 20
+    missing = sorted(n for n in names if n not in doc)
+    assert not missing, missing
+
+
 def test_options_mirror_matches_library_defaults():
     """The Python Options structure has the C layout: every field read back
     from capac_options_default is the documented default."""
