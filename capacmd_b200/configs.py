@@ -61,6 +61,10 @@ WORKLOADS = {
     "c1_field": Workload("c1_field", [3], 0, 6.0, seed=0, ensemble="nve", steps=1000,
                          efield_vnm=(0.0, 0.0, 0.5)),
     "c2": Workload("c2", [4], 3000, 4.5, seed=1, steps=5000),
+    # the same system under the Berendsen thermostat the workload's
+    # description names (the reference has only the Nose-Hoover chain, so
+    # "c2" keeps that for comparisons with it)
+    "c2_berendsen": Workload("c2_berendsen", [4], 3000, 4.5, seed=1, ensemble="berendsen", steps=5000),
     # the same system without thermostat, for energy-drift measurements, with
     # two more seeds and, per seed, a variant without CPIM (the floor of the
     # integrator and RATTLE alone)

@@ -119,6 +119,9 @@ void md_step(capac_ctx *c)
     if (nvt) {
         launch_nhc(c);
         launch_scale_velocities(c);
+    } else if (c->ensemble == CAPAC_BERENDSEN) {
+        launch_berendsen(c);
+        launch_scale_velocities(c);
     }
     launch_remove_com(c);
     launch_kinetic(c);
@@ -265,6 +268,8 @@ int capac_create(const capac_desc *d, const capac_options *opt, capac_ctx **out)
                 d->np_start[k] > d->np_end[k])
                 throw Error(CAPAC_ERR_INVALID, "START_END_CHG range outside MM_METAL");
         if (d->n_nps > 256) throw Error(CAPAC_ERR_UNSUPPORTED, "more than 256 nanoparticles");
+        if (d->ensemble == CAPAC_BERENDSEN && !(d->tau_temp > 0.0))
+            throw Error(CAPAC_ERR_INVALID, "tau_T_in_ps must be positive for the Berendsen thermostat");
         int ndev = 0;
         if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
             throw Error(CAPAC_ERR_NO_DEVICE, "no CUDA device");
@@ -298,6 +303,7 @@ int capac_create(const capac_desc *d, const capac_options *opt, capac_ctx **out)
             c->n_save = d->n_save > 0 ? d->n_save : 1;
             c->n_heating = d->n_heating;
             c->dt = d->dt;
+            if (d->ensemble == CAPAC_BERENDSEN) c->dt_over_tau = d->dt / d->tau_temp;
             c->run_type = d->run_type;
             c->em_length = d->em_length;
             c->em_tol = d->em_tol;

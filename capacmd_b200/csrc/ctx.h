@@ -106,6 +106,7 @@ struct capac_ctx {
     int ensemble = 0, fix_metal = 0, use_cpff = 0, n_save = 1, n_heating = 0;
     int metal_min = 0;
     double dt = 0.0;
+    double dt_over_tau = 0.0;  // Berendsen coupling: dt / tau_T_in_ps
     // energy minimisation (mpi-main.c:700-865): run type, step length, tolerance
     int run_type = 0;
     double em_length = 0.0, em_tol = 0.0;
@@ -369,6 +370,7 @@ void launch_md_drift(capac_ctx *c);
 void launch_rattle(capac_ctx *c, int second);
 void launch_kinetic(capac_ctx *c);
 void launch_nhc(capac_ctx *c);
+void launch_berendsen(capac_ctx *c);
 void launch_scale_velocities(capac_ctx *c);
 void launch_remove_com(capac_ctx *c);
 void launch_apply_pbc(capac_ctx *c);

@@ -86,6 +86,7 @@ void read_mdset(const char *path, capac_desc *d)
             else throw Error(CAPAC_ERR_IO, "unknown run_type " + v);
         } else if (k == "ensemble") {
             if (v == "nvt") d->ensemble = CAPAC_NVT;
+            else if (v == "berendsen") d->ensemble = CAPAC_BERENDSEN;  // no counterpart in the reference
             else d->ensemble = CAPAC_NVE;  // the reference thermostats only on "nvt"
         } else if (k == "em_steps") d->em_steps = atoi(val);
         else if (k == "em_length_in_nm") d->em_length = atof(val);

@@ -85,6 +85,22 @@ __global__ void k_nhc(ThermoState *th, MdParams m)
     th->inst_temp *= scale * scale;
 }
 
+// Berendsen weak coupling (no counterpart in the reference, whose only
+// thermostat is the Nose-Hoover chain): lambda = sqrt(1 + dt/tau (T0/T - 1))
+// from the temperature after the second RATTLE (Berendsen et al., J. Chem.
+// Phys. 81, 3684 (1984)), lambda^2 held to [0.64, 1.5625] and lambda = 1 at
+// T = 0; the scale is left in th->scale for k_scale_velocities.
+__global__ void k_berendsen(ThermoState *th, double dt_over_tau)
+{
+    const double T = th->inst_temp;
+    double s2 = 1.0;
+    if (T > 0.0) s2 = fmin(fmax(1.0 + dt_over_tau * (th->ref_temp / T - 1.0), 0.64), 1.5625);
+    const double s = sqrt(s2);
+    th->scale = s;
+    th->eksum *= s * s;
+    th->inst_temp *= s * s;
+}
+
 // Optional thermostat scaling of every velocity, then v += dt/2 F/m for
 // atoms that move (mpi-main.c:900-913).
 __global__ void k_half_kick(MdParams m, const unsigned char *is_metal, const double *inv_mass,
@@ -571,6 +587,12 @@ void launch_heating(capac_ctx *c, long step)
 void launch_nhc(capac_ctx *c)
 {
     k_nhc<<<1, 1, 0, c->stream>>>(c->th, md_params(c));
+    ++c->launches;
+}
+
+void launch_berendsen(capac_ctx *c)
+{
+    k_berendsen<<<1, 1, 0, c->stream>>>(c->th, c->dt_over_tau);
     ++c->launches;
 }
 

@@ -67,6 +67,15 @@ const char *capac_last_error(void);
 #define CAPAC_BT_DIHEDRAL_RB 7    /* par: c0..c5 (periodic funct 1/4/9 are given as their RB form) */
 #define CAPAC_NVE 0
 #define CAPAC_NVT 1
+/* Berendsen weak coupling, "ensemble berendsen" in mdset.txt.  No counterpart
+ * in the reference: its only thermostat is the Nose-Hoover chain
+ * (thermostat.c:117-191), and its MD loop thermostats only on "nvt"
+ * (mpi-main.c:894, 975).  Once a step, after the second RATTLE, every
+ * velocity is scaled by lambda = sqrt(1 + dt/tau (T0/T - 1)) (Berendsen et
+ * al., J. Chem. Phys. 81, 3684 (1984)), T the instantaneous temperature, T0
+ * the reference temperature of the heating ramp, tau = tau_T_in_ps; lambda is
+ * held to [0.8, 1.25], and to 1 when T is zero. */
+#define CAPAC_BERENDSEN 2
 
 #define CAPAC_PREC_FP64 0   /* plain FP64 path: reference arithmetic on the GPU */
 #define CAPAC_PREC_MIXED 1  /* FP32 pair terms, FP32 CPIM matrix/SpMV, FP64 refinement */
@@ -80,7 +89,7 @@ const char *capac_last_error(void);
 typedef struct capac_desc {
     /* mdset.txt (RunSet, typedef.h:200-242; keys file.c:90-124) */
     int run_type;     /* CAPAC_RUN_* */
-    int ensemble;     /* CAPAC_NVE / CAPAC_NVT */
+    int ensemble;     /* CAPAC_NVE / CAPAC_NVT / CAPAC_BERENDSEN */
     int n_steps, n_save, n_heating, em_steps;
     double dt, r_cut, w_alpha, ref_temp, tau_temp, em_length, em_tol;
     int use_vdw;      /* 1: shifted-force LJ ("shifted"), 0: plain cut-off */

@@ -852,6 +852,23 @@ static void nhc(orc *o)
     o->inst_temp *= scale * scale;
 }
 
+/* Berendsen weak coupling (Berendsen et al., J. Chem. Phys. 81, 3684 (1984));
+ * no counterpart in the reference, which thermostats only with the chain
+ * above: lambda = sqrt(1 + dt/tau (T0/T - 1)), lambda^2 held to
+ * [0.64, 1.5625], lambda = 1 at T = 0, applied to every velocity. */
+static void berendsen(orc *o)
+{
+    double s2 = 1.0;
+    if (o->inst_temp > 0.0) {
+        s2 = 1.0 + o->d->dt / o->d->tau_temp * (o->ref_temp / o->inst_temp - 1.0);
+        s2 = s2 < 0.64 ? 0.64 : (s2 > 1.5625 ? 1.5625 : s2);
+    }
+    const double s = sqrt(s2);
+    for (int i = 0; i < o->N; ++i) { o->vx[i] *= s; o->vy[i] *= s; o->vz[i] *= s; }
+    o->eksum *= s * s;
+    o->inst_temp *= s * s;
+}
+
 /* rattle_1st force.c:1907-1997 and rattle_2nd force.c:2004-2090. */
 static int rattle(orc *o, int second)
 {
@@ -1078,6 +1095,7 @@ int orc_md_steps(orc *o, int n)
         if (rc) return rc;
         kinetic(o);
         if (d->ensemble == CAPAC_NVT) nhc(o);
+        else if (d->ensemble == CAPAC_BERENDSEN) berendsen(o);
         remove_com(o);
         kinetic(o);
         if (step % d->n_save == 0) {

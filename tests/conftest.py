@@ -83,6 +83,7 @@ def variant(case: str, out_dir: str, par=None, mds=None) -> dict:
     src = golden_paths(case)
     names = {"gro": "init.gro", "par": "param.txt", "mds": "mdset.txt"}
     edit = {"par": par, "mds": mds}
+    os.makedirs(str(out_dir), exist_ok=True)
     out = {}
     for k, p in src.items():
         text = open(p).read()
@@ -101,3 +102,21 @@ def impossible_constraints(text: str) -> str:
     constraints together: no geometry satisfies it, so RATTLE cannot converge
     (the reference stops with "RATTLE_1 not converged!", force.c:1990-1994)."""
     return text.replace("1 2   0.163298", "1 2   0.300000")
+
+
+def berendsen(tau: float, ref_t: float | None = None):
+    """An mdset.txt edit selecting the Berendsen thermostat with coupling time
+    tau (ps) and, if given, another reference temperature (K)."""
+    def edit(text: str) -> str:
+        out = []
+        for line in text.splitlines():
+            key = line.split()[0] if line.split() else ""
+            if key == "ensemble":
+                line = "ensemble          berendsen"
+            elif key == "tau_T_in_ps":
+                line = f"tau_T_in_ps       {tau!r}"
+            elif key == "ref_T_in_K" and ref_t is not None:
+                line = f"ref_T_in_K        {ref_t!r}"
+            out.append(line)
+        return "\n".join(out) + "\n"
+    return edit
