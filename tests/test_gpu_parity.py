@@ -130,28 +130,6 @@ def test_md_100_steps_energy_trace(case):
     assert rel_err(s.get("rx"), o.get("rx")) < 1e-8
 
 
-def test_berendsen_md_trace(tmp_path):
-    """The Berendsen thermostat (no counterpart in the reference) against
-    the oracle's restatement: 20 steps of the water system coupled to 400 K
-    with tau = 5 fs, so every step scales the velocities by several per cent."""
-    from conftest import berendsen, variant
-    d = cm.Desc.from_paths(variant("t_water", tmp_path, mds=berendsen(0.005, 400.0)))
-    s, o = cm.Simulation(d), Oracle(d)
-    s.md_init()
-    assert o.force() == 0
-    o.md_init()
-    ts, to = [], []
-    for _ in range(20):
-        s.md_steps(1)
-        assert o.md_steps(1) == 0
-        ts.append(s.get("thermo")[1])
-        to.append(o.get("thermo")[1])
-    assert to[-1] > 350.0  # the coupling is active: heated from 300 K towards 400 K
-    assert rel_err(ts, to) < 1e-9
-    for k in ("rx", "vx", "vz"):
-        assert rel_err(s.get(k), o.get(k)) < 1e-9
-
-
 @pytest.mark.parametrize("case", ["c1", "t_water", "t_morse_buck"])
 def test_reference_md_trace_without_solve_noise(case):
     d, s, o = _pair(case)
