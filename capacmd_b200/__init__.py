@@ -35,6 +35,9 @@ ERR_NO_DEVICE = -8
 PREC_FP64 = 0
 PREC_MIXED = 1
 
+# thermostats (CAPAC_NVE / CAPAC_NVT / CAPAC_BERENDSEN of capacmd.h), as mdset.txt's ensemble selects
+NVE, NVT, BERENDSEN = 0, 1, 2
+
 # bonded term kinds (CAPAC_BT_* of capacmd.h)
 BT_BOND_HARMONIC, BT_BOND_MORSE, BT_PAIR_14, BT_PAIR_USER = 1, 2, 3, 4
 BT_ANGLE_HARMONIC, BT_ANGLE_UB, BT_DIHEDRAL_RB = 5, 6, 7

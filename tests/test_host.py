@@ -45,6 +45,21 @@ def test_every_state_name_is_documented():
     assert not missing, missing
 
 
+def test_python_constants_match_the_header():
+    """Every status, precision, bonded-term and thermostat value the Python
+    mirror names equals the header's #define of the same name."""
+    src = open(os.path.join(ROOT, "include", "capacmd.h")).read()
+    defs = {k: int(v) for k, v in re.findall(r"#define CAPAC_([A-Z_0-9]+)\s+\(?(-?\d+)\)?", src)}
+    checked = 0
+    for name, value in vars(cm).items():
+        if isinstance(value, int) and not isinstance(value, bool) and name in defs:
+            assert value == defs[name], name
+            checked += 1
+    for name in ("OK", "ERR_INVALID", "ERR_CAPACITY", "PREC_MIXED", "BT_DIHEDRAL_RB", "NVT", "BERENDSEN"):
+        assert name in defs and getattr(cm, name) == defs[name], name
+    assert checked >= 20
+
+
 def test_options_mirror_matches_library_defaults():
     """The Python Options structure has the C layout: every field read back
     from capac_options_default is the documented default."""
