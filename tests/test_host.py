@@ -127,6 +127,16 @@ def test_parser_errors(tmp_path):
     with pytest.raises(cm.CapacError) as e:
         cm.Desc(str(short), p["par"], p["mds"])
     assert e.value.code == cm.ERR_IO
+    # an atom count that is not the topology's: the reference's own check and
+    # wording (mpi-main.c:527-532)
+    lines = open(p["gro"]).readlines()
+    n = int(lines[1])
+    lines[1] = f"{n + 1}\n"
+    other = tmp_path / "other.gro"
+    other.write_text("".join(lines))
+    with pytest.raises(cm.CapacError) as e:
+        cm.Desc(str(other), p["par"], p["mds"])
+    assert e.value.code == cm.ERR_IO and f"groNAtoms({n + 1}) not equal to nAtoms({n})" in str(e.value)
 
 
 @pytest.mark.parametrize("section,line", [("SOL_BONDS", "0 1 7 0.1 1000.0"),
