@@ -51,6 +51,22 @@ WORKLOAD_DESC = {
 }
 
 
+def max_over_ranks(ms: float, device) -> float:
+    """The slowest rank's time: independent replicas are timed together as
+    the slowest one (every rank takes part in the same all-reduce)."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([ms], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(n_atoms: int, steps: int, world: int, ms: float) -> float:
+    """Whole-job atom-steps/s of `world` replicas of an n_atoms system, each
+    running `steps` MD steps, timed as the slowest replica's ms."""
+    return n_atoms * steps * world / (ms / 1e3)
+
+
 def _peaks() -> tuple[float, str]:
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -286,11 +302,9 @@ def main() -> int:
     clk = clocks.stop()
     torch.cuda.synchronize()
     if world > 1:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+        ms = max_over_ranks(ms, "cuda")
         dist.barrier()
-    value = N * args.steps * world / (ms / 1e3)
+    value = replica_value(N, args.steps, world, ms)
     st = sim.stats()
 
     # dominant kernel and its roofline, and the persistent solve's beside it
